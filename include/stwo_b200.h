@@ -1,0 +1,225 @@
+/*
+ * stwo_b200 — Blackwell-native (sm_100a) CUDA backend for the Stwo circle-STARK
+ * prover's hot path: M31 circle FFT, FRI folds, DEEP quotients, batch inverse,
+ * Blake2s Merkle commitment, accumulation and the wide-Fibonacci composition.
+ *
+ * Two tiers of `extern "C"` entry points are exported by libstwo_b200.so:
+ *
+ *  1. Reference-compatible entry points. Their names, argument order and
+ *     argument meaning are exactly those the reference's Rust FFI binds
+ *     (NethermindEth/stwo-gpu, stwo_gpu_backend/src/cuda/bindings.rs:75-271), so
+ *     the reference's trait impls link against this library unchanged. Like the
+ *     reference they run on the legacy default stream and return after the work
+ *     is done. Failures are recorded for stwo_last_error() instead of printed.
+ *
+ *  2. Native entry points (stwo_*): asynchronous on a caller-supplied CUDA stream
+ *     (a cudaStream_t passed as void*, NULL = legacy default stream), returning a
+ *     status code (STWO_OK = 0). They take host arrays of device column pointers
+ *     (passed to the kernels by value, so the calls are CUDA-graph capturable),
+ *     accept columns of mixed power-of-two sizes where the reference assumed one
+ *     size, and fuse steps the reference ran as separate passes.
+ *
+ * Conventions. An M31 element is a uint32_t in [0, 2^31 - 1). A QM31 value is
+ * stwo_qm31 {a, b, c, d} = (a + b i) + (c + d i) u, the reference's repr(C)
+ * CudaSecureField (bindings.rs:8-14). "SoA QM31 columns" are four M31 device
+ * arrays (SecureColumnByCoords); "AoS QM31" is 16 contiguous bytes per element
+ * (SecureFieldVec). Evaluations are in bit-reversed order. Twiddle trees are the
+ * layout PolyOps::precompute_twiddles produces (twiddles.cu:29-73): the layers
+ * of the root coset's doublings, concatenated, followed by a single 1.
+ */
+#ifndef STWO_B200_H
+#define STWO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- types */
+typedef struct { uint32_t x, y; } stwo_point;          /* CirclePointBaseField, bindings.rs:45-58 */
+typedef struct { uint32_t a, b, c, d; } stwo_qm31;      /* CudaSecureField, bindings.rs:8-14 */
+typedef struct { stwo_qm31 x, y; } stwo_spoint;         /* CirclePointSecureField, bindings.rs:60-73 */
+typedef struct { uint32_t s[8]; } stwo_blake2s_hash;    /* Blake2sHash, cuda/include/utils.cuh:7-9 */
+
+enum {
+    STWO_OK = 0,
+    STWO_ERR_INVALID_ARGUMENT = 1,
+    STWO_ERR_UNSUPPORTED_SIZE = 2,
+    STWO_ERR_OUT_OF_MEMORY = 3,
+    STWO_ERR_CUDA = 4,
+};
+
+/* =====================================================================
+ * Tier 1: reference-compatible entry points (bindings.rs:75-271)
+ * ===================================================================== */
+
+/* Device memory and copies. Replaces cuda/src/utils.cu:14-80 (bindings.rs:77-99,196-216). */
+void copy_uint32_t_vec_from_device_to_host(const uint32_t *device_ptr, uint32_t *host_ptr, uint32_t size);
+uint32_t *copy_uint32_t_vec_from_host_to_device(const uint32_t *host_ptr, uint32_t size);
+uint32_t *copy_uint32_t_vec_from_device_to_device(const uint32_t *from, uint32_t *dst, uint32_t size);
+uint32_t *cuda_malloc_uint32_t(uint32_t size);
+stwo_blake2s_hash *cuda_malloc_blake_2s_hash(size_t size);
+uint32_t *cuda_alloc_zeroes_uint32_t(uint32_t size);
+stwo_blake2s_hash *cuda_alloc_zeroes_blake_2s_hash(size_t size);
+void cuda_free_memory(void *device_ptr);
+stwo_blake2s_hash *copy_blake_2s_hash_vec_from_host_to_device(const stwo_blake2s_hash *from, size_t size);
+void copy_blake_2s_hash_vec_from_device_to_host(const stwo_blake2s_hash *from, stwo_blake2s_hash *to, size_t size);
+void copy_blake_2s_hash_vec_from_device_to_device(const stwo_blake2s_hash *from, stwo_blake2s_hash *dst, size_t size);
+uint32_t **copy_device_pointer_vec_from_host_to_device(uint32_t *const *from, size_t size);
+
+/* ColumnOps::bit_reverse_column. Replaces cuda/src/bit_reverse.cu:18-33 (bindings.rs:101-103). */
+void bit_reverse_base_field(uint32_t *array, size_t size);
+void bit_reverse_secure_field(uint32_t *array, size_t size);
+
+/* FieldOps::batch_inverse. Replaces cuda/src/batch_inverse.cu:157-177 (bindings.rs:105-107). */
+void batch_inverse_base_field(const uint32_t *from, uint32_t *dst, size_t size);
+void batch_inverse_secure_field(const uint32_t *from, uint32_t *dst, size_t size);
+
+/* PolyOps::new_canonical_ordered. Replaces cuda/src/poly/twiddles.cu:17-27 (bindings.rs:109-112).
+ * Returns a new device buffer owned by the caller (free with cuda_free_memory). */
+uint32_t *sort_values_and_permute_with_bit_reverse_order(const uint32_t *from, size_t size);
+
+/* PolyOps::precompute_twiddles. Replaces cuda/src/poly/twiddles.cu:50-73 (bindings.rs:114-118).
+ * Returns a new device buffer of total_size twiddles owned by the caller. */
+uint32_t *precompute_twiddles(stwo_point initial, stwo_point step, size_t total_size);
+
+/* PolyOps::interpolate / interpolate_columns / evaluate / evaluate_polynomials.
+ * Replace cuda/src/poly/ifft.cu:41-163 and rfft.cu:45-141 (bindings.rs:120-152).
+ * eval_domain_size is the domain's half-coset size; values are in place. In
+ * interpolate_columns `values` is a host array of `values_size` device column
+ * pointers of `number_of_rows` elements; evaluate_columns accepts per-column sizes. */
+void interpolate(uint32_t eval_domain_size, uint32_t *values, const uint32_t *inverse_twiddles_tree,
+                 uint32_t inverse_twiddle_tree_size, uint32_t values_size);
+void interpolate_columns(uint32_t eval_domain_size, uint32_t *const *values, const uint32_t *inverse_twiddles_tree,
+                         uint32_t inverse_twiddle_tree_size, uint32_t values_size, uint32_t number_of_rows);
+void evaluate(uint32_t eval_domain_size, uint32_t *values, const uint32_t *twiddles_tree,
+              uint32_t twiddle_tree_size, uint32_t values_size);
+void evaluate_columns(const uint32_t *eval_domain_sizes, uint32_t *const *values, const uint32_t *twiddles_tree,
+                      uint32_t twiddle_tree_size, uint32_t number_of_columns, const uint32_t *column_sizes);
+
+/* PolyOps::eval_at_point. Replaces cuda/src/poly/eval_at_point.cu:99-155 (bindings.rs:154-159). */
+stwo_qm31 eval_at_point(const uint32_t *coeffs, uint32_t coeffs_size, stwo_qm31 point_x, stwo_qm31 point_y);
+
+/* FriOps::fold_line / fold_circle_into_line. Replace cuda/src/fri/fold_line.cu:36-53 and
+ * fold_circle_into_line.cu:48-69 (bindings.rs:161-177). gpu_domain is the itwiddles tree,
+ * eval_values / folded_values are host arrays of the 4 SoA coordinate columns. */
+void fold_line(const uint32_t *gpu_domain, size_t twiddle_offset, size_t n, uint32_t *const *eval_values,
+               stwo_qm31 alpha, uint32_t *const *folded_values);
+void fold_circle_into_line(const uint32_t *gpu_domain, size_t twiddle_offset, size_t n, uint32_t *const *eval_values,
+                           stwo_qm31 alpha, uint32_t *const *folded_values);
+
+/* AccumulationOps::accumulate. Replaces cuda/src/accumulate.cu:15-26 (bindings.rs:179). */
+void accumulate(uint32_t size, uint32_t *const *left_columns, uint32_t *const *right_columns);
+
+/* MerkleOps<Blake2sMerkleHasher>::commit_on_layer. Replaces cuda/src/blake2s.cu:157-170
+ * (bindings.rs:181-194). `columns` is a DEVICE array of device column pointers. */
+void commit_on_first_layer(size_t size, size_t amount_of_columns, uint32_t *const *columns, stwo_blake2s_hash *result);
+void commit_on_layer_with_previous(size_t size, size_t amount_of_columns, uint32_t *const *columns,
+                                   const stwo_blake2s_hash *previous_layer, stwo_blake2s_hash *result);
+
+/* QuotientOps::accumulate_quotients. Replaces cuda/src/quotients.cu:180-270
+ * (bindings.rs:218-236). `columns` is a DEVICE array of device column pointers;
+ * sample arrays are host memory; batches may have different sizes. */
+void accumulate_quotients(uint32_t half_coset_initial_index, uint32_t half_coset_step_size, uint32_t domain_size,
+                          uint32_t *const *columns, size_t number_of_columns, stwo_qm31 random_coeff,
+                          const uint32_t *sample_points, const uint32_t *sample_columns_indexes,
+                          uint32_t sample_columns_indexes_size, const stwo_qm31 *sample_column_values,
+                          const uint32_t *sample_column_and_values_sizes, uint32_t sample_size,
+                          uint32_t *result_column_0, uint32_t *result_column_1, uint32_t *result_column_2,
+                          uint32_t *result_column_3, uint32_t flattened_line_coeffs_size);
+
+/* Wide-Fibonacci composition (ComponentProver::evaluate_constraint_quotients_on_domain).
+ * Replaces cuda/src/examples/wide_fibonacci.cu:40-66 (bindings.rs:260-270).
+ * trace_evaluations is a host array of device pointers; random_coeff_powers is a device
+ * AoS QM31 array; denominator_inverses a device M31 array (bit-reversed order). */
+void evaluate_wide_fibonacci_constraint_quotients_on_domain(
+    uint32_t *quotients_0, uint32_t *quotients_1, uint32_t *quotients_2, uint32_t *quotients_3,
+    uint32_t *const *trace_evaluations, const uint32_t *random_coeff_powers, const uint32_t *denominator_inverses,
+    uint32_t extended_domain_size, uint32_t number_of_columns);
+
+/* =====================================================================
+ * Tier 2: native asynchronous entry points
+ * ===================================================================== */
+
+/* Message of the last failure on the calling thread ("" if none); the record is
+ * sticky until stwo_clear_last_error(). The void reference-compatible entry points
+ * report failures only through this record. */
+const char *stwo_last_error(void);
+void stwo_clear_last_error(void);
+/* Waits for all work on `stream`; returns STWO_ERR_CUDA if any of it failed. */
+int stwo_stream_synchronize(void *stream);
+
+/* Twiddle tree of the coset {root_initial_index, root_step_size, 2^root_log_size}
+ * into twiddles[2^root_log_size] and its element-wise inverse into itwiddles
+ * (either output may be NULL). Replaces twiddles.cu:29-73 plus the batch_inverse
+ * call of poly.rs:181-186. */
+int stwo_precompute_twiddles(uint32_t root_initial_index, uint32_t root_step_size, uint32_t root_log_size,
+                             uint32_t *twiddles, uint32_t *itwiddles, void *stream);
+
+/* In-place circle FFTs over columns of mixed sizes; column i has 2^log_sizes[i]
+ * elements and its domain's half coset is a doubling of the tree's root coset.
+ * Inverse FFTs include the 2^-log rescale. */
+int stwo_interpolate_columns(uint32_t *const *columns, const uint32_t *log_sizes, uint32_t n_columns,
+                             const uint32_t *itwiddles, uint64_t tree_size, void *stream);
+int stwo_evaluate_columns(uint32_t *const *columns, const uint32_t *log_sizes, uint32_t n_columns,
+                          const uint32_t *twiddles, uint64_t tree_size, void *stream);
+/* Fused PolyOps::extend + evaluate: reads 2^coeff_log_sizes[i] coefficients from coeffs[i]
+ * and writes the 2^(coeff_log_sizes[i] + log_blowup) evaluations to outputs[i] (distinct
+ * buffers); the zero padding is never materialised. */
+int stwo_extend_evaluate_columns(const uint32_t *const *coeffs, const uint32_t *coeff_log_sizes,
+                                 uint32_t *const *outputs, uint32_t log_blowup, uint32_t n_columns,
+                                 const uint32_t *twiddles, uint64_t tree_size, void *stream);
+
+/* ColumnOps / FieldOps. qm31 arrays are AoS. */
+int stwo_bit_reverse_m31(uint32_t *column, uint64_t n, void *stream);
+int stwo_bit_reverse_qm31(uint32_t *column, uint64_t n, void *stream);
+int stwo_new_canonical_ordered(const uint32_t *src, uint32_t *dst, uint32_t log_size, void *stream);
+int stwo_batch_inverse_m31(const uint32_t *src, uint32_t *dst, uint64_t n, void *stream);
+int stwo_batch_inverse_qm31(const uint32_t *src, uint32_t *dst, uint64_t n, void *stream);
+
+/* PolyOps::eval_at_point for n_polys polynomials, each at its own point; results
+ * (device, AoS QM31) in results[i]. `scratch` is caller-owned device memory of at
+ * least stwo_eval_at_points_scratch_bytes() bytes (per-block partial sums and
+ * completion tickets); concurrent calls need distinct scratch. */
+size_t stwo_eval_at_points_scratch_bytes(const uint32_t *log_sizes, uint32_t n_polys);
+int stwo_eval_at_points(const uint32_t *const *coeffs, const uint32_t *log_sizes, uint32_t n_polys,
+                        const stwo_spoint *points, stwo_qm31 *results, void *scratch, size_t scratch_bytes,
+                        void *stream);
+
+/* FriOps on SoA QM31 columns; itwiddles + twiddle_offset as in fri.rs:24-26,56. */
+int stwo_fold_line(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha, const uint32_t *itwiddles,
+                   uint64_t twiddle_offset, uint32_t *const *dst4, void *stream);
+int stwo_fold_circle_into_line(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha, const uint32_t *itwiddles,
+                               uint64_t twiddle_offset, uint32_t *const *dst4, void *stream);
+
+/* AccumulationOps::accumulate on SoA QM31 columns: left += right. */
+int stwo_accumulate(uint32_t *const *left4, const uint32_t *const *right4, uint64_t n, void *stream);
+
+/* One Merkle layer of 2^log_size Blake2s nodes (32 bytes each). prev_layer (2^(log_size+1)
+ * nodes) may be NULL for the leaf layer; columns is a host array of device pointers to
+ * columns of 2^log_size elements. */
+int stwo_merkle_commit_layer(uint32_t log_size, const uint32_t *prev_layer, const uint32_t *const *columns,
+                             uint32_t n_columns, uint32_t *out, void *stream);
+
+/* DEEP quotient accumulation over the circle domain with half coset
+ * {initial_index, step_size, 2^(domain_log_size-1)}. Batch b samples batch_sizes[b]
+ * columns (indices in column_indices, values in sampled_values, flattened) at
+ * sample_points[b]. Host arrays; columns is a host array of device pointers; out4 are
+ * the four SoA result columns. */
+int stwo_accumulate_quotients(uint32_t half_coset_initial_index, uint32_t half_coset_step_size,
+                              uint32_t domain_log_size, const uint32_t *const *columns, uint32_t n_columns,
+                              stwo_qm31 random_coeff, const stwo_spoint *sample_points, const uint32_t *batch_sizes,
+                              const uint32_t *column_indices, const stwo_qm31 *sampled_values, uint32_t n_batches,
+                              uint32_t *const *out4, void *stream);
+
+/* Wide-Fibonacci composition: out = den_inv * sum_i (c_i^2 + c_{i+1}^2 - c_{i+2}) * powers[N-3-i]. */
+int stwo_wide_fib_composition(const uint32_t *const *trace, uint32_t n_columns, uint32_t ext_log_size,
+                              const stwo_qm31 *coeff_powers, const uint32_t *den_inv, uint32_t *const *out4,
+                              void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STWO_B200_H */

@@ -1,0 +1,12 @@
+"""stwo_gpu_b200 — Blackwell-native CUDA backend for the Stwo prover's hot path.
+
+The compute lives in libstwo_b200.so (CUDA for sm_100a behind the C ABI of
+include/stwo_b200.h); this package is the host-side mirror of the reference's
+backend traits (backend.py) and the ctypes binding (_lib.py).
+"""
+from . import _lib  # noqa: F401
+from .backend import (  # noqa: F401
+    BaseFieldVec, Blake2sHashVec, CanonicCoset, CircleDomain, CircleEvaluation, CirclePoly, ColumnSampleBatch,
+    Coset, CudaBackend, LineDomain, LineEvaluation, SecureColumnByCoords, SecureEvaluation, SecureFieldVec,
+    TwiddleTree, index_to_point,
+)

@@ -1,0 +1,232 @@
+// ColumnOps::bit_reverse_column and FieldOps::batch_inverse.
+//
+// Bit reversal (reference: one thread per swap with uncoalesced 4/16-byte
+// accesses, cuda/src/bit_reverse.cu:6-33). Here, for n = 2^L with L >= 10, the index
+// splits as (a | b | c) with a and c of 5 bits: bitrev(a|b|c) = (rev c | rev b | rev a).
+// A CTA takes the 32x32 block of (a, c) for middle b and the block for rev(b),
+// loads both with 128-byte row reads, and writes each transposed-and-reversed into
+// the other, so every HBM access is a full line and in-place is safe.
+//
+// Batch inverse (reference: per-block product tree in shared memory,
+// cuda/src/batch_inverse.cu:25-155). Here each thread keeps prefix products of its
+// 8 elements in registers, a block-wide multiplicative scan (warp shuffles, then
+// one value per warp) gives the products before and after every thread, one field
+// inversion per CTA inverts the block product, and the back-substitution recovers
+// every inverse: 3 multiplications per element and one inversion per 2048 elements.
+#include "common.cuh"
+
+namespace stwo {
+namespace {
+
+template <int WORDS>
+struct Elem { uint32_t w[WORDS]; };
+
+template <int WORDS>
+__global__ void bitrev_simple_kernel(Elem<WORDS> *a, uint32_t L) {
+    const uint64_t n = 1ull << L;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t j = bit_reverse_bits((uint32_t)i, L);
+        if (j > i) {
+            Elem<WORDS> t = a[i];
+            a[i] = a[j];
+            a[j] = t;
+        }
+    }
+}
+
+// One CTA per (b, rev b) pair with b <= rev b; 256 threads; WORDS words per element.
+template <int WORDS>
+__global__ void __launch_bounds__(256) bitrev_tiled_kernel(uint32_t *a, uint32_t L, const uint32_t *pairs) {
+    __shared__ uint32_t t0[32][32 * WORDS + 1];
+    __shared__ uint32_t t1[32][32 * WORDS + 1];
+    const uint32_t mb = L - 10;  // middle bits
+    const uint32_t b0 = pairs[blockIdx.x];
+    const uint32_t b1 = bit_reverse_bits(b0, mb);
+    const uint32_t tid = threadIdx.x;
+    // Element (a, b, c) lives at index (a << (L-5)) | (b << 5) | c.
+    for (uint32_t e = tid; e < 32 * 32 * WORDS; e += 256) {
+        uint32_t row = e / (32 * WORDS), col = e % (32 * WORDS);
+        uint64_t base0 = (((uint64_t)row << (L - 5)) | ((uint64_t)b0 << 5)) * WORDS;
+        uint64_t base1 = (((uint64_t)row << (L - 5)) | ((uint64_t)b1 << 5)) * WORDS;
+        t0[row][col] = a[base0 + col];
+        t1[row][col] = a[base1 + col];
+    }
+    __syncthreads();
+    // Destination of (a, b0, c) is (rev c, rev b0 = b1, rev a): row rev c of block b1, column rev a.
+    for (uint32_t e = tid; e < 32 * 32 * WORDS; e += 256) {
+        uint32_t row = e / (32 * WORDS), col = e % (32 * WORDS);
+        uint32_t ci = col / WORDS, w = col % WORDS;  // ci = element column within the row
+        uint32_t src_row = bit_reverse_bits(ci, 5), src_c = bit_reverse_bits(row, 5);
+        uint64_t base1 = (((uint64_t)row << (L - 5)) | ((uint64_t)b1 << 5)) * WORDS;
+        uint64_t base0 = (((uint64_t)row << (L - 5)) | ((uint64_t)b0 << 5)) * WORDS;
+        a[base1 + col] = t0[src_row][src_c * WORDS + w];
+        a[base0 + col] = t1[src_row][src_c * WORDS + w];
+    }
+}
+
+// ---------------------------------------------------------------- batch inverse
+constexpr int BI_THREADS = 256;
+constexpr int BI_PER_THREAD = 8;
+
+template <typename F>
+struct FieldT;
+template <>
+struct FieldT<uint32_t> {
+    __device__ static uint32_t one() { return 1u; }
+    __device__ static uint32_t mul(uint32_t a, uint32_t b) { return m31_mul(a, b); }
+    __device__ static uint32_t inv(uint32_t a) { return m31_inv(a); }
+    __device__ static uint32_t shfl_up(uint32_t v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+    __device__ static uint32_t shfl_down(uint32_t v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+};
+template <>
+struct FieldT<qm31> {
+    __device__ static qm31 one() { return qm31_one(); }
+    __device__ static qm31 mul(qm31 a, qm31 b) { return qm31_mul(a, b); }
+    __device__ static qm31 inv(qm31 a) { return qm31_inv(a); }
+    __device__ static qm31 shfl_up(qm31 v, int d) {
+        return {{__shfl_up_sync(0xffffffffu, v.a.a, d), __shfl_up_sync(0xffffffffu, v.a.b, d)},
+                {__shfl_up_sync(0xffffffffu, v.b.a, d), __shfl_up_sync(0xffffffffu, v.b.b, d)}};
+    }
+    __device__ static qm31 shfl_down(qm31 v, int d) {
+        return {{__shfl_down_sync(0xffffffffu, v.a.a, d), __shfl_down_sync(0xffffffffu, v.a.b, d)},
+                {__shfl_down_sync(0xffffffffu, v.b.a, d), __shfl_down_sync(0xffffffffu, v.b.b, d)}};
+    }
+};
+
+template <typename F>
+__global__ void __launch_bounds__(BI_THREADS) batch_inverse_kernel(const F *__restrict__ src, F *__restrict__ dst,
+                                                                    uint64_t n) {
+    using T = FieldT<F>;
+    __shared__ F warp_pre[BI_THREADS / 32], warp_suf[BI_THREADS / 32];
+    __shared__ F block_inv;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint64_t base = (uint64_t)blockIdx.x * (BI_THREADS * BI_PER_THREAD) + (uint64_t)tid * BI_PER_THREAD;
+    F v[BI_PER_THREAD], pre[BI_PER_THREAD];
+    F run = T::one();
+#pragma unroll
+    for (int i = 0; i < BI_PER_THREAD; i++) {
+        v[i] = (base + i < n) ? src[base + i] : T::one();
+        run = T::mul(run, v[i]);
+        pre[i] = run;
+    }
+    // Inclusive warp scans of thread totals, forward and backward.
+    F inc = run, suf = run;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        F u = T::shfl_up(inc, d);
+        F w = T::shfl_down(suf, d);
+        if (lane >= (uint32_t)d) inc = T::mul(inc, u);
+        if (lane + d < 32u) suf = T::mul(suf, w);
+    }
+    if (lane == 31) warp_pre[warp] = inc;
+    if (lane == 0) warp_suf[warp] = suf;
+    __syncthreads();
+    // Products of whole warps before / after this warp.
+    F before_w = T::one(), after_w = T::one();
+    for (uint32_t w = 0; w < BI_THREADS / 32; w++) {
+        if (w < warp) before_w = T::mul(before_w, warp_pre[w]);
+        if (w > warp) after_w = T::mul(after_w, warp_suf[w]);
+    }
+    if (tid == 0) {
+        F total = T::one();
+        for (uint32_t w = 0; w < BI_THREADS / 32; w++) total = T::mul(total, warp_pre[w]);
+        block_inv = T::inv(total);
+    }
+    // Exclusive products within the warp.
+    F ex_pre = T::shfl_up(inc, 1), ex_suf = T::shfl_down(suf, 1);
+    if (lane == 0) ex_pre = T::one();
+    if (lane == 31) ex_suf = T::one();
+    __syncthreads();
+    // inverse of this thread's product = block_inv * (everything before) * (everything after)
+    F r = T::mul(T::mul(block_inv, T::mul(before_w, ex_pre)), T::mul(ex_suf, after_w));
+#pragma unroll
+    for (int i = BI_PER_THREAD - 1; i >= 0; i--) {
+        F inv_i = i > 0 ? T::mul(r, pre[i - 1]) : r;
+        if (base + i < n) dst[base + i] = inv_i;
+        r = T::mul(r, v[i]);
+    }
+}
+
+}  // namespace
+
+int bit_reverse_async(uint32_t *col, uint64_t n, uint32_t words, cudaStream_t st) {
+    STWO_REQUIRE(is_pow2(n) && n <= (1ull << 31), STWO_ERR_INVALID_ARGUMENT, "bit reverse of %llu elements",
+                 (unsigned long long)n);
+    STWO_REQUIRE(words == 1 || words == 4, STWO_ERR_INVALID_ARGUMENT, "element of %u words", words);
+    uint32_t L = log2_u64(n);
+    if (L < 10) {
+        uint32_t blocks = (uint32_t)((n + 255) / 256);
+        if (words == 1) bitrev_simple_kernel<1><<<blocks, 256, 0, st>>>(reinterpret_cast<Elem<1> *>(col), L);
+        else bitrev_simple_kernel<4><<<blocks, 256, 0, st>>>(reinterpret_cast<Elem<4> *>(col), L);
+        STWO_LAUNCH_CHECK("bitrev_simple_kernel");
+        return STWO_OK;
+    }
+    // Middle indices b with b <= rev(b): built on the host once per size and cached.
+    static uint32_t *pairs_dev[32] = {nullptr};
+    static uint32_t pairs_cnt[32] = {0};
+    uint32_t mb = L - 10;
+    if (!pairs_dev[L]) {
+        uint32_t m = 1u << mb, cnt = 0;
+        uint32_t *h = (uint32_t *)malloc(sizeof(uint32_t) * m);
+        for (uint32_t b = 0; b < m; b++)
+            if (b <= bit_reverse_bits(b, mb)) h[cnt++] = b;
+        uint32_t *d = nullptr;
+        cudaError_t e = cudaMalloc(&d, sizeof(uint32_t) * cnt);
+        if (e == cudaSuccess) e = cudaMemcpy(d, h, sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice);
+        free(h);
+        if (e != cudaSuccess) return set_error(STWO_ERR_CUDA, "bit reverse table: %s", cudaGetErrorString(e));
+        pairs_dev[L] = d;
+        pairs_cnt[L] = cnt;
+    }
+    if (words == 1) bitrev_tiled_kernel<1><<<pairs_cnt[L], 256, 0, st>>>(col, L, pairs_dev[L]);
+    else bitrev_tiled_kernel<4><<<pairs_cnt[L], 256, 0, st>>>(col, L, pairs_dev[L]);
+    STWO_LAUNCH_CHECK("bitrev_tiled_kernel");
+    return STWO_OK;
+}
+
+int batch_inverse_m31_async(const uint32_t *src, uint32_t *dst, uint64_t n, cudaStream_t st) {
+    if (n == 0) return STWO_OK;
+    uint64_t blocks = (n + BI_THREADS * BI_PER_THREAD - 1) / (BI_THREADS * BI_PER_THREAD);
+    batch_inverse_kernel<uint32_t><<<(unsigned)blocks, BI_THREADS, 0, st>>>(src, dst, n);
+    STWO_LAUNCH_CHECK("batch_inverse_kernel<m31>");
+    return STWO_OK;
+}
+
+int batch_inverse_qm31_async(const uint32_t *src, uint32_t *dst, uint64_t n, cudaStream_t st) {
+    if (n == 0) return STWO_OK;
+    uint64_t blocks = (n + BI_THREADS * BI_PER_THREAD - 1) / (BI_THREADS * BI_PER_THREAD);
+    batch_inverse_kernel<qm31><<<(unsigned)blocks, BI_THREADS, 0, st>>>(reinterpret_cast<const qm31 *>(src),
+                                                                         reinterpret_cast<qm31 *>(dst), n);
+    STWO_LAUNCH_CHECK("batch_inverse_kernel<qm31>");
+    return STWO_OK;
+}
+
+}  // namespace stwo
+
+using namespace stwo;
+
+extern "C" {
+
+int stwo_bit_reverse_m31(uint32_t *column, uint64_t n, void *stream) {
+    return bit_reverse_async(column, n, 1, as_stream(stream));
+}
+int stwo_bit_reverse_qm31(uint32_t *column, uint64_t n, void *stream) {
+    return bit_reverse_async(column, n, 4, as_stream(stream));
+}
+int stwo_batch_inverse_m31(const uint32_t *src, uint32_t *dst, uint64_t n, void *stream) {
+    return batch_inverse_m31_async(src, dst, n, as_stream(stream));
+}
+int stwo_batch_inverse_qm31(const uint32_t *src, uint32_t *dst, uint64_t n, void *stream) {
+    return batch_inverse_qm31_async(src, dst, n, as_stream(stream));
+}
+
+void bit_reverse_base_field(uint32_t *array, size_t size) { sync_default_stream(bit_reverse_async(array, size, 1, 0)); }
+void bit_reverse_secure_field(uint32_t *array, size_t size) { sync_default_stream(bit_reverse_async(array, size, 4, 0)); }
+void batch_inverse_base_field(const uint32_t *from, uint32_t *dst, size_t size) {
+    sync_default_stream(batch_inverse_m31_async(from, dst, size, 0));
+}
+void batch_inverse_secure_field(const uint32_t *from, uint32_t *dst, size_t size) {
+    sync_default_stream(batch_inverse_qm31_async(from, dst, size, 0));
+}
+
+}  // extern "C"

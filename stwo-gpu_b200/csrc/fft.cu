@@ -1,0 +1,387 @@
+// Circle FFT (evaluate / interpolate) over M31 columns in bit-reversed order.
+//
+// Semantics follow PolyOps::evaluate / interpolate of the reference
+// (cuda/src/poly/rfft.cu:5-141, ifft.cu:3-163, poly/utils.cu:3-22): layer k >= 1
+// of a size-2^N transform pairs indices that differ in bit k, with twiddle
+// line_twiddles[k-1][i >> (k+1)] read from the suffix of the twiddle tree that
+// belongs to the domain; layer 0 (the circle layer) derives its twiddle from the
+// first line layer's pairs [x, y] as [y, -y, -x, x]. Evaluate runs layers N-1..0
+// with butterfly (a + t b, a - t b); interpolate runs 0..N-1 with
+// (a + b, (a - b) t) and rescales by 2^-N.
+//
+// B200 design (not the reference's one-launch-per-layer scheme):
+//  * A pass applies a contiguous range of layers [lo, hi) to tiles of up to 2^15
+//    elements (128 KB) held in shared memory. The bottom pass works on contiguous
+//    tiles; passes for higher layers use "strided" tiles of 2^(hi-lo) rows x 2^c
+//    contiguous words (c >= 5, full 128-byte lines), so every HBM access is a
+//    coalesced 16-byte vector access. A 2^24 column takes 2 passes, not 24.
+//  * Inside a tile each thread owns 2^e elements (e <= 6) and applies up to e
+//    layers per round in registers, touching shared memory once per round.
+//    The XOR swizzle S(j) = j ^ ((j>>5 ^ j>>10) & 31) keeps every access pattern
+//    used here (consecutive lanes on any 5-bit window below bit 15) free of bank
+//    conflicts.
+//  * Twiddles are read from the tree through the read-only path and doubled once
+//    for the shift-free M31 product (field.cuh).
+//  * Zero extension for evaluate is fused into the first pass (the upper layers
+//    of a zero-padded input only copy it), the 2^-N rescale into the last pass.
+//  * One launch serves many columns of the same size; columns of different sizes
+//    use separate launches on the same stream.
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+
+namespace stwo {
+namespace {
+
+constexpr int MAX_TILE_LOG = 15;
+constexpr int MAX_THREADS_LOG = 9;
+constexpr int MAX_COLS_PER_LAUNCH = 64;
+
+struct FftColumn {
+    const uint32_t *src;
+    uint32_t *dst;
+};
+
+struct FftLaunch {
+    FftColumn cols[MAX_COLS_PER_LAUNCH];
+    const uint32_t *tw;   // suffix of the tree for a size-2^N domain (2^(N-1) entries)
+    uint32_t N;           // log size of the (virtual) transform
+    uint32_t lo, hi;      // layers [lo, hi) applied by this pass
+    uint32_t c;           // low global bits [0, c) spanned by a tile row
+    uint32_t tile_log;    // log2 of tile elements = c + (hi - lo)
+    uint32_t src_mask;    // src index mask (2^L - 1 for an extension read, else all ones)
+    uint32_t scale2;      // 2 * scale factor applied on store, 0 = none
+};
+
+__device__ __forceinline__ uint32_t swz(uint32_t j) { return j ^ (((j >> 5) ^ (j >> 10)) & 31u); }
+
+// Doubled twiddle for layer k, group h.
+__device__ __forceinline__ uint32_t twiddle2(const uint32_t *__restrict__ tw, uint32_t N, uint32_t k, uint32_t h) {
+    if (k == 0) {
+        uint32_t q = h >> 2, r = h & 3u;
+        uint32_t v = __ldg(tw + 2 * q + ((r >> 1) ^ 1u));
+        if (r == 1u || r == 2u) v = m31_neg(v);
+        return v << 1;
+    }
+    uint32_t off = (1u << (N - 1)) - (1u << (N - k));
+    return __ldg(tw + off + h) << 1;
+}
+
+template <bool INV>
+__device__ __forceinline__ void butterfly(uint32_t &a, uint32_t &b, uint32_t t2) {
+    if (INV) {
+        uint32_t s = m31_add(a, b), d = m31_sub(a, b);
+        a = s;
+        b = m31_mul2(d, t2);
+    } else {
+        uint32_t t = m31_mul2(b, t2);
+        b = m31_sub(a, t);
+        a = m31_add(a, t);
+    }
+}
+
+struct TileGeom {
+    uint32_t gfix, cmask, c, lo;
+    __device__ __forceinline__ uint32_t gidx(uint32_t j) const { return gfix | (j & cmask) | ((j >> c) << lo); }
+};
+
+// One round: each thread applies the RB layers of tile bits [a, a+RB) to its
+// 2^LOG_E elements (2^(LOG_E-RB) groups of 2^RB).
+template <int RB, int LOG_E, bool INV>
+__device__ __forceinline__ void fft_round(uint32_t *sm, const FftLaunch &p, const TileGeom &g, uint32_t a,
+                                          uint32_t W) {
+    constexpr int R = 1 << RB;
+    constexpr int GROUPS = 1 << (LOG_E - RB);
+    const uint32_t amask = (1u << a) - 1u;
+    const uint32_t k0 = p.lo + (a - p.c);  // global layer of bit a
+#pragma unroll 1
+    for (int grp = 0; grp < GROUPS; grp++) {
+        uint32_t x = threadIdx.x | ((uint32_t)grp << W);
+        uint32_t jb = (x & amask) | ((x >> a) << (a + RB));
+        uint32_t gb = g.gidx(jb);
+        uint32_t v[R];
+#pragma unroll
+        for (int m = 0; m < R; m++) v[m] = sm[swz(jb | ((uint32_t)m << a))];
+#pragma unroll
+        for (int uu = 0; uu < RB; uu++) {
+            const int u = INV ? uu : RB - 1 - uu;
+            const uint32_t k = k0 + u;
+            const uint32_t hb = gb >> (k + 1);
+#pragma unroll
+            for (int q = 0; q < (R >> (u + 1)); q++) {
+                uint32_t t2 = twiddle2(p.tw, p.N, k, hb + q);
+#pragma unroll
+                for (int l = 0; l < (1 << u); l++) {
+                    const int m0 = (q << (u + 1)) | l;
+                    butterfly<INV>(v[m0], v[m0 | (1 << u)], t2);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < R; m++) sm[swz(jb | ((uint32_t)m << a))] = v[m];
+    }
+}
+
+template <int LOG_E, bool INV>
+__device__ __forceinline__ void fft_round_dispatch(int rb, uint32_t *sm, const FftLaunch &p, const TileGeom &g,
+                                                   uint32_t a, uint32_t W) {
+    switch (rb) {
+    case 1: fft_round<1, LOG_E, INV>(sm, p, g, a, W); break;
+    case 2: if constexpr (LOG_E >= 2) fft_round<2, LOG_E, INV>(sm, p, g, a, W); break;
+    case 3: if constexpr (LOG_E >= 3) fft_round<3, LOG_E, INV>(sm, p, g, a, W); break;
+    case 4: if constexpr (LOG_E >= 4) fft_round<4, LOG_E, INV>(sm, p, g, a, W); break;
+    case 5: if constexpr (LOG_E >= 5) fft_round<5, LOG_E, INV>(sm, p, g, a, W); break;
+    case 6: if constexpr (LOG_E >= 6) fft_round<6, LOG_E, INV>(sm, p, g, a, W); break;
+    default: break;
+    }
+}
+
+template <int LOG_E, bool INV>
+__global__ void __launch_bounds__(1 << MAX_THREADS_LOG) fft_pass_kernel(const __grid_constant__ FftLaunch p) {
+    extern __shared__ uint32_t sm[];
+    const uint32_t tile = 1u << p.tile_log;
+    const uint32_t W = p.tile_log - LOG_E;  // log2(threads)
+    const uint32_t tiles_log = p.N - p.tile_log;
+    const uint32_t col = blockIdx.x >> tiles_log;
+    const uint32_t T = blockIdx.x & ((1u << tiles_log) - 1u);
+    const uint32_t low_fixed = p.lo - p.c;  // fixed bits [c, lo)
+    TileGeom g;
+    g.c = p.c;
+    g.lo = p.lo;
+    g.cmask = (1u << p.c) - 1u;
+    g.gfix = ((T & ((1u << low_fixed) - 1u)) << p.c) | ((T >> low_fixed) << p.hi);
+
+    const uint32_t *__restrict__ src = p.cols[col].src;
+    uint32_t *__restrict__ dst = p.cols[col].dst;
+
+    // Global -> shared: 4 consecutive tile elements are 4 consecutive words.
+    for (uint32_t j = threadIdx.x * 4; j < tile; j += blockDim.x * 4) {
+        uint32_t gi = g.gidx(j) & p.src_mask;
+        uint4 v = __ldg(reinterpret_cast<const uint4 *>(src + gi));
+        sm[swz(j)] = v.x;
+        sm[swz(j + 1)] = v.y;
+        sm[swz(j + 2)] = v.z;
+        sm[swz(j + 3)] = v.w;
+    }
+    __syncthreads();
+
+    const int g_bits = (int)(p.hi - p.lo);
+    if (INV) {
+        for (int s = 0; s < g_bits; s += LOG_E) {
+            int rb = min(LOG_E, g_bits - s);
+            fft_round_dispatch<LOG_E, INV>(rb, sm, p, g, p.c + s, W);
+            __syncthreads();
+        }
+    } else {
+        for (int top = g_bits; top > 0; top -= LOG_E) {
+            int rb = min(LOG_E, top);
+            fft_round_dispatch<LOG_E, INV>(rb, sm, p, g, p.c + (top - rb), W);
+            __syncthreads();
+        }
+    }
+
+    for (uint32_t j = threadIdx.x * 4; j < tile; j += blockDim.x * 4) {
+        uint4 v;
+        v.x = sm[swz(j)];
+        v.y = sm[swz(j + 1)];
+        v.z = sm[swz(j + 2)];
+        v.w = sm[swz(j + 3)];
+        if (p.scale2) {
+            v.x = m31_mul2(v.x, p.scale2);
+            v.y = m31_mul2(v.y, p.scale2);
+            v.z = m31_mul2(v.z, p.scale2);
+            v.w = m31_mul2(v.w, p.scale2);
+        }
+        *reinterpret_cast<uint4 *>(dst + g.gidx(j)) = v;
+    }
+}
+
+// Transforms of 2 and 4 elements. The circle twiddle is y of the half coset's
+// first point, which the tree does not store for these sizes; it is derived from
+// the first line layer of the next larger domain ([x', y'] with y = 2 x' y'), so
+// the tree must cover at least an 8-element domain.
+struct TinyLaunch {
+    FftColumn cols[MAX_COLS_PER_LAUNCH];
+    uint32_t N;
+    uint32_t t_x, t_y;   // (i)twiddles: x and y of the first half-coset point (or inverses)
+    uint32_t scale;
+};
+
+template <bool INV>
+__global__ void fft_tiny_kernel(const __grid_constant__ TinyLaunch p) {
+    uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= gridDim.x * blockDim.x) return;
+    if (p.cols[col].src == nullptr) return;
+    const uint32_t *src = p.cols[col].src;
+    uint32_t *dst = p.cols[col].dst;
+    uint32_t y2 = p.t_y << 1, ny2 = m31_neg(p.t_y) << 1, x2 = p.t_x << 1;
+    if (p.N == 1) {
+        uint32_t a = src[0], b = src[1];
+        butterfly<INV>(a, b, y2);
+        if (INV) { a = m31_mul(a, p.scale); b = m31_mul(b, p.scale); }
+        dst[0] = a;
+        dst[1] = b;
+    } else {
+        uint32_t v0 = src[0], v1 = src[1], v2 = src[2], v3 = src[3];
+        if (INV) {
+            butterfly<true>(v0, v1, y2);
+            butterfly<true>(v2, v3, ny2);
+            butterfly<true>(v0, v2, x2);
+            butterfly<true>(v1, v3, x2);
+            v0 = m31_mul(v0, p.scale); v1 = m31_mul(v1, p.scale);
+            v2 = m31_mul(v2, p.scale); v3 = m31_mul(v3, p.scale);
+        } else {
+            butterfly<false>(v0, v2, x2);
+            butterfly<false>(v1, v3, x2);
+            butterfly<false>(v0, v1, y2);
+            butterfly<false>(v2, v3, ny2);
+        }
+        dst[0] = v0; dst[1] = v1; dst[2] = v2; dst[3] = v3;
+    }
+}
+
+template <int LOG_E, bool INV>
+int launch_pass_t(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
+    const uint32_t threads = 1u << (p.tile_log - LOG_E);
+    const size_t smem = sizeof(uint32_t) << p.tile_log;
+    auto kern = fft_pass_kernel<LOG_E, INV>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        STWO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(sizeof(uint32_t) << MAX_TILE_LOG)));
+        attr_set = true;
+    }
+    const uint64_t blocks = (uint64_t)n_cols << (p.N - p.tile_log);
+    STWO_REQUIRE(blocks < (1ull << 31), STWO_ERR_UNSUPPORTED_SIZE, "fft grid too large");
+    kern<<<(unsigned)blocks, threads, smem, st>>>(p);
+    STWO_LAUNCH_CHECK("fft_pass_kernel");
+    return STWO_OK;
+}
+
+int launch_pass(const FftLaunch &p, uint32_t n_cols, bool inv, cudaStream_t st) {
+    // Threads per tile: up to 512, at least 4 elements per thread.
+    uint32_t W = std::min<uint32_t>(MAX_THREADS_LOG, p.tile_log >= 2 ? p.tile_log - 2 : 0);
+    int log_e = (int)(p.tile_log - W);
+    switch (log_e) {
+#define STWO_FFT_CASE(E) \
+    case E: return inv ? launch_pass_t<E, true>(p, n_cols, st) : launch_pass_t<E, false>(p, n_cols, st);
+        STWO_FFT_CASE(2)
+        STWO_FFT_CASE(3)
+        STWO_FFT_CASE(4)
+        STWO_FFT_CASE(5)
+        STWO_FFT_CASE(6)
+#undef STWO_FFT_CASE
+    default:
+        return set_error(STWO_ERR_UNSUPPORTED_SIZE, "fft tile of 2^%u elements unsupported", p.tile_log);
+    }
+}
+
+struct PassSpec { uint32_t lo, hi, c, tile_log; };
+
+// Layer ranges for a transform whose non-trivial layers are [0, L): a bottom
+// contiguous pass of up to 15 layers and strided passes of up to 10 layers above.
+std::vector<PassSpec> plan_passes(uint32_t L) {
+    std::vector<PassSpec> v;
+    if (L <= (uint32_t)MAX_TILE_LOG) {
+        v.push_back({0, L, 0, L});
+        return v;
+    }
+    v.push_back({0, (uint32_t)MAX_TILE_LOG, 0, (uint32_t)MAX_TILE_LOG});
+    uint32_t lo = MAX_TILE_LOG;
+    const uint32_t max_g = MAX_TILE_LOG - 5;
+    while (lo < L) {
+        uint32_t rem = L - lo;
+        uint32_t chunks = (rem + max_g - 1) / max_g;
+        uint32_t g = (rem + chunks - 1) / chunks;
+        v.push_back({lo, lo + g, MAX_TILE_LOG - g, (uint32_t)MAX_TILE_LOG});
+        lo += g;
+    }
+    return v;
+}
+
+// Derives (x, y) of the first point of the half coset of a 2^N domain (N <= 2)
+// from the tree's first line layer of the 8-element domain: [x8, y8] with
+// (x, y) of the 4-element half coset point = (2 x8^2 - 1, 2 x8 y8) and the
+// 2-element one its double. For the inverse tree the inverses are derived.
+int tiny_twiddles(const uint32_t *tree, uint64_t tree_size, uint32_t N, bool inv, uint32_t *tx, uint32_t *ty,
+                  cudaStream_t st) {
+    STWO_REQUIRE(tree_size >= 4, STWO_ERR_UNSUPPORTED_SIZE,
+                 "a 2^%u-point transform needs a twiddle tree of at least 4 entries", N);
+    uint32_t l8[2];
+    STWO_CUDA_TRY(cudaMemcpyAsync(l8, tree + tree_size - 4, sizeof(l8), cudaMemcpyDeviceToHost, st));
+    STWO_CUDA_TRY(cudaStreamSynchronize(st));
+    uint32_t x8 = inv ? m31_inv(l8[0]) : l8[0];
+    uint32_t y8 = inv ? m31_inv(l8[1]) : l8[1];
+    uint32_t x = m31_sub(m31_add(m31_sqr(x8), m31_sqr(x8)), 1), y = m31_mul(m31_add(x8, x8), y8);
+    if (N == 1) {
+        uint32_t nx = m31_sub(m31_add(m31_sqr(x), m31_sqr(x)), 1), ny = m31_mul(m31_add(x, x), y);
+        x = nx;
+        y = ny;
+    }
+    *tx = inv ? m31_inv(x) : x;
+    *ty = inv ? m31_inv(y) : y;
+    return STWO_OK;
+}
+
+}  // namespace
+
+// Runs a transform over n_cols columns of one size. src[i] may equal dst[i]
+// (in place); for an extension read (L < N) src holds 2^L coefficients.
+int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
+                const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st) {
+    if (n_cols == 0) return STWO_OK;
+    STWO_REQUIRE(N >= 1 && N <= 30 && L <= N, STWO_ERR_UNSUPPORTED_SIZE, "fft log size %u unsupported", N);
+    STWO_REQUIRE(tree != nullptr, STWO_ERR_INVALID_ARGUMENT, "null twiddle tree");
+    if (N <= 2) {
+        STWO_REQUIRE(L == N, STWO_ERR_UNSUPPORTED_SIZE, "extension to a 2^%u domain unsupported", N);
+        TinyLaunch t{};
+        t.N = N;
+        int rc = tiny_twiddles(tree, tree_size, N, inv, &t.t_x, &t.t_y, st);
+        if (rc) return rc;
+        t.scale = m31_inv_pow2(N);
+        for (uint32_t base = 0; base < n_cols; base += MAX_COLS_PER_LAUNCH) {
+            uint32_t cnt = std::min<uint32_t>(MAX_COLS_PER_LAUNCH, n_cols - base);
+            for (uint32_t i = 0; i < MAX_COLS_PER_LAUNCH; i++)
+                t.cols[i] = i < cnt ? FftColumn{srcs[base + i], dsts[base + i]} : FftColumn{nullptr, nullptr};
+            if (inv) fft_tiny_kernel<true><<<1, cnt, 0, st>>>(t);
+            else fft_tiny_kernel<false><<<1, cnt, 0, st>>>(t);
+            STWO_LAUNCH_CHECK("fft_tiny_kernel");
+        }
+        return STWO_OK;
+    }
+    STWO_REQUIRE(tree_size >= (1ull << (N - 1)), STWO_ERR_INVALID_ARGUMENT,
+                 "twiddle tree of %llu entries is smaller than the 2^%u domain's half coset",
+                 (unsigned long long)tree_size, N);
+    STWO_REQUIRE(L >= 2, STWO_ERR_UNSUPPORTED_SIZE, "extension from fewer than 4 coefficients unsupported");
+    for (uint32_t i = 0; i < n_cols; i++) {
+        STWO_REQUIRE(srcs[i] && dsts[i], STWO_ERR_INVALID_ARGUMENT, "null column pointer");
+        STWO_REQUIRE(((uintptr_t)srcs[i] & 15) == 0 && ((uintptr_t)dsts[i] & 15) == 0, STWO_ERR_INVALID_ARGUMENT,
+                     "column pointers must be 16-byte aligned");
+    }
+    FftLaunch p{};
+    p.tw = tree + (tree_size - (1ull << (N - 1)));
+    p.N = N;
+    std::vector<PassSpec> passes = plan_passes(L);
+    if (!inv) std::reverse(passes.begin(), passes.end());
+    for (size_t pi = 0; pi < passes.size(); pi++) {
+        const PassSpec &ps = passes[pi];
+        p.lo = ps.lo;
+        p.hi = ps.hi;
+        p.c = ps.c;
+        p.tile_log = ps.tile_log;
+        bool first = pi == 0, last = pi + 1 == passes.size();
+        p.src_mask = (first && L < N) ? ((1u << L) - 1u) : 0xffffffffu;
+        p.scale2 = (inv && last) ? (m31_inv_pow2(N) << 1) : 0u;
+        for (uint32_t base = 0; base < n_cols; base += MAX_COLS_PER_LAUNCH) {
+            uint32_t cnt = std::min<uint32_t>(MAX_COLS_PER_LAUNCH, n_cols - base);
+            for (uint32_t i = 0; i < cnt; i++)
+                p.cols[i] = FftColumn{first ? srcs[base + i] : dsts[base + i], dsts[base + i]};
+            int rc = launch_pass(p, cnt, inv, st);
+            if (rc) return rc;
+        }
+    }
+    return STWO_OK;
+}
+
+}  // namespace stwo

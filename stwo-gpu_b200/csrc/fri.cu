@@ -1,0 +1,150 @@
+// FriOps::fold_line and FriOps::fold_circle_into_line on SoA QM31 columns.
+//
+// fold_line (cuda/src/fri/fold_line.cu:5-53, stwo_gpu_backend/src/fri.rs:16-43):
+//   out[i] = (f[2i] + f[2i+1]) + alpha * (f[2i] - f[2i+1]) * itw[off + i]
+// fold_circle_into_line (fold_circle_into_line.cu:7-69, fri.rs:45-66):
+//   f' = same with the circle itwiddle of (itw + off) at i (pattern [y,-y,-x,x]),
+//   dst[i] = dst[i] * alpha^2 + f'.
+// Each thread folds two adjacent outputs, reading one 16-byte vector per input
+// coordinate column and writing one 8-byte vector per output column.
+#include "common.cuh"
+
+namespace stwo {
+namespace {
+
+struct Cols4 { const uint32_t *c[4]; };
+struct MutCols4 { uint32_t *c[4]; };
+
+__device__ __forceinline__ uint32_t circle_itw(const uint32_t *__restrict__ lt0, uint64_t h) {
+    uint64_t q = h >> 2;
+    uint32_t r = (uint32_t)(h & 3u);
+    uint32_t v = __ldg(lt0 + 2 * q + ((r >> 1) ^ 1u));
+    return (r == 1u || r == 2u) ? m31_neg(v) : v;
+}
+
+__device__ __forceinline__ qm31 fold_pair(qm31 a, qm31 b, uint32_t t, qm31 alpha) {
+    qm31 s = qm31_add(a, b);
+    qm31 d = qm31_scale(qm31_sub(a, b), t);
+    return qm31_add(s, qm31_mul(alpha, d));
+}
+
+template <bool CIRCLE>
+__global__ void fold_kernel(const __grid_constant__ Cols4 src, const __grid_constant__ MutCols4 dst, uint64_t n_out,
+                            const uint32_t *__restrict__ tw, qm31 alpha, qm31 alpha_sq) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; 2 * k < n_out;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = 2 * k;  // outputs i, i+1 <- inputs 2i .. 2i+3
+        uint32_t in[4][4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            uint4 v = __ldg(reinterpret_cast<const uint4 *>(src.c[c]) + k);
+            in[c][0] = v.x; in[c][1] = v.y; in[c][2] = v.z; in[c][3] = v.w;
+        }
+        qm31 f0 = {{in[0][0], in[1][0]}, {in[2][0], in[3][0]}};
+        qm31 f1 = {{in[0][1], in[1][1]}, {in[2][1], in[3][1]}};
+        qm31 f2 = {{in[0][2], in[1][2]}, {in[2][2], in[3][2]}};
+        qm31 f3 = {{in[0][3], in[1][3]}, {in[2][3], in[3][3]}};
+        uint32_t t0, t1;
+        if (CIRCLE) {
+            t0 = circle_itw(tw, i);
+            t1 = circle_itw(tw, i + 1);
+        } else {
+            uint2 tt = __ldg(reinterpret_cast<const uint2 *>(tw + i));
+            t0 = tt.x;
+            t1 = tt.y;
+        }
+        qm31 r0 = fold_pair(f0, f1, t0, alpha);
+        qm31 r1 = fold_pair(f2, f3, t1, alpha);
+        if (CIRCLE) {
+            uint2 d[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++) d[c] = *(reinterpret_cast<const uint2 *>(dst.c[c]) + k);
+            qm31 p0 = {{d[0].x, d[1].x}, {d[2].x, d[3].x}};
+            qm31 p1 = {{d[0].y, d[1].y}, {d[2].y, d[3].y}};
+            r0 = qm31_add(qm31_mul(p0, alpha_sq), r0);
+            r1 = qm31_add(qm31_mul(p1, alpha_sq), r1);
+        }
+        *(reinterpret_cast<uint2 *>(dst.c[0]) + k) = make_uint2(r0.a.a, r1.a.a);
+        *(reinterpret_cast<uint2 *>(dst.c[1]) + k) = make_uint2(r0.a.b, r1.a.b);
+        *(reinterpret_cast<uint2 *>(dst.c[2]) + k) = make_uint2(r0.b.a, r1.b.a);
+        *(reinterpret_cast<uint2 *>(dst.c[3]) + k) = make_uint2(r0.b.b, r1.b.b);
+    }
+}
+
+// Tiny folds (n_out == 1) use a scalar path.
+template <bool CIRCLE>
+__global__ void fold_one_kernel(const __grid_constant__ Cols4 src, const __grid_constant__ MutCols4 dst,
+                                const uint32_t *__restrict__ tw, qm31 alpha, qm31 alpha_sq) {
+    qm31 a = {{src.c[0][0], src.c[1][0]}, {src.c[2][0], src.c[3][0]}};
+    qm31 b = {{src.c[0][1], src.c[1][1]}, {src.c[2][1], src.c[3][1]}};
+    uint32_t t = CIRCLE ? circle_itw(tw, 0) : tw[0];
+    qm31 r = fold_pair(a, b, t, alpha);
+    if (CIRCLE) {
+        qm31 p = {{dst.c[0][0], dst.c[1][0]}, {dst.c[2][0], dst.c[3][0]}};
+        r = qm31_add(qm31_mul(p, alpha_sq), r);
+    }
+    dst.c[0][0] = r.a.a; dst.c[1][0] = r.a.b; dst.c[2][0] = r.b.a; dst.c[3][0] = r.b.b;
+}
+
+}  // namespace
+
+int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const uint32_t *itw, uint64_t off,
+               uint32_t *const *dst4, bool circle, cudaStream_t st) {
+    STWO_REQUIRE(n >= 2 && is_pow2(n), STWO_ERR_INVALID_ARGUMENT, "fold of %llu values", (unsigned long long)n);
+    Cols4 s;
+    MutCols4 d;
+    for (int c = 0; c < 4; c++) {
+        s.c[c] = src4[c];
+        d.c[c] = dst4[c];
+        STWO_REQUIRE(((uintptr_t)s.c[c] & 15) == 0 && ((uintptr_t)d.c[c] & 7) == 0, STWO_ERR_INVALID_ARGUMENT,
+                     "fold columns must be 16-byte aligned");
+    }
+    qm31 alpha = {{alpha_c.a, alpha_c.b}, {alpha_c.c, alpha_c.d}};
+    qm31 a2 = qm31_mul(alpha, alpha);
+    const uint32_t *tw = itw + off;
+    uint64_t n_out = n / 2;
+    if (n_out == 1) {
+        if (circle) fold_one_kernel<true><<<1, 1, 0, st>>>(s, d, tw, alpha, a2);
+        else fold_one_kernel<false><<<1, 1, 0, st>>>(s, d, tw, alpha, a2);
+        STWO_LAUNCH_CHECK("fold_one_kernel");
+        return STWO_OK;
+    }
+    STWO_REQUIRE(circle || ((uintptr_t)tw & 7) == 0, STWO_ERR_INVALID_ARGUMENT,
+                 "fold_line twiddle offset must be even");
+    uint64_t threads = n_out / 2;
+    uint32_t blocks = (uint32_t)((threads + 255) / 256);
+    uint32_t cap = (uint32_t)device_sm_count() * 16;
+    if (blocks > cap) blocks = cap;
+    if (circle) fold_kernel<true><<<blocks, 256, 0, st>>>(s, d, n_out, tw, alpha, a2);
+    else fold_kernel<false><<<blocks, 256, 0, st>>>(s, d, n_out, tw, alpha, a2);
+    STWO_LAUNCH_CHECK("fold_kernel");
+    return STWO_OK;
+}
+
+}  // namespace stwo
+
+using namespace stwo;
+
+extern "C" {
+
+int stwo_fold_line(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha, const uint32_t *itwiddles,
+                   uint64_t twiddle_offset, uint32_t *const *dst4, void *stream) {
+    return fold_async(src4, n, alpha, itwiddles, twiddle_offset, dst4, false, as_stream(stream));
+}
+
+int stwo_fold_circle_into_line(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha, const uint32_t *itwiddles,
+                               uint64_t twiddle_offset, uint32_t *const *dst4, void *stream) {
+    return fold_async(src4, n, alpha, itwiddles, twiddle_offset, dst4, true, as_stream(stream));
+}
+
+void fold_line(const uint32_t *gpu_domain, size_t twiddle_offset, size_t n, uint32_t *const *eval_values,
+               stwo_qm31 alpha, uint32_t *const *folded_values) {
+    sync_default_stream(fold_async(eval_values, n, alpha, gpu_domain, twiddle_offset, folded_values, false, 0));
+}
+
+void fold_circle_into_line(const uint32_t *gpu_domain, size_t twiddle_offset, size_t n, uint32_t *const *eval_values,
+                           stwo_qm31 alpha, uint32_t *const *folded_values) {
+    sync_default_stream(fold_async(eval_values, n, alpha, gpu_domain, twiddle_offset, folded_values, true, 0));
+}
+
+}  // extern "C"

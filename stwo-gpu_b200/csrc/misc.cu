@@ -1,0 +1,210 @@
+// AccumulationOps::accumulate and the wide-Fibonacci composition kernel.
+//
+// accumulate (cuda/src/accumulate.cu:4-26): SoA QM31 left += right, 16-byte vectors.
+//
+// Wide-Fibonacci composition (cuda/src/examples/wide_fibonacci.cu:3-66,
+// stwo_gpu_backend/src/examples/wide_fibonacci.rs:90-141): for every row of the
+// extended domain
+//   out = den_inv * sum_{i < N-2} (c_i^2 + c_{i+1}^2 - c_{i+2}) * powers[N-3-i].
+// The reference launches it with grid and block swapped and clones the column
+// pointer array with the wrong length (.cu:48,54); here the pointers travel in the
+// parameter block, each thread does four consecutive rows (16-byte loads per
+// column), and each QM31 coordinate of the sum accumulates unreduced partial
+// products in 64 bits, reduced once per row.
+#include <memory>
+
+#include "common.cuh"
+
+namespace stwo {
+namespace {
+
+struct Acc4 { uint32_t *l[4]; const uint32_t *r[4]; };
+
+__global__ void accumulate_kernel(const __grid_constant__ Acc4 p, uint64_t n4, uint64_t n) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n4; k += (uint64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            if (4 * k + 3 < n) {
+                uint4 a = reinterpret_cast<const uint4 *>(p.l[c])[k];
+                uint4 b = __ldg(reinterpret_cast<const uint4 *>(p.r[c]) + k);
+                a.x = m31_add(a.x, b.x); a.y = m31_add(a.y, b.y); a.z = m31_add(a.z, b.z); a.w = m31_add(a.w, b.w);
+                reinterpret_cast<uint4 *>(p.l[c])[k] = a;
+            } else {
+                for (uint64_t i = 4 * k; i < n; i++) p.l[c][i] = m31_add(p.l[c][i], p.r[c][i]);
+            }
+        }
+    }
+}
+
+constexpr int WF_MAX_COLS = 2048;
+
+struct WideFibParams {
+    const uint32_t *trace[WF_MAX_COLS];
+    uint32_t *out[4];
+    const uint32_t *den_inv;
+    const qm31 *powers_dev;  // device powers (reference ABI) or null
+    uint32_t n_cols;
+    uint32_t log_size;
+};
+
+__constant__ qm31 c_wf_powers2[WF_MAX_COLS];  // doubled coordinates, host-supplied powers
+
+__device__ __forceinline__ uint32_t mul_lazy_wf(uint32_t a, uint32_t b2) {
+    uint64_t w = (uint64_t)a * b2;
+    return (uint32_t)(w >> 32) + ((uint32_t)w >> 1);
+}
+__device__ __forceinline__ uint32_t reduce64_wf(uint64_t x) {
+    uint64_t s = (x & P) + (x >> 31);
+    s = (s & P) + (s >> 31);
+    return reduce_once((uint32_t)s);
+}
+
+template <bool POWERS_ON_DEVICE>
+__global__ void __launch_bounds__(256) wide_fib_kernel(const __grid_constant__ WideFibParams p) {
+    const uint64_t n = 1ull << p.log_size;
+    const uint64_t quads = (n + 3) / 4;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < quads; k += (uint64_t)gridDim.x * blockDim.x) {
+        const bool full = 4 * k + 3 < n;
+        uint64_t acc[4][4] = {};
+        uint32_t c0[4], c1[4];
+        auto load = [&](uint32_t col, uint32_t *v) {
+            if (full) {
+                uint4 t = __ldg(reinterpret_cast<const uint4 *>(p.trace[col]) + k);
+                v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+            } else {
+                for (int r = 0; r < 4; r++) v[r] = (4 * k + r < n) ? p.trace[col][4 * k + r] : 0u;
+            }
+        };
+        load(0, c0);
+        load(1, c1);
+        uint32_t s0[4], s1[4];
+        for (int r = 0; r < 4; r++) { s0[r] = m31_sqr(c0[r]); s1[r] = m31_sqr(c1[r]); }
+        for (uint32_t i = 0; i + 2 < p.n_cols; i++) {
+            uint32_t c2[4];
+            load(i + 2, c2);
+            qm31 w2;
+            if (POWERS_ON_DEVICE) {
+                qm31 w = p.powers_dev[p.n_cols - 3 - i];
+                w2 = {{w.a.a << 1, w.a.b << 1}, {w.b.a << 1, w.b.b << 1}};
+            } else {
+                w2 = c_wf_powers2[p.n_cols - 3 - i];
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                uint32_t cons = m31_sub(m31_add(s0[r], s1[r]), c2[r]);
+                acc[r][0] += mul_lazy_wf(cons, w2.a.a);
+                acc[r][1] += mul_lazy_wf(cons, w2.a.b);
+                acc[r][2] += mul_lazy_wf(cons, w2.b.a);
+                acc[r][3] += mul_lazy_wf(cons, w2.b.b);
+                s0[r] = s1[r];
+                s1[r] = m31_sqr(c2[r]);
+            }
+        }
+        uint32_t o[4][4];
+        for (int r = 0; r < 4; r++) {
+            uint32_t d = (4 * k + r < n) ? __ldg(p.den_inv + 4 * k + r) : 0u;
+            uint32_t d2 = d << 1;
+            for (int c = 0; c < 4; c++) o[c][r] = m31_mul2(reduce64_wf(acc[r][c]), d2);
+        }
+        for (int c = 0; c < 4; c++) {
+            if (full) reinterpret_cast<uint4 *>(p.out[c])[k] = make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
+            else
+                for (int r = 0; r < 4; r++)
+                    if (4 * k + r < n) p.out[c][4 * k + r] = o[c][r];
+        }
+    }
+}
+
+}  // namespace
+
+int accumulate_async(uint32_t *const *left4, const uint32_t *const *right4, uint64_t n, cudaStream_t st) {
+    Acc4 p;
+    for (int c = 0; c < 4; c++) {
+        p.l[c] = left4[c];
+        p.r[c] = right4[c];
+        STWO_REQUIRE(((uintptr_t)p.l[c] & 15) == 0 && ((uintptr_t)p.r[c] & 15) == 0, STWO_ERR_INVALID_ARGUMENT,
+                     "accumulate columns must be 16-byte aligned");
+    }
+    if (n == 0) return STWO_OK;
+    uint64_t n4 = (n + 3) / 4;
+    uint64_t blocks = (n4 + 255) / 256, cap = (uint64_t)device_sm_count() * 16;
+    if (blocks > cap) blocks = cap;
+    accumulate_kernel<<<(unsigned)blocks, 256, 0, st>>>(p, n4, n);
+    STWO_LAUNCH_CHECK("accumulate_kernel");
+    return STWO_OK;
+}
+
+int wide_fib_async(const uint32_t *const *trace, uint32_t n_cols, uint32_t log_size, const stwo_qm31 *powers_host,
+                   const uint32_t *powers_dev, const uint32_t *den_inv, uint32_t *const *out4, cudaStream_t st) {
+    STWO_REQUIRE(n_cols >= 2 && n_cols <= (uint32_t)WF_MAX_COLS, STWO_ERR_UNSUPPORTED_SIZE,
+                 "wide-Fibonacci composition over %u columns", n_cols);
+    STWO_REQUIRE(log_size <= 31, STWO_ERR_UNSUPPORTED_SIZE, "domain log size %u", log_size);
+    auto p = std::make_unique<WideFibParams>();
+    for (uint32_t i = 0; i < n_cols; i++) {
+        p->trace[i] = trace[i];
+        STWO_REQUIRE(((uintptr_t)trace[i] & 15) == 0, STWO_ERR_INVALID_ARGUMENT, "trace columns must be 16-byte aligned");
+    }
+    for (int c = 0; c < 4; c++) p->out[c] = out4[c];
+    p->den_inv = den_inv;
+    p->n_cols = n_cols;
+    p->log_size = log_size;
+    p->powers_dev = reinterpret_cast<const qm31 *>(powers_dev);
+    uint64_t n = 1ull << log_size, quads = (n + 3) / 4;
+    uint64_t blocks = (quads + 255) / 256, cap = (uint64_t)device_sm_count() * 8;
+    if (blocks > cap) blocks = cap;
+    if (n_cols < 3) {
+        // No constraints: the composition is zero.
+        for (int c = 0; c < 4; c++) STWO_CUDA_TRY(cudaMemsetAsync(out4[c], 0, n * 4, st));
+        return STWO_OK;
+    }
+    if (powers_dev) {
+        wide_fib_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(*p);
+    } else {
+        std::unique_ptr<qm31[]> w2(new qm31[n_cols]);
+        for (uint32_t i = 0; i + 2 < n_cols; i++) {
+            stwo_qm31 v = powers_host[i];
+            w2[i] = {{v.a << 1, v.b << 1}, {v.c << 1, v.d << 1}};
+        }
+        STWO_CUDA_TRY(cudaMemcpyToSymbolAsync(c_wf_powers2, w2.get(), sizeof(qm31) * (n_cols - 2), 0,
+                                              cudaMemcpyHostToDevice, st));
+        wide_fib_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(*p);
+    }
+    STWO_LAUNCH_CHECK("wide_fib_kernel");
+    return STWO_OK;
+}
+
+}  // namespace stwo
+
+using namespace stwo;
+
+extern "C" {
+
+int stwo_accumulate(uint32_t *const *left4, const uint32_t *const *right4, uint64_t n, void *stream) {
+    return accumulate_async(left4, right4, n, as_stream(stream));
+}
+
+void accumulate(uint32_t size, uint32_t *const *left_columns, uint32_t *const *right_columns) {
+    sync_default_stream(accumulate_async(left_columns, const_cast<const uint32_t *const *>(right_columns), size, 0));
+}
+
+int stwo_wide_fib_composition(const uint32_t *const *trace, uint32_t n_columns, uint32_t ext_log_size,
+                              const stwo_qm31 *coeff_powers, const uint32_t *den_inv, uint32_t *const *out4,
+                              void *stream) {
+    return wide_fib_async(trace, n_columns, ext_log_size, coeff_powers, nullptr, den_inv, out4, as_stream(stream));
+}
+
+void evaluate_wide_fibonacci_constraint_quotients_on_domain(
+    uint32_t *quotients_0, uint32_t *quotients_1, uint32_t *quotients_2, uint32_t *quotients_3,
+    uint32_t *const *trace_evaluations, const uint32_t *random_coeff_powers, const uint32_t *denominator_inverses,
+    uint32_t extended_domain_size, uint32_t number_of_columns) {
+    if (!is_pow2(extended_domain_size)) {
+        set_error(STWO_ERR_INVALID_ARGUMENT, "domain size %u is not a power of two", extended_domain_size);
+        return;
+    }
+    uint32_t *out[4] = {quotients_0, quotients_1, quotients_2, quotients_3};
+    sync_default_stream(wide_fib_async(const_cast<const uint32_t *const *>(trace_evaluations), number_of_columns,
+                                       log2_u64(extended_domain_size), nullptr, random_coeff_powers,
+                                       denominator_inverses, out, 0));
+}
+
+}  // extern "C"

@@ -1,0 +1,454 @@
+// PolyOps entry points: twiddle trees, canonic -> bit-reversed reordering,
+// interpolate / evaluate (reference-compatible and native), eval_at_point.
+#include <algorithm>
+#include <map>
+#include <vector>
+
+#include "common.cuh"
+
+namespace stwo {
+
+int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
+                const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st);
+int batch_inverse_m31_async(const uint32_t *src, uint32_t *dst, uint64_t n, cudaStream_t st);
+int bit_reverse_async(uint32_t *col, uint64_t n, uint32_t words, cudaStream_t st);
+
+namespace {
+
+// ------------------------------------------------------------------ twiddles
+// Tree layer j of root coset (I, S, m): entries h < 2^(m-j-1) at offset
+// 2^m - 2^(m-j) hold x(I^(2^j) * S^(2^j * bitrev_{m-j-1}(h))) (twiddles.cu:29-73).
+// Points are products of table entries: pows[b] = S^(2^b), inits[j] = I^(2^j).
+struct TwiddleParams {
+    cpoint pows[32];
+    cpoint inits[32];
+    uint32_t m;
+};
+
+__global__ void twiddle_tree_kernel(const __grid_constant__ TwiddleParams p, uint32_t *tw) {
+    const uint64_t size = 1ull << p.m;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i + 1 < size;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        // layer j: offset 2^m - 2^(m-j) <= i < 2^m - 2^(m-j-1)
+        uint32_t j = 0;
+        while (i >= size - (size >> (j + 1))) j++;
+        uint64_t off = size - (size >> j);
+        uint32_t hl = p.m - j - 1;
+        uint32_t e = bit_reverse_bits((uint32_t)(i - off), hl);
+        cpoint r = p.inits[j];
+        for (uint32_t b = 0; b < hl; b++)
+            if ((e >> b) & 1u) r = point_mul(r, p.pows[b + j]);
+        tw[i] = r.x;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) tw[size - 1] = 1u;
+}
+
+int precompute_tree(cpoint initial, cpoint step, uint32_t m, uint32_t *tw, uint32_t *itw, cudaStream_t st) {
+    STWO_REQUIRE(m <= 30, STWO_ERR_UNSUPPORTED_SIZE, "root coset of log size %u unsupported", m);
+    STWO_REQUIRE(tw || itw, STWO_ERR_INVALID_ARGUMENT, "no output buffer");
+    TwiddleParams p{};
+    p.m = m;
+    cpoint s = step, ini = initial;
+    for (uint32_t b = 0; b < 32; b++) {
+        p.pows[b] = s;
+        p.inits[b] = ini;
+        s = point_mul(s, s);
+        ini = point_mul(ini, ini);
+    }
+    uint64_t size = 1ull << m;
+    uint32_t *dst = tw;
+    uint32_t *tmp = nullptr;
+    if (!dst) {
+        STWO_CUDA_TRY(cudaMallocAsync((void **)&tmp, size * 4, st));
+        dst = tmp;
+    }
+    uint32_t blocks = (uint32_t)std::min<uint64_t>((size + 255) / 256, (uint64_t)device_sm_count() * 16);
+    twiddle_tree_kernel<<<std::max(1u, blocks), 256, 0, st>>>(p, dst);
+    STWO_LAUNCH_CHECK("twiddle_tree_kernel");
+    int rc = STWO_OK;
+    if (itw) rc = batch_inverse_m31_async(dst, itw, size, st);
+    if (tmp) cudaFreeAsync(tmp, st);
+    return rc;
+}
+
+// ------------------------------------------------------------------ canonic order
+// new_canonical_ordered (twiddles.cu:4-27): position br(q) <- src[2q] for q < n/2,
+// src[n - 1 - 2(q - n/2)] otherwise; written as a gather over output positions.
+__global__ void canonic_to_bitrev_kernel(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst, uint32_t L) {
+    const uint64_t n = 1ull << L, half = n >> 1;
+    for (uint64_t pos = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; pos < n; pos += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t q = bit_reverse_bits((uint32_t)pos, L);
+        uint64_t s = q < half ? (q << 1) : (n - 1 - ((q - half) << 1));
+        dst[pos] = __ldg(src + s);
+    }
+}
+
+// ------------------------------------------------------------------ eval_at_point
+// p(P) = sum_i c_i prod_{bit b of i} f_b with f_0 = y, f_1 = x, f_b = pi^(b-1)(x),
+// pi(x) = 2x^2 - 1 (eval_at_point.cu:99-109). Each CTA folds a chunk of 2^CHUNK_LOG
+// coefficients (bits 0..CHUNK_LOG-1) and multiplies by the factors of its chunk
+// index; the last CTA of each polynomial (atomic ticket) adds the partials.
+constexpr int EAP_THREADS = 256;
+constexpr int EAP_PER_THREAD_LOG = 3;
+constexpr int EAP_CHUNK_LOG = 11;  // 256 threads x 8 coefficients
+constexpr int EAP_MAX_POLYS = 32;
+
+struct EapParams {
+    const uint32_t *coeffs[EAP_MAX_POLYS];
+    qm31 factors[EAP_MAX_POLYS][32];
+    uint32_t log_size[EAP_MAX_POLYS];
+    uint32_t block_start[EAP_MAX_POLYS + 1];  // prefix sum of CTAs per polynomial
+    uint32_t n_polys;
+    qm31 *partials;                            // one per CTA
+    uint32_t *tickets;                         // one per polynomial, zero on entry, reset on exit
+    qm31 *results;
+};
+
+__device__ __forceinline__ qm31 shfl_xor_q(qm31 v, int m) {
+    v.a.a = __shfl_xor_sync(0xffffffffu, v.a.a, m);
+    v.a.b = __shfl_xor_sync(0xffffffffu, v.a.b, m);
+    v.b.a = __shfl_xor_sync(0xffffffffu, v.b.a, m);
+    v.b.b = __shfl_xor_sync(0xffffffffu, v.b.b, m);
+    return v;
+}
+
+__global__ void __launch_bounds__(EAP_THREADS) eval_at_point_kernel(const __grid_constant__ EapParams p) {
+    __shared__ qm31 warp_vals[EAP_THREADS / 32];
+    __shared__ bool is_last;
+    uint32_t poly = 0;
+    while (poly + 1 < p.n_polys && blockIdx.x >= p.block_start[poly + 1]) poly++;
+    const uint32_t chunk = blockIdx.x - p.block_start[poly];
+    const uint32_t L = p.log_size[poly];
+    const qm31 *f = p.factors[poly];
+    const uint32_t *c = p.coeffs[poly];
+    const uint32_t tid = threadIdx.x;
+    const uint64_t n = 1ull << L;
+    const uint64_t base = ((uint64_t)chunk << EAP_CHUNK_LOG) + ((uint64_t)tid << EAP_PER_THREAD_LOG);
+
+    // Per-thread fold of 8 coefficients (bits 0..2); bits beyond L read as absent.
+    qm31 acc = qm31_zero();
+    if (base < n) {
+        uint32_t v[8];
+        const uint32_t cnt = (n - base) < 8 ? (uint32_t)(n - base) : 8u;
+        for (uint32_t i = 0; i < 8; i++) v[i] = i < cnt ? __ldg(c + base + i) : 0u;
+        qm31 lvl[4];
+        for (int i = 0; i < 4; i++) {
+            // v[2i] + v[2i+1] * f0
+            qm31 t = qm31_scale(f[0], v[2 * i + 1]);
+            t.a.a = m31_add(t.a.a, v[2 * i]);
+            lvl[i] = t;
+        }
+        lvl[0] = qm31_add(lvl[0], qm31_mul(lvl[1], f[1]));
+        lvl[2] = qm31_add(lvl[2], qm31_mul(lvl[3], f[1]));
+        acc = qm31_add(lvl[0], qm31_mul(lvl[2], f[2]));
+    }
+    // Across lanes: bits 3..7 (lane bit j <-> factor 3 + j).
+    const uint32_t lane = tid & 31u;
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+        qm31 other = shfl_xor_q(acc, 1 << j);
+        // lane with bit j clear keeps lo + hi * f; the other result is discarded.
+        qm31 lo = (lane >> j) & 1u ? other : acc;
+        qm31 hi = (lane >> j) & 1u ? acc : other;
+        acc = qm31_add(lo, qm31_mul(hi, f[3 + j]));
+    }
+    if (lane == 0) warp_vals[tid >> 5] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        // Warps: bits 8..10.
+        qm31 w[8];
+        for (int i = 0; i < 8; i++) w[i] = warp_vals[i];
+        for (int lvl = 0; lvl < 3; lvl++)
+            for (int i = 0; i < (8 >> (lvl + 1)); i++)
+                w[i] = qm31_add(w[2 * i], qm31_mul(w[2 * i + 1], f[8 + lvl]));
+        qm31 s = w[0];
+        // Chunk index bits -> factors 11.. .
+        for (uint32_t b = 0; EAP_CHUNK_LOG + b < L; b++)
+            if ((chunk >> b) & 1u) s = qm31_mul(s, f[EAP_CHUNK_LOG + b]);
+        p.partials[blockIdx.x] = s;
+        __threadfence();
+        uint32_t nblk = p.block_start[poly + 1] - p.block_start[poly];
+        uint32_t t = atomicAdd(&p.tickets[poly], 1u);
+        is_last = (t == nblk - 1);
+    }
+    __syncthreads();
+    if (is_last && tid == 0) {
+        __threadfence();
+        qm31 s = qm31_zero();
+        for (uint32_t b = p.block_start[poly]; b < p.block_start[poly + 1]; b++) {
+            qm31 v;
+            const volatile uint32_t *pv = reinterpret_cast<const volatile uint32_t *>(&p.partials[b]);
+            v.a.a = pv[0]; v.a.b = pv[1]; v.b.a = pv[2]; v.b.b = pv[3];
+            s = qm31_add(s, v);
+        }
+        p.results[poly] = s;
+        p.tickets[poly] = 0;  // ready for the next launch
+    }
+}
+
+inline qm31 to_q(stwo_qm31 v) { return {{v.a, v.b}, {v.c, v.d}}; }
+inline stwo_qm31 from_q(qm31 v) { return {v.a.a, v.a.b, v.b.a, v.b.b}; }
+
+void eap_factors(qm31 *f, stwo_spoint pt, uint32_t L) {
+    // f_0 = y, f_1 = x, f_b = pi^(b-1)(x)
+    for (uint32_t b = 0; b < 32; b++) f[b] = qm31_zero();
+    f[0] = to_q(pt.y);
+    qm31 x = to_q(pt.x);
+    for (uint32_t b = 1; b < std::max<uint32_t>(L, 2u) && b < 32; b++) {
+        f[b] = x;
+        qm31 sq = qm31_mul(x, x);
+        x = qm31_sub(qm31_add(sq, sq), qm31_one());
+    }
+}
+
+uint32_t eap_blocks(uint32_t L) { return L <= (uint32_t)EAP_CHUNK_LOG ? 1u : 1u << (L - EAP_CHUNK_LOG); }
+
+}  // namespace
+
+size_t eval_at_points_scratch_bytes(const uint32_t *log_sizes, uint32_t n_polys) {
+    size_t blocks = 0;
+    for (uint32_t i = 0; i < n_polys; i++) blocks += eap_blocks(log_sizes[i]);
+    return blocks * sizeof(qm31) + ((size_t)n_polys * 4 + 15) / 16 * 16 + 256;
+}
+
+// scratch: partials followed by zeroed tickets (the kernel leaves them zero).
+int eval_at_points_async(const uint32_t *const *coeffs, const uint32_t *log_sizes, uint32_t n_polys,
+                         const stwo_spoint *points, stwo_qm31 *results, void *scratch, size_t scratch_bytes,
+                         bool tickets_zeroed, cudaStream_t st) {
+    STWO_REQUIRE(scratch_bytes >= eval_at_points_scratch_bytes(log_sizes, n_polys), STWO_ERR_INVALID_ARGUMENT,
+                 "eval_at_point scratch too small");
+    size_t blocks_total = 0;
+    for (uint32_t i = 0; i < n_polys; i++) {
+        STWO_REQUIRE(log_sizes[i] <= 30, STWO_ERR_UNSUPPORTED_SIZE, "polynomial of log size %u unsupported", log_sizes[i]);
+        blocks_total += eap_blocks(log_sizes[i]);
+    }
+    uint32_t *tickets = reinterpret_cast<uint32_t *>(static_cast<char *>(scratch) + blocks_total * sizeof(qm31));
+    if (!tickets_zeroed) STWO_CUDA_TRY(cudaMemsetAsync(tickets, 0, (size_t)n_polys * 4, st));
+    qm31 *partials = static_cast<qm31 *>(scratch);
+    uint32_t done = 0;
+    size_t part_off = 0;
+    while (done < n_polys) {
+        EapParams p{};
+        uint32_t cnt = std::min<uint32_t>(EAP_MAX_POLYS, n_polys - done);
+        uint32_t b = 0;
+        for (uint32_t i = 0; i < cnt; i++) {
+            uint32_t L = log_sizes[done + i];
+            p.coeffs[i] = coeffs[done + i];
+            p.log_size[i] = L;
+            eap_factors(p.factors[i], points[done + i], L);
+            p.block_start[i] = b;
+            b += eap_blocks(L);
+        }
+        p.block_start[cnt] = b;
+        p.n_polys = cnt;
+        p.partials = partials + part_off;
+        p.tickets = tickets + done;
+        p.results = reinterpret_cast<qm31 *>(results) + done;
+        eval_at_point_kernel<<<b, EAP_THREADS, 0, st>>>(p);
+        STWO_LAUNCH_CHECK("eval_at_point_kernel");
+        part_off += b;
+        done += cnt;
+    }
+    return STWO_OK;
+}
+
+int extend_evaluate_async(const uint32_t *const *coeffs, const uint32_t *coeff_logs, uint32_t *const *outs,
+                          uint32_t log_blowup, uint32_t n, const uint32_t *tw, uint64_t tree_size, cudaStream_t st) {
+    // Group columns by size so each size is one launch sequence.
+    std::map<uint32_t, std::vector<uint32_t>> by_size;
+    for (uint32_t i = 0; i < n; i++) by_size[coeff_logs[i]].push_back(i);
+    for (auto &kv : by_size) {
+        std::vector<const uint32_t *> s;
+        std::vector<uint32_t *> d;
+        for (uint32_t i : kv.second) {
+            s.push_back(coeffs[i]);
+            d.push_back(outs[i]);
+        }
+        uint32_t L = kv.first, N = L + log_blowup;
+        int rc;
+        if (L == N || N <= 2) {
+            // No extension (or a tiny one): copy then transform in place.
+            for (size_t i = 0; i < s.size(); i++) {
+                if (s[i] != d[i]) STWO_CUDA_TRY(cudaMemcpyAsync(d[i], s[i], 4ull << L, cudaMemcpyDeviceToDevice, st));
+                if (N > L) STWO_CUDA_TRY(cudaMemsetAsync(d[i] + (1ull << L), 0, (4ull << N) - (4ull << L), st));
+            }
+            rc = fft_columns(d.data(), d.data(), (uint32_t)d.size(), N, N, tw, tree_size, false, st);
+        } else {
+            rc = fft_columns(s.data(), d.data(), (uint32_t)d.size(), N, L, tw, tree_size, false, st);
+        }
+        if (rc) return rc;
+    }
+    return STWO_OK;
+}
+
+int columns_fft_async(uint32_t *const *cols, const uint32_t *logs, uint32_t n, const uint32_t *tree,
+                      uint64_t tree_size, bool inv, cudaStream_t st) {
+    std::map<uint32_t, std::vector<uint32_t *>> by_size;
+    for (uint32_t i = 0; i < n; i++) by_size[logs[i]].push_back(cols[i]);
+    for (auto &kv : by_size) {
+        int rc = fft_columns(kv.second.data(), kv.second.data(), (uint32_t)kv.second.size(), kv.first, kv.first,
+                             tree, tree_size, inv, st);
+        if (rc) return rc;
+    }
+    return STWO_OK;
+}
+
+}  // namespace stwo
+
+using namespace stwo;
+
+extern "C" {
+
+int stwo_precompute_twiddles(uint32_t root_initial_index, uint32_t root_step_size, uint32_t root_log_size,
+                             uint32_t *twiddles, uint32_t *itwiddles, void *stream) {
+    return precompute_tree(index_to_point(root_initial_index), index_to_point(root_step_size), root_log_size,
+                           twiddles, itwiddles, as_stream(stream));
+}
+
+uint32_t *precompute_twiddles(stwo_point initial, stwo_point step, size_t total_size) {
+    if (!is_pow2(total_size)) {
+        set_error(STWO_ERR_INVALID_ARGUMENT, "twiddle tree size %zu is not a power of two", total_size);
+        return nullptr;
+    }
+    uint32_t *tw = cuda_malloc_uint32_t((uint32_t)total_size);
+    if (!tw) return nullptr;
+    int rc = precompute_tree({initial.x, initial.y}, {step.x, step.y}, log2_u64(total_size), tw, nullptr, 0);
+    if (sync_default_stream(rc) != STWO_OK) {
+        cudaFree(tw);
+        return nullptr;
+    }
+    return tw;
+}
+
+int stwo_new_canonical_ordered(const uint32_t *src, uint32_t *dst, uint32_t log_size, void *stream) {
+    STWO_REQUIRE(log_size >= 1 && log_size <= 31, STWO_ERR_UNSUPPORTED_SIZE, "log size %u unsupported", log_size);
+    STWO_REQUIRE(src != dst, STWO_ERR_INVALID_ARGUMENT, "new_canonical_ordered is out of place");
+    uint64_t n = 1ull << log_size;
+    uint32_t blocks = (uint32_t)std::min<uint64_t>((n + 255) / 256, (uint64_t)device_sm_count() * 32);
+    canonic_to_bitrev_kernel<<<blocks, 256, 0, as_stream(stream)>>>(src, dst, log_size);
+    STWO_LAUNCH_CHECK("canonic_to_bitrev_kernel");
+    return STWO_OK;
+}
+
+uint32_t *sort_values_and_permute_with_bit_reverse_order(const uint32_t *from, size_t size) {
+    if (!is_pow2(size) || size < 2) {
+        set_error(STWO_ERR_INVALID_ARGUMENT, "size %zu is not a power of two >= 2", size);
+        return nullptr;
+    }
+    uint32_t *dst = cuda_malloc_uint32_t((uint32_t)size);
+    if (!dst) return nullptr;
+    if (sync_default_stream(stwo_new_canonical_ordered(from, dst, log2_u64(size), nullptr)) != STWO_OK) {
+        cudaFree(dst);
+        return nullptr;
+    }
+    return dst;
+}
+
+int stwo_interpolate_columns(uint32_t *const *columns, const uint32_t *log_sizes, uint32_t n_columns,
+                             const uint32_t *itwiddles, uint64_t tree_size, void *stream) {
+    return columns_fft_async(columns, log_sizes, n_columns, itwiddles, tree_size, true, as_stream(stream));
+}
+
+int stwo_evaluate_columns(uint32_t *const *columns, const uint32_t *log_sizes, uint32_t n_columns,
+                          const uint32_t *twiddles, uint64_t tree_size, void *stream) {
+    return columns_fft_async(columns, log_sizes, n_columns, twiddles, tree_size, false, as_stream(stream));
+}
+
+int stwo_extend_evaluate_columns(const uint32_t *const *coeffs, const uint32_t *coeff_log_sizes,
+                                 uint32_t *const *outputs, uint32_t log_blowup, uint32_t n_columns,
+                                 const uint32_t *twiddles, uint64_t tree_size, void *stream) {
+    for (uint32_t i = 0; i < n_columns; i++)
+        STWO_REQUIRE(log_blowup == 0 || coeffs[i] != outputs[i], STWO_ERR_INVALID_ARGUMENT,
+                     "extend_evaluate needs distinct coefficient and output buffers");
+    return extend_evaluate_async(coeffs, coeff_log_sizes, outputs, log_blowup, n_columns, twiddles, tree_size,
+                                 as_stream(stream));
+}
+
+// Reference-compatible forms: eval_domain_size is the half-coset size, i.e. half
+// of values_size; the column is transformed in place (ifft.cu:41-65, rfft.cu:45-64).
+void interpolate(uint32_t eval_domain_size, uint32_t *values, const uint32_t *inverse_twiddles_tree,
+                 uint32_t inverse_twiddle_tree_size, uint32_t values_size) {
+    (void)eval_domain_size;
+    if (!is_pow2(values_size) || values_size < 2) {
+        set_error(STWO_ERR_INVALID_ARGUMENT, "values_size %u is not a power of two >= 2", values_size);
+        return;
+    }
+    uint32_t L = log2_u64(values_size);
+    sync_default_stream(columns_fft_async(&values, &L, 1, inverse_twiddles_tree, inverse_twiddle_tree_size, true, 0));
+}
+
+void interpolate_columns(uint32_t eval_domain_size, uint32_t *const *values, const uint32_t *inverse_twiddles_tree,
+                         uint32_t inverse_twiddle_tree_size, uint32_t values_size, uint32_t number_of_rows) {
+    (void)eval_domain_size;
+    if (!is_pow2(number_of_rows) || number_of_rows < 2) {
+        set_error(STWO_ERR_INVALID_ARGUMENT, "number_of_rows %u is not a power of two >= 2", number_of_rows);
+        return;
+    }
+    std::vector<uint32_t> logs(values_size, log2_u64(number_of_rows));
+    sync_default_stream(columns_fft_async(values, logs.data(), values_size, inverse_twiddles_tree,
+                                          inverse_twiddle_tree_size, true, 0));
+}
+
+void evaluate(uint32_t eval_domain_size, uint32_t *values, const uint32_t *twiddles_tree, uint32_t twiddle_tree_size,
+              uint32_t values_size) {
+    (void)eval_domain_size;
+    if (!is_pow2(values_size) || values_size < 2) {
+        set_error(STWO_ERR_INVALID_ARGUMENT, "values_size %u is not a power of two >= 2", values_size);
+        return;
+    }
+    uint32_t L = log2_u64(values_size);
+    sync_default_stream(columns_fft_async(&values, &L, 1, twiddles_tree, twiddle_tree_size, false, 0));
+}
+
+void evaluate_columns(const uint32_t *eval_domain_sizes, uint32_t *const *values, const uint32_t *twiddles_tree,
+                      uint32_t twiddle_tree_size, uint32_t number_of_columns, const uint32_t *column_sizes) {
+    (void)eval_domain_sizes;
+    std::vector<uint32_t> logs(number_of_columns);
+    for (uint32_t i = 0; i < number_of_columns; i++) {
+        if (!is_pow2(column_sizes[i]) || column_sizes[i] < 2) {
+            set_error(STWO_ERR_INVALID_ARGUMENT, "column size %u is not a power of two >= 2", column_sizes[i]);
+            return;
+        }
+        logs[i] = log2_u64(column_sizes[i]);
+    }
+    sync_default_stream(columns_fft_async(values, logs.data(), number_of_columns, twiddles_tree, twiddle_tree_size,
+                                          false, 0));
+}
+
+size_t stwo_eval_at_points_scratch_bytes(const uint32_t *log_sizes, uint32_t n_polys) {
+    return eval_at_points_scratch_bytes(log_sizes, n_polys);
+}
+
+int stwo_eval_at_points(const uint32_t *const *coeffs, const uint32_t *log_sizes, uint32_t n_polys,
+                        const stwo_spoint *points, stwo_qm31 *results, void *scratch, size_t scratch_bytes,
+                        void *stream) {
+    return eval_at_points_async(coeffs, log_sizes, n_polys, points, results, scratch, scratch_bytes, false,
+                                as_stream(stream));
+}
+
+// Reference-compatible: allocates its scratch per call, as eval_at_point.cu:118 does.
+stwo_qm31 eval_at_point(const uint32_t *coeffs, uint32_t coeffs_size, stwo_qm31 point_x, stwo_qm31 point_y) {
+    stwo_qm31 out = {0, 0, 0, 0};
+    if (!is_pow2(coeffs_size)) {
+        set_error(STWO_ERR_INVALID_ARGUMENT, "coeffs_size %u is not a power of two", coeffs_size);
+        return out;
+    }
+    uint32_t L = log2_u64(coeffs_size);
+    stwo_spoint pt = {point_x, point_y};
+    const size_t need = eval_at_points_scratch_bytes(&L, 1);
+    char *scratch = nullptr;
+    if (cudaMalloc((void **)&scratch, need + 256) != cudaSuccess) {
+        set_error(STWO_ERR_OUT_OF_MEMORY, "eval_at_point scratch allocation failed");
+        return out;
+    }
+    stwo_qm31 *res = reinterpret_cast<stwo_qm31 *>(scratch);  // result slot, then the kernel scratch
+    int rc = eval_at_points_async(&coeffs, &L, 1, &pt, res, scratch + 256, need, false, 0);
+    if (rc == STWO_OK) {
+        if (cudaMemcpy(&out, res, sizeof(out), cudaMemcpyDeviceToHost) != cudaSuccess)
+            set_error(STWO_ERR_CUDA, "eval_at_point copy failed");
+    }
+    cudaFree(scratch);
+    return out;
+}
+
+}  // extern "C"

@@ -1,0 +1,244 @@
+// QuotientOps::accumulate_quotients (DEEP quotients).
+//
+// Semantics (cuda/src/quotients.cu:49-178, stwo_gpu_backend/src/quotient.rs:17-115):
+// for row r with domain point p = domain.at(bitrev(r)):
+//   acc = sum over batches b, in order: acc * rc^|b| + den_b(p)^-1 * num_b(p),
+//   num_b(p) = sum_j c_j col_j[r] - (a_j p.y + b_j),
+//   (a_j, b_j, c_j) = rc^(j+1) * (conj(v)-v, v*c - a*P.y, conj(P.y)-P.y) of sample j,
+//   den_b(p) = (Pr.x - p.x) Pi.y - (Pr.y - p.y) Pi.x in CM31 (P = Pr + u Pi).
+// Line coefficients use each batch's own cumulative offset (the CpuBackend
+// semantics; the reference kernel mis-indexes batches of different sizes).
+//
+// Design: the per-batch sums of a_j and b_j and the doubled c_j are computed once
+// on the host and passed by value. A thread handles rows 2k and 2k+1, whose
+// domain points are P and conj(P), so one point evaluation (a product of table
+// powers of the circle generator) serves two rows. All 2 x n_batches CM31
+// denominators of the thread are inverted with one field inversion (Montgomery's
+// trick). The column terms accumulate unreduced 33-bit partial products in 64-bit
+// registers and reduce once per batch.
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+
+namespace stwo {
+namespace {
+
+constexpr int QUOT_MAX_COLS = 512;
+constexpr int QUOT_MAX_SAMPLES = 512;
+constexpr int QUOT_MAX_BATCHES = 16;
+
+struct QuotParams {
+    const uint32_t *cols[QUOT_MAX_COLS];
+    qm31 c2[QUOT_MAX_SAMPLES];            // c_j with every coordinate doubled (for m31_mul2)
+    uint16_t col_idx[QUOT_MAX_SAMPLES];
+    qm31 a_sum[QUOT_MAX_BATCHES], b_sum[QUOT_MAX_BATCHES], batch_coeff[QUOT_MAX_BATCHES];
+    cm31 prx[QUOT_MAX_BATCHES], pry[QUOT_MAX_BATCHES], pix[QUOT_MAX_BATCHES], piy[QUOT_MAX_BATCHES];
+    uint32_t batch_end[QUOT_MAX_BATCHES];  // cumulative sample counts
+    uint32_t n_batches;
+    uint32_t half_init, half_step;        // half coset indices
+    uint32_t log_size;                    // domain log size
+    uint32_t *out[4];
+};
+
+__constant__ cpoint c_gen_pows[31];  // GEN^(2^b)
+
+__device__ __forceinline__ cpoint point_at_index(uint32_t idx) {
+    cpoint r = {1, 0};
+#pragma unroll 1
+    for (int b = 0; b < 31; b++)
+        if ((idx >> b) & 1u) r = point_mul(r, c_gen_pows[b]);
+    return r;
+}
+
+// Unreduced product: value congruent to a*b, in [0, 2p].
+__device__ __forceinline__ uint32_t mul_lazy(uint32_t a, uint32_t b2) {
+    uint64_t w = (uint64_t)a * b2;
+    return (uint32_t)(w >> 32) + ((uint32_t)w >> 1);
+}
+__device__ __forceinline__ uint32_t reduce64(uint64_t x) {
+    // x < 2^62: fold twice
+    uint64_t s = (x & P) + (x >> 31);
+    s = (s & P) + (s >> 31);
+    return reduce_once((uint32_t)s);
+}
+
+template <bool COLS_ON_DEVICE>
+__global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ QuotParams p,
+                                                        const uint32_t *const *__restrict__ dev_cols) {
+    const uint64_t n_pairs = 1ull << (p.log_size - 1);
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_pairs;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t hidx = bit_reverse_bits((uint32_t)k, p.log_size - 1);
+        cpoint pt = point_at_index(p.half_init + p.half_step * hidx);
+        // Denominators for both rows (y and -y), then one shared inversion.
+        cm31 den[2][QUOT_MAX_BATCHES];
+        cm31 prefix = {1, 0};
+        cm31 pre[2][QUOT_MAX_BATCHES];
+        const uint32_t ys[2] = {pt.y, m31_neg(pt.y)};
+        for (uint32_t b = 0; b < p.n_batches; b++) {
+            for (int s = 0; s < 2; s++) {
+                cm31 t1 = {m31_sub(p.prx[b].a, pt.x), p.prx[b].b};
+                cm31 t2 = {m31_sub(p.pry[b].a, ys[s]), p.pry[b].b};
+                den[s][b] = cm31_sub(cm31_mul(t1, p.piy[b]), cm31_mul(t2, p.pix[b]));
+                prefix = cm31_mul(prefix, den[s][b]);
+                pre[s][b] = prefix;
+            }
+        }
+        cm31 inv = cm31_inv(prefix);
+        for (int b = (int)p.n_batches - 1; b >= 0; b--) {
+            for (int s = 1; s >= 0; s--) {
+                cm31 prev = (s == 1) ? pre[0][b] : (b > 0 ? pre[1][b - 1] : cm31{1, 0});
+                cm31 d = den[s][b];
+                den[s][b] = cm31_mul(inv, prev);  // inverse of d
+                inv = cm31_mul(inv, d);
+            }
+        }
+        qm31 acc[2] = {qm31_zero(), qm31_zero()};
+        uint32_t j0 = 0;
+        for (uint32_t b = 0; b < p.n_batches; b++) {
+            uint64_t s0[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+            const uint32_t j1 = p.batch_end[b];
+            for (uint32_t j = j0; j < j1; j++) {
+                const uint32_t *col = COLS_ON_DEVICE ? dev_cols[p.col_idx[j]] : p.cols[p.col_idx[j]];
+                uint2 v = __ldg(reinterpret_cast<const uint2 *>(col) + k);
+                qm31 c2 = p.c2[j];
+                s0[0][0] += mul_lazy(v.x, c2.a.a); s0[0][1] += mul_lazy(v.x, c2.a.b);
+                s0[0][2] += mul_lazy(v.x, c2.b.a); s0[0][3] += mul_lazy(v.x, c2.b.b);
+                s0[1][0] += mul_lazy(v.y, c2.a.a); s0[1][1] += mul_lazy(v.y, c2.a.b);
+                s0[1][2] += mul_lazy(v.y, c2.b.a); s0[1][3] += mul_lazy(v.y, c2.b.b);
+            }
+            j0 = j1;
+            for (int s = 0; s < 2; s++) {
+                qm31 num = {{reduce64(s0[s][0]), reduce64(s0[s][1])}, {reduce64(s0[s][2]), reduce64(s0[s][3])}};
+                qm31 lin = qm31_add(qm31_scale(p.a_sum[b], ys[s]), p.b_sum[b]);
+                num = qm31_sub(num, lin);
+                acc[s] = qm31_add(qm31_mul(acc[s], p.batch_coeff[b]), qm31_mul_cm31(num, den[s][b]));
+            }
+        }
+        reinterpret_cast<uint2 *>(p.out[0])[k] = make_uint2(acc[0].a.a, acc[1].a.a);
+        reinterpret_cast<uint2 *>(p.out[1])[k] = make_uint2(acc[0].a.b, acc[1].a.b);
+        reinterpret_cast<uint2 *>(p.out[2])[k] = make_uint2(acc[0].b.a, acc[1].b.a);
+        reinterpret_cast<uint2 *>(p.out[3])[k] = make_uint2(acc[0].b.b, acc[1].b.b);
+    }
+}
+
+inline qm31 to_q(stwo_qm31 v) { return {{v.a, v.b}, {v.c, v.d}}; }
+
+int gen_table_ready() {
+    static bool done = false;
+    if (done) return STWO_OK;
+    cpoint t[31];
+    cpoint g = {CIRCLE_GEN_X, CIRCLE_GEN_Y};
+    for (int b = 0; b < 31; b++) {
+        t[b] = g;
+        g = point_mul(g, g);
+    }
+    STWO_CUDA_TRY(cudaMemcpyToSymbol(c_gen_pows, t, sizeof(t)));
+    done = true;
+    return STWO_OK;
+}
+
+}  // namespace
+
+int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, const uint32_t *const *cols,
+                    uint32_t n_cols, bool cols_on_device, stwo_qm31 rc_c, const stwo_spoint *pts,
+                    const uint32_t *bsz, const uint32_t *cidx, const stwo_qm31 *vals, uint32_t n_batches,
+                    uint32_t *const *out4, cudaStream_t st) {
+    STWO_REQUIRE(log_size >= 1 && log_size <= 31, STWO_ERR_UNSUPPORTED_SIZE, "domain log size %u", log_size);
+    STWO_REQUIRE(n_batches <= (uint32_t)QUOT_MAX_BATCHES, STWO_ERR_UNSUPPORTED_SIZE, "at most %d sample batches",
+                 QUOT_MAX_BATCHES);
+    STWO_REQUIRE(cols_on_device || n_cols <= (uint32_t)QUOT_MAX_COLS, STWO_ERR_UNSUPPORTED_SIZE,
+                 "at most %d columns", QUOT_MAX_COLS);
+    int rc = gen_table_ready();
+    if (rc) return rc;
+    QuotParams *p = new QuotParams();
+    std::unique_ptr<QuotParams> guard(p);
+    p->n_batches = n_batches;
+    p->half_init = half_init;
+    p->half_step = half_step;
+    p->log_size = log_size;
+    for (int c = 0; c < 4; c++) p->out[c] = out4[c];
+    if (!cols_on_device)
+        for (uint32_t i = 0; i < n_cols; i++) p->cols[i] = cols[i];
+    qm31 rcq = to_q(rc_c);
+    uint32_t off = 0;
+    for (uint32_t b = 0; b < n_batches; b++) {
+        STWO_REQUIRE(off + bsz[b] <= (uint32_t)QUOT_MAX_SAMPLES, STWO_ERR_UNSUPPORTED_SIZE, "at most %d samples",
+                     QUOT_MAX_SAMPLES);
+        qm31 px = to_q(pts[b].x), py = to_q(pts[b].y);
+        p->prx[b] = px.a;
+        p->pix[b] = px.b;
+        p->pry[b] = py.a;
+        p->piy[b] = py.b;
+        p->batch_coeff[b] = qm31_pow(rcq, bsz[b]);
+        qm31 alpha = qm31_one(), as = qm31_zero(), bs = qm31_zero();
+        for (uint32_t j = 0; j < bsz[b]; j++) {
+            alpha = qm31_mul(alpha, rcq);
+            qm31 v = to_q(vals[off + j]);
+            qm31 a = qm31_sub(qm31_conj(v), v);
+            qm31 c = qm31_sub(qm31_conj(py), py);
+            qm31 bb = qm31_sub(qm31_mul(v, c), qm31_mul(a, py));
+            a = qm31_mul(alpha, a);
+            bb = qm31_mul(alpha, bb);
+            c = qm31_mul(alpha, c);
+            as = qm31_add(as, a);
+            bs = qm31_add(bs, bb);
+            p->c2[off + j] = {{c.a.a << 1, c.a.b << 1}, {c.b.a << 1, c.b.b << 1}};
+            STWO_REQUIRE(cidx[off + j] < n_cols, STWO_ERR_INVALID_ARGUMENT, "sample column index %u out of range",
+                         cidx[off + j]);
+            p->col_idx[off + j] = (uint16_t)cidx[off + j];
+        }
+        p->a_sum[b] = as;
+        p->b_sum[b] = bs;
+        off += bsz[b];
+        p->batch_end[b] = off;
+    }
+    uint64_t pairs = 1ull << (log_size - 1);
+    uint64_t blocks = (pairs + 255) / 256;
+    uint64_t cap = (uint64_t)device_sm_count() * 8;
+    if (blocks > cap) blocks = cap;
+    if (cols_on_device) quotients_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(*p, cols);
+    else quotients_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(*p, nullptr);
+    STWO_LAUNCH_CHECK("quotients_kernel");
+    return STWO_OK;
+}
+
+}  // namespace stwo
+
+using namespace stwo;
+
+extern "C" {
+
+int stwo_accumulate_quotients(uint32_t half_coset_initial_index, uint32_t half_coset_step_size,
+                              uint32_t domain_log_size, const uint32_t *const *columns, uint32_t n_columns,
+                              stwo_qm31 random_coeff, const stwo_spoint *sample_points, const uint32_t *batch_sizes,
+                              const uint32_t *column_indices, const stwo_qm31 *sampled_values, uint32_t n_batches,
+                              uint32_t *const *out4, void *stream) {
+    return quotients_async(half_coset_initial_index, half_coset_step_size, domain_log_size, columns, n_columns, false,
+                           random_coeff, sample_points, batch_sizes, column_indices, sampled_values, n_batches, out4,
+                           as_stream(stream));
+}
+
+void accumulate_quotients(uint32_t half_coset_initial_index, uint32_t half_coset_step_size, uint32_t domain_size,
+                          uint32_t *const *columns, size_t number_of_columns, stwo_qm31 random_coeff,
+                          const uint32_t *sample_points, const uint32_t *sample_columns_indexes,
+                          uint32_t sample_columns_indexes_size, const stwo_qm31 *sample_column_values,
+                          const uint32_t *sample_column_and_values_sizes, uint32_t sample_size,
+                          uint32_t *result_column_0, uint32_t *result_column_1, uint32_t *result_column_2,
+                          uint32_t *result_column_3, uint32_t flattened_line_coeffs_size) {
+    (void)sample_columns_indexes_size;
+    (void)flattened_line_coeffs_size;
+    if (!is_pow2(domain_size) || domain_size < 2) {
+        set_error(STWO_ERR_INVALID_ARGUMENT, "domain size %u is not a power of two >= 2", domain_size);
+        return;
+    }
+    uint32_t *out[4] = {result_column_0, result_column_1, result_column_2, result_column_3};
+    sync_default_stream(quotients_async(half_coset_initial_index, half_coset_step_size, log2_u64(domain_size),
+                                        const_cast<const uint32_t *const *>(columns), (uint32_t)number_of_columns,
+                                        true, random_coeff, reinterpret_cast<const stwo_spoint *>(sample_points),
+                                        sample_column_and_values_sizes, sample_columns_indexes, sample_column_values,
+                                        sample_size, out, 0));
+}
+
+}  // extern "C"

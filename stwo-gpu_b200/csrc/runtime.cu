@@ -1,0 +1,131 @@
+// Error reporting, device memory and copy entry points.
+//
+// The reference's memory helpers (cuda/include/utils.cuh:39-78, cuda/src/utils.cu:14-80)
+// print CUDA failures and carry on. Here every failure is recorded per thread and
+// returned as a status by the native API; the reference-compatible entry points keep
+// their void / pointer signatures and return NULL on failure.
+#include <cstdarg>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace stwo {
+
+static thread_local char g_last_error[512] = "";
+
+int set_error(int status, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+void clear_error() { g_last_error[0] = 0; }
+
+int device_sm_count() {
+    static int count = 0;
+    if (count == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            count = NUM_SMS_B200;
+    }
+    return count;
+}
+
+int sync_default_stream(int status) {
+    if (status != STWO_OK) return status;
+    cudaError_t e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) return set_error(STWO_ERR_CUDA, "device error: %s", cudaGetErrorString(e));
+    return STWO_OK;
+}
+
+template <typename T>
+static T *dev_alloc(size_t count, bool zero) {
+    void *p = nullptr;
+    size_t bytes = count * sizeof(T);
+    if (bytes == 0) bytes = sizeof(T);
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        set_error(STWO_ERR_OUT_OF_MEMORY, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        return nullptr;
+    }
+    if (zero && cudaMemset(p, 0, bytes) != cudaSuccess) {
+        set_error(STWO_ERR_CUDA, "cudaMemset failed");
+        cudaFree(p);
+        return nullptr;
+    }
+    return static_cast<T *>(p);
+}
+
+static void copy_sync(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) {
+    cudaError_t e = cudaMemcpy(dst, src, bytes, kind);
+    if (e != cudaSuccess) set_error(STWO_ERR_CUDA, "cudaMemcpy(%zu) failed: %s", bytes, cudaGetErrorString(e));
+}
+
+}  // namespace stwo
+
+using namespace stwo;
+
+extern "C" {
+
+const char *stwo_last_error(void) { return g_last_error; }
+
+void stwo_clear_last_error(void) { clear_error(); }
+
+int stwo_stream_synchronize(void *stream) {
+    cudaError_t e = cudaStreamSynchronize(as_stream(stream));
+    if (e != cudaSuccess) return set_error(STWO_ERR_CUDA, "device error: %s", cudaGetErrorString(e));
+    return STWO_OK;
+}
+
+void copy_uint32_t_vec_from_device_to_host(const uint32_t *device_ptr, uint32_t *host_ptr, uint32_t size) {
+    copy_sync(host_ptr, device_ptr, (size_t)size * 4, cudaMemcpyDeviceToHost);
+}
+
+uint32_t *copy_uint32_t_vec_from_host_to_device(const uint32_t *host_ptr, uint32_t size) {
+    uint32_t *d = dev_alloc<uint32_t>(size, false);
+    if (d) copy_sync(d, host_ptr, (size_t)size * 4, cudaMemcpyHostToDevice);
+    return d;
+}
+
+uint32_t *copy_uint32_t_vec_from_device_to_device(const uint32_t *from, uint32_t *dst, uint32_t size) {
+    copy_sync(dst, from, (size_t)size * 4, cudaMemcpyDeviceToDevice);
+    return dst;
+}
+
+uint32_t *cuda_malloc_uint32_t(uint32_t size) { return dev_alloc<uint32_t>(size, false); }
+
+stwo_blake2s_hash *cuda_malloc_blake_2s_hash(size_t size) { return dev_alloc<stwo_blake2s_hash>(size, false); }
+
+uint32_t *cuda_alloc_zeroes_uint32_t(uint32_t size) { return dev_alloc<uint32_t>(size, true); }
+
+stwo_blake2s_hash *cuda_alloc_zeroes_blake_2s_hash(size_t size) { return dev_alloc<stwo_blake2s_hash>(size, true); }
+
+void cuda_free_memory(void *device_ptr) {
+    if (!device_ptr) return;
+    cudaError_t e = cudaFree(device_ptr);
+    if (e != cudaSuccess) set_error(STWO_ERR_CUDA, "cudaFree failed: %s", cudaGetErrorString(e));
+}
+
+stwo_blake2s_hash *copy_blake_2s_hash_vec_from_host_to_device(const stwo_blake2s_hash *from, size_t size) {
+    stwo_blake2s_hash *d = dev_alloc<stwo_blake2s_hash>(size, false);
+    if (d) copy_sync(d, from, size * sizeof(stwo_blake2s_hash), cudaMemcpyHostToDevice);
+    return d;
+}
+
+void copy_blake_2s_hash_vec_from_device_to_host(const stwo_blake2s_hash *from, stwo_blake2s_hash *to, size_t size) {
+    copy_sync(to, from, size * sizeof(stwo_blake2s_hash), cudaMemcpyDeviceToHost);
+}
+
+void copy_blake_2s_hash_vec_from_device_to_device(const stwo_blake2s_hash *from, stwo_blake2s_hash *dst, size_t size) {
+    copy_sync(dst, from, size * sizeof(stwo_blake2s_hash), cudaMemcpyDeviceToDevice);
+}
+
+uint32_t **copy_device_pointer_vec_from_host_to_device(uint32_t *const *from, size_t size) {
+    uint32_t **d = dev_alloc<uint32_t *>(size, false);
+    if (d) copy_sync(d, from, size * sizeof(uint32_t *), cudaMemcpyHostToDevice);
+    return d;
+}
+
+}  // extern "C"
