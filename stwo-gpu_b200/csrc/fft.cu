@@ -27,6 +27,7 @@
 //  * One launch serves many columns of the same size; columns of different sizes
 //    use separate launches on the same stream.
 #include <algorithm>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -197,6 +198,193 @@ __global__ void __launch_bounds__(1 << MAX_THREADS_LOG) fft_pass_kernel(const __
     }
 }
 
+// ---------------------------------------------------------------------------
+// Specialised pass over 2^15-element tiles (512 threads x 64 elements).
+//
+// Tile index bits: [0, C) columns of a strided tile (consecutive global words),
+// [C, C+G) the G layer bits of the pass, [C+G, 15) "slots": for a single-pass
+// transform of a 2^G column (G < 15) a CTA holds 2^(15-G) independent tiles.
+// Everything about the round structure is a compile-time constant: the first
+// round loads straight from global memory into registers (lanes on consecutive
+// words), the last round stores straight back, and only the rounds in between go
+// through shared memory, where the swizzled address is one XOR with a constant
+// (S is linear over GF(2) and the round's own bits are disjoint from the others).
+// ---------------------------------------------------------------------------
+constexpr int T15 = 15, W15 = 9, E15 = 6;
+
+__host__ __device__ constexpr uint32_t swz_c(uint32_t j) { return j ^ (((j >> 5) ^ (j >> 10)) & 31u); }
+
+template <int G, bool INV, int R>
+struct Round15 {
+    static constexpr int NR = (G + E15 - 1) / E15;
+    static constexpr int REM = G - E15 * R;
+    static constexpr int RB = REM < E15 ? REM : E15;
+    static constexpr int A = INV ? E15 * R : REM - RB;  // first owned layer bit (row bit)
+};
+
+struct Geo15 {
+    const FftLaunch *p;
+    uint32_t tiles_log, low_fixed;
+};
+
+template <int G, int C>
+__device__ __forceinline__ void tile_locate(const Geo15 &geo, uint32_t jb, uint32_t &col, uint32_t &gidx) {
+    constexpr int SLOT_BITS = T15 - C - G;
+    const uint32_t tile_id = (blockIdx.x << SLOT_BITS) | (jb >> (C + G));
+    const uint32_t T = tile_id & ((1u << geo.tiles_log) - 1u);
+    col = tile_id >> geo.tiles_log;
+    const uint32_t jl = jb & ((1u << (C + G)) - 1u);
+    const uint32_t gfix = ((T & ((1u << geo.low_fixed) - 1u)) << C) | ((T >> geo.low_fixed) << geo.p->hi);
+    if constexpr (C == 0) gidx = gfix | jl;  // contiguous pass: lo = 0
+    else gidx = gfix | (jl & ((1u << C) - 1u)) | ((jl >> C) << geo.p->lo);
+}
+
+template <int G, int C, bool INV, int R>
+__device__ __forceinline__ void round15(uint32_t *sm, const Geo15 &geo) {
+    using RI = Round15<G, INV, R>;
+    constexpr int RB = RI::RB, A = RI::A, OA = C + A, RR = 1 << RB, GROUPS = 1 << (E15 - RB);
+    constexpr bool FIRST = R == 0, LAST = R == RI::NR - 1;
+    const FftLaunch &p = *geo.p;
+    const uint32_t lo = (C == 0) ? 0u : p.lo;
+#pragma unroll 1
+    for (int grp = 0; grp < GROUPS; grp++) {
+        const uint32_t x = threadIdx.x | ((uint32_t)grp << W15);
+        const uint32_t jb = (x & ((1u << OA) - 1u)) | ((x >> OA) << (OA + RB));
+        uint32_t col, gb;
+        tile_locate<G, C>(geo, jb, col, gb);
+        const uint32_t sh = lo + A;  // global bit of the round's first owned bit
+        uint32_t v[RR];
+        if constexpr (FIRST) {
+            const uint32_t *__restrict__ src = p.cols[col].src;
+            const uint32_t base = gb & p.src_mask;
+            if constexpr (C == 0 && A == 0 && RR >= 4) {
+#pragma unroll
+                for (int m = 0; m < RR; m += 4) {
+                    uint4 t = __ldg(reinterpret_cast<const uint4 *>(src + base + m));
+                    v[m] = t.x; v[m + 1] = t.y; v[m + 2] = t.z; v[m + 3] = t.w;
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < RR; m++) v[m] = __ldg(src + base + ((uint32_t)m << sh));
+            }
+        } else {
+            const uint32_t sj = swz_c(jb);
+#pragma unroll
+            for (int m = 0; m < RR; m++) v[m] = sm[sj ^ swz_c((uint32_t)m << OA)];
+        }
+#pragma unroll
+        for (int uu = 0; uu < RB; uu++) {
+            const int u = INV ? uu : RB - 1 - uu;
+            const uint32_t k = sh + u;
+            const uint32_t hb = gb >> (k + 1);
+            const uint32_t *tk = nullptr;
+            if (!(C == 0 && A + u == 0)) tk = p.tw + ((1u << (p.N - 1)) - (1u << (p.N - k))) + hb;
+#pragma unroll
+            for (int q = 0; q < (RR >> (u + 1)); q++) {
+                uint32_t t2;
+                if (C == 0 && A + u == 0) t2 = twiddle2(p.tw, p.N, 0, hb + q);
+                else t2 = __ldg(tk + q) << 1;
+#pragma unroll
+                for (int l = 0; l < (1 << u); l++) {
+                    const int m0 = (q << (u + 1)) | l;
+                    butterfly<INV>(v[m0], v[m0 | (1 << u)], t2);
+                }
+            }
+        }
+        if constexpr (LAST) {
+            uint32_t *__restrict__ dst = p.cols[col].dst;
+            if (INV && p.scale2) {
+#pragma unroll
+                for (int m = 0; m < RR; m++) v[m] = m31_mul2(v[m], p.scale2);
+            }
+            if constexpr (C == 0 && A == 0 && RR >= 4) {
+#pragma unroll
+                for (int m = 0; m < RR; m += 4)
+                    *reinterpret_cast<uint4 *>(dst + gb + m) = make_uint4(v[m], v[m + 1], v[m + 2], v[m + 3]);
+            } else {
+#pragma unroll
+                for (int m = 0; m < RR; m++) dst[gb + ((uint32_t)m << sh)] = v[m];
+            }
+        } else {
+            const uint32_t sj = swz_c(jb);
+#pragma unroll
+            for (int m = 0; m < RR; m++) sm[sj ^ swz_c((uint32_t)m << OA)] = v[m];
+        }
+    }
+}
+
+template <int G, int C, bool INV, int... Rs>
+__device__ __forceinline__ void rounds15(uint32_t *sm, const Geo15 &geo, std::integer_sequence<int, Rs...>) {
+    (
+        [&] {
+            round15<G, C, INV, Rs>(sm, geo);
+            if constexpr (Rs + 1 < Round15<G, INV, 0>::NR) __syncthreads();
+        }(),
+        ...);
+}
+
+template <int G, int C, bool INV>
+__global__ void __launch_bounds__(1 << W15, 1) fft15_kernel(const __grid_constant__ FftLaunch p) {
+    extern __shared__ uint32_t sm[];
+    Geo15 geo;
+    geo.p = &p;
+    geo.tiles_log = p.N - (C + G);
+    geo.low_fixed = (C == 0) ? 0u : p.lo - C;
+    rounds15<G, C, INV>(sm, geo, std::make_integer_sequence<int, Round15<G, INV, 0>::NR>{});
+}
+
+template <int G, int C, bool INV>
+int launch15_t(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
+    constexpr int NR = Round15<G, INV, 0>::NR;
+    const size_t smem = NR > 1 ? (sizeof(uint32_t) << T15) : 0;
+    auto kern = fft15_kernel<G, C, INV>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        STWO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(sizeof(uint32_t) << T15)));
+        attr_set = true;
+    }
+    // total tiles = n_cols * 2^(N - C - G); 2^(15 - C - G) tiles per CTA
+    const uint64_t tiles = (uint64_t)n_cols << (p.N - C - G);
+    const uint64_t per_cta = 1ull << (T15 - C - G);
+    STWO_REQUIRE(tiles % per_cta == 0, STWO_ERR_UNSUPPORTED_SIZE, "fft tile packing");
+    const uint64_t blocks = tiles / per_cta;
+    kern<<<(unsigned)blocks, 1 << W15, smem, st>>>(p);
+    STWO_LAUNCH_CHECK("fft15_kernel");
+    return STWO_OK;
+}
+
+// Dispatch over (G, C): contiguous passes G = 11..15 (C = 0), strided passes
+// G = 1..10 with C = 15 - G.
+template <bool INV>
+int launch15(const FftLaunch &p, uint32_t n_cols, uint32_t G, uint32_t C, cudaStream_t st) {
+    if (C == 0) {
+        switch (G) {
+        case 11: return launch15_t<11, 0, INV>(p, n_cols, st);
+        case 12: return launch15_t<12, 0, INV>(p, n_cols, st);
+        case 13: return launch15_t<13, 0, INV>(p, n_cols, st);
+        case 14: return launch15_t<14, 0, INV>(p, n_cols, st);
+        case 15: return launch15_t<15, 0, INV>(p, n_cols, st);
+        default: break;
+        }
+    } else if (C + G == 15) {
+        switch (G) {
+        case 1: return launch15_t<1, 14, INV>(p, n_cols, st);
+        case 2: return launch15_t<2, 13, INV>(p, n_cols, st);
+        case 3: return launch15_t<3, 12, INV>(p, n_cols, st);
+        case 4: return launch15_t<4, 11, INV>(p, n_cols, st);
+        case 5: return launch15_t<5, 10, INV>(p, n_cols, st);
+        case 6: return launch15_t<6, 9, INV>(p, n_cols, st);
+        case 7: return launch15_t<7, 8, INV>(p, n_cols, st);
+        case 8: return launch15_t<8, 7, INV>(p, n_cols, st);
+        case 9: return launch15_t<9, 6, INV>(p, n_cols, st);
+        case 10: return launch15_t<10, 5, INV>(p, n_cols, st);
+        default: break;
+        }
+    }
+    return set_error(STWO_ERR_UNSUPPORTED_SIZE, "no specialised fft pass for G=%u C=%u", G, C);
+}
+
 // Transforms of 2 and 4 elements. The circle twiddle is y of the half coset's
 // first point, which the tree does not store for these sizes; it is derived from
 // the first line layer of the next larger domain ([x', y'] with y = 2 x' y'), so
@@ -300,16 +488,22 @@ std::vector<PassSpec> plan_passes(uint32_t L) {
     return v;
 }
 
-// Derives (x, y) of the first point of the half coset of a 2^N domain (N <= 2)
-// from the tree's first line layer of the 8-element domain: [x8, y8] with
-// (x, y) of the 4-element half coset point = (2 x8^2 - 1, 2 x8 y8) and the
-// 2-element one its double. For the inverse tree the inverses are derived.
-int tiny_twiddles(const uint32_t *tree, uint64_t tree_size, uint32_t N, bool inv, uint32_t *tx, uint32_t *ty,
-                  cudaStream_t st) {
-    STWO_REQUIRE(tree_size >= 4, STWO_ERR_UNSUPPORTED_SIZE,
-                 "a 2^%u-point transform needs a twiddle tree of at least 4 entries", N);
+}  // namespace
+
+// (x, y) of the first point of the half coset of a 2^N-point circle domain, N <= 2,
+// as twiddles (inv = false) or inverse twiddles (inv = true). The tree does not
+// store y for these sizes (CpuBackend reads it from the domain itself), so it is
+// derived from the first line layer of the 8-point domain, which holds the pair
+// [x8, y8] of that domain's first point P8 (the [x, y] pairing the circle
+// twiddles rely on, poly/utils.cu:3-14): P4 = P8^2 = (2 x8^2 - 1, 2 x8 y8) and
+// P2 = P4^2. `suffix_end` points one past the 2^N domain's suffix of the tree;
+// the 8-point domain's first line layer is the two entries 4 before it.
+int small_circle_point(const uint32_t *suffix_end, uint64_t avail, uint32_t N, bool inv, uint32_t *tx,
+                       uint32_t *ty, cudaStream_t st) {
+    STWO_REQUIRE(avail >= 4, STWO_ERR_UNSUPPORTED_SIZE,
+                 "a 2^%u-point circle domain needs a twiddle tree that also covers the 8-point domain", N);
     uint32_t l8[2];
-    STWO_CUDA_TRY(cudaMemcpyAsync(l8, tree + tree_size - 4, sizeof(l8), cudaMemcpyDeviceToHost, st));
+    STWO_CUDA_TRY(cudaMemcpyAsync(l8, suffix_end - 4, sizeof(l8), cudaMemcpyDeviceToHost, st));
     STWO_CUDA_TRY(cudaStreamSynchronize(st));
     uint32_t x8 = inv ? m31_inv(l8[0]) : l8[0];
     uint32_t y8 = inv ? m31_inv(l8[1]) : l8[1];
@@ -324,8 +518,6 @@ int tiny_twiddles(const uint32_t *tree, uint64_t tree_size, uint32_t N, bool inv
     return STWO_OK;
 }
 
-}  // namespace
-
 // Runs a transform over n_cols columns of one size. src[i] may equal dst[i]
 // (in place); for an extension read (L < N) src holds 2^L coefficients.
 int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
@@ -337,7 +529,7 @@ int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_c
         STWO_REQUIRE(L == N, STWO_ERR_UNSUPPORTED_SIZE, "extension to a 2^%u domain unsupported", N);
         TinyLaunch t{};
         t.N = N;
-        int rc = tiny_twiddles(tree, tree_size, N, inv, &t.t_x, &t.t_y, st);
+        int rc = small_circle_point(tree + tree_size, tree_size, N, inv, &t.t_x, &t.t_y, st);
         if (rc) return rc;
         t.scale = m31_inv_pow2(N);
         for (uint32_t base = 0; base < n_cols; base += MAX_COLS_PER_LAUNCH) {
@@ -377,7 +569,13 @@ int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_c
             uint32_t cnt = std::min<uint32_t>(MAX_COLS_PER_LAUNCH, n_cols - base);
             for (uint32_t i = 0; i < cnt; i++)
                 p.cols[i] = FftColumn{first ? srcs[base + i] : dsts[base + i], dsts[base + i]};
-            int rc = launch_pass(p, cnt, inv, st);
+            const uint32_t G = ps.hi - ps.lo;
+            // Specialised 2^15 tiles: strided passes, or contiguous passes of >= 11 layers whose
+            // tiles pack evenly into CTAs.
+            const bool spec = (ps.c > 0 && ps.tile_log == 15) ||
+                              (ps.c == 0 && G >= 11 && ((uint64_t)cnt << (N - G)) % (1ull << (15 - G)) == 0);
+            int rc = spec ? (inv ? launch15<true>(p, cnt, G, ps.c, st) : launch15<false>(p, cnt, G, ps.c, st))
+                          : launch_pass(p, cnt, inv, st);
             if (rc) return rc;
         }
     }

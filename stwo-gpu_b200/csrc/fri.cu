@@ -10,6 +10,10 @@
 #include "common.cuh"
 
 namespace stwo {
+
+int small_circle_point(const uint32_t *suffix_end, uint64_t avail, uint32_t N, bool inv, uint32_t *tx, uint32_t *ty,
+                       cudaStream_t st);
+
 namespace {
 
 struct Cols4 { const uint32_t *c[4]; };
@@ -71,19 +75,22 @@ __global__ void fold_kernel(const __grid_constant__ Cols4 src, const __grid_cons
     }
 }
 
-// Tiny folds (n_out == 1) use a scalar path.
+// Folds with one or two outputs take their (inverse) twiddles by value: for the
+// circle fold of a 2- or 4-point domain they are +-1/y of the half coset's first
+// point, which the tree does not hold at those sizes (see small_circle_point).
 template <bool CIRCLE>
-__global__ void fold_one_kernel(const __grid_constant__ Cols4 src, const __grid_constant__ MutCols4 dst,
-                                const uint32_t *__restrict__ tw, qm31 alpha, qm31 alpha_sq) {
-    qm31 a = {{src.c[0][0], src.c[1][0]}, {src.c[2][0], src.c[3][0]}};
-    qm31 b = {{src.c[0][1], src.c[1][1]}, {src.c[2][1], src.c[3][1]}};
-    uint32_t t = CIRCLE ? circle_itw(tw, 0) : tw[0];
-    qm31 r = fold_pair(a, b, t, alpha);
-    if (CIRCLE) {
-        qm31 p = {{dst.c[0][0], dst.c[1][0]}, {dst.c[2][0], dst.c[3][0]}};
-        r = qm31_add(qm31_mul(p, alpha_sq), r);
+__global__ void fold_small_kernel(const __grid_constant__ Cols4 src, const __grid_constant__ MutCols4 dst,
+                                  uint32_t n_out, uint32_t t0, uint32_t t1, qm31 alpha, qm31 alpha_sq) {
+    for (uint32_t i = 0; i < n_out; i++) {
+        qm31 a = {{src.c[0][2 * i], src.c[1][2 * i]}, {src.c[2][2 * i], src.c[3][2 * i]}};
+        qm31 b = {{src.c[0][2 * i + 1], src.c[1][2 * i + 1]}, {src.c[2][2 * i + 1], src.c[3][2 * i + 1]}};
+        qm31 r = fold_pair(a, b, i == 0 ? t0 : t1, alpha);
+        if (CIRCLE) {
+            qm31 p = {{dst.c[0][i], dst.c[1][i]}, {dst.c[2][i], dst.c[3][i]}};
+            r = qm31_add(qm31_mul(p, alpha_sq), r);
+        }
+        dst.c[0][i] = r.a.a; dst.c[1][i] = r.a.b; dst.c[2][i] = r.b.a; dst.c[3][i] = r.b.b;
     }
-    dst.c[0][0] = r.a.a; dst.c[1][0] = r.a.b; dst.c[2][0] = r.b.a; dst.c[3][0] = r.b.b;
 }
 
 }  // namespace
@@ -103,10 +110,21 @@ int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const
     qm31 a2 = qm31_mul(alpha, alpha);
     const uint32_t *tw = itw + off;
     uint64_t n_out = n / 2;
-    if (n_out == 1) {
-        if (circle) fold_one_kernel<true><<<1, 1, 0, st>>>(s, d, tw, alpha, a2);
-        else fold_one_kernel<false><<<1, 1, 0, st>>>(s, d, tw, alpha, a2);
-        STWO_LAUNCH_CHECK("fold_one_kernel");
+    if (n_out <= 2) {
+        uint32_t t[2] = {0, 0};
+        if (circle) {
+            uint32_t ix, iy;
+            int rc = small_circle_point(tw + n / 2, off + n / 2, log2_u64(n), true, &ix, &iy, st);
+            if (rc) return rc;
+            t[0] = iy;
+            t[1] = m31_neg(iy);
+        } else {
+            STWO_CUDA_TRY(cudaMemcpyAsync(t, tw, sizeof(uint32_t) * n_out, cudaMemcpyDeviceToHost, st));
+            STWO_CUDA_TRY(cudaStreamSynchronize(st));
+        }
+        if (circle) fold_small_kernel<true><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, t[0], t[1], alpha, a2);
+        else fold_small_kernel<false><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, t[0], t[1], alpha, a2);
+        STWO_LAUNCH_CHECK("fold_small_kernel");
         return STWO_OK;
     }
     STWO_REQUIRE(circle || ((uintptr_t)tw & 7) == 0, STWO_ERR_INVALID_ARGUMENT,

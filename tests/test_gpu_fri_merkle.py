@@ -49,7 +49,7 @@ def test_fold_line_more_than_once(stwo, oracle):
         assert (g == e).all()
 
 
-@pytest.mark.parametrize("log_size", [2, 3, 13, 21])
+@pytest.mark.parametrize("log_size", [1, 2, 3, 13, 21])
 def test_fold_circle_into_line(stwo, oracle, log_size):
     """fri.rs:260 (2^13, values 4i..4i+3, alpha (1,3,5,7)) plus random sizes."""
     B = stwo.CudaBackend
@@ -66,12 +66,24 @@ def test_fold_circle_into_line(stwo, oracle, log_size):
         dst0 = [m31(r, n // 2) for _ in range(4)]
     circle = stwo.CanonicCoset(log_size).circle_domain()
     line = stwo.LineDomain(circle.half_coset)
-    tree = B.precompute_twiddles(line.coset)
+    # For 2- and 4-point circle domains the tree must also cover the 8-point domain
+    # (the circle twiddle 1/y is derived from it); larger folds use the reference's tree.
+    tree = B.precompute_twiddles(line.coset if log_size > 2 else stwo.CanonicCoset(4).half_coset())
     dst = stwo.LineEvaluation(line, stwo.SecureColumnByCoords.from_numpy(dst0))
     B.fold_circle_into_line(dst, stwo.SecureEvaluation(circle, stwo.SecureColumnByCoords.from_numpy(src)), alpha, tree)
     expect = oracle.fold_circle_into_line(dst0, src, _oc(oracle, circle.half_coset), alpha)
     for g, e in zip(dst.values.to_numpy(), expect):
         assert (g == e).all()
+
+
+def test_fold_circle_into_line_tiny_domain_needs_larger_tree(stwo):
+    circle = stwo.CanonicCoset(2).circle_domain()
+    line = stwo.LineDomain(circle.half_coset)
+    tree = stwo.CudaBackend.precompute_twiddles(line.coset)
+    dst = stwo.LineEvaluation(line, stwo.SecureColumnByCoords.zeros(2))
+    src = stwo.SecureEvaluation(circle, stwo.SecureColumnByCoords.zeros(4))
+    with pytest.raises(stwo._lib.StwoError, match="8-point"):
+        stwo.CudaBackend.fold_circle_into_line(dst, src, (1, 2, 3, 4), tree)
 
 
 def test_fold_circle_into_line_fibonacci_literals(stwo, oracle):
