@@ -199,57 +199,121 @@ __global__ void __launch_bounds__(1 << MAX_THREADS_LOG) fft_pass_kernel(const __
 }
 
 // ---------------------------------------------------------------------------
-// Specialised pass over 2^15-element tiles (512 threads x 64 elements).
+// Specialised pass over 2^14-element tiles: 256 threads x 64 elements, two CTAs
+// per SM so that one CTA's global loads and stores overlap the other's butterflies
+// (the transform is bound by integer issue, not by HBM).
 //
 // Tile index bits: [0, C) columns of a strided tile (consecutive global words),
-// [C, C+G) the G layer bits of the pass, [C+G, 15) "slots": for a single-pass
-// transform of a 2^G column (G < 15) a CTA holds 2^(15-G) independent tiles.
-// Everything about the round structure is a compile-time constant: the first
-// round loads straight from global memory into registers (lanes on consecutive
-// words), the last round stores straight back, and only the rounds in between go
-// through shared memory, where the swizzled address is one XOR with a constant
-// (S is linear over GF(2) and the round's own bits are disjoint from the others).
+// [C, C+G) the G layer bits of the pass, [C+G, 14) "slots": for a single-pass
+// transform of a 2^G column (G < 14) a CTA holds 2^(14-G) independent tiles.
+// The round structure is compile-time: the first round loads straight from global
+// memory into registers, the last round stores straight back, and only the rounds
+// in between go through shared memory, where the swizzled address is one XOR with
+// a constant (S is linear over GF(2); a round's own bits are disjoint from the
+// others). Middle rounds map warp lanes onto 5 tile bits whose bank images under
+// S are independent, so every shared-memory access is conflict free.
+// CTA order: contiguous passes run the same tile position of all columns back to
+// back (their twiddles are then L2 hits); strided passes run the 2^(N-hi) copies of
+// an extension read back to back (the coefficient tile is then an L2 hit).
 // ---------------------------------------------------------------------------
-constexpr int T15 = 15, W15 = 9, E15 = 6;
+constexpr int TT = 14, WT = 8, ET = 6;
 
 __host__ __device__ constexpr uint32_t swz_c(uint32_t j) { return j ^ (((j >> 5) ^ (j >> 10)) & 31u); }
 
 template <int G, bool INV, int R>
-struct Round15 {
-    static constexpr int NR = (G + E15 - 1) / E15;
-    static constexpr int REM = G - E15 * R;
-    static constexpr int RB = REM < E15 ? REM : E15;
-    static constexpr int A = INV ? E15 * R : REM - RB;  // first owned layer bit (row bit)
+struct RoundT {
+    static constexpr int NR = (G + ET - 1) / ET;
+    // balanced split of the G bits into NR rounds
+    static constexpr int before(int r) { return r == 0 ? 0 : before(r - 1) + (G - before(r - 1) + (NR - r)) / (NR - r + 1); }
+    static constexpr int RB = before(R + 1) - before(R);
+    static constexpr int A = INV ? before(R) : G - before(R + 1);  // first owned layer (row) bit
 };
 
-struct Geo15 {
+// Bank-bit image of tile bit b under S.
+__host__ __device__ constexpr uint32_t bank_vec(int b) {
+    return (b < 5 ? 1u << b : 0u) ^ (b >= 5 && b < 10 ? 1u << (b - 5) : 0u) ^ (b >= 10 && b < 15 ? 1u << (b - 10) : 0u);
+}
+
+struct BitMap { int pos[TT]; };
+
+// Positions (tile bits) of the thread-index bits of a round owning [OA, OA+RB):
+// lanes first (the lowest other bits, or for middle rounds the lowest bits with
+// independent bank images), then the remaining other bits in increasing order.
+__host__ __device__ constexpr BitMap make_map(int OA, int RB, bool pick_lanes) {
+    BitMap m{};
+    int other[TT] = {};
+    int n = 0;
+    for (int b = 0; b < TT; b++)
+        if (b < OA || b >= OA + RB) other[n++] = b;
+    bool used[TT] = {};
+    int k = 0;
+    if (pick_lanes) {
+        uint32_t basis[5] = {0, 0, 0, 0, 0};
+        int nb = 0;
+        for (int i = 0; i < n && k < 5; i++) {
+            uint32_t v = bank_vec(other[i]);
+            for (int t = 0; t < nb; t++)
+                if ((v ^ basis[t]) < v) v ^= basis[t];
+            if (v) {
+                basis[nb++] = v;
+                // keep the basis sorted by leading bit for the reduction above
+                for (int t = nb - 1; t > 0 && basis[t] > basis[t - 1]; t--) {
+                    uint32_t tmp = basis[t]; basis[t] = basis[t - 1]; basis[t - 1] = tmp;
+                }
+                m.pos[k++] = other[i];
+                used[i] = true;
+            }
+        }
+    }
+    for (int i = 0; i < n; i++)
+        if (!used[i]) m.pos[k++] = other[i];
+    return m;
+}
+
+template <int N_BITS>
+__device__ __forceinline__ uint32_t deposit(uint32_t x, const BitMap &m) {
+    uint32_t r = 0;
+#pragma unroll
+    for (int i = 0; i < N_BITS; i++) r |= ((x >> i) & 1u) << m.pos[i];
+    return r;
+}
+
+struct GeoT {
     const FftLaunch *p;
-    uint32_t tiles_log, low_fixed;
+    uint32_t tiles_log, low_fixed, n_high, n_cols;
 };
 
 template <int G, int C>
-__device__ __forceinline__ void tile_locate(const Geo15 &geo, uint32_t jb, uint32_t &col, uint32_t &gidx) {
-    constexpr int SLOT_BITS = T15 - C - G;
+__device__ __forceinline__ void tile_locate(const GeoT &geo, uint32_t jb, uint32_t &col, uint32_t &gidx) {
+    constexpr int SLOT_BITS = TT - C - G;
     const uint32_t tile_id = (blockIdx.x << SLOT_BITS) | (jb >> (C + G));
-    const uint32_t T = tile_id & ((1u << geo.tiles_log) - 1u);
-    col = tile_id >> geo.tiles_log;
     const uint32_t jl = jb & ((1u << (C + G)) - 1u);
-    const uint32_t gfix = ((T & ((1u << geo.low_fixed) - 1u)) << C) | ((T >> geo.low_fixed) << geo.p->hi);
-    if constexpr (C == 0) gidx = gfix | jl;  // contiguous pass: lo = 0
-    else gidx = gfix | (jl & ((1u << C) - 1u)) | ((jl >> C) << geo.p->lo);
+    if constexpr (C == 0) {
+        // contiguous pass: tile position major, column minor
+        const uint32_t T = tile_id / geo.n_cols;
+        col = tile_id - T * geo.n_cols;
+        gidx = (T << G) | jl;
+    } else {
+        col = tile_id >> geo.tiles_log;
+        const uint32_t t = tile_id & ((1u << geo.tiles_log) - 1u);
+        const uint32_t th = t & ((1u << geo.n_high) - 1u), tl = t >> geo.n_high;
+        gidx = (tl << C) | (th << geo.p->hi) | (jl & ((1u << C) - 1u)) | ((jl >> C) << geo.p->lo);
+    }
 }
 
 template <int G, int C, bool INV, int R>
-__device__ __forceinline__ void round15(uint32_t *sm, const Geo15 &geo) {
-    using RI = Round15<G, INV, R>;
-    constexpr int RB = RI::RB, A = RI::A, OA = C + A, RR = 1 << RB, GROUPS = 1 << (E15 - RB);
+__device__ __forceinline__ void roundT(uint32_t *sm, const GeoT &geo) {
+    using RI = RoundT<G, INV, R>;
+    constexpr int RB = RI::RB, A = RI::A, OA = C + A, RR = 1 << RB, GROUPS = 1 << (ET - RB);
     constexpr bool FIRST = R == 0, LAST = R == RI::NR - 1;
+    constexpr int XBITS = TT - RB;
+    constexpr BitMap M = make_map(OA, RB, !FIRST && !LAST);
     const FftLaunch &p = *geo.p;
     const uint32_t lo = (C == 0) ? 0u : p.lo;
+    const uint32_t jt = deposit<WT>(threadIdx.x, M);
 #pragma unroll 1
     for (int grp = 0; grp < GROUPS; grp++) {
-        const uint32_t x = threadIdx.x | ((uint32_t)grp << W15);
-        const uint32_t jb = (x & ((1u << OA) - 1u)) | ((x >> OA) << (OA + RB));
+        const uint32_t jb = jt | deposit<XBITS>((uint32_t)grp << WT, M);
         uint32_t col, gb;
         tile_locate<G, C>(geo, jb, col, gb);
         const uint32_t sh = lo + A;  // global bit of the round's first owned bit
@@ -314,71 +378,71 @@ __device__ __forceinline__ void round15(uint32_t *sm, const Geo15 &geo) {
 }
 
 template <int G, int C, bool INV, int... Rs>
-__device__ __forceinline__ void rounds15(uint32_t *sm, const Geo15 &geo, std::integer_sequence<int, Rs...>) {
+__device__ __forceinline__ void roundsT(uint32_t *sm, const GeoT &geo, std::integer_sequence<int, Rs...>) {
     (
         [&] {
-            round15<G, C, INV, Rs>(sm, geo);
-            if constexpr (Rs + 1 < Round15<G, INV, 0>::NR) __syncthreads();
+            roundT<G, C, INV, Rs>(sm, geo);
+            if constexpr (Rs + 1 < RoundT<G, INV, 0>::NR) __syncthreads();
         }(),
         ...);
 }
 
 template <int G, int C, bool INV>
-__global__ void __launch_bounds__(1 << W15, 1) fft15_kernel(const __grid_constant__ FftLaunch p) {
+__global__ void __launch_bounds__(1 << WT, 2) fftT_kernel(const __grid_constant__ FftLaunch p, uint32_t n_cols) {
     extern __shared__ uint32_t sm[];
-    Geo15 geo;
+    GeoT geo;
     geo.p = &p;
     geo.tiles_log = p.N - (C + G);
     geo.low_fixed = (C == 0) ? 0u : p.lo - C;
-    rounds15<G, C, INV>(sm, geo, std::make_integer_sequence<int, Round15<G, INV, 0>::NR>{});
+    geo.n_high = p.N - p.hi;
+    geo.n_cols = n_cols;
+    roundsT<G, C, INV>(sm, geo, std::make_integer_sequence<int, RoundT<G, INV, 0>::NR>{});
 }
 
 template <int G, int C, bool INV>
-int launch15_t(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
-    constexpr int NR = Round15<G, INV, 0>::NR;
-    const size_t smem = NR > 1 ? (sizeof(uint32_t) << T15) : 0;
-    auto kern = fft15_kernel<G, C, INV>;
+int launchT_t(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
+    constexpr int NR = RoundT<G, INV, 0>::NR;
+    const size_t smem = NR > 1 ? (sizeof(uint32_t) << TT) : 0;
+    auto kern = fftT_kernel<G, C, INV>;
     static bool attr_set = false;
     if (!attr_set) {
         STWO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)(sizeof(uint32_t) << T15)));
+                                           (int)(sizeof(uint32_t) << TT)));
         attr_set = true;
     }
-    // total tiles = n_cols * 2^(N - C - G); 2^(15 - C - G) tiles per CTA
     const uint64_t tiles = (uint64_t)n_cols << (p.N - C - G);
-    const uint64_t per_cta = 1ull << (T15 - C - G);
+    const uint64_t per_cta = 1ull << (TT - C - G);
     STWO_REQUIRE(tiles % per_cta == 0, STWO_ERR_UNSUPPORTED_SIZE, "fft tile packing");
     const uint64_t blocks = tiles / per_cta;
-    kern<<<(unsigned)blocks, 1 << W15, smem, st>>>(p);
-    STWO_LAUNCH_CHECK("fft15_kernel");
+    kern<<<(unsigned)blocks, 1 << WT, smem, st>>>(p, n_cols);
+    STWO_LAUNCH_CHECK("fftT_kernel");
     return STWO_OK;
 }
 
-// Dispatch over (G, C): contiguous passes G = 11..15 (C = 0), strided passes
-// G = 1..10 with C = 15 - G.
+// Dispatch over (G, C): contiguous passes G = 11..14 (C = 0), strided passes
+// G = 1..10 with C = 14 - G.
 template <bool INV>
-int launch15(const FftLaunch &p, uint32_t n_cols, uint32_t G, uint32_t C, cudaStream_t st) {
+int launchT(const FftLaunch &p, uint32_t n_cols, uint32_t G, uint32_t C, cudaStream_t st) {
     if (C == 0) {
         switch (G) {
-        case 11: return launch15_t<11, 0, INV>(p, n_cols, st);
-        case 12: return launch15_t<12, 0, INV>(p, n_cols, st);
-        case 13: return launch15_t<13, 0, INV>(p, n_cols, st);
-        case 14: return launch15_t<14, 0, INV>(p, n_cols, st);
-        case 15: return launch15_t<15, 0, INV>(p, n_cols, st);
+        case 11: return launchT_t<11, 0, INV>(p, n_cols, st);
+        case 12: return launchT_t<12, 0, INV>(p, n_cols, st);
+        case 13: return launchT_t<13, 0, INV>(p, n_cols, st);
+        case 14: return launchT_t<14, 0, INV>(p, n_cols, st);
         default: break;
         }
-    } else if (C + G == 15) {
+    } else if (C + G == TT) {
         switch (G) {
-        case 1: return launch15_t<1, 14, INV>(p, n_cols, st);
-        case 2: return launch15_t<2, 13, INV>(p, n_cols, st);
-        case 3: return launch15_t<3, 12, INV>(p, n_cols, st);
-        case 4: return launch15_t<4, 11, INV>(p, n_cols, st);
-        case 5: return launch15_t<5, 10, INV>(p, n_cols, st);
-        case 6: return launch15_t<6, 9, INV>(p, n_cols, st);
-        case 7: return launch15_t<7, 8, INV>(p, n_cols, st);
-        case 8: return launch15_t<8, 7, INV>(p, n_cols, st);
-        case 9: return launch15_t<9, 6, INV>(p, n_cols, st);
-        case 10: return launch15_t<10, 5, INV>(p, n_cols, st);
+        case 1: return launchT_t<1, 13, INV>(p, n_cols, st);
+        case 2: return launchT_t<2, 12, INV>(p, n_cols, st);
+        case 3: return launchT_t<3, 11, INV>(p, n_cols, st);
+        case 4: return launchT_t<4, 10, INV>(p, n_cols, st);
+        case 5: return launchT_t<5, 9, INV>(p, n_cols, st);
+        case 6: return launchT_t<6, 8, INV>(p, n_cols, st);
+        case 7: return launchT_t<7, 7, INV>(p, n_cols, st);
+        case 8: return launchT_t<8, 6, INV>(p, n_cols, st);
+        case 9: return launchT_t<9, 5, INV>(p, n_cols, st);
+        case 10: return launchT_t<10, 4, INV>(p, n_cols, st);
         default: break;
         }
     }
@@ -468,21 +532,22 @@ int launch_pass(const FftLaunch &p, uint32_t n_cols, bool inv, cudaStream_t st) 
 struct PassSpec { uint32_t lo, hi, c, tile_log; };
 
 // Layer ranges for a transform whose non-trivial layers are [0, L): a bottom
-// contiguous pass of up to 15 layers and strided passes of up to 10 layers above.
+// contiguous pass of up to 14 layers and strided passes of up to 10 layers above,
+// each over 2^14-element tiles (rows of >= 16 contiguous words).
 std::vector<PassSpec> plan_passes(uint32_t L) {
     std::vector<PassSpec> v;
-    if (L <= (uint32_t)MAX_TILE_LOG) {
+    if (L <= (uint32_t)TT) {
         v.push_back({0, L, 0, L});
         return v;
     }
-    v.push_back({0, (uint32_t)MAX_TILE_LOG, 0, (uint32_t)MAX_TILE_LOG});
-    uint32_t lo = MAX_TILE_LOG;
-    const uint32_t max_g = MAX_TILE_LOG - 5;
+    v.push_back({0, (uint32_t)TT, 0, (uint32_t)TT});
+    uint32_t lo = TT;
+    const uint32_t max_g = TT - 4;
     while (lo < L) {
         uint32_t rem = L - lo;
         uint32_t chunks = (rem + max_g - 1) / max_g;
         uint32_t g = (rem + chunks - 1) / chunks;
-        v.push_back({lo, lo + g, MAX_TILE_LOG - g, (uint32_t)MAX_TILE_LOG});
+        v.push_back({lo, lo + g, TT - g, (uint32_t)TT});
         lo += g;
     }
     return v;
@@ -572,9 +637,10 @@ int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_c
             const uint32_t G = ps.hi - ps.lo;
             // Specialised 2^15 tiles: strided passes, or contiguous passes of >= 11 layers whose
             // tiles pack evenly into CTAs.
-            const bool spec = (ps.c > 0 && ps.tile_log == 15) ||
-                              (ps.c == 0 && G >= 11 && ((uint64_t)cnt << (N - G)) % (1ull << (15 - G)) == 0);
-            int rc = spec ? (inv ? launch15<true>(p, cnt, G, ps.c, st) : launch15<false>(p, cnt, G, ps.c, st))
+            const bool spec = (ps.c > 0 && ps.tile_log == (uint32_t)TT) ||
+                              (ps.c == 0 && G >= 11 && G <= (uint32_t)TT &&
+                               ((uint64_t)cnt << (N - G)) % (1ull << (TT - G)) == 0);
+            int rc = spec ? (inv ? launchT<true>(p, cnt, G, ps.c, st) : launchT<false>(p, cnt, G, ps.c, st))
                           : launch_pass(p, cnt, inv, st);
             if (rc) return rc;
         }
