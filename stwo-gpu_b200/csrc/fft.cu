@@ -27,6 +27,7 @@
 //  * One launch serves many columns of the same size; columns of different sizes
 //    use separate launches on the same stream.
 #include <algorithm>
+#include <cstdlib>
 #include <utility>
 #include <vector>
 
@@ -216,13 +217,13 @@ __global__ void __launch_bounds__(1 << MAX_THREADS_LOG) fft_pass_kernel(const __
 // back (their twiddles are then L2 hits); strided passes run the 2^(N-hi) copies of
 // an extension read back to back (the coefficient tile is then an L2 hit).
 // ---------------------------------------------------------------------------
-constexpr int TT = 14, WT = 8, ET = 6;
+constexpr int TT = 14;  // tile = 2^14 elements; a thread owns 2^E of them (E = 5 or 6)
 
 __host__ __device__ constexpr uint32_t swz_c(uint32_t j) { return j ^ (((j >> 5) ^ (j >> 10)) & 31u); }
 
-template <int G, bool INV, int R>
+template <int G, bool INV, int R, int E>
 struct RoundT {
-    static constexpr int NR = (G + ET - 1) / ET;
+    static constexpr int NR = (G + E - 1) / E;
     // balanced split of the G bits into NR rounds
     static constexpr int before(int r) { return r == 0 ? 0 : before(r - 1) + (G - before(r - 1) + (NR - r)) / (NR - r + 1); }
     static constexpr int RB = before(R + 1) - before(R);
@@ -301,94 +302,154 @@ __device__ __forceinline__ void tile_locate(const GeoT &geo, uint32_t jb, uint32
     }
 }
 
-template <int G, int C, bool INV, int R>
+// The butterflies of one layer (bit u of the round) on one group of 2^RB registers.
+template <int C, int A, int RB, bool INV, int U>
+__device__ __forceinline__ void layer_butterflies(uint32_t (&v)[1 << RB], const FftLaunch &p, uint32_t gb,
+                                                  uint32_t sh) {
+    constexpr int RR = 1 << RB;
+    constexpr int NQ = RR >> (U + 1);  // twiddles of this layer: consecutive and aligned to NQ
+    constexpr bool CIRCLE = (C == 0 && A + U == 0);
+    const uint32_t k = sh + U;
+    const uint32_t hb = gb >> (k + 1);
+    uint32_t tws[NQ];
+    if constexpr (CIRCLE) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) tws[q] = twiddle2(p.tw, p.N, 0, hb + q);
+    } else {
+        const uint32_t *tk = p.tw + ((1u << (p.N - 1)) - (1u << (p.N - k))) + hb;
+        if constexpr (NQ >= 4) {
+#pragma unroll
+            for (int q = 0; q < NQ; q += 4) {
+                uint4 t = __ldg(reinterpret_cast<const uint4 *>(tk + q));
+                tws[q] = t.x << 1; tws[q + 1] = t.y << 1; tws[q + 2] = t.z << 1; tws[q + 3] = t.w << 1;
+            }
+        } else if constexpr (NQ == 2) {
+            uint2 t = __ldg(reinterpret_cast<const uint2 *>(tk));
+            tws[0] = t.x << 1;
+            tws[1] = t.y << 1;
+        } else {
+            tws[0] = __ldg(tk) << 1;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+#pragma unroll
+        for (int l = 0; l < (1 << U); l++) {
+            const int m0 = (q << (U + 1)) | l;
+            butterfly<INV>(v[m0], v[m0 | (1 << U)], tws[q]);
+        }
+    }
+}
+
+// All layers of one round on one group: evaluate runs them top-down, interpolate
+// bottom-up. gb is the global index of the group's first element and sh the
+// global bit of the round's first layer.
+template <int C, int A, int RB, bool INV, int... Us>
+__device__ __forceinline__ void round_butterflies_seq(uint32_t (&v)[1 << RB], const FftLaunch &p, uint32_t gb,
+                                                      uint32_t sh, std::integer_sequence<int, Us...>) {
+    (layer_butterflies<C, A, RB, INV, INV ? Us : RB - 1 - Us>(v, p, gb, sh), ...);
+}
+
+template <int C, int A, int RB, bool INV>
+__device__ __forceinline__ void round_butterflies(uint32_t (&v)[1 << RB], const FftLaunch &p, uint32_t gb,
+                                                  uint32_t sh) {
+    round_butterflies_seq<C, A, RB, INV>(v, p, gb, sh, std::make_integer_sequence<int, RB>{});
+}
+
+template <int C, int A, int RB, bool INV>
+__device__ __forceinline__ void store_global(uint32_t (&v)[1 << RB], const FftLaunch &p, uint32_t *__restrict__ dst,
+                                             uint32_t gb, uint32_t sh) {
+    constexpr int RR = 1 << RB;
+    if (INV && p.scale2) {
+#pragma unroll
+        for (int m = 0; m < RR; m++) v[m] = m31_mul2(v[m], p.scale2);
+    }
+    if constexpr (C == 0 && A == 0 && RR >= 4) {
+#pragma unroll
+        for (int m = 0; m < RR; m += 4)
+            *reinterpret_cast<uint4 *>(dst + gb + m) = make_uint4(v[m], v[m + 1], v[m + 2], v[m + 3]);
+    } else {
+#pragma unroll
+        for (int m = 0; m < RR; m++) dst[gb + ((uint32_t)m << sh)] = v[m];
+    }
+}
+
+template <int G, int C, bool INV, int R, int E>
 __device__ __forceinline__ void roundT(uint32_t *sm, const GeoT &geo) {
-    using RI = RoundT<G, INV, R>;
-    constexpr int RB = RI::RB, A = RI::A, OA = C + A, RR = 1 << RB, GROUPS = 1 << (ET - RB);
+    using RI = RoundT<G, INV, R, E>;
+    constexpr int RB = RI::RB, A = RI::A, OA = C + A, RR = 1 << RB, GROUPS = 1 << (E - RB), W = TT - E;
     constexpr bool FIRST = R == 0, LAST = R == RI::NR - 1;
     constexpr int XBITS = TT - RB;
     constexpr BitMap M = make_map(OA, RB, !FIRST && !LAST);
     const FftLaunch &p = *geo.p;
     const uint32_t lo = (C == 0) ? 0u : p.lo;
-    const uint32_t jt = deposit<WT>(threadIdx.x, M);
-#pragma unroll 1
-    for (int grp = 0; grp < GROUPS; grp++) {
-        const uint32_t jb = jt | deposit<XBITS>((uint32_t)grp << WT, M);
-        uint32_t col, gb;
-        tile_locate<G, C>(geo, jb, col, gb);
-        const uint32_t sh = lo + A;  // global bit of the round's first owned bit
-        uint32_t v[RR];
-        if constexpr (FIRST) {
-            const uint32_t *__restrict__ src = p.cols[col].src;
-            const uint32_t base = gb & p.src_mask;
+    const uint32_t sh = lo + A;  // global bit of the round's first owned bit
+    const uint32_t jt = deposit<W>(threadIdx.x, M);
+    if constexpr (FIRST) {
+        // Issue every global load of the round before the first butterfly.
+        uint32_t v[GROUPS][RR];
+        uint32_t gbs[GROUPS], cols[GROUPS];
+#pragma unroll
+        for (int grp = 0; grp < GROUPS; grp++) {
+            const uint32_t jb = jt | deposit<XBITS>((uint32_t)grp << W, M);
+            tile_locate<G, C>(geo, jb, cols[grp], gbs[grp]);
+            const uint32_t *__restrict__ src = p.cols[cols[grp]].src;
+            const uint32_t base = gbs[grp] & p.src_mask;
             if constexpr (C == 0 && A == 0 && RR >= 4) {
 #pragma unroll
                 for (int m = 0; m < RR; m += 4) {
                     uint4 t = __ldg(reinterpret_cast<const uint4 *>(src + base + m));
-                    v[m] = t.x; v[m + 1] = t.y; v[m + 2] = t.z; v[m + 3] = t.w;
+                    v[grp][m] = t.x; v[grp][m + 1] = t.y; v[grp][m + 2] = t.z; v[grp][m + 3] = t.w;
                 }
             } else {
 #pragma unroll
-                for (int m = 0; m < RR; m++) v[m] = __ldg(src + base + ((uint32_t)m << sh));
+                for (int m = 0; m < RR; m++) v[grp][m] = __ldg(src + base + ((uint32_t)m << sh));
             }
-        } else {
+        }
+#pragma unroll
+        for (int grp = 0; grp < GROUPS; grp++) {
+            round_butterflies<C, A, RB, INV>(v[grp], p, gbs[grp], sh);
+            if constexpr (LAST) {
+                store_global<C, A, RB, INV>(v[grp], p, p.cols[cols[grp]].dst, gbs[grp], sh);
+            } else {
+                const uint32_t sj = swz_c(jt | deposit<XBITS>((uint32_t)grp << W, M));
+#pragma unroll
+                for (int m = 0; m < RR; m++) sm[sj ^ swz_c((uint32_t)m << OA)] = v[grp][m];
+            }
+        }
+    } else {
+#pragma unroll 1
+        for (int grp = 0; grp < GROUPS; grp++) {
+            const uint32_t jb = jt | deposit<XBITS>((uint32_t)grp << W, M);
+            uint32_t col, gb;
+            tile_locate<G, C>(geo, jb, col, gb);
+            uint32_t v[RR];
             const uint32_t sj = swz_c(jb);
 #pragma unroll
             for (int m = 0; m < RR; m++) v[m] = sm[sj ^ swz_c((uint32_t)m << OA)];
-        }
-#pragma unroll
-        for (int uu = 0; uu < RB; uu++) {
-            const int u = INV ? uu : RB - 1 - uu;
-            const uint32_t k = sh + u;
-            const uint32_t hb = gb >> (k + 1);
-            const uint32_t *tk = nullptr;
-            if (!(C == 0 && A + u == 0)) tk = p.tw + ((1u << (p.N - 1)) - (1u << (p.N - k))) + hb;
-#pragma unroll
-            for (int q = 0; q < (RR >> (u + 1)); q++) {
-                uint32_t t2;
-                if (C == 0 && A + u == 0) t2 = twiddle2(p.tw, p.N, 0, hb + q);
-                else t2 = __ldg(tk + q) << 1;
-#pragma unroll
-                for (int l = 0; l < (1 << u); l++) {
-                    const int m0 = (q << (u + 1)) | l;
-                    butterfly<INV>(v[m0], v[m0 | (1 << u)], t2);
-                }
-            }
-        }
-        if constexpr (LAST) {
-            uint32_t *__restrict__ dst = p.cols[col].dst;
-            if (INV && p.scale2) {
-#pragma unroll
-                for (int m = 0; m < RR; m++) v[m] = m31_mul2(v[m], p.scale2);
-            }
-            if constexpr (C == 0 && A == 0 && RR >= 4) {
-#pragma unroll
-                for (int m = 0; m < RR; m += 4)
-                    *reinterpret_cast<uint4 *>(dst + gb + m) = make_uint4(v[m], v[m + 1], v[m + 2], v[m + 3]);
+            round_butterflies<C, A, RB, INV>(v, p, gb, sh);
+            if constexpr (LAST) {
+                store_global<C, A, RB, INV>(v, p, p.cols[col].dst, gb, sh);
             } else {
 #pragma unroll
-                for (int m = 0; m < RR; m++) dst[gb + ((uint32_t)m << sh)] = v[m];
+                for (int m = 0; m < RR; m++) sm[sj ^ swz_c((uint32_t)m << OA)] = v[m];
             }
-        } else {
-            const uint32_t sj = swz_c(jb);
-#pragma unroll
-            for (int m = 0; m < RR; m++) sm[sj ^ swz_c((uint32_t)m << OA)] = v[m];
         }
     }
 }
 
-template <int G, int C, bool INV, int... Rs>
+template <int G, int C, bool INV, int E, int... Rs>
 __device__ __forceinline__ void roundsT(uint32_t *sm, const GeoT &geo, std::integer_sequence<int, Rs...>) {
     (
         [&] {
-            roundT<G, C, INV, Rs>(sm, geo);
-            if constexpr (Rs + 1 < RoundT<G, INV, 0>::NR) __syncthreads();
+            roundT<G, C, INV, Rs, E>(sm, geo);
+            if constexpr (Rs + 1 < RoundT<G, INV, 0, E>::NR) __syncthreads();
         }(),
         ...);
 }
 
-template <int G, int C, bool INV>
-__global__ void __launch_bounds__(1 << WT, 2) fftT_kernel(const __grid_constant__ FftLaunch p, uint32_t n_cols) {
+template <int G, int C, bool INV, int E>
+__global__ void __launch_bounds__(1 << (TT - E), 2) fftT_kernel(const __grid_constant__ FftLaunch p, uint32_t n_cols) {
     extern __shared__ uint32_t sm[];
     GeoT geo;
     geo.p = &p;
@@ -396,14 +457,14 @@ __global__ void __launch_bounds__(1 << WT, 2) fftT_kernel(const __grid_constant_
     geo.low_fixed = (C == 0) ? 0u : p.lo - C;
     geo.n_high = p.N - p.hi;
     geo.n_cols = n_cols;
-    roundsT<G, C, INV>(sm, geo, std::make_integer_sequence<int, RoundT<G, INV, 0>::NR>{});
+    roundsT<G, C, INV, E>(sm, geo, std::make_integer_sequence<int, RoundT<G, INV, 0, E>::NR>{});
 }
 
-template <int G, int C, bool INV>
-int launchT_t(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
-    constexpr int NR = RoundT<G, INV, 0>::NR;
+template <int G, int C, bool INV, int E>
+int launchT_e(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
+    constexpr int NR = RoundT<G, INV, 0, E>::NR;
     const size_t smem = NR > 1 ? (sizeof(uint32_t) << TT) : 0;
-    auto kern = fftT_kernel<G, C, INV>;
+    auto kern = fftT_kernel<G, C, INV, E>;
     static bool attr_set = false;
     if (!attr_set) {
         STWO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -414,9 +475,24 @@ int launchT_t(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
     const uint64_t per_cta = 1ull << (TT - C - G);
     STWO_REQUIRE(tiles % per_cta == 0, STWO_ERR_UNSUPPORTED_SIZE, "fft tile packing");
     const uint64_t blocks = tiles / per_cta;
-    kern<<<(unsigned)blocks, 1 << WT, smem, st>>>(p, n_cols);
+    kern<<<(unsigned)blocks, 1 << (TT - E), smem, st>>>(p, n_cols);
     STWO_LAUNCH_CHECK("fftT_kernel");
     return STWO_OK;
+}
+
+// Elements per thread: 2^5 (512 threads, 32 warps per SM at two CTAs) by default;
+// STWO_FFT_EPT_LOG=6 selects 2^6 (256 threads, more registers per thread).
+inline int fft_ept_log() {
+    static int v = [] {
+        const char *e = getenv("STWO_FFT_EPT_LOG");
+        return (e && atoi(e) == 6) ? 6 : 5;
+    }();
+    return v;
+}
+
+template <int G, int C, bool INV>
+int launchT_t(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
+    return fft_ept_log() == 6 ? launchT_e<G, C, INV, 6>(p, n_cols, st) : launchT_e<G, C, INV, 5>(p, n_cols, st);
 }
 
 // Dispatch over (G, C): contiguous passes G = 11..14 (C = 0), strided passes
@@ -637,9 +713,11 @@ int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_c
             const uint32_t G = ps.hi - ps.lo;
             // Specialised 2^15 tiles: strided passes, or contiguous passes of >= 11 layers whose
             // tiles pack evenly into CTAs.
-            const bool spec = (ps.c > 0 && ps.tile_log == (uint32_t)TT) ||
-                              (ps.c == 0 && G >= 11 && G <= (uint32_t)TT &&
-                               ((uint64_t)cnt << (N - G)) % (1ull << (TT - G)) == 0);
+            // (vector twiddle loads need the tree suffix 16-byte aligned)
+            const bool spec = ((uintptr_t)p.tw & 15) == 0 &&
+                              ((ps.c > 0 && ps.tile_log == (uint32_t)TT) ||
+                               (ps.c == 0 && G >= 11 && G <= (uint32_t)TT &&
+                                ((uint64_t)cnt << (N - G)) % (1ull << (TT - G)) == 0));
             int rc = spec ? (inv ? launchT<true>(p, cnt, G, ps.c, st) : launchT<false>(p, cnt, G, ps.c, st))
                           : launch_pass(p, cnt, inv, st);
             if (rc) return rc;
