@@ -116,6 +116,54 @@ def cpu_baseline(O, log_size, log_blowup, threads):
     return dt
 
 
+def reference_gpu_timing(args, evals, lg, lb, ncols, tw, itw, tree_size):
+    """The reference's own CUDA library (oracle/_ref, built unmodified from its sources)
+    on the same step through its own API path: interpolate_columns, then, as
+    PolyOps::evaluate_polynomials does (poly.rs:128-168), extend every polynomial into
+    a fresh zeroed buffer and evaluate_columns. Reported beside our numbers."""
+    import ctypes as C
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        import reflib
+    except ImportError:
+        return None
+    if not reflib.available():
+        return None
+    R = reflib.lib()
+    N = lg + lb
+    ptrs = (C.c_void_p * ncols)(*[t.data_ptr() for t in evals])
+
+    def step():
+        R.interpolate_columns(1 << (lg - 1), ptrs, itw.data_ptr(), tree_size, ncols, 1 << lg)
+        ext = []
+        for t in evals:
+            d = R.cuda_alloc_zeroes_uint32_t(1 << N)
+            R.copy_uint32_t_vec_from_device_to_device(t.data_ptr(), d, 1 << lg)
+            ext.append(d)
+        eptr = (C.c_void_p * ncols)(*ext)
+        sizes = (C.c_int * ncols)(*([1 << N] * ncols))
+        dom = (C.c_int * ncols)(*([1 << (N - 1)] * ncols))
+        R.evaluate_columns(dom, eptr, tw.data_ptr(), tree_size, ncols, sizes)
+        for d in ext:
+            R.cuda_free_memory(d)
+
+    torch.cuda.synchronize()
+    step()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    s.record(torch.cuda.default_stream())
+    for _ in range(reps):
+        step()
+    e.record(torch.cuda.default_stream())
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / reps
+    return {"ms_per_step": ms, "value": ncols / (ms / 1e3), "unit": UNIT,
+            "what": "reference CUDA library (oracle/_ref) on this GPU: interpolate_columns + extend + "
+                    "evaluate_columns, same 8 x 2^24 step"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -256,6 +304,8 @@ def run_ours(args, rank, world, local_rank):
         e2e_ms = float(t.item())
     e2e_value = world * ncols / (e2e_ms / 1e3)
 
+    ref_gpu = reference_gpu_timing(args, evals, lg, lb, ncols, tw, itw, tree_size) if rank == 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         O = load_oracle()
@@ -281,6 +331,7 @@ def run_ours(args, rank, world, local_rank):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ncols * (1 << lg) * 4,
                     "d2h_bytes_per_step": ncols * (1 << N) * 4, "ms_per_step": e2e_ms},
+            "reference_gpu": ref_gpu,
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
         }
