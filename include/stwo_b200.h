@@ -188,6 +188,20 @@ int stwo_eval_at_points(const uint32_t *const *coeffs, const uint32_t *log_sizes
                         const stwo_spoint *points, stwo_qm31 *results, void *scratch, size_t scratch_bytes,
                         void *stream);
 
+/* PolyOps::eval_at_point that allocates nothing. It has no counterpart in the
+ * reference (whose eval_at_point mallocs and frees scratch on every call); it is
+ * for callers that cannot call cudaMalloc, for example a server whose device memory
+ * all belongs to its own pool, or a loop that cannot afford cudaMalloc/cudaFree's
+ * implicit synchronisation. The scratch is a fixed 512.5 KiB array inside the library,
+ * held on every GPU that loads it until the process exits, so polynomials are
+ * limited to 2^26 coefficients (larger sizes return STWO_ERR_UNSUPPORTED_SIZE).
+ * result is a device pointer to one QM31; the call is asynchronous on `stream`.
+ * The first call on each device looks the array's device address up (make it
+ * before any stream capture). All calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller. */
+int stwo_eval_at_point_no_alloc(const uint32_t *coeffs, uint32_t log_size, stwo_qm31 point_x, stwo_qm31 point_y,
+                                stwo_qm31 *result, void *stream);
+
 /* FriOps on SoA QM31 columns; itwiddles + twiddle_offset as in fri.rs:24-26,56. */
 int stwo_fold_line(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha, const uint32_t *itwiddles,
                    uint64_t twiddle_offset, uint32_t *const *dst4, void *stream);

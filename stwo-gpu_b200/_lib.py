@@ -84,6 +84,7 @@ SIGNATURES = [
     ("stwo_batch_inverse_qm31", C.c_int, [vp, vp, u64, vp]),
     ("stwo_eval_at_points_scratch_bytes", sz, [vp, u32]),
     ("stwo_eval_at_points", C.c_int, [vp, vp, u32, vp, vp, vp, sz, vp]),
+    ("stwo_eval_at_point_no_alloc", C.c_int, [vp, u32, QM31, QM31, vp, vp]),
     ("stwo_fold_line", C.c_int, [vp, u64, QM31, vp, u64, vp, vp]),
     ("stwo_fold_circle_into_line", C.c_int, [vp, u64, QM31, vp, u64, vp, vp]),
     ("stwo_accumulate", C.c_int, [vp, vp, u64, vp]),

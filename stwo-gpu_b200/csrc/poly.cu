@@ -2,6 +2,7 @@
 // interpolate / evaluate (reference-compatible and native), eval_at_point.
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -452,3 +453,71 @@ stwo_qm31 eval_at_point(const uint32_t *coeffs, uint32_t coeffs_size, stwo_qm31 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// eval_at_point without any allocation.
+//
+// Some callers cannot call cudaMalloc: a proof server that hands every byte of
+// HBM to its own pool at start-up and admits jobs against that fixed budget, a
+// host library embedded in a process whose allocator owns the device, or a
+// latency-critical loop that must not pay the implicit device-wide
+// synchronisation of cudaMalloc/cudaFree. For them this entry point evaluates a
+// polynomial at a point with its per-block partial sums and completion tickets in
+// a fixed device array of this library instead of freshly allocated memory.
+//
+// The array is a file-scope __device__ variable: every GPU that loads the library
+// holds its 512.5 KiB until the process exits. Host code only knows a stand-in symbol
+// for it, so its device address is looked up with cudaGetSymbolAddress once per
+// device, on that device's first call (which therefore should come before any
+// stream capture), and the address is what the kernel receives.
+// All calls share the one array, so calls whose work overlaps on the GPU (two
+// streams, or two host threads) race and must be serialised by the caller; the
+// completion tickets are cleared at the start of every call, and the partial sums
+// are fully rewritten before they are read.
+// ---------------------------------------------------------------------------
+constexpr uint32_t EAP_NOALLOC_MAX_LOG = 26;  // 2^26 coefficients, 2^15 partial sums
+constexpr size_t EAP_NOALLOC_BYTES =
+    (((size_t)1 << (EAP_NOALLOC_MAX_LOG - EAP_CHUNK_LOG)) * sizeof(qm31) + 16 + 256 + 255) / 256 * 256;
+
+static __device__ __align__(256) unsigned char g_eap_noalloc_scratch[EAP_NOALLOC_BYTES];
+
+namespace {
+
+constexpr int EAP_NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[EAP_NOALLOC_MAX_DEVICES] = {};
+
+// Device address of the scratch array on the current device (looked up once).
+int noalloc_scratch(void **out) {
+    int dev = 0;
+    STWO_CUDA_TRY(cudaGetDevice(&dev));
+    STWO_REQUIRE(dev >= 0 && dev < EAP_NOALLOC_MAX_DEVICES, STWO_ERR_UNSUPPORTED_SIZE, "device ordinal %d", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_eap_noalloc_scratch);
+        if (e != cudaSuccess || ptr == nullptr)
+            return set_error(STWO_ERR_CUDA, "cudaGetSymbolAddress of the eval_at_point scratch failed: %s",
+                             cudaGetErrorString(e));
+        g_noalloc_addr[dev] = ptr;
+    }
+    *out = g_noalloc_addr[dev];
+    return STWO_OK;
+}
+
+}  // namespace
+
+extern "C" int stwo_eval_at_point_no_alloc(const uint32_t *coeffs, uint32_t log_size, stwo_qm31 point_x,
+                                           stwo_qm31 point_y, stwo_qm31 *result, void *stream) {
+    STWO_REQUIRE(log_size <= EAP_NOALLOC_MAX_LOG, STWO_ERR_UNSUPPORTED_SIZE,
+                 "stwo_eval_at_point_no_alloc handles at most 2^%u coefficients (got 2^%u); use eval_at_point",
+                 EAP_NOALLOC_MAX_LOG, log_size);
+    STWO_REQUIRE(coeffs != nullptr && result != nullptr, STWO_ERR_INVALID_ARGUMENT, "null coefficient or result pointer");
+    void *scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    const stwo_spoint pt = {point_x, point_y};
+    // tickets_zeroed = false: the ticket words are cleared with cudaMemsetAsync first.
+    return eval_at_points_async(&coeffs, &log_size, 1, &pt, result, scratch, EAP_NOALLOC_BYTES, false,
+                                as_stream(stream));
+}
