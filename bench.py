@@ -164,6 +164,196 @@ def reference_gpu_timing(args, evals, lg, lb, ncols, tw, itw, tree_size):
                     "evaluate_columns, same 8 x 2^24 step"}
 
 
+def replica_throughput(local_ms, units_per_rank, world, device=None):
+    """Whole-job throughput of `world` independent replicas (no data-path collective):
+    the step time is the maximum over ranks, and every rank processed
+    `units_per_rank` units. Returns (max_ms, units per second)."""
+    if world > 1:
+        import torch
+        t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        local_ms = float(t.item())
+    return local_ms, world * units_per_rank / (local_ms / 1e3)
+
+
+def kernel_suite(stwo, reps=5):
+    """Config-1 per-kernel sweep (seeded uniform data) on cuda:0, ours and the reference
+    CUDA library (oracle/_ref) on the same device inputs. Times are CUDA-event means over
+    `reps` runs after one warm-up; algorithmic bytes are defined per kernel below."""
+    import ctypes as C
+    import torch
+    L = stwo._lib
+    lib = L.lib()
+    dev = torch.device("cuda", 0)
+    peak, _ = measured_peaks()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    R = None
+    try:
+        import reflib
+        if reflib.available():
+            R = reflib.lib()
+    except ImportError:
+        pass
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(99)
+
+    def rand(n, nonzero=False):
+        lo = 1 if nonzero else 0
+        return torch.randint(lo, P, (n,), dtype=torch.int64, device=dev, generator=gen).to(torch.int32)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(torch.cuda.current_stream())
+        for _ in range(reps):
+            fn()
+        e.record(torch.cuda.current_stream())
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    def ptrs(ts):
+        return (C.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+
+    out = {}
+    sptr = torch.cuda.current_stream(dev).cuda_stream
+
+    # (b) Blake2s Merkle tree over 64 columns of 2^22 (leaf = 64 words): leaf layer + 22 node layers.
+    lg, nc = 22, 64
+    cols = [rand(1 << lg) for _ in range(nc)]
+    layers = [torch.empty((1 << l) * 8, dtype=torch.int32, device=dev) for l in range(lg + 1)]
+    cptr = ptrs(cols)
+
+    def merkle_ours():
+        L.check(lib.stwo_merkle_commit_layer(lg, None, cptr, nc, layers[lg].data_ptr(), sptr))
+        for l in range(lg - 1, -1, -1):
+            L.check(lib.stwo_merkle_commit_layer(l, layers[l + 1].data_ptr(), None, 0, layers[l].data_ptr(), sptr))
+
+    t = timed(merkle_ours)
+    nodes = (1 << (lg + 1)) - 1
+    b = nc * (1 << lg) * 4 + nodes * 32 + ((1 << lg) - 1) * 64
+    comp = (1 << lg) * (nc // 16) + ((1 << lg) - 1)
+    rec = {"ms": t, "gbs": b / t / 1e6, "frac_hbm": b / t / 1e6 / peak, "compressions_per_s": comp / (t / 1e3),
+           "workload": "64 cols x 2^22, full tree"}
+    if R is not None:
+        dcols = R.copy_device_pointer_vec_from_host_to_device(cptr, nc)
+        rl = [torch.empty((1 << l) * 8, dtype=torch.int32, device=dev) for l in range(lg + 1)]
+
+        def merkle_ref():
+            R.commit_on_first_layer(1 << lg, nc, dcols, rl[lg].data_ptr())
+            for l in range(lg - 1, -1, -1):
+                R.commit_on_layer_with_previous(1 << l, 0, dcols, rl[l + 1].data_ptr(), rl[l].data_ptr())
+
+        rec["reference_ms"] = timed(merkle_ref)
+        rec["root_equal"] = bool(torch.equal(rl[0], layers[0]))
+        R.cuda_free_memory(dcols)
+    out["merkle"] = rec
+    del cols, layers
+
+    # (c) batch inverse of 2^24 nonzero QM31 (AoS).
+    n = 1 << 24
+    src = rand(4 * n, nonzero=True)
+    dst = torch.empty_like(src)
+    t = timed(lambda: L.check(lib.stwo_batch_inverse_qm31(src.data_ptr(), dst.data_ptr(), n, sptr)))
+    rec = {"ms": t, "gbs": n * 32 / t / 1e6, "frac_hbm": n * 32 / t / 1e6 / peak, "workload": "2^24 QM31"}
+    if R is not None:
+        rdst = torch.empty_like(src)
+        rec["reference_ms"] = timed(lambda: R.batch_inverse_secure_field(src.data_ptr(), rdst.data_ptr(), n))
+        rec["equal"] = bool(torch.equal(rdst, dst))
+    out["batch_inverse_qm31"] = rec
+    del src, dst
+
+    # (d) FRI: fold_circle_into_line 2^24 -> 2^23, then fold_line down to 2^4.
+    lg = 24
+    hc = stwo.CanonicCoset(lg).half_coset()  # circle domain 2^24; line domain = its half coset
+    tree = torch.empty(1 << hc.log_size, dtype=torch.int32, device=dev)
+    itree = torch.empty_like(tree)
+    L.check(lib.stwo_precompute_twiddles(hc.initial_index, hc.step_size, hc.log_size, tree.data_ptr(),
+                                         itree.data_ptr(), sptr))
+    src = [rand(1 << lg) for _ in range(4)]
+    bufs = [[torch.empty(1 << l, dtype=torch.int32, device=dev) for _ in range(4)] for l in range(lg)]
+    alpha = L.QM31(12345, 678, 91011, 1213)
+    tsz = 1 << hc.log_size
+
+    def fri_ours():
+        L.check(lib.stwo_fold_circle_into_line(ptrs(src), 1 << lg, alpha, itree.data_ptr(), 0, ptrs(bufs[lg - 1]),
+                                               sptr))
+        for l in range(lg - 1, 4, -1):
+            L.check(lib.stwo_fold_line(ptrs(bufs[l]), 1 << l, alpha, itree.data_ptr(), tsz - (1 << l),
+                                       ptrs(bufs[l - 1]), sptr))
+
+    t = timed(fri_ours)
+    b = (1 << (lg - 1)) * 68 + sum((1 << (l - 1)) * 52 for l in range(lg - 1, 4, -1))
+    rec = {"ms": t, "gbs": b / t / 1e6, "frac_hbm": b / t / 1e6 / peak, "workload": "circle fold 2^24 + line folds to 2^4"}
+    if R is not None:
+        rb_ = [[torch.empty(1 << l, dtype=torch.int32, device=dev) for _ in range(4)] for l in range(lg)]
+
+        def fri_ref():
+            R.fold_circle_into_line(itree.data_ptr(), 0, 1 << lg, ptrs(src), reflib.QM31(12345, 678, 91011, 1213),
+                                    ptrs(rb_[lg - 1]))
+            for l in range(lg - 1, 4, -1):
+                R.fold_line(itree.data_ptr(), tsz - (1 << l), 1 << l, ptrs(rb_[l]),
+                            reflib.QM31(12345, 678, 91011, 1213), ptrs(rb_[l - 1]))
+
+        for bb in rb_[lg - 1]:
+            bb.zero_()
+        for bb in bufs[lg - 1]:
+            bb.zero_()
+        fri_ref()
+        fri_ours()
+        torch.cuda.synchronize()
+        rec["equal_after_one_chain"] = all(torch.equal(a, c) for a, c in zip(rb_[4], bufs[4]))
+        rec["reference_ms"] = timed(fri_ref)
+    out["fri_fold_chain"] = rec
+    del src, bufs
+
+    # (e) DEEP quotients: 32 columns over a 2^22 domain, 4 sample points each sampling all 32 columns.
+    lg, nc, nb = 22, 32, 4
+    dom = stwo.CanonicCoset(lg).circle_domain()
+    cols = [rand(1 << lg) for _ in range(nc)]
+    outq = [torch.empty(1 << lg, dtype=torch.int32, device=dev) for _ in range(4)]
+    import random
+    rr = random.Random(5)
+
+    def rq():
+        return L.QM31(*[rr.randrange(P) for _ in range(4)])
+
+    sp = (L.SPoint * nb)(*[L.SPoint(rq(), rq()) for _ in range(nb)])  # any QM31 pair works for timing
+    sizes = (C.c_uint32 * nb)(*([nc] * nb))
+    idx = (C.c_uint32 * (nc * nb))(*(list(range(nc)) * nb))
+    vals = (L.QM31 * (nc * nb))(*[rq() for _ in range(nc * nb)])
+    rcoef = rq()
+    cp = ptrs(cols)
+
+    def quot_ours():
+        L.check(lib.stwo_accumulate_quotients(dom.half_coset.initial_index, dom.half_coset.step_size, lg, cp, nc,
+                                              rcoef, sp, sizes, idx, vals, nb, ptrs(outq), sptr))
+
+    t = timed(quot_ours)
+    b = (1 << lg) * (4 * nc + 16)
+    rec = {"ms": t, "gbs": b / t / 1e6, "frac_hbm": b / t / 1e6 / peak, "workload": "32 cols x 2^22, 4 points"}
+    if R is not None:
+        dcols = R.copy_device_pointer_vec_from_host_to_device(cp, nc)
+        rout = [torch.empty(1 << lg, dtype=torch.int32, device=dev) for _ in range(4)]
+        flat_pts = (C.c_uint32 * (8 * nb))(*[v for q in sp for v in (q.x.a, q.x.b, q.x.c, q.x.d,
+                                                                      q.y.a, q.y.b, q.y.c, q.y.d)])
+        rvals = (reflib.QM31 * (nc * nb))(*[reflib.QM31(v.a, v.b, v.c, v.d) for v in vals])
+
+        def quot_ref():
+            R.accumulate_quotients(dom.half_coset.initial_index, dom.half_coset.step_size, 1 << lg, dcols, nc,
+                                   reflib.QM31(rcoef.a, rcoef.b, rcoef.c, rcoef.d), flat_pts, idx, nc * nb, rvals,
+                                   sizes, nb, *[o.data_ptr() for o in rout], nc * nb * 3)
+
+        rec["reference_ms"] = timed(quot_ref)
+        rec["equal"] = all(torch.equal(a, c) for a, c in zip(rout, outq))
+        R.cuda_free_memory(dcols)
+    out["quotients"] = rec
+    for k, v in out.items():
+        if "reference_ms" in v:
+            v["speedup_vs_reference"] = v["reference_ms"] / v["ms"]
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -253,12 +443,7 @@ def run_ours(args, rank, world, local_rank):
     total_ms = start.elapsed_time(end)
     t_interp = sum(a.elapsed_time(b) for a, b, _ in ev) / args.steps
     t_eval = sum(b.elapsed_time(c) for _, b, c in ev) / args.steps
-    ms_step = total_ms / args.steps
-    if world > 1:
-        t = torch.tensor([ms_step], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_step = float(t.item())
-    value = world * ncols / (ms_step / 1e3)
+    ms_step, value = replica_throughput(total_ms / args.steps, ncols, world, dev)
 
     # Roofline of the FFT kernel: algorithmic bytes = one read + one write per
     # element (interpolate: 8 B per element; evaluate: 4 B per coefficient read +
@@ -297,14 +482,14 @@ def run_ours(args, rank, world, local_rank):
         e2e_step()
     e2.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = s2.elapsed_time(e2) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * ncols / (e2e_ms / 1e3)
+    e2e_ms, e2e_value = replica_throughput(s2.elapsed_time(e2) / e2e_steps, ncols, world, dev)
 
     ref_gpu = reference_gpu_timing(args, evals, lg, lb, ncols, tw, itw, tree_size) if rank == 0 else None
+    kernels = None
+    if rank == 0 and world == 1 and not args.no_suite:
+        del evals, outs, h_in, h_out
+        torch.cuda.empty_cache()
+        kernels = kernel_suite(stwo)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -332,6 +517,7 @@ def run_ours(args, rank, world, local_rank):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ncols * (1 << lg) * 4,
                     "d2h_bytes_per_step": ncols * (1 << N) * 4, "ms_per_step": e2e_ms},
             "reference_gpu": ref_gpu,
+            "kernels": kernels,
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
         }
@@ -349,6 +535,7 @@ def main():
     ap.add_argument("--log-size", type=int, default=24)
     ap.add_argument("--log-blowup", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-suite", action="store_true", help="skip the config-1 per-kernel sweep")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
