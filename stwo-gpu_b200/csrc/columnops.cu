@@ -8,11 +8,12 @@
 // the other, so every HBM access is a full line and in-place is safe.
 //
 // Batch inverse (reference: per-block product tree in shared memory,
-// cuda/src/batch_inverse.cu:25-155). Here each thread keeps prefix products of its
-// 8 elements in registers, a block-wide multiplicative scan (warp shuffles, then
-// one value per warp) gives the products before and after every thread, one field
-// inversion per CTA inverts the block product, and the back-substitution recovers
-// every inverse: 3 multiplications per element and one inversion per 2048 elements.
+// cuda/src/batch_inverse.cu:25-155). Here each warp owns 256 elements with
+// coalesced accesses (lane l takes elements l, l+32, ...): prefix products in
+// registers, a multiplicative scan of the lane products in both directions with
+// shuffles, one field inversion of the warp product (computed by every lane, so no
+// barrier is needed) and back-substitution: 3 multiplications per element and one
+// inversion per 256 elements.
 #include "common.cuh"
 
 namespace stwo {
@@ -93,23 +94,28 @@ struct FieldT<qm31> {
     }
 };
 
+// Warp-level Montgomery batch inverse: each warp owns 32 x BI_PER_THREAD elements,
+// lane l holding elements base + i*32 + l (coalesced loads and stores). Prefix
+// products in registers, inclusive scans of the lane products in both directions
+// with shuffles, and one field inversion of the warp product per warp (computed
+// redundantly by every lane, so there is no barrier and no shared memory).
 template <typename F>
 __global__ void __launch_bounds__(BI_THREADS) batch_inverse_kernel(const F *__restrict__ src, F *__restrict__ dst,
                                                                     uint64_t n) {
     using T = FieldT<F>;
-    __shared__ F warp_pre[BI_THREADS / 32], warp_suf[BI_THREADS / 32];
-    __shared__ F block_inv;
-    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    const uint64_t base = (uint64_t)blockIdx.x * (BI_THREADS * BI_PER_THREAD) + (uint64_t)tid * BI_PER_THREAD;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp_global = ((uint64_t)blockIdx.x * BI_THREADS + threadIdx.x) >> 5;
+    const uint64_t base = warp_global * (32 * BI_PER_THREAD) + lane;
     F v[BI_PER_THREAD], pre[BI_PER_THREAD];
     F run = T::one();
 #pragma unroll
     for (int i = 0; i < BI_PER_THREAD; i++) {
-        v[i] = (base + i < n) ? src[base + i] : T::one();
+        const uint64_t idx = base + (uint64_t)i * 32;
+        v[i] = (idx < n) ? src[idx] : T::one();
         run = T::mul(run, v[i]);
         pre[i] = run;
     }
-    // Inclusive warp scans of thread totals, forward and backward.
+    // Inclusive scans of lane products, forward (prefix) and backward (suffix).
     F inc = run, suf = run;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -118,31 +124,17 @@ __global__ void __launch_bounds__(BI_THREADS) batch_inverse_kernel(const F *__re
         if (lane >= (uint32_t)d) inc = T::mul(inc, u);
         if (lane + d < 32u) suf = T::mul(suf, w);
     }
-    if (lane == 31) warp_pre[warp] = inc;
-    if (lane == 0) warp_suf[warp] = suf;
-    __syncthreads();
-    // Products of whole warps before / after this warp.
-    F before_w = T::one(), after_w = T::one();
-    for (uint32_t w = 0; w < BI_THREADS / 32; w++) {
-        if (w < warp) before_w = T::mul(before_w, warp_pre[w]);
-        if (w > warp) after_w = T::mul(after_w, warp_suf[w]);
-    }
-    if (tid == 0) {
-        F total = T::one();
-        for (uint32_t w = 0; w < BI_THREADS / 32; w++) total = T::mul(total, warp_pre[w]);
-        block_inv = T::inv(total);
-    }
-    // Exclusive products within the warp.
+    const F total = T::shfl_down(inc, 31 - lane);  // lane 31's inclusive prefix, broadcast via shuffles
     F ex_pre = T::shfl_up(inc, 1), ex_suf = T::shfl_down(suf, 1);
     if (lane == 0) ex_pre = T::one();
     if (lane == 31) ex_suf = T::one();
-    __syncthreads();
-    // inverse of this thread's product = block_inv * (everything before) * (everything after)
-    F r = T::mul(T::mul(block_inv, T::mul(before_w, ex_pre)), T::mul(ex_suf, after_w));
+    // inverse of this lane's product = inv(total) * (product before) * (product after)
+    F r = T::mul(T::inv(total), T::mul(ex_pre, ex_suf));
 #pragma unroll
     for (int i = BI_PER_THREAD - 1; i >= 0; i--) {
         F inv_i = i > 0 ? T::mul(r, pre[i - 1]) : r;
-        if (base + i < n) dst[base + i] = inv_i;
+        const uint64_t idx = base + (uint64_t)i * 32;
+        if (idx < n) dst[idx] = inv_i;
         r = T::mul(r, v[i]);
     }
 }

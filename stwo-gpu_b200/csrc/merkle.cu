@@ -21,14 +21,23 @@ __device__ __forceinline__ uint32_t rotr(uint32_t x, uint32_t c) { return __funn
 __device__ constexpr uint32_t IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
                             0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
 
+// c + d as an integer multiply-add by a runtime 1: it issues to the FMA pipe,
+// which the rotate/xor/add-heavy compression otherwise leaves idle while the ALU
+// pipe saturates.
+__device__ __forceinline__ uint32_t add_on_fma(uint32_t c, uint32_t d, uint32_t one) {
+    uint32_t r;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(d), "r"(one), "r"(c));
+    return r;
+}
+
 #define STWO_G(a, b, c, d, x, y)    \
     a = a + b + (x);                \
     d = rotr(d ^ a, 16);            \
-    c = c + d;                      \
+    c = add_on_fma(c, d, one);      \
     b = rotr(b ^ c, 12);            \
     a = a + b + (y);                \
     d = rotr(d ^ a, 8);             \
-    c = c + d;                      \
+    c = add_on_fma(c, d, one);      \
     b = rotr(b ^ c, 7);
 
 // One BLAKE2s round with message permutation s0..s15 (RFC 7693 SIGMA rows).
@@ -42,7 +51,7 @@ __device__ constexpr uint32_t IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0x
       STWO_G(v2, v7, v8, v13, m[s12], m[s13])                                          \
       STWO_G(v3, v4, v9, v14, m[s14], m[s15]) }
 
-__device__ __forceinline__ void compress(uint32_t h[8], const uint32_t m[16]) {
+__device__ __forceinline__ void compress(uint32_t h[8], const uint32_t m[16], uint32_t one) {
     uint32_t v0 = h[0], v1 = h[1], v2 = h[2], v3 = h[3], v4 = h[4], v5 = h[5], v6 = h[6], v7 = h[7];
     uint32_t v8 = IV[0], v9 = IV[1], v10 = IV[2], v11 = IV[3], v12 = IV[4], v13 = IV[5], v14 = IV[6], v15 = IV[7];
     STWO_ROUND(0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15)
@@ -75,7 +84,7 @@ template <bool COLS_ON_DEVICE>
 __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, const uint4 *__restrict__ prev,
                                                            const __grid_constant__ MerkleCols cols,
                                                            const uint32_t *const *__restrict__ dev_cols,
-                                                           uint32_t n_cols, uint4 *__restrict__ out) {
+                                                           uint32_t n_cols, uint4 *__restrict__ out, uint32_t one) {
     const uint64_t n = 1ull << log_size;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -87,7 +96,7 @@ __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, co
                 uint4 v = __ldg(p + q);
                 m[4 * q] = v.x; m[4 * q + 1] = v.y; m[4 * q + 2] = v.z; m[4 * q + 3] = v.w;
             }
-            compress(h, m);
+            compress(h, m, one);
         }
         for (uint32_t c0 = 0; c0 < n_cols; c0 += 16) {
 #pragma unroll
@@ -97,7 +106,7 @@ __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, co
                 if (cj < n_cols) col = COLS_ON_DEVICE ? dev_cols[cj] : cols.c[cj];
                 m[j] = col ? __ldg(col + i) : 0u;
             }
-            compress(h, m);
+            compress(h, m, one);
         }
         out[2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
         out[2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
@@ -122,10 +131,10 @@ int merkle_layer_async(uint32_t log_size, const uint32_t *prev, const uint32_t *
     if (blocks > cap) blocks = cap;
     if (cols_on_device)
         merkle_layer_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(log_size, reinterpret_cast<const uint4 *>(prev), mc,
-                                                                    cols, n_cols, reinterpret_cast<uint4 *>(out));
+                                                                    cols, n_cols, reinterpret_cast<uint4 *>(out), 1u);
     else
         merkle_layer_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(log_size, reinterpret_cast<const uint4 *>(prev), mc,
-                                                                     nullptr, n_cols, reinterpret_cast<uint4 *>(out));
+                                                                     nullptr, n_cols, reinterpret_cast<uint4 *>(out), 1u);
     STWO_LAUNCH_CHECK("merkle_layer_kernel");
     return STWO_OK;
 }
