@@ -148,6 +148,8 @@ void evaluate_wide_fibonacci_constraint_quotients_on_domain(
  * report failures only through this record. */
 const char *stwo_last_error(void);
 void stwo_clear_last_error(void);
+/* Number of kernel launches the library has made in this process (all threads). */
+uint64_t stwo_kernel_launches(void);
 /* Waits for all work on `stream`; returns STWO_ERR_CUDA if any of it failed. */
 int stwo_stream_synchronize(void *stream);
 
@@ -232,6 +234,88 @@ int stwo_accumulate_quotients(uint32_t half_coset_initial_index, uint32_t half_c
 int stwo_wide_fib_composition(const uint32_t *const *trace, uint32_t n_columns, uint32_t ext_log_size,
                               const stwo_qm31 *coeff_powers, const uint32_t *den_inv, uint32_t *const *out4,
                               void *stream);
+
+/* =====================================================================
+ * Tier 3: the wide-Fibonacci STARK prover and the proof server. The reference has
+ * no C entry point for these: its prover is stwo's Rust prove() driving CudaBackend
+ * (stwo_gpu_backend/src/examples/wide_fibonacci.rs:205-250).
+ * ===================================================================== */
+
+/* One wide-Fibonacci proof: the trace has 2^log_n_rows rows of n_columns columns
+ * (row r: a0[r], a1[r], then a_{j+2} = a_j^2 + a_{j+1}^2), proved with
+ * PcsConfig{pow_bits, FriConfig{log_last_layer_degree_bound = 0, log_blowup, n_queries}}
+ * and a Blake2s channel starting from the zero digest. Limits: 3 <= n_columns <= 1024,
+ * 1 <= log_blowup <= 4, 2 <= log_n_rows, log_n_rows + 1 + log_blowup <= 27,
+ * 1 <= n_queries <= 1024, pow_bits <= 40. */
+typedef struct {
+    uint32_t log_n_rows;
+    uint32_t n_columns;
+    uint32_t log_blowup;
+    uint32_t n_queries;
+    uint32_t pow_bits;
+} stwo_wide_fib_job;
+
+/* Per-phase host wall-clock times of one proof (each phase ends on a device
+ * synchronisation, so device work is included), and what the proof used. */
+typedef struct {
+    double trace_ms;        /* trace generation, interpolation, evaluation, tree */
+    double composition_ms;  /* composition polynomial and its tree */
+    double oods_ms;         /* out-of-domain sampling and the constraint check */
+    double fri_ms;          /* DEEP quotients and the FRI commitment */
+    double decommit_ms;     /* proof of work, queries, decommitments, serialisation */
+    double total_ms;
+    uint64_t device_bytes;    /* device memory the proof allocated */
+    uint64_t kernel_launches; /* kernels it launched */
+    uint64_t proof_bytes;
+} stwo_prove_stats;
+
+/* Upper bound of the device bytes stwo_wide_fib_prove allocates for `job` (0 if the
+ * job is unsupported); with_own_twiddles: the call builds its own twiddle tree. */
+uint64_t stwo_wide_fib_prove_device_bytes(const stwo_wide_fib_job *job, int with_own_twiddles);
+
+/* Proves one job on `stream`. a0, a1: the first two trace columns, 2^log_n_rows M31
+ * values each, in host or device memory. twiddles/itwiddles: NULL, or a tree of
+ * tree_size entries for the half coset of a canonic domain of log size at least
+ * log_n_rows + 1 + log_blowup (stwo_precompute_twiddles). On success *proof is a
+ * malloc'd buffer of *proof_len bytes (free with stwo_free_proof): the
+ * CommitmentSchemeProof fields in declaration order, little endian, vectors prefixed
+ * by a u64 length. stats may be NULL. Blocks the calling thread until the proof is
+ * done; calls on distinct streams from distinct threads run concurrently. */
+int stwo_wide_fib_prove(const stwo_wide_fib_job *job, const uint32_t *a0, const uint32_t *a1,
+                        const uint32_t *twiddles, const uint32_t *itwiddles, uint64_t tree_size, uint8_t **proof,
+                        uint64_t *proof_len, stwo_prove_stats *stats, void *stream);
+void stwo_free_proof(uint8_t *proof);
+
+/* Proof server on the current device: n_workers jobs in flight at most, admitted in
+ * arrival order while their device bound fits device_budget_bytes (smaller later jobs
+ * pass a job that does not fit), each on its own stream; one shared twiddle tree for
+ * domains up to log size max_domain_log. */
+typedef struct stwo_prover_server stwo_prover_server;
+
+typedef struct {
+    uint64_t job_id;
+    int status;          /* STWO_OK or the prover's error status */
+    char error[256];     /* the error message when status != STWO_OK */
+    uint8_t *proof;      /* malloc'd proof bytes (free with stwo_free_proof), NULL on error */
+    uint64_t proof_len;
+    double submit_ms, start_ms, done_ms; /* stwo_server_now_ms() clock */
+    stwo_prove_stats stats;
+} stwo_server_result;
+
+stwo_prover_server *stwo_server_create(uint32_t n_workers, uint64_t device_budget_bytes, uint32_t max_domain_log);
+/* Queues a job (a0, a1 are host arrays, copied before the call returns). Fails when
+ * the job is unsupported or can never fit the budget. */
+int stwo_server_submit(stwo_prover_server *server, uint64_t job_id, const stwo_wide_fib_job *job, const uint32_t *a0,
+                       const uint32_t *a1);
+/* Moves up to max_results finished jobs into out and returns their number. Waits up to
+ * timeout_ms for one (negative: until one finishes or nothing is queued or running). */
+uint32_t stwo_server_poll(stwo_prover_server *server, stwo_server_result *out, uint32_t max_results,
+                          int32_t timeout_ms);
+void stwo_server_stats(stwo_prover_server *server, uint32_t *pending, uint32_t *running,
+                       uint64_t *device_bytes_in_use);
+double stwo_server_now_ms(void);
+/* Drops queued jobs, waits for running ones, frees everything (including unpolled proofs). */
+void stwo_server_destroy(stwo_prover_server *server);
 
 #ifdef __cplusplus
 }

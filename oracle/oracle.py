@@ -40,6 +40,11 @@ class Coset(C.Structure):
     _fields_ = [("initial_index", C.c_uint32), ("step_size", C.c_uint32), ("log_size", C.c_uint32)]
 
 
+class WideFibJob(C.Structure):
+    _fields_ = [("log_n_rows", C.c_uint32), ("n_columns", C.c_uint32), ("log_blowup", C.c_uint32),
+                ("n_queries", C.c_uint32), ("pow_bits", C.c_uint32)]
+
+
 def build():
     import subprocess
     subprocess.check_call(["make", "-s", "-C", HERE])
@@ -75,6 +80,9 @@ def lib():
         L.or_evaluate.argtypes = [Coset, _u32p, _u32p, C.c_size_t]
         L.or_evaluate_direct.argtypes = [Coset, _u32p, C.c_uint32, _u32p]
         L.or_precompute_twiddles.argtypes = [Coset, _u32p, _u32p]
+        L.or_wide_fib_prove.argtypes = [C.POINTER(WideFibJob), C.c_void_p, C.c_void_p,
+                                        C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t)]
+        L.or_free.argtypes = [C.c_void_p]
         L.or_eval_at_point.restype = QM31
         L.or_eval_at_point.argtypes = [_u32p, C.c_uint32, SPoint]
         L.or_line_eval_at_point.restype = QM31
@@ -337,3 +345,20 @@ def qm31_inv(x):
 
 def qm31_pow(x, e):
     return qm31_tuple(lib().or_qm31_pow(qm31(x), e))
+
+
+def wide_fib_prove(log_n_rows, n_columns, a0, a1, log_blowup=1, n_queries=3, pow_bits=5):
+    """The oracle prover's proof bytes (stwo_oracle_prover.c) and its status (0, or
+    -2 / -3 when the OODS / last-layer check failed)."""
+    a0 = np.ascontiguousarray(a0, dtype=np.uint32)
+    a1 = np.ascontiguousarray(a1, dtype=np.uint32)
+    out = C.POINTER(C.c_uint8)()
+    ln = C.c_size_t()
+    job = WideFibJob(log_n_rows, n_columns, log_blowup, n_queries, pow_bits)
+    rc = lib().or_wide_fib_prove(C.byref(job), a0.ctypes.data, a1.ctypes.data, C.byref(out), C.byref(ln))
+    if rc == -1:
+        raise ValueError("unsupported wide-Fibonacci job")
+    try:
+        return C.string_at(out, ln.value), rc
+    finally:
+        lib().or_free(out)

@@ -90,6 +90,15 @@ void or_wide_fib_composition(const m31_t *const *trace_evals, size_t n_columns, 
                              const qm31_t *coeff_powers, const m31_t *den_inv,
                              m31_t *const out[4]);
 
+/* ---- wide-Fibonacci prover (stwo_oracle_prover.c) ---- */
+typedef struct { uint32_t log_n_rows, n_columns, log_blowup, n_queries, pow_bits; } or_wide_fib_job;
+/* Proof bytes in *proof (free with or_free). Returns 0, or -1 for unsupported
+ * parameters, -2 / -3 when the OODS check / the last-layer degree check fails (the
+ * bytes are still produced). */
+int or_wide_fib_prove(const or_wide_fib_job *job, const uint32_t *a0, const uint32_t *a1, uint8_t **proof,
+                      size_t *proof_len);
+void or_free(void *p);
+
 /* ---- threading for the timed CPU baseline ---- */
 void or_set_threads(int n);
 int  or_get_threads(void);

@@ -2,7 +2,8 @@
 
 The compute lives in libstwo_b200.so (CUDA for sm_100a behind the C ABI of
 include/stwo_b200.h); this package is the host-side mirror of the reference's
-backend traits (backend.py) and the ctypes binding (_lib.py).
+backend traits (backend.py), the wide-Fibonacci prover and proof server
+(prover.py), a plain-Python verifier (verifier.py) and the ctypes binding (_lib.py).
 """
 from . import _lib  # noqa: F401
 from .backend import (  # noqa: F401
@@ -10,3 +11,5 @@ from .backend import (  # noqa: F401
     Coset, CudaBackend, LineDomain, LineEvaluation, SecureColumnByCoords, SecureEvaluation, SecureFieldVec,
     TwiddleTree, index_to_point,
 )
+from .prover import ProofServer, WideFibJob, kernel_launches, prove_wide_fib, wide_fib_inputs  # noqa: F401
+from .verifier import VerificationError, verify  # noqa: F401

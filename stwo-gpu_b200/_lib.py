@@ -32,6 +32,29 @@ class SPoint(C.Structure):
     _fields_ = [("x", QM31), ("y", QM31)]
 
 
+class WideFibJob(C.Structure):
+    """stwo_wide_fib_job: one wide-Fibonacci proof's parameters."""
+    _fields_ = [("log_n_rows", u32), ("n_columns", u32), ("log_blowup", u32), ("n_queries", u32),
+                ("pow_bits", u32)]
+
+
+class ProveStats(C.Structure):
+    """stwo_prove_stats: per-phase wall-clock times and resources of one proof."""
+    _fields_ = [("trace_ms", C.c_double), ("composition_ms", C.c_double), ("oods_ms", C.c_double),
+                ("fri_ms", C.c_double), ("decommit_ms", C.c_double), ("total_ms", C.c_double),
+                ("device_bytes", u64), ("kernel_launches", u64), ("proof_bytes", u64)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class ServerResult(C.Structure):
+    """stwo_server_result: one finished job of the proof server."""
+    _fields_ = [("job_id", u64), ("status", C.c_int), ("error", C.c_char * 256), ("proof", C.POINTER(C.c_uint8)),
+                ("proof_len", u64), ("submit_ms", C.c_double), ("start_ms", C.c_double), ("done_ms", C.c_double),
+                ("stats", ProveStats)]
+
+
 class StwoError(RuntimeError):
     pass
 
@@ -91,6 +114,18 @@ SIGNATURES = [
     ("stwo_merkle_commit_layer", C.c_int, [u32, vp, vp, u32, vp, vp]),
     ("stwo_accumulate_quotients", C.c_int, [u32, u32, u32, vp, u32, QM31, vp, vp, vp, vp, u32, vp, vp]),
     ("stwo_wide_fib_composition", C.c_int, [vp, u32, u32, vp, vp, vp, vp]),
+    ("stwo_kernel_launches", u64, []),
+    # prover tier
+    ("stwo_wide_fib_prove_device_bytes", u64, [C.POINTER(WideFibJob), C.c_int]),
+    ("stwo_wide_fib_prove", C.c_int, [C.POINTER(WideFibJob), vp, vp, vp, vp, u64, C.POINTER(C.POINTER(C.c_uint8)),
+                                      C.POINTER(u64), C.POINTER(ProveStats), vp]),
+    ("stwo_free_proof", None, [vp]),
+    ("stwo_server_create", vp, [u32, u64, u32]),
+    ("stwo_server_submit", C.c_int, [vp, u64, C.POINTER(WideFibJob), vp, vp]),
+    ("stwo_server_poll", u32, [vp, C.POINTER(ServerResult), u32, C.c_int32]),
+    ("stwo_server_stats", None, [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u64)]),
+    ("stwo_server_now_ms", C.c_double, []),
+    ("stwo_server_destroy", None, [vp]),
 ]
 
 _lib = None

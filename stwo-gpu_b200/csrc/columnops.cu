@@ -14,6 +14,10 @@
 // shuffles, one field inversion of the warp product (computed by every lane, so no
 // barrier is needed) and back-substitution: 3 multiplications per element and one
 // inversion per 256 elements.
+#include <map>
+#include <mutex>
+#include <vector>
+
 #include "common.cuh"
 
 namespace stwo {
@@ -153,25 +157,33 @@ int bit_reverse_async(uint32_t *col, uint64_t n, uint32_t words, cudaStream_t st
         STWO_LAUNCH_CHECK("bitrev_simple_kernel");
         return STWO_OK;
     }
-    // Middle indices b with b <= rev(b): built on the host once per size and cached.
-    static uint32_t *pairs_dev[32] = {nullptr};
-    static uint32_t pairs_cnt[32] = {0};
-    uint32_t mb = L - 10;
-    if (!pairs_dev[L]) {
-        uint32_t m = 1u << mb, cnt = 0;
-        uint32_t *h = (uint32_t *)malloc(sizeof(uint32_t) * m);
-        for (uint32_t b = 0; b < m; b++)
-            if (b <= bit_reverse_bits(b, mb)) h[cnt++] = b;
-        uint32_t *d = nullptr;
-        cudaError_t e = cudaMalloc(&d, sizeof(uint32_t) * cnt);
-        if (e == cudaSuccess) e = cudaMemcpy(d, h, sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice);
-        free(h);
-        if (e != cudaSuccess) return set_error(STWO_ERR_CUDA, "bit reverse table: %s", cudaGetErrorString(e));
-        pairs_dev[L] = d;
-        pairs_cnt[L] = cnt;
+    // Middle indices b with b <= rev(b): built on the host once per device and size, and
+    // cached (the cache is shared by all threads and streams, under a lock).
+    static std::mutex mu;
+    static std::map<std::pair<int, uint32_t>, std::pair<uint32_t *, uint32_t>> cache;
+    int dev = 0;
+    STWO_CUDA_TRY(cudaGetDevice(&dev));
+    uint32_t *pairs = nullptr, cnt = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find({dev, L});
+        if (it == cache.end()) {
+            uint32_t mb = L - 10, m = 1u << mb;
+            std::vector<uint32_t> h;
+            h.reserve(m);
+            for (uint32_t b = 0; b < m; b++)
+                if (b <= bit_reverse_bits(b, mb)) h.push_back(b);
+            uint32_t *d = nullptr;
+            cudaError_t e = cudaMalloc(&d, sizeof(uint32_t) * h.size());
+            if (e == cudaSuccess) e = cudaMemcpy(d, h.data(), sizeof(uint32_t) * h.size(), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return set_error(STWO_ERR_CUDA, "bit reverse table: %s", cudaGetErrorString(e));
+            it = cache.emplace(std::make_pair(dev, L), std::make_pair(d, (uint32_t)h.size())).first;
+        }
+        pairs = it->second.first;
+        cnt = it->second.second;
     }
-    if (words == 1) bitrev_tiled_kernel<1><<<pairs_cnt[L], 256, 0, st>>>(col, L, pairs_dev[L]);
-    else bitrev_tiled_kernel<4><<<pairs_cnt[L], 256, 0, st>>>(col, L, pairs_dev[L]);
+    if (words == 1) bitrev_tiled_kernel<1><<<cnt, 256, 0, st>>>(col, L, pairs);
+    else bitrev_tiled_kernel<4><<<cnt, 256, 0, st>>>(col, L, pairs);
     STWO_LAUNCH_CHECK("bitrev_tiled_kernel");
     return STWO_OK;
 }

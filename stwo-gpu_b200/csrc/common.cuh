@@ -1,6 +1,7 @@
 // Shared plumbing for the C ABI: status codes, the per-thread last-error record,
 // launch checks and small device helpers.
 #pragma once
+#include <atomic>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -16,6 +17,14 @@ namespace stwo {
 int set_error(int status, const char *fmt, ...);
 void clear_error();
 
+// Counts of kernel launches made by the library: process-wide and per host thread.
+extern std::atomic<uint64_t> g_kernel_launches;
+extern thread_local uint64_t t_kernel_launches;
+inline void count_launch() {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    t_kernel_launches++;
+}
+
 #define STWO_CUDA_TRY(expr)                                                               \
     do {                                                                                  \
         cudaError_t _e = (expr);                                                          \
@@ -24,8 +33,10 @@ void clear_error();
                                      cudaGetErrorString(_e), __FILE__, __LINE__);         \
     } while (0)
 
+// Follows every kernel launch: counts it (stwo_kernel_launches) and checks it.
 #define STWO_LAUNCH_CHECK(name)                                                           \
     do {                                                                                  \
+        ::stwo::count_launch();                                                           \
         cudaError_t _e = cudaGetLastError();                                              \
         if (_e != cudaSuccess)                                                            \
             return ::stwo::set_error(STWO_ERR_CUDA, "launch of %s failed: %s", name,      \
@@ -48,6 +59,39 @@ constexpr int NUM_SMS_B200 = 148;
 
 // Number of SMs of the current device (cached per process; the library drives one device).
 int device_sm_count();
+
+// Runs f() (a status-returning setup step such as cudaFuncSetAttribute) once per device:
+// bit d of `done` records device d. Concurrent first calls may both run f, so f must be
+// idempotent.
+template <class F>
+int once_per_device(std::atomic<uint64_t> &done, F f) {
+    int dev = 0;
+    STWO_CUDA_TRY(cudaGetDevice(&dev));
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return STWO_OK;
+    int rc = f();
+    if (rc == STWO_OK) done.fetch_or(bit, std::memory_order_release);
+    return rc;
+}
+
+// The library's stream-ordered memory pool on the current device, created on first use
+// with an unbounded release threshold: memory a job frees is reused by the next job
+// instead of going back to the driver at every synchronisation.
+int library_pool(cudaMemPool_t *pool);
+// cudaMallocFromPoolAsync from the library pool (free with cudaFreeAsync).
+int pool_alloc(void **p, size_t bytes, cudaStream_t st);
+
+// Waits for all work on `st`. A thread that sets t_blocking_wait yields its CPU core
+// while it waits (a blocking-sync event) instead of spinning; the proof server's
+// workers do, so many in-flight jobs do not compete for host cores.
+extern thread_local bool t_blocking_wait;
+int wait_stream(cudaStream_t st);
+
+// Pinned host memory of at least `bytes`, owned by the calling thread and reused by its
+// next call: the staging area of the small device<->host copies (roots, sampled values,
+// decommitment words), which from pageable memory serialise on the driver's staging
+// buffer across threads. Valid until the thread's next host_stage call.
+int host_stage(size_t bytes, void **out);
 
 // Stream handle conversion for the C ABI.
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }

@@ -465,12 +465,13 @@ int launchT_e(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
     constexpr int NR = RoundT<G, INV, 0, E>::NR;
     const size_t smem = NR > 1 ? (sizeof(uint32_t) << TT) : 0;
     auto kern = fftT_kernel<G, C, INV, E>;
-    static bool attr_set = false;
-    if (!attr_set) {
+    static std::atomic<uint64_t> attr_set{0};
+    int rc = once_per_device(attr_set, [&] {
         STWO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)(sizeof(uint32_t) << TT)));
-        attr_set = true;
-    }
+        return (int)STWO_OK;
+    });
+    if (rc) return rc;
     const uint64_t tiles = (uint64_t)n_cols << (p.N - C - G);
     const uint64_t per_cta = 1ull << (TT - C - G);
     STWO_REQUIRE(tiles % per_cta == 0, STWO_ERR_UNSUPPORTED_SIZE, "fft tile packing");
@@ -575,12 +576,13 @@ int launch_pass_t(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
     const uint32_t threads = 1u << (p.tile_log - LOG_E);
     const size_t smem = sizeof(uint32_t) << p.tile_log;
     auto kern = fft_pass_kernel<LOG_E, INV>;
-    static bool attr_set = false;
-    if (!attr_set) {
+    static std::atomic<uint64_t> attr_set{0};
+    int rc = once_per_device(attr_set, [&] {
         STWO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)(sizeof(uint32_t) << MAX_TILE_LOG)));
-        attr_set = true;
-    }
+        return (int)STWO_OK;
+    });
+    if (rc) return rc;
     const uint64_t blocks = (uint64_t)n_cols << (p.N - p.tile_log);
     STWO_REQUIRE(blocks < (1ull << 31), STWO_ERR_UNSUPPORTED_SIZE, "fft grid too large");
     kern<<<(unsigned)blocks, threads, smem, st>>>(p);
@@ -645,8 +647,13 @@ int small_circle_point(const uint32_t *suffix_end, uint64_t avail, uint32_t N, b
     STWO_REQUIRE(avail >= 4, STWO_ERR_UNSUPPORTED_SIZE,
                  "a 2^%u-point circle domain needs a twiddle tree that also covers the 8-point domain", N);
     uint32_t l8[2];
-    STWO_CUDA_TRY(cudaMemcpyAsync(l8, suffix_end - 4, sizeof(l8), cudaMemcpyDeviceToHost, st));
-    STWO_CUDA_TRY(cudaStreamSynchronize(st));
+    void *stage = nullptr;
+    int wrc = host_stage(sizeof(l8), &stage);
+    if (wrc) return wrc;
+    STWO_CUDA_TRY(cudaMemcpyAsync(stage, suffix_end - 4, sizeof(l8), cudaMemcpyDeviceToHost, st));
+    wrc = wait_stream(st);
+    if (wrc) return wrc;
+    memcpy(l8, stage, sizeof(l8));
     uint32_t x8 = inv ? m31_inv(l8[0]) : l8[0];
     uint32_t y8 = inv ? m31_inv(l8[1]) : l8[1];
     uint32_t x = m31_sub(m31_add(m31_sqr(x8), m31_sqr(x8)), 1), y = m31_mul(m31_add(x8, x8), y8);

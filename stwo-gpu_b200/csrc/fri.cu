@@ -80,7 +80,12 @@ __global__ void fold_kernel(const __grid_constant__ Cols4 src, const __grid_cons
 // point, which the tree does not hold at those sizes (see small_circle_point).
 template <bool CIRCLE>
 __global__ void fold_small_kernel(const __grid_constant__ Cols4 src, const __grid_constant__ MutCols4 dst,
-                                  uint32_t n_out, uint32_t t0, uint32_t t1, qm31 alpha, qm31 alpha_sq) {
+                                  uint32_t n_out, uint32_t t0, uint32_t t1, const uint32_t *tw, qm31 alpha,
+                                  qm31 alpha_sq) {
+    if (tw) {  // line fold: the inverse x twiddles are read from the tree
+        t0 = tw[0];
+        t1 = n_out > 1 ? tw[1] : 0u;
+    }
     for (uint32_t i = 0; i < n_out; i++) {
         qm31 a = {{src.c[0][2 * i], src.c[1][2 * i]}, {src.c[2][2 * i], src.c[3][2 * i]}};
         qm31 b = {{src.c[0][2 * i + 1], src.c[1][2 * i + 1]}, {src.c[2][2 * i + 1], src.c[3][2 * i + 1]}};
@@ -118,12 +123,9 @@ int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const
             if (rc) return rc;
             t[0] = iy;
             t[1] = m31_neg(iy);
-        } else {
-            STWO_CUDA_TRY(cudaMemcpyAsync(t, tw, sizeof(uint32_t) * n_out, cudaMemcpyDeviceToHost, st));
-            STWO_CUDA_TRY(cudaStreamSynchronize(st));
         }
-        if (circle) fold_small_kernel<true><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, t[0], t[1], alpha, a2);
-        else fold_small_kernel<false><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, t[0], t[1], alpha, a2);
+        if (circle) fold_small_kernel<true><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, t[0], t[1], nullptr, alpha, a2);
+        else fold_small_kernel<false><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, 0u, 0u, tw, alpha, a2);
         STWO_LAUNCH_CHECK("fold_small_kernel");
         return STWO_OK;
     }

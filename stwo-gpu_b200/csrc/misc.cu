@@ -42,12 +42,10 @@ struct WideFibParams {
     const uint32_t *trace[WF_MAX_COLS];
     uint32_t *out[4];
     const uint32_t *den_inv;
-    const qm31 *powers_dev;  // device powers (reference ABI) or null
+    const qm31 *powers_dev;  // device powers
     uint32_t n_cols;
     uint32_t log_size;
 };
-
-__constant__ qm31 c_wf_powers2[WF_MAX_COLS];  // doubled coordinates, host-supplied powers
 
 __device__ __forceinline__ uint32_t mul_lazy_wf(uint32_t a, uint32_t b2) {
     uint64_t w = (uint64_t)a * b2;
@@ -59,7 +57,9 @@ __device__ __forceinline__ uint32_t reduce64_wf(uint64_t x) {
     return reduce_once((uint32_t)s);
 }
 
-template <bool POWERS_ON_DEVICE>
+// Powers on the device: plain QM31 (the reference ABI) or, when DOUBLED, with every
+// coordinate already doubled for m31_mul2.
+template <bool DOUBLED>
 __global__ void __launch_bounds__(256) wide_fib_kernel(const __grid_constant__ WideFibParams p) {
     const uint64_t n = 1ull << p.log_size;
     const uint64_t quads = (n + 3) / 4;
@@ -82,13 +82,8 @@ __global__ void __launch_bounds__(256) wide_fib_kernel(const __grid_constant__ W
         for (uint32_t i = 0; i + 2 < p.n_cols; i++) {
             uint32_t c2[4];
             load(i + 2, c2);
-            qm31 w2;
-            if (POWERS_ON_DEVICE) {
-                qm31 w = p.powers_dev[p.n_cols - 3 - i];
-                w2 = {{w.a.a << 1, w.a.b << 1}, {w.b.a << 1, w.b.b << 1}};
-            } else {
-                w2 = c_wf_powers2[p.n_cols - 3 - i];
-            }
+            qm31 w2 = p.powers_dev[p.n_cols - 3 - i];
+            if (!DOUBLED) w2 = {{w2.a.a << 1, w2.a.b << 1}, {w2.b.a << 1, w2.b.b << 1}};
 #pragma unroll
             for (int r = 0; r < 4; r++) {
                 uint32_t cons = m31_sub(m31_add(s0[r], s1[r]), c2[r]);
@@ -158,18 +153,31 @@ int wide_fib_async(const uint32_t *const *trace, uint32_t n_cols, uint32_t log_s
         return STWO_OK;
     }
     if (powers_dev) {
-        wide_fib_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(*p);
-    } else {
-        std::unique_ptr<qm31[]> w2(new qm31[n_cols]);
-        for (uint32_t i = 0; i + 2 < n_cols; i++) {
-            stwo_qm31 v = powers_host[i];
-            w2[i] = {{v.a << 1, v.b << 1}, {v.c << 1, v.d << 1}};
-        }
-        STWO_CUDA_TRY(cudaMemcpyToSymbolAsync(c_wf_powers2, w2.get(), sizeof(qm31) * (n_cols - 2), 0,
-                                              cudaMemcpyHostToDevice, st));
         wide_fib_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(*p);
+        STWO_LAUNCH_CHECK("wide_fib_kernel");
+        return STWO_OK;
     }
-    STWO_LAUNCH_CHECK("wide_fib_kernel");
+    // Host powers: staged, doubled, into a stream-ordered buffer private to this call,
+    // so concurrent calls on other streams never see each other's powers.
+    std::unique_ptr<qm31[]> w2(new qm31[n_cols - 2]);
+    for (uint32_t i = 0; i + 2 < n_cols; i++) {
+        stwo_qm31 v = powers_host[i];
+        w2[i] = {{v.a << 1, v.b << 1}, {v.c << 1, v.d << 1}};
+    }
+    void *buf = nullptr;
+    {
+        int arc = pool_alloc(&buf, sizeof(qm31) * (n_cols - 2), st);
+        if (arc) return arc;
+    }
+    cudaError_t e = cudaMemcpyAsync(buf, w2.get(), sizeof(qm31) * (n_cols - 2), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        p->powers_dev = static_cast<const qm31 *>(buf);
+        wide_fib_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(*p);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(buf, st);
+    if (e != cudaSuccess) return set_error(STWO_ERR_CUDA, "wide_fib_kernel: %s", cudaGetErrorString(e));
     return STWO_OK;
 }
 

@@ -60,7 +60,8 @@ int precompute_tree(cpoint initial, cpoint step, uint32_t m, uint32_t *tw, uint3
     uint32_t *dst = tw;
     uint32_t *tmp = nullptr;
     if (!dst) {
-        STWO_CUDA_TRY(cudaMallocAsync((void **)&tmp, size * 4, st));
+        int arc = pool_alloc((void **)&tmp, size * 4, st);
+        if (arc) return arc;
         dst = tmp;
     }
     uint32_t blocks = (uint32_t)std::min<uint64_t>((size + 255) / 256, (uint64_t)device_sm_count() * 16);

@@ -39,15 +39,14 @@ struct QuotParams {
     uint32_t half_init, half_step;        // half coset indices
     uint32_t log_size;                    // domain log size
     uint32_t *out[4];
+    cpoint gen_pows[31];                  // GEN^(2^b), so the kernel shares no state between calls
 };
 
-__constant__ cpoint c_gen_pows[31];  // GEN^(2^b)
-
-__device__ __forceinline__ cpoint point_at_index(uint32_t idx) {
+__device__ __forceinline__ cpoint point_at_index(const cpoint *gen_pows, uint32_t idx) {
     cpoint r = {1, 0};
 #pragma unroll 1
     for (int b = 0; b < 31; b++)
-        if ((idx >> b) & 1u) r = point_mul(r, c_gen_pows[b]);
+        if ((idx >> b) & 1u) r = point_mul(r, gen_pows[b]);
     return r;
 }
 
@@ -70,7 +69,7 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_pairs;
          k += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t hidx = bit_reverse_bits((uint32_t)k, p.log_size - 1);
-        cpoint pt = point_at_index(p.half_init + p.half_step * hidx);
+        cpoint pt = point_at_index(p.gen_pows, p.half_init + p.half_step * hidx);
         // Denominators for both rows (y and -y), then one shared inversion.
         cm31 den[2][QUOT_MAX_BATCHES];
         cm31 prefix = {1, 0};
@@ -125,19 +124,6 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
 
 inline qm31 to_q(stwo_qm31 v) { return {{v.a, v.b}, {v.c, v.d}}; }
 
-int gen_table_ready() {
-    static bool done = false;
-    if (done) return STWO_OK;
-    cpoint t[31];
-    cpoint g = {CIRCLE_GEN_X, CIRCLE_GEN_Y};
-    for (int b = 0; b < 31; b++) {
-        t[b] = g;
-        g = point_mul(g, g);
-    }
-    STWO_CUDA_TRY(cudaMemcpyToSymbol(c_gen_pows, t, sizeof(t)));
-    done = true;
-    return STWO_OK;
-}
 
 }  // namespace
 
@@ -150,10 +136,15 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
                  QUOT_MAX_BATCHES);
     STWO_REQUIRE(cols_on_device || n_cols <= (uint32_t)QUOT_MAX_COLS, STWO_ERR_UNSUPPORTED_SIZE,
                  "at most %d columns", QUOT_MAX_COLS);
-    int rc = gen_table_ready();
-    if (rc) return rc;
     QuotParams *p = new QuotParams();
     std::unique_ptr<QuotParams> guard(p);
+    {
+        cpoint g = {CIRCLE_GEN_X, CIRCLE_GEN_Y};
+        for (int b = 0; b < 31; b++) {
+            p->gen_pows[b] = g;
+            g = point_mul(g, g);
+        }
+    }
     p->n_batches = n_batches;
     p->half_init = half_init;
     p->half_step = half_step;

@@ -23,6 +23,9 @@ int set_error(int status, const char *fmt, ...) {
 
 void clear_error() { g_last_error[0] = 0; }
 
+std::atomic<uint64_t> g_kernel_launches{0};
+thread_local uint64_t t_kernel_launches = 0;
+
 int device_sm_count() {
     static int count = 0;
     if (count == 0) {
@@ -31,6 +34,97 @@ int device_sm_count() {
             count = NUM_SMS_B200;
     }
     return count;
+}
+
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+
+struct BlockingEvent {
+    cudaEvent_t ev = nullptr;
+    int device = -1;
+    ~BlockingEvent() {
+        if (ev) cudaEventDestroy(ev);
+    }
+};
+thread_local BlockingEvent t_event;
+
+struct HostStage {
+    void *p = nullptr;
+    size_t cap = 0;
+    ~HostStage() {
+        if (p) cudaFreeHost(p);
+    }
+};
+thread_local HostStage t_stage;
+}  // namespace
+
+int host_stage(size_t bytes, void **out) {
+    if (t_stage.cap < bytes) {
+        size_t cap = 1 << 16;
+        while (cap < bytes) cap <<= 1;
+        if (t_stage.p) cudaFreeHost(t_stage.p);
+        t_stage.p = nullptr;
+        t_stage.cap = 0;
+        STWO_CUDA_TRY(cudaMallocHost(&t_stage.p, cap));
+        t_stage.cap = cap;
+    }
+    *out = t_stage.p;
+    return STWO_OK;
+}
+
+thread_local bool t_blocking_wait = false;
+
+int library_pool(cudaMemPool_t *pool) {
+    int dev = 0;
+    STWO_CUDA_TRY(cudaGetDevice(&dev));
+    STWO_REQUIRE(dev >= 0 && dev < 64, STWO_ERR_CUDA, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        STWO_CUDA_TRY(cudaMemPoolCreate(&p, &props));
+        uint64_t threshold = ~0ull;
+        STWO_CUDA_TRY(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &threshold));
+        g_pools[dev] = p;
+    }
+    *pool = g_pools[dev];
+    return STWO_OK;
+}
+
+int pool_alloc(void **p, size_t bytes, cudaStream_t st) {
+    cudaMemPool_t pool;
+    int rc = library_pool(&pool);
+    if (rc) return rc;
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return set_error(e == cudaErrorMemoryAllocation ? STWO_ERR_OUT_OF_MEMORY : STWO_ERR_CUDA,
+                         "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    return STWO_OK;
+}
+
+int wait_stream(cudaStream_t st) {
+    if (!t_blocking_wait) {
+        STWO_CUDA_TRY(cudaStreamSynchronize(st));
+        return STWO_OK;
+    }
+    int dev = 0;
+    STWO_CUDA_TRY(cudaGetDevice(&dev));
+    if (!t_event.ev || t_event.device != dev) {
+        if (t_event.ev) cudaEventDestroy(t_event.ev);
+        t_event.ev = nullptr;
+        STWO_CUDA_TRY(cudaEventCreateWithFlags(&t_event.ev, cudaEventBlockingSync | cudaEventDisableTiming));
+        t_event.device = dev;
+    }
+    STWO_CUDA_TRY(cudaEventRecord(t_event.ev, st));
+    STWO_CUDA_TRY(cudaEventSynchronize(t_event.ev));
+    return STWO_OK;
 }
 
 int sync_default_stream(int status) {
@@ -72,6 +166,8 @@ extern "C" {
 const char *stwo_last_error(void) { return g_last_error; }
 
 void stwo_clear_last_error(void) { clear_error(); }
+
+uint64_t stwo_kernel_launches(void) { return g_kernel_launches.load(std::memory_order_relaxed); }
 
 int stwo_stream_synchronize(void *stream) {
     cudaError_t e = cudaStreamSynchronize(as_stream(stream));

@@ -1,0 +1,232 @@
+// Proof server: continuous batching of wide-Fibonacci proof jobs on one GPU.
+//
+// Jobs are submitted at any time and queue in arrival order. A job is admitted when a
+// worker is free and its device-memory bound (stwo_wide_fib_prove_device_bytes) fits
+// in what the budget has left; a job that does not fit lets later, smaller jobs pass
+// (backfill), so one large job does not idle the device. Each worker is a host thread
+// with its own CUDA stream; a job keeps its trace, twiddle references, trees and FRI
+// layers on the device from the trace commitment to the last decommitment, and its
+// kernels interleave on the device with the other admitted jobs' kernels while its
+// thread waits on the channel. All jobs share one twiddle tree, built at creation for
+// the largest domain the server accepts. A job's proof bytes do not depend on what
+// else is running: each job's arithmetic is confined to its own buffers and stream.
+#include <chrono>
+#include <condition_variable>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+
+namespace stwo {
+
+int wide_fib_prove(const stwo_wide_fib_job *job, const uint32_t *a0, const uint32_t *a1, const uint32_t *tw,
+                   const uint32_t *itw, uint64_t tree_size, std::vector<uint8_t> &proof, stwo_prove_stats *stats,
+                   cudaStream_t st);
+uint64_t wide_fib_job_device_bytes(const stwo_wide_fib_job *job, bool own_twiddles);
+
+namespace {
+
+double steady_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct PendingJob {
+    uint64_t id;
+    stwo_wide_fib_job job;
+    std::vector<uint32_t> a0, a1;
+    uint64_t bytes;
+    double submit_ms;
+};
+
+}  // namespace
+}  // namespace stwo
+
+using namespace stwo;
+
+struct stwo_prover_server {
+    int device = 0;
+    uint64_t budget = 0, in_use = 0;
+    uint32_t max_domain_log = 0;
+    uint32_t *tw = nullptr, *itw = nullptr;
+    uint64_t tree_size = 0;
+    bool stopping = false;
+    bool blocking_wait = true;  // workers yield their core while waiting on the device
+    uint32_t running = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<PendingJob> pending;
+    std::deque<stwo_server_result> done;
+    std::vector<std::thread> workers;
+
+    // The first pending job (in arrival order) whose bound fits the budget's remainder.
+    bool take(PendingJob &out) {
+        for (auto it = pending.begin(); it != pending.end(); ++it) {
+            if (in_use + it->bytes <= budget) {
+                out = std::move(*it);
+                pending.erase(it);
+                in_use += out.bytes;
+                return true;
+            }
+        }
+        return false;
+    }
+
+    void worker() {
+        cudaSetDevice(device);
+        t_blocking_wait = blocking_wait;
+        cudaStream_t st = nullptr;
+        cudaError_t se = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        for (;;) {
+            PendingJob j;
+            {
+                std::unique_lock<std::mutex> lock(mu);
+                cv_work.wait(lock, [&] { return stopping || (!pending.empty() && take(j)); });
+                if (stopping && j.a0.empty()) break;
+                running++;
+            }
+            stwo_server_result r{};
+            r.job_id = j.id;
+            r.submit_ms = j.submit_ms;
+            r.start_ms = steady_ms();
+            std::vector<uint8_t> proof;
+            if (se != cudaSuccess) {
+                r.status = set_error(STWO_ERR_CUDA, "worker stream creation failed: %s", cudaGetErrorString(se));
+            } else {
+                clear_error();
+                r.status = wide_fib_prove(&j.job, j.a0.data(), j.a1.data(), tw, itw, tree_size, proof, &r.stats, st);
+            }
+            if (r.status == STWO_OK) {
+                r.proof = static_cast<uint8_t *>(malloc(proof.size()));
+                if (r.proof) {
+                    memcpy(r.proof, proof.data(), proof.size());
+                    r.proof_len = proof.size();
+                } else {
+                    r.status = STWO_ERR_OUT_OF_MEMORY;
+                }
+            } else {
+                strncpy(r.error, stwo_last_error(), sizeof(r.error) - 1);
+            }
+            r.done_ms = steady_ms();
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                in_use -= j.bytes;
+                running--;
+                done.push_back(r);
+            }
+            cv_work.notify_all();  // freed budget may admit waiting jobs
+            cv_done.notify_all();
+        }
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+extern "C" {
+
+double stwo_server_now_ms(void) { return steady_ms(); }
+
+stwo_prover_server *stwo_server_create(uint32_t n_workers, uint64_t device_budget_bytes, uint32_t max_domain_log) {
+    clear_error();
+    if (n_workers == 0 || n_workers > 256 || max_domain_log < 4 || max_domain_log > 28) {
+        set_error(STWO_ERR_INVALID_ARGUMENT, "server needs 1..256 workers and a domain log size in 4..28");
+        return nullptr;
+    }
+    auto *s = new stwo_prover_server();
+    if (cudaGetDevice(&s->device) != cudaSuccess) {
+        set_error(STWO_ERR_CUDA, "no CUDA device");
+        delete s;
+        return nullptr;
+    }
+    s->budget = device_budget_bytes;
+    if (const char *w = getenv("STWO_SERVER_WAIT")) s->blocking_wait = strcmp(w, "spin") != 0;
+    s->max_domain_log = max_domain_log;
+    // One twiddle tree for CanonicCoset(max_domain_log).half_coset serves every smaller
+    // canonic domain: its doublings are the smaller domains' half cosets.
+    s->tree_size = 1ull << (max_domain_log - 1);
+    if (cudaMalloc(&s->tw, s->tree_size * 4) != cudaSuccess || cudaMalloc(&s->itw, s->tree_size * 4) != cudaSuccess) {
+        set_error(STWO_ERR_OUT_OF_MEMORY, "server twiddle tree allocation failed");
+        cudaFree(s->tw);
+        delete s;
+        return nullptr;
+    }
+    const uint32_t init = 1u << (30 - max_domain_log);
+    const uint32_t step = (uint32_t)((1ull << (32 - max_domain_log)) & 0x7fffffffu);
+    if (stwo_precompute_twiddles(init, step, max_domain_log - 1, s->tw, s->itw, nullptr) != STWO_OK ||
+        cudaStreamSynchronize(0) != cudaSuccess) {
+        cudaFree(s->tw);
+        cudaFree(s->itw);
+        delete s;
+        return nullptr;
+    }
+    for (uint32_t i = 0; i < n_workers; i++) s->workers.emplace_back([s] { s->worker(); });
+    return s;
+}
+
+int stwo_server_submit(stwo_prover_server *s, uint64_t job_id, const stwo_wide_fib_job *job, const uint32_t *a0,
+                       const uint32_t *a1) {
+    STWO_REQUIRE(s && job && a0 && a1, STWO_ERR_INVALID_ARGUMENT, "null argument");
+    const uint64_t bytes = wide_fib_job_device_bytes(job, false);
+    STWO_REQUIRE(bytes, STWO_ERR_UNSUPPORTED_SIZE, "job parameters unsupported");
+    STWO_REQUIRE(job->log_n_rows + 1 + job->log_blowup <= s->max_domain_log, STWO_ERR_UNSUPPORTED_SIZE,
+                 "job domain log size %u exceeds the server's %u", job->log_n_rows + 1 + job->log_blowup,
+                 s->max_domain_log);
+    STWO_REQUIRE(bytes <= s->budget, STWO_ERR_OUT_OF_MEMORY, "job needs %llu device bytes, budget is %llu",
+                 (unsigned long long)bytes, (unsigned long long)s->budget);
+    PendingJob j;
+    j.id = job_id;
+    j.job = *job;
+    const size_t rows = 1ull << job->log_n_rows;
+    j.a0.assign(a0, a0 + rows);
+    j.a1.assign(a1, a1 + rows);
+    j.bytes = bytes;
+    j.submit_ms = steady_ms();
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        STWO_REQUIRE(!s->stopping, STWO_ERR_INVALID_ARGUMENT, "server is shutting down");
+        s->pending.push_back(std::move(j));
+    }
+    s->cv_work.notify_one();
+    return STWO_OK;
+}
+
+uint32_t stwo_server_poll(stwo_prover_server *s, stwo_server_result *out, uint32_t max_results, int32_t timeout_ms) {
+    if (!s || !out || max_results == 0) return 0;
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto ready = [&] { return !s->done.empty() || (s->pending.empty() && s->running == 0); };
+    if (timeout_ms < 0) s->cv_done.wait(lock, ready);
+    else if (timeout_ms > 0) s->cv_done.wait_for(lock, std::chrono::milliseconds(timeout_ms), ready);
+    uint32_t n = 0;
+    while (n < max_results && !s->done.empty()) {
+        out[n++] = s->done.front();
+        s->done.pop_front();
+    }
+    return n;
+}
+
+void stwo_server_stats(stwo_prover_server *s, uint32_t *pending, uint32_t *running, uint64_t *device_bytes_in_use) {
+    if (!s) return;
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (pending) *pending = (uint32_t)s->pending.size();
+    if (running) *running = s->running;
+    if (device_bytes_in_use) *device_bytes_in_use = s->in_use;
+}
+
+void stwo_server_destroy(stwo_prover_server *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stopping = true;
+        s->pending.clear();
+    }
+    s->cv_work.notify_all();
+    for (auto &t : s->workers) t.join();
+    for (auto &r : s->done) free(r.proof);
+    cudaFree(s->tw);
+    cudaFree(s->itw);
+    delete s;
+}
+
+}  // extern "C"

@@ -1,0 +1,153 @@
+"""The GPU prover (csrc/prover.cu) and proof server (csrc/server.cu): proof bytes
+identical to the oracle prover's, proofs that verify, identical proofs alone and in a
+concurrent mix."""
+import numpy as np
+import pytest
+
+from conftest import load_package
+
+pytestmark = pytest.mark.gpu
+
+JOBS = [
+    # (log_n_rows, n_columns, log_blowup, n_queries, pow_bits)
+    (2, 3, 1, 1, 0),
+    (3, 4, 1, 3, 5),
+    (4, 8, 1, 3, 5),
+    (5, 3, 1, 3, 0),
+    (6, 16, 2, 5, 3),
+    (3, 20, 3, 9, 2),
+    (7, 33, 4, 20, 8),
+    (9, 17, 1, 7, 11),
+    (10, 100, 2, 3, 5),
+    (11, 64, 1, 30, 1),
+    (12, 64, 1, 3, 5),   # 64 columns, 2^12 rows: the reference CpuBackend's single proof
+    (14, 16, 1, 3, 10),
+]
+
+
+def job_of(t):
+    stwo = load_package()
+    return stwo.WideFibJob(*t)
+
+
+@pytest.mark.parametrize("t", JOBS, ids=lambda j: "L%d_N%d_B%d_q%d_pow%d" % j)
+def test_gpu_proof_equals_oracle_proof(oracle, t):
+    stwo = load_package()
+    a0, a1 = stwo.wide_fib_inputs(t[0], 2000 + t[0] * 7 + t[1])
+    proof, stats = stwo.prove_wide_fib(job_of(t), a0, a1)
+    want, rc = oracle.wide_fib_prove(t[0], t[1], a0, a1, t[2], t[3], t[4])
+    assert rc == 0
+    assert proof == want
+    assert stats["proof_bytes"] == len(proof)
+    assert stats["kernel_launches"] > 0
+    assert 0 < stats["device_bytes"] <= job_of(t).device_bytes(own_twiddles=True)
+    assert stats["total_ms"] >= stats["trace_ms"] > 0
+    assert stwo.verify(proof, *t)
+
+
+def test_gpu_proof_with_shared_twiddles_is_identical():
+    stwo = load_package()
+    t = (8, 12, 1, 3, 5)
+    a0, a1 = stwo.wide_fib_inputs(8, 5)
+    own, _ = stwo.prove_wide_fib(job_of(t), a0, a1)
+    tree = stwo.CudaBackend.precompute_twiddles(stwo.CanonicCoset(16).half_coset())
+    shared, _ = stwo.prove_wide_fib(job_of(t), a0, a1, twiddles=tree)
+    assert own == shared
+
+
+def test_gpu_prover_accepts_device_inputs():
+    stwo = load_package()
+    t = (6, 9, 1, 3, 5)
+    a0, a1 = stwo.wide_fib_inputs(6, 8)
+    host, _ = stwo.prove_wide_fib(job_of(t), a0, a1)
+    d0, d1 = stwo.BaseFieldVec.from_numpy(a0), stwo.BaseFieldVec.from_numpy(a1)
+    import ctypes as C
+    L = stwo._lib
+    out, ln, st = C.POINTER(C.c_uint8)(), C.c_uint64(), L.ProveStats()
+    L.check(L.lib().stwo_wide_fib_prove(C.byref(job_of(t).c()), d0.device_ptr, d1.device_ptr, None, None, 0,
+                                        C.byref(out), C.byref(ln), C.byref(st), None))
+    dev = C.string_at(out, ln.value)
+    L.lib().stwo_free_proof(out)
+    assert dev == host
+
+
+@pytest.mark.parametrize("bad", [(2, 2, 1, 3, 5), (1, 8, 1, 3, 5), (4, 8, 0, 3, 5), (4, 8, 5, 3, 5),
+                                 (4, 8, 1, 0, 5), (4, 2000, 1, 3, 5), (26, 8, 1, 3, 5)])
+def test_gpu_prover_rejects_unsupported_jobs(bad):
+    stwo = load_package()
+    n = 1 << min(bad[0], 4)
+    with pytest.raises((stwo._lib.StwoError, ValueError)):
+        stwo.prove_wide_fib(job_of(bad), np.zeros(n, np.uint32), np.zeros(n, np.uint32))
+    # the library stays usable
+    a0, a1 = stwo.wide_fib_inputs(4, 1)
+    proof, _ = stwo.prove_wide_fib(job_of((4, 8, 1, 3, 5)), a0, a1)
+    assert stwo.verify(proof, 4, 8, 1, 3, 5)
+
+
+def test_large_proof_verifies():
+    """256 columns, 2^18 rows: checked by the verifier (the oracle is too slow here)."""
+    stwo = load_package()
+    t = (18, 256, 1, 3, 10)
+    a0, a1 = stwo.wide_fib_inputs(18, 99)
+    proof, stats = stwo.prove_wide_fib(job_of(t), a0, a1)
+    assert stwo.verify(proof, *t)
+    proof2, _ = stwo.prove_wide_fib(job_of(t), a0, a1)
+    assert proof2 == proof
+
+
+def _mixed_jobs(n, seed):
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(n):
+        L = int(rng.integers(4, 13))
+        N = int(rng.choice([3, 8, 16, 33, 64]))
+        B = int(rng.choice([1, 1, 2]))
+        jobs.append((i, (L, N, B, int(rng.integers(1, 8)), int(rng.integers(0, 9))), 500 + i))
+    return jobs
+
+
+def test_server_proofs_equal_single_job_proofs():
+    stwo = load_package()
+    jobs = _mixed_jobs(24, 3)
+    alone = {}
+    for jid, t, seed in jobs:
+        a0, a1 = stwo.wide_fib_inputs(t[0], seed)
+        alone[jid] = stwo.prove_wide_fib(job_of(t), a0, a1)[0]
+    with stwo.ProofServer(n_workers=8, device_budget_bytes=8 << 30, max_domain_log=16) as srv:
+        for jid, t, seed in jobs:
+            a0, a1 = stwo.wide_fib_inputs(t[0], seed)
+            srv.submit(jid, job_of(t), a0, a1)
+        got = {}
+        while len(got) < len(jobs):
+            for r in srv.poll(timeout_ms=-1):
+                assert r["status"] == 0, r["error"]
+                got[r["job_id"]] = r
+        assert srv.stats()["running"] == 0
+    for jid, t, _ in jobs:
+        assert got[jid]["proof"] == alone[jid], (jid, t)
+        r = got[jid]
+        assert r["submit_ms"] <= r["start_ms"] <= r["done_ms"]
+
+
+def test_server_respects_the_memory_budget():
+    stwo = load_package()
+    t = (10, 32, 1, 3, 5)
+    need = job_of(t).device_bytes(own_twiddles=False)
+    with stwo.ProofServer(n_workers=4, device_budget_bytes=need + need // 2, max_domain_log=12) as srv:
+        for i in range(6):
+            a0, a1 = stwo.wide_fib_inputs(10, i)
+            srv.submit(i, job_of(t), a0, a1)
+        results = []
+        while len(results) < 6:
+            st = srv.stats()
+            assert st["device_bytes_in_use"] <= need + need // 2
+            assert st["running"] <= 1
+            results += srv.poll(timeout_ms=5)
+        # one job at a time fits: their runs do not overlap
+        spans = sorted((r["start_ms"], r["done_ms"]) for r in results)
+        for (s0, e0), (s1, e1) in zip(spans, spans[1:]):
+            assert s1 >= e0 - 1e-6
+        with pytest.raises(stwo._lib.StwoError):
+            big = (11, 64, 1, 3, 5)
+            a0, a1 = stwo.wide_fib_inputs(11, 0)
+            srv.submit(99, job_of(big), a0, a1)
