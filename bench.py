@@ -1,19 +1,27 @@
-"""Benchmark: M31 circle FFT on B200 (the BASELINE metric's "FFT % HBM peak" leg).
+"""Benchmark: wide-Fibonacci proof serving on one B200 (the BASELINE metric:
+"bit-exact proofs/s & p99 latency: batched server vs per-job; FFT % HBM peak").
 
-Workload (per GPU, weak scaling): 8 M31 columns at log_size 24 — each step
-interpolates the 8 evaluations (2^24 each, in place) and evaluates the resulting
-coefficients on the blowup-4 domain (2^24 coefficients -> 2^26 evaluations) with
-the extension fused into the FFT. One "column" of the metric = one such
-interpolate + extend-evaluate. Inputs (512 MB) and outputs (2 GB) exceed the
-126 MB L2, so no flush is needed between steps.
+Workload: a seeded stream of wide-Fibonacci proof jobs shaped like the serving
+config: log_n_rows uniform in {12..20} (log-uniform row counts), columns uniform in
+{16..256}, log_blowup 1, 3 queries, pow_bits 5, Blake2s channel. A step is one batch
+of --jobs jobs (default 48) admitted at once to the proof server (csrc/server.cu:
+--workers jobs in flight, 150 GB device budget). `value` is the server's proofs/s
+with the job inputs already resident in HBM; `e2e` submits host inputs instead.
+Alongside: the same jobs proved one at a time (per_job), every batched proof
+compared byte for byte with its one-at-a-time proof, Poisson-arrival latency
+(p50/p99/p99.9) at three loads for both modes, the single proofs of the 64-column x
+2^12 and 256-column x 2^20 cases with their phase breakdown, the M31 circle FFT
+roofline (8 columns at log 24, blowup 4; roofline.frac = FFT % HBM peak) and the
+per-kernel sweep against the reference's own CUDA library.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
---impl reference times the oracle port of the reference's CPU path (CpuBackend
-restated in C, oracle/stwo_oracle.c) on all host cores, one column per step.
-Prints one JSON line (rank 0).
+--impl reference times the oracle port of the reference's CPU prover (CpuBackend
+restated in C, oracle/stwo_oracle_prover.c) on the same job stream on all host
+cores, a bounded sample per step. Prints one JSON line (rank 0).
 """
 import argparse
+import dataclasses
 import importlib.util
 import json
 import os
@@ -25,8 +33,10 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "stwo-gpu_b200")
 P = (1 << 31) - 1
-METRIC = "circle FFT columns/s at log_size 24 (interpolate + blowup-4 evaluate); FFT % HBM peak in roofline.frac"
-UNIT = "columns/s"
+METRIC = "bit-exact proofs/s & p99 latency: batched server vs per-job; FFT % HBM peak"
+UNIT = "proofs/s"
+FFT_UNIT = "columns/s"
+BUDGET = 150 << 30  # device-memory budget of the serving config
 
 
 def load_package():
@@ -159,7 +169,7 @@ def reference_gpu_timing(args, evals, lg, lb, ncols, tw, itw, tree_size):
     e.record(torch.cuda.default_stream())
     torch.cuda.synchronize()
     ms = s.elapsed_time(e) / reps
-    return {"ms_per_step": ms, "value": ncols / (ms / 1e3), "unit": UNIT,
+    return {"ms_per_step": ms, "value": ncols / (ms / 1e3), "unit": FFT_UNIT,
             "what": "reference CUDA library (oracle/_ref) on this GPU: interpolate_columns + extend + "
                     "evaluate_columns, same 8 x 2^24 step"}
 
@@ -354,44 +364,77 @@ def kernel_suite(stwo, reps=5):
     return out
 
 
+def job_stream(n, seed):
+    """n seeded jobs: (log_n_rows, n_columns, input seed)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return [(int(rng.integers(12, 21)), int(rng.integers(16, 257)), int(rng.integers(0, 1 << 62))) for _ in range(n)]
+
+
+def job_of(stwo, t):
+    return stwo.WideFibJob(t[0], t[1], 1, 3, 5)
+
+
+def job_desc(n_jobs):
+    return (f"seeded wide-Fibonacci proof stream: log_n_rows U{{12..20}}, columns U{{16..256}}, log_blowup 1, "
+            f"3 queries, pow_bits 5; {n_jobs} jobs per step admitted at once")
+
+
+def cpu_stream_sample(O, stwo, jobs, budget_s, threads):
+    """The oracle prover on jobs of the stream, in order, until budget_s of CPU work
+    (at least one job). Returns (jobs done, seconds, description)."""
+    O.set_threads(threads)
+    done, t0 = 0, time.perf_counter()
+    for t in jobs:
+        a0, a1 = stwo.wide_fib_inputs(t[0], t[2])
+        O.wide_fib_prove(t[0], t[1], a0, a1, 1, 3, 5)
+        done += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    O.set_threads(1)
+    return done, dt, f"first {done} jobs of the stream, oracle prover on {threads} host threads"
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
     O = load_oracle()
+    stwo = load_package()
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_baseline(O, args.log_size, args.log_blowup, threads)
-    times = [cpu_baseline(O, args.log_size, args.log_blowup, threads) for _ in range(args.steps)]
-    per_col = sum(times) / len(times)
-    value = 1.0 / per_col
+    for w in range(args.warmup):  # warm-up: one 64-column x 2^12 job each
+        cpu_stream_sample(O, stwo, [(12, 64, 7000 + w)], 0.0, threads)
+    n_total, t_total = 0, 0.0
+    for s in range(args.steps):
+        n, dt, _ = cpu_stream_sample(O, stwo, job_stream(args.jobs, 1000 + s), args.cpu_budget, threads)
+        n_total += n
+        t_total += dt
+    value = n_total / t_total
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_col * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "m31 (u32)", "data": "synthetic (seeded uniform M31)",
-        "config": {"workload": f"1 column at log_size {args.log_size}: interpolate + evaluate blowup "
-                               f"{1 << args.log_blowup} (CPU sample of the 8-column GPU step)",
-                   "columns": 1, "log_size": args.log_size, "log_blowup": args.log_blowup},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_total / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "m31 (u32)",
+        "data": "synthetic (seeded SplitMix64 M31 trace inputs)",
+        "config": {"workload": job_desc(args.jobs) + f" (CPU: a bounded sample of each step, ~{args.cpu_budget:.0f} s)",
+                   "jobs_per_step": args.jobs},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"1 column of 2^{args.log_size} per step"},
+                         "sample": f"{n_total} jobs over {args.steps} steps, each step the stream's first jobs "
+                                   f"within {args.cpu_budget:.0f} s (oracle prover, {threads} threads)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, rank, world, local_rank):
-    import numpy as np
+def fft_roofline(stwo, dev, rank, args):
+    """The M31 circle FFT step (8 columns at log 24: interpolate, extend-evaluate
+    blowup 4), its HBM roofline and the reference CUDA library on the same step."""
     import torch
-
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    stwo = load_package()
     L = stwo._lib
     lib = L.lib()
-    ncols, lg, lb = args.cols, args.log_size, args.log_blowup
+    ncols, lg, lb = 8, 24, 2
     N = lg + lb
     stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
-
     hc = stwo.CanonicCoset(N).half_coset()
     tree_size = 1 << hc.log_size
     tw = torch.empty(tree_size, dtype=torch.int32, device=dev)
@@ -413,41 +456,24 @@ def run_ours(args, rank, world, local_rank):
     def extend_eval():
         L.check(lib.stwo_extend_evaluate_columns(ev_ptrs, logs, out_ptrs, lb, ncols, tw.data_ptr(), tree_size, sptr))
 
-    launches_per_step = 4  # 2 passes interpolate + 2 passes evaluate (log 24, 8 columns)
-
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-
-    for _ in range(args.warmup):
+    for _ in range(3):
         interp()
         extend_eval()
     torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-
+    reps = 5
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
-        start.record(stream)
-        for e0, e1, e2 in ev:
-            e0.record(stream)
-            interp()
-            e1.record(stream)
-            extend_eval()
-            e2.record(stream)
-        end.record(stream)
-        torch.cuda.synchronize()
-    barrier()
-    total_ms = start.elapsed_time(end)
-    t_interp = sum(a.elapsed_time(b) for a, b, _ in ev) / args.steps
-    t_eval = sum(b.elapsed_time(c) for _, b, c in ev) / args.steps
-    ms_step, value = replica_throughput(total_ms / args.steps, ncols, world, dev)
-
-    # Roofline of the FFT kernel: algorithmic bytes = one read + one write per
-    # element (interpolate: 8 B per element; evaluate: 4 B per coefficient read +
-    # 4 B per evaluation written); twiddle reads are not counted.
+           torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for e0, e1, e2 in ev:
+        e0.record(stream)
+        interp()
+        e1.record(stream)
+        extend_eval()
+        e2.record(stream)
+    torch.cuda.synchronize()
+    t_interp = sum(a.elapsed_time(b) for a, b, _ in ev) / reps
+    t_eval = sum(b.elapsed_time(c) for _, b, c in ev) / reps
+    # algorithmic bytes: one read + one write per element (interpolate 8 B per element;
+    # evaluate 4 B per coefficient read + 4 B per evaluation written); twiddles not counted
     b_interp = ncols * (1 << lg) * 8
     b_eval = ncols * ((1 << lg) * 4 + (1 << N) * 4)
     achieved = (b_interp + b_eval) / ((t_interp + t_eval) / 1e3) / 1e9
@@ -456,84 +482,233 @@ def run_ours(args, rank, world, local_rank):
     tf = os.path.join(ROOT, "profiles", "fft_traffic.json")
     if os.path.exists(tf):
         traffic = json.load(open(tf)).get("dram_bytes_per_launch")
+    ref_gpu = None
+    if rank == 0 and not args.no_suite:
+        ns = argparse.Namespace(**vars(args))
+        ref_gpu = reference_gpu_timing(ns, evals, lg, lb, ncols, tw, itw, tree_size)
+    roof = {"bound": "hbm", "kernel": "fftT_kernel / fft_pass_kernel (circle FFT, 8 columns x 2^24, blowup 4)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": traffic, "interpolate_ms": t_interp, "evaluate_ms": t_eval,
+            "algorithmic_bytes_per_step": b_interp + b_eval}
+    fft = {"columns_per_s": ncols / ((t_interp + t_eval) / 1e3), "unit": FFT_UNIT, "reference_gpu": ref_gpu}
+    del evals, outs, tw, itw
+    torch.cuda.empty_cache()
+    return roof, fft
 
-    # End to end through the C ABI with host buffers: pinned H2D of the 8 input
-    # columns, interpolate, extend-evaluate, D2H of the 8 evaluated columns.
-    h_in = [torch.empty(1 << lg, dtype=torch.int32, pin_memory=True) for _ in range(ncols)]
-    h_out = [torch.empty(1 << N, dtype=torch.int32, pin_memory=True) for _ in range(ncols)]
-    for h, d in zip(h_in, evals):
-        h.copy_(d)
-    e2e_steps = max(2, min(args.steps, 5))
 
-    def e2e_step():
-        for h, d in zip(h_in, evals):
-            d.copy_(h, non_blocking=True)
-        interp()
-        extend_eval()
-        for h, d in zip(h_out, outs):
-            h.copy_(d, non_blocking=True)
+class StreamRunner:
+    """Submits jobs to a ProofServer (resident device inputs or host inputs) and
+    collects every result on a polling thread."""
 
-    e2e_step()
+    def __init__(self, stwo, workers, max_domain_log=22):
+        self.stwo = stwo
+        self.srv = stwo.ProofServer(n_workers=workers, device_budget_bytes=BUDGET, max_domain_log=max_domain_log)
+
+    def run(self, jobs, inputs, resident, arrivals_ms=None):
+        """jobs: list of (L, N, seed); inputs[i] = (host a0, host a1, dev a0, dev a1).
+        arrivals_ms: offsets from the start (None: all at once). Returns (results by
+        index, wall ms from the first submit to the last completion)."""
+        stwo, srv = self.stwo, self.srv
+        results = {}
+        done = threading.Event()
+
+        def poller():
+            while len(results) < len(jobs):
+                for r in srv.poll(timeout_ms=50):
+                    results[int(r["job_id"])] = r
+            done.set()
+
+        th = threading.Thread(target=poller, daemon=True)
+        th.start()
+        t0 = srv.now_ms()
+        for i, t in enumerate(jobs):
+            if arrivals_ms is not None:
+                wait = t0 + arrivals_ms[i] - srv.now_ms()
+                if wait > 0:
+                    time.sleep(wait / 1e3)
+            h0, h1, d0, d1 = inputs[i]
+            if resident:
+                srv.submit_device(i, job_of(stwo, t), d0.data_ptr(), d1.data_ptr())
+            else:
+                srv.submit(i, job_of(stwo, t), h0, h1)
+        done.wait()
+        th.join()
+        bad = [r for r in results.values() if r["status"] != 0]
+        if bad:
+            raise RuntimeError(f"proof failed: {bad[0]['error']}")
+        end = max(r["done_ms"] for r in results.values())
+        return results, end - t0
+
+    def close(self):
+        self.srv.close()
+
+
+def percentiles(xs):
+    import numpy as np
+    a = np.array(xs)
+    return {"p50_ms": float(np.percentile(a, 50)), "p99_ms": float(np.percentile(a, 99)),
+            "p999_ms": float(np.percentile(a, 99.9)), "mean_ms": float(a.mean())}
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stwo = load_package()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def inputs_for(jobs):
+        out = []
+        for t in jobs:
+            a0, a1 = stwo.wide_fib_inputs(t[0], t[2])
+            out.append((a0, a1, torch.from_numpy(a0.view(np.int32)).to(dev), torch.from_numpy(a1.view(np.int32)).to(dev)))
+        return out
+
+    # Per-rank streams (weak scaling): rank r proves its own seeded jobs.
+    steps = [job_stream(args.jobs, 1000 + s + 7919 * rank) for s in range(args.steps)]
+    warm = [job_stream(max(4, args.workers), 7000 + w + 7919 * rank) for w in range(args.warmup)]
+    step_inputs = [inputs_for(js) for js in steps]
+    warm_inputs = [inputs_for(js) for js in warm]
+    torch.cuda.synchronize()
+
+    batched = StreamRunner(stwo, args.workers)
+    for js, ins in zip(warm, warm_inputs):
+        batched.run(js, ins, resident=True)
     torch.cuda.synchronize()
     barrier()
-    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s2.record(stream)
-    for _ in range(e2e_steps):
-        e2e_step()
-    e2.record(stream)
     torch.cuda.synchronize()
-    e2e_ms, e2e_value = replica_throughput(s2.elapsed_time(e2) / e2e_steps, ncols, world, dev)
 
-    ref_gpu = reference_gpu_timing(args, evals, lg, lb, ncols, tw, itw, tree_size) if rank == 0 else None
-    kernels = None
-    if rank == 0 and world == 1 and not args.no_suite:
-        del evals, outs, h_in, h_out
-        torch.cuda.empty_cache()
-        kernels = kernel_suite(stwo)
+    # ---- timed: the batched server, inputs resident in HBM
+    launches0 = stwo.kernel_launches()
+    step_ms, batched_results = [], []
+    with ClockSampler(local_rank) as clk:
+        for js, ins in zip(steps, step_inputs):
+            res, ms = batched.run(js, ins, resident=True)
+            step_ms.append(ms)
+            batched_results.append(res)
+        torch.cuda.synchronize()
+    barrier()
+    launches = stwo.kernel_launches() - launches0
+    local_ms = sum(step_ms) / len(step_ms)
+    ms_step, value = replica_throughput(local_ms, args.jobs, world, dev)
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        O = load_oracle()
-        threads = os.cpu_count() or 1
-        dt = cpu_baseline(O, lg, lb, threads)
-        cpu = {"value": 1.0 / dt, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"1 column of 2^{lg}: interpolate + evaluate blowup {1 << lb} (oracle, {threads} threads)"}
+    # ---- end to end: host inputs copied in by the server
+    e2e_ms = []
+    for js, ins in zip(steps, step_inputs):
+        _, ms = batched.run(js, ins, resident=False)
+        e2e_ms.append(ms)
+    e2e_step, e2e_value = replica_throughput(sum(e2e_ms) / len(e2e_ms), args.jobs, world, dev)
+    h2d = sum(8 << t[0] for t in steps[0])
+    d2h = sum(len(r["proof"]) for r in batched_results[0].values())
+
+    # ---- one job at a time on the same jobs (one worker), and byte-for-byte comparison
+    single = StreamRunner(stwo, 1)
+    single.run(warm[0], warm_inputs[0], resident=True)
+    per_ms, identical, compared = [], True, 0
+    for js, ins, bres in zip(steps, step_inputs, batched_results):
+        res, ms = single.run(js, ins, resident=True)
+        per_ms.append(ms)
+        for i in res:
+            compared += 1
+            identical = identical and res[i]["proof"] == bres[i]["proof"]
+    per_step, per_value = replica_throughput(sum(per_ms) / len(per_ms), args.jobs, world, dev)
+
+    # ---- Poisson arrivals at three loads (fractions of the one-at-a-time throughput)
+    latency = {}
+    lat_jobs = job_stream(args.latency_jobs, 4242 + 7919 * rank)
+    lat_inputs = inputs_for(lat_jobs)
+    rng = np.random.default_rng(99)
+    per_rate = per_value / world  # proofs/s of one GPU one at a time
+    for load in (0.5, 0.9, 1.5):
+        gaps = rng.exponential(1e3 / (load * per_rate), size=len(lat_jobs))
+        arrivals = np.cumsum(gaps) - gaps[0]
+        entry = {"arrival_rate_per_s": load * per_rate}
+        for name, runner in (("batched", batched), ("per_job", single)):
+            res, ms = runner.run(lat_jobs, lat_inputs, resident=True, arrivals_ms=list(arrivals))
+            lat = [r["done_ms"] - r["submit_ms"] for r in res.values()]
+            entry[name] = dict(percentiles(lat), proofs_per_s=len(res) / (ms / 1e3))
+        latency[f"load_{load}x"] = entry
+    single.close()
+    batched.close()
+    del step_inputs, warm_inputs, lat_inputs
+    torch.cuda.empty_cache()
+
+    # ---- single proofs, FFT roofline, kernel sweep, CPU baseline (rank 0, 1 GPU)
+    roof, fft = fft_roofline(stwo, dev, rank, args)
+    singles, kernels, cpu, verified = None, None, None, None
+    if rank == 0:
+        O = load_oracle() if not args.no_cpu_baseline else None
+        singles = {}
+        for name, t in (("cols64_log12", (12, 64, 1, 3, 5)), ("cols256_log20", (20, 256, 1, 3, 10))):
+            job = stwo.WideFibJob(*t)
+            a0, a1 = stwo.wide_fib_inputs(t[0], 1)
+            stwo.prove_wide_fib(job, a0, a1)
+            times, stats = [], None
+            for _ in range(5):
+                t0 = time.perf_counter()
+                proof, stats = stwo.prove_wide_fib(job, a0, a1)
+                times.append((time.perf_counter() - t0) * 1e3)
+            ent = {"job": dict(zip(["log_n_rows", "n_columns", "log_blowup", "n_queries", "pow_bits"], t)),
+                   "ms_median": float(np.median(times)), "phases_ms": {k: stats[k] for k in
+                   ("trace_ms", "composition_ms", "oods_ms", "fri_ms", "decommit_ms")},
+                   "kernel_launches": stats["kernel_launches"], "proof_bytes": len(proof),
+                   "verified": bool(stwo.verify(proof, *t))}
+            if O is not None and t[0] <= 12:
+                t0 = time.perf_counter()
+                want, _ = O.wide_fib_prove(t[0], t[1], a0, a1, *t[2:])
+                ent["oracle_ms"] = (time.perf_counter() - t0) * 1e3
+                ent["equal_to_oracle"] = want == proof
+            singles[name] = ent
+        verified = all(stwo.verify(batched_results[0][i]["proof"], *dataclasses.astuple(job_of(stwo, steps[0][i])))
+                       for i in range(min(2, args.jobs)))
+        if world == 1 and not args.no_suite:
+            kernels = kernel_suite(stwo)
+        if O is not None and world == 1:
+            threads = os.cpu_count() or 1
+            n, dt, desc = cpu_stream_sample(O, stwo, steps[0], args.cpu_budget, threads)
+            cpu = {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "m31 (u32)", "data": "synthetic (seeded uniform M31)",
-            "config": {"workload": f"{ncols} columns x log_size {lg}: interpolate + extend-evaluate blowup {1 << lb}",
-                       "columns_per_gpu": ncols, "log_size": lg, "log_blowup": lb,
-                       "l2": "inputs 512 MB + outputs 2 GB > 126 MB L2 (no flush needed)",
+            "vs_baseline": None, "dtype": "m31 (u32)", "data": "synthetic (seeded SplitMix64 M31 trace inputs)",
+            "config": {"workload": job_desc(args.jobs), "jobs_per_step": args.jobs, "workers": args.workers,
+                       "device_budget_gb": BUDGET >> 30, "inputs": "resident in HBM before the timed region",
+                       "l2": "each job's columns and trees are freshly written; the stream's working set "
+                             "(GBs) exceeds the 126 MB L2",
                        "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "hbm", "kernel": "fft_pass_kernel (interpolate + evaluate transforms)",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": traffic,
-                         "interpolate_ms": t_interp, "evaluate_ms": t_eval,
-                         "algorithmic_bytes_per_step": b_interp + b_eval},
+            "serving": {"per_job_proofs_per_s": per_value, "batched_vs_per_job": value / per_value,
+                        "bit_identical": identical, "proofs_compared": compared, "verified_sample": verified,
+                        "latency": latency, "latency_jobs": args.latency_jobs},
+            "single_proofs": singles,
+            "roofline": roof,
+            "fft": fft,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ncols * (1 << lg) * 4,
-                    "d2h_bytes_per_step": ncols * (1 << N) * 4, "ms_per_step": e2e_ms},
-            "reference_gpu": ref_gpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_step},
             "kernels": kernels,
-            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches": launches,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
-    del np
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cols", type=int, default=8)
-    ap.add_argument("--log-size", type=int, default=24)
-    ap.add_argument("--log-blowup", type=int, default=2)
+    ap.add_argument("--jobs", type=int, default=48, help="jobs per step")
+    ap.add_argument("--workers", type=int, default=8, help="proof server jobs in flight")
+    ap.add_argument("--latency-jobs", type=int, default=200, help="jobs per Poisson load level")
+    ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds of oracle work per CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-suite", action="store_true", help="skip the config-1 per-kernel sweep")
     args = ap.parse_args()

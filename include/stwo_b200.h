@@ -148,6 +148,9 @@ void evaluate_wide_fibonacci_constraint_quotients_on_domain(
  * report failures only through this record. */
 const char *stwo_last_error(void);
 void stwo_clear_last_error(void);
+/* Grows the library's device memory pool (which keeps what it holds) to at least
+ * `bytes`, so allocations up to that total map no new memory later. */
+int stwo_reserve_device_memory(uint64_t bytes);
 /* Number of kernel launches the library has made in this process (all threads). */
 uint64_t stwo_kernel_launches(void);
 /* Waits for all work on `stream`; returns STWO_ERR_CUDA if any of it failed. */
@@ -309,6 +312,10 @@ int stwo_server_submit(stwo_prover_server *server, uint64_t job_id, const stwo_w
                        const uint32_t *a1);
 /* Moves up to max_results finished jobs into out and returns their number. Waits up to
  * timeout_ms for one (negative: until one finishes or nothing is queued or running). */
+/* Queues a job whose inputs are already in device memory; the caller keeps a0_dev and
+ * a1_dev valid until the job's result has been polled. */
+int stwo_server_submit_device(stwo_prover_server *server, uint64_t job_id, const stwo_wide_fib_job *job,
+                              const uint32_t *a0_dev, const uint32_t *a1_dev);
 uint32_t stwo_server_poll(stwo_prover_server *server, stwo_server_result *out, uint32_t max_results,
                           int32_t timeout_ms);
 void stwo_server_stats(stwo_prover_server *server, uint32_t *pending, uint32_t *running,

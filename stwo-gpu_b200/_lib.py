@@ -115,6 +115,7 @@ SIGNATURES = [
     ("stwo_accumulate_quotients", C.c_int, [u32, u32, u32, vp, u32, QM31, vp, vp, vp, vp, u32, vp, vp]),
     ("stwo_wide_fib_composition", C.c_int, [vp, u32, u32, vp, vp, vp, vp]),
     ("stwo_kernel_launches", u64, []),
+    ("stwo_reserve_device_memory", C.c_int, [u64]),
     # prover tier
     ("stwo_wide_fib_prove_device_bytes", u64, [C.POINTER(WideFibJob), C.c_int]),
     ("stwo_wide_fib_prove", C.c_int, [C.POINTER(WideFibJob), vp, vp, vp, vp, u64, C.POINTER(C.POINTER(C.c_uint8)),
@@ -122,6 +123,7 @@ SIGNATURES = [
     ("stwo_free_proof", None, [vp]),
     ("stwo_server_create", vp, [u32, u64, u32]),
     ("stwo_server_submit", C.c_int, [vp, u64, C.POINTER(WideFibJob), vp, vp]),
+    ("stwo_server_submit_device", C.c_int, [vp, u64, C.POINTER(WideFibJob), vp, vp]),
     ("stwo_server_poll", u32, [vp, C.POINTER(ServerResult), u32, C.c_int32]),
     ("stwo_server_stats", None, [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u64)]),
     ("stwo_server_now_ms", C.c_double, []),

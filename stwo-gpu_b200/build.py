@@ -59,7 +59,7 @@ def build(force=False, verbose=False, extra=None):
     objs = [o for o, _ in results]
     changed = any(c for _, c in results)
     if changed or force or not os.path.exists(LIB):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-Xlinker", "--no-undefined", "-o", LIB] + objs + ["-lcudart"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -43,9 +43,13 @@ __device__ __forceinline__ uint32_t add_on_fma(uint32_t c, uint32_t d, uint32_t 
       STWO_G(v2, v7, v8, v13, m[s12], m[s13])                                          \
       STWO_G(v3, v4, v9, v14, m[s14], m[s15]) }
 
-__device__ __forceinline__ void compress(uint32_t h[8], const uint32_t m[16], uint32_t one) {
+// Compression with byte counter t (low word) and finalisation flag f0; the Merkle
+// hasher and the nonce mixing use t = f0 = 0.
+__device__ __forceinline__ void compress_tf(uint32_t h[8], const uint32_t m[16], uint32_t t, uint32_t f0,
+                                            uint32_t one) {
     uint32_t v0 = h[0], v1 = h[1], v2 = h[2], v3 = h[3], v4 = h[4], v5 = h[5], v6 = h[6], v7 = h[7];
-    uint32_t v8 = IV[0], v9 = IV[1], v10 = IV[2], v11 = IV[3], v12 = IV[4], v13 = IV[5], v14 = IV[6], v15 = IV[7];
+    uint32_t v8 = IV[0], v9 = IV[1], v10 = IV[2], v11 = IV[3], v12 = IV[4] ^ t, v13 = IV[5], v14 = IV[6] ^ f0,
+             v15 = IV[7];
     STWO_ROUND(0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15)
     STWO_ROUND(14, 10, 4, 8, 9, 15, 13, 6, 1, 12, 0, 2, 11, 7, 5, 3)
     STWO_ROUND(11, 8, 12, 0, 5, 2, 15, 13, 10, 14, 3, 6, 7, 1, 9, 4)
@@ -64,6 +68,10 @@ __device__ __forceinline__ void compress(uint32_t h[8], const uint32_t m[16], ui
     h[5] ^= v5 ^ v13;
     h[6] ^= v6 ^ v14;
     h[7] ^= v7 ^ v15;
+}
+
+__device__ __forceinline__ void compress(uint32_t h[8], const uint32_t m[16], uint32_t one) {
+    compress_tf(h, m, 0u, 0u, one);
 }
 
 }  // namespace blake

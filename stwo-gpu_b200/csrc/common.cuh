@@ -78,6 +78,9 @@ int once_per_device(std::atomic<uint64_t> &done, F f) {
 // with an unbounded release threshold: memory a job frees is reused by the next job
 // instead of going back to the driver at every synchronisation.
 int library_pool(cudaMemPool_t *pool);
+// Grows the library pool to hold at least `bytes` (allocated and freed once), so
+// later allocations up to that total map no new physical memory.
+int reserve_pool(uint64_t bytes);
 // cudaMallocFromPoolAsync from the library pool (free with cudaFreeAsync).
 int pool_alloc(void **p, size_t bytes, cudaStream_t st);
 

@@ -32,9 +32,15 @@ __device__ __forceinline__ qm31 fold_pair(qm31 a, qm31 b, uint32_t t, qm31 alpha
     return qm31_add(s, qm31_mul(alpha, d));
 }
 
+// alpha_dev: when set, alpha is read from device memory (a challenge the device
+// channel drew) instead of the by-value argument.
 template <bool CIRCLE>
 __global__ void fold_kernel(const __grid_constant__ Cols4 src, const __grid_constant__ MutCols4 dst, uint64_t n_out,
-                            const uint32_t *__restrict__ tw, qm31 alpha, qm31 alpha_sq) {
+                            const uint32_t *__restrict__ tw, qm31 alpha, qm31 alpha_sq, const qm31 *alpha_dev) {
+    if (alpha_dev) {
+        alpha = *alpha_dev;
+        alpha_sq = qm31_mul(alpha, alpha);
+    }
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; 2 * k < n_out;
          k += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t i = 2 * k;  // outputs i, i+1 <- inputs 2i .. 2i+3
@@ -81,7 +87,11 @@ __global__ void fold_kernel(const __grid_constant__ Cols4 src, const __grid_cons
 template <bool CIRCLE>
 __global__ void fold_small_kernel(const __grid_constant__ Cols4 src, const __grid_constant__ MutCols4 dst,
                                   uint32_t n_out, uint32_t t0, uint32_t t1, const uint32_t *tw, qm31 alpha,
-                                  qm31 alpha_sq) {
+                                  qm31 alpha_sq, const qm31 *alpha_dev) {
+    if (alpha_dev) {
+        alpha = *alpha_dev;
+        alpha_sq = qm31_mul(alpha, alpha);
+    }
     if (tw) {  // line fold: the inverse x twiddles are read from the tree
         t0 = tw[0];
         t1 = n_out > 1 ? tw[1] : 0u;
@@ -101,7 +111,8 @@ __global__ void fold_small_kernel(const __grid_constant__ Cols4 src, const __gri
 }  // namespace
 
 int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const uint32_t *itw, uint64_t off,
-               uint32_t *const *dst4, bool circle, cudaStream_t st) {
+               uint32_t *const *dst4, bool circle, cudaStream_t st, const void *alpha_dev) {
+    const qm31 *ad = static_cast<const qm31 *>(alpha_dev);
     STWO_REQUIRE(n >= 2 && is_pow2(n), STWO_ERR_INVALID_ARGUMENT, "fold of %llu values", (unsigned long long)n);
     Cols4 s;
     MutCols4 d;
@@ -124,8 +135,8 @@ int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const
             t[0] = iy;
             t[1] = m31_neg(iy);
         }
-        if (circle) fold_small_kernel<true><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, t[0], t[1], nullptr, alpha, a2);
-        else fold_small_kernel<false><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, 0u, 0u, tw, alpha, a2);
+        if (circle) fold_small_kernel<true><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, t[0], t[1], nullptr, alpha, a2, ad);
+        else fold_small_kernel<false><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, 0u, 0u, tw, alpha, a2, ad);
         STWO_LAUNCH_CHECK("fold_small_kernel");
         return STWO_OK;
     }
@@ -135,8 +146,8 @@ int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const
     uint32_t blocks = (uint32_t)((threads + 255) / 256);
     uint32_t cap = (uint32_t)device_sm_count() * 16;
     if (blocks > cap) blocks = cap;
-    if (circle) fold_kernel<true><<<blocks, 256, 0, st>>>(s, d, n_out, tw, alpha, a2);
-    else fold_kernel<false><<<blocks, 256, 0, st>>>(s, d, n_out, tw, alpha, a2);
+    if (circle) fold_kernel<true><<<blocks, 256, 0, st>>>(s, d, n_out, tw, alpha, a2, ad);
+    else fold_kernel<false><<<blocks, 256, 0, st>>>(s, d, n_out, tw, alpha, a2, ad);
     STWO_LAUNCH_CHECK("fold_kernel");
     return STWO_OK;
 }
@@ -149,22 +160,22 @@ extern "C" {
 
 int stwo_fold_line(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha, const uint32_t *itwiddles,
                    uint64_t twiddle_offset, uint32_t *const *dst4, void *stream) {
-    return fold_async(src4, n, alpha, itwiddles, twiddle_offset, dst4, false, as_stream(stream));
+    return fold_async(src4, n, alpha, itwiddles, twiddle_offset, dst4, false, as_stream(stream), nullptr);
 }
 
 int stwo_fold_circle_into_line(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha, const uint32_t *itwiddles,
                                uint64_t twiddle_offset, uint32_t *const *dst4, void *stream) {
-    return fold_async(src4, n, alpha, itwiddles, twiddle_offset, dst4, true, as_stream(stream));
+    return fold_async(src4, n, alpha, itwiddles, twiddle_offset, dst4, true, as_stream(stream), nullptr);
 }
 
 void fold_line(const uint32_t *gpu_domain, size_t twiddle_offset, size_t n, uint32_t *const *eval_values,
                stwo_qm31 alpha, uint32_t *const *folded_values) {
-    sync_default_stream(fold_async(eval_values, n, alpha, gpu_domain, twiddle_offset, folded_values, false, 0));
+    sync_default_stream(fold_async(eval_values, n, alpha, gpu_domain, twiddle_offset, folded_values, false, 0, nullptr));
 }
 
 void fold_circle_into_line(const uint32_t *gpu_domain, size_t twiddle_offset, size_t n, uint32_t *const *eval_values,
                            stwo_qm31 alpha, uint32_t *const *folded_values) {
-    sync_default_stream(fold_async(eval_values, n, alpha, gpu_domain, twiddle_offset, folded_values, true, 0));
+    sync_default_stream(fold_async(eval_values, n, alpha, gpu_domain, twiddle_offset, folded_values, true, 0, nullptr));
 }
 
 }  // extern "C"

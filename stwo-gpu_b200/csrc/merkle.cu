@@ -9,6 +9,8 @@
 // One thread per node; the 16-word message and the 16-word working state stay in
 // registers (the round permutation is resolved at compile time). Column reads are
 // coalesced across the threads of a warp (consecutive nodes, consecutive words).
+#include <algorithm>
+
 #include "blake2s.cuh"
 #include "common.cuh"
 
@@ -19,93 +21,130 @@ using blake::compress;
 
 constexpr int MERKLE_MAX_COLS = 2048;
 
+// Column pointers by value, in a parameter block sized to the call (a launch copies
+// its whole parameter block, so small calls use a small one).
+template <int CAP>
 struct MerkleCols {
-    const uint32_t *c[MERKLE_MAX_COLS];
+    const uint32_t *c[CAP];
 };
 
-// COLS_ON_DEVICE: column pointers come from a device array (reference ABI);
-// otherwise from the kernel parameter block.
-template <bool COLS_ON_DEVICE>
+// Hashes node i of a layer: children (if prev) then n_cols column words, 16 per
+// compression, the last chunk zero-padded.
+template <class ColAt>
+__device__ __forceinline__ void merkle_node(uint64_t i, const uint4 *prev, ColAt col_at, uint32_t n_cols, uint4 *out,
+                                            uint32_t one) {
+    uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t m[16];
+    if (prev) {
+        const uint4 *p = prev + 4 * i;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            uint4 v = p[q];
+            m[4 * q] = v.x; m[4 * q + 1] = v.y; m[4 * q + 2] = v.z; m[4 * q + 3] = v.w;
+        }
+        compress(h, m, one);
+    }
+    for (uint32_t c0 = 0; c0 < n_cols; c0 += 16) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            uint32_t cj = c0 + j;
+            m[j] = cj < n_cols ? __ldg(col_at(cj) + i) : 0u;
+        }
+        compress(h, m, one);
+    }
+    out[2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
+    out[2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+}
+
+// One layer, one thread per node. COLS_ON_DEVICE: column pointers come from a device
+// array (reference ABI); otherwise from the parameter block.
+template <bool COLS_ON_DEVICE, int CAP>
 __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, const uint4 *__restrict__ prev,
-                                                           const __grid_constant__ MerkleCols cols,
+                                                           const __grid_constant__ MerkleCols<CAP> cols,
                                                            const uint32_t *const *__restrict__ dev_cols,
                                                            uint32_t n_cols, uint4 *__restrict__ out, uint32_t one) {
     const uint64_t n = 1ull << log_size;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        uint32_t m[16];
-        if (prev) {
-            const uint4 *p = prev + 4 * i;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                uint4 v = __ldg(p + q);
-                m[4 * q] = v.x; m[4 * q + 1] = v.y; m[4 * q + 2] = v.z; m[4 * q + 3] = v.w;
-            }
-            compress(h, m, one);
-        }
-        for (uint32_t c0 = 0; c0 < n_cols; c0 += 16) {
-#pragma unroll
-            for (int j = 0; j < 16; j++) {
-                uint32_t cj = c0 + j;
-                const uint32_t *col = nullptr;
-                if (cj < n_cols) col = COLS_ON_DEVICE ? dev_cols[cj] : cols.c[cj];
-                m[j] = col ? __ldg(col + i) : 0u;
-            }
-            compress(h, m, one);
-        }
-        out[2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
-        out[2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+        if (COLS_ON_DEVICE)
+            merkle_node(i, prev, [&](uint32_t c) { return dev_cols[c]; }, n_cols, out, one);
+        else
+            merkle_node(i, prev, [&](uint32_t c) { return cols.c[c]; }, n_cols, out, one);
     }
 }
 
-// The column-free top of a tree in one launch of one CTA: layers top_log .. 0, each
-// node the compression of its two children. The children of layer top_log come from
-// `prev`; later layers read the layer this CTA wrote before the barrier.
-struct TopLayers {
-    uint4 *layer[32];  // layer[l]: 2^l nodes (2 uint4 each)
+// Up to 9 layers in one launch. CTA c owns nodes [c*256 >> j, (c+1)*256 >> j) of level
+// j (layer top_log - j): exactly the parents of the nodes it owned one level up, which
+// it wrote itself before the barrier. Level j hashes the children (absent on the leaf
+// layer) and the layer's columns (device pointer tables, one per level).
+constexpr int MERKLE_SUB_THREADS = 256;
+constexpr int MERKLE_SUB_LEVELS = 9;  // 256 nodes -> 1 node
+
+struct SubtreeParams {
+    uint4 *layer[32];                                   // layer[l]: 2^l nodes
+    const uint32_t *const *cols[MERKLE_SUB_LEVELS];     // device column tables per level
+    uint32_t n_cols[MERKLE_SUB_LEVELS];
+    uint32_t top_log, levels, has_prev;
 };
 
-constexpr int MERKLE_TOP_THREADS = 512;
-
-__global__ void __launch_bounds__(MERKLE_TOP_THREADS) merkle_top_kernel(const uint4 *prev,
-                                                                       const __grid_constant__ TopLayers t,
-                                                                       uint32_t top_log, uint32_t one) {
-    const uint4 *src = prev;
-    for (int l = (int)top_log; l >= 0; l--) {
-        uint4 *dst = t.layer[l];
-        for (uint32_t i = threadIdx.x; i < (1u << l); i += blockDim.x) {
-            uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            uint32_t m[16];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                uint4 v = src[4 * i + q];
-                m[4 * q] = v.x; m[4 * q + 1] = v.y; m[4 * q + 2] = v.z; m[4 * q + 3] = v.w;
-            }
-            compress(h, m, one);
-            dst[2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
-            dst[2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
-        }
-        __syncthreads();  // this layer's global writes are visible to the whole CTA
-        src = dst;
+__global__ void __launch_bounds__(MERKLE_SUB_THREADS) merkle_subtree_kernel(const __grid_constant__ SubtreeParams p,
+                                                                           uint32_t one) {
+    for (uint32_t j = 0; j < p.levels; j++) {
+        const uint32_t l = p.top_log - j;
+        const uint64_t per_cta = (uint64_t)MERKLE_SUB_THREADS >> j;
+        const uint64_t first = blockIdx.x * per_cta, n_l = 1ull << l;
+        const uint4 *prev = (j > 0 || p.has_prev) ? p.layer[l + 1] : nullptr;
+        const uint32_t *const *ct = p.cols[j];
+        for (uint64_t k = threadIdx.x; k < per_cta && first + k < n_l; k += blockDim.x)
+            merkle_node(first + k, prev, [&](uint32_t c) { return ct[c]; }, p.n_cols[j], p.layer[l], one);
+        __syncthreads();  // this level's global writes are visible to the whole CTA
     }
+}
+
+template <int CAP>
+void launch_layer(uint32_t log_size, const uint32_t *prev, const uint32_t *const *cols, uint32_t n_cols,
+                  bool cols_on_device, uint32_t *out, unsigned blocks, cudaStream_t st) {
+    MerkleCols<CAP> mc;  // parameter block (host stack)
+    if (!cols_on_device)
+        for (uint32_t i = 0; i < n_cols; i++) mc.c[i] = cols[i];
+    if (cols_on_device)
+        merkle_layer_kernel<true, CAP><<<blocks, 256, 0, st>>>(log_size, reinterpret_cast<const uint4 *>(prev), mc,
+                                                               cols, n_cols, reinterpret_cast<uint4 *>(out), 1u);
+    else
+        merkle_layer_kernel<false, CAP><<<blocks, 256, 0, st>>>(log_size, reinterpret_cast<const uint4 *>(prev), mc,
+                                                                nullptr, n_cols, reinterpret_cast<uint4 *>(out), 1u);
 }
 
 }  // namespace
 
-// Hashes layers prev_log-1 .. 0 of a tree whose layers (host array of device
-// pointers, indexed by log size) are all column-free below prev_log.
-int merkle_top_async(uint32_t prev_log, uint32_t *const *layers, cudaStream_t st) {
-    STWO_REQUIRE(prev_log >= 1 && prev_log <= 16, STWO_ERR_UNSUPPORTED_SIZE, "merkle top from log size %u", prev_log);
-    TopLayers t{};
-    for (uint32_t l = 0; l < prev_log; l++) {
-        t.layer[l] = reinterpret_cast<uint4 *>(layers[l]);
+// A whole tree whose per-layer columns are device pointer tables: level_cols[l],
+// level_ncols[l] for layer l (table may be null when the count is 0); layers[l] the
+// 2^l-node outputs. ceil((max_log + 1) / 9) launches.
+int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_cols, const uint32_t *level_ncols,
+                          uint32_t *const *layers, cudaStream_t st) {
+    STWO_REQUIRE(max_log <= 30, STWO_ERR_UNSUPPORTED_SIZE, "merkle tree of log size %u", max_log);
+    SubtreeParams p{};
+    for (uint32_t l = 0; l <= max_log; l++) {
+        p.layer[l] = reinterpret_cast<uint4 *>(layers[l]);
         STWO_REQUIRE(((uintptr_t)layers[l] & 15) == 0, STWO_ERR_INVALID_ARGUMENT, "hash buffers must be 16-byte aligned");
     }
-    STWO_REQUIRE(((uintptr_t)layers[prev_log] & 15) == 0, STWO_ERR_INVALID_ARGUMENT,
-                 "hash buffers must be 16-byte aligned");
-    merkle_top_kernel<<<1, MERKLE_TOP_THREADS, 0, st>>>(reinterpret_cast<const uint4 *>(layers[prev_log]), t,
-                                                         prev_log - 1, 1u);
-    STWO_LAUNCH_CHECK("merkle_top_kernel");
+    int top = (int)max_log;
+    while (top >= 0) {
+        const uint32_t levels = (uint32_t)std::min(top + 1, MERKLE_SUB_LEVELS);
+        p.top_log = (uint32_t)top;
+        p.levels = levels;
+        p.has_prev = top < (int)max_log;
+        for (uint32_t j = 0; j < levels; j++) {
+            p.cols[j] = level_cols[top - j];
+            p.n_cols[j] = level_ncols[top - j];
+        }
+        const uint64_t nodes = 1ull << top;
+        const uint64_t blocks = nodes > (uint64_t)MERKLE_SUB_THREADS ? nodes / MERKLE_SUB_THREADS : 1;
+        STWO_REQUIRE(levels == (uint32_t)MERKLE_SUB_LEVELS || blocks == 1, STWO_ERR_UNSUPPORTED_SIZE,
+                     "merkle subtree partition");
+        merkle_subtree_kernel<<<(unsigned)blocks, MERKLE_SUB_THREADS, 0, st>>>(p, 1u);
+        STWO_LAUNCH_CHECK("merkle_subtree_kernel");
+        top -= (int)levels;
+    }
     return STWO_OK;
 }
 
@@ -116,19 +155,13 @@ int merkle_layer_async(uint32_t log_size, const uint32_t *prev, const uint32_t *
                  "at most %d columns per merkle layer call", MERKLE_MAX_COLS);
     STWO_REQUIRE(((uintptr_t)out & 15) == 0 && ((uintptr_t)prev & 15) == 0, STWO_ERR_INVALID_ARGUMENT,
                  "hash buffers must be 16-byte aligned");
-    MerkleCols mc;  // parameter block (host stack)
-    if (!cols_on_device)
-        for (uint32_t i = 0; i < n_cols; i++) mc.c[i] = cols[i];
     uint64_t n = 1ull << log_size;
     uint64_t blocks = (n + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 16;
     if (blocks > cap) blocks = cap;
-    if (cols_on_device)
-        merkle_layer_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(log_size, reinterpret_cast<const uint4 *>(prev), mc,
-                                                                    cols, n_cols, reinterpret_cast<uint4 *>(out), 1u);
-    else
-        merkle_layer_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(log_size, reinterpret_cast<const uint4 *>(prev), mc,
-                                                                     nullptr, n_cols, reinterpret_cast<uint4 *>(out), 1u);
+    if (cols_on_device || n_cols <= 16) launch_layer<16>(log_size, prev, cols, n_cols, cols_on_device, out, (unsigned)blocks, st);
+    else if (n_cols <= 256) launch_layer<256>(log_size, prev, cols, n_cols, false, out, (unsigned)blocks, st);
+    else launch_layer<MERKLE_MAX_COLS>(log_size, prev, cols, n_cols, false, out, (unsigned)blocks, st);
     STWO_LAUNCH_CHECK("merkle_layer_kernel");
     return STWO_OK;
 }

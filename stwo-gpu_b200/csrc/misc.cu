@@ -37,9 +37,14 @@ __global__ void accumulate_kernel(const __grid_constant__ Acc4 p, uint64_t n4, u
 }
 
 constexpr int WF_MAX_COLS = 2048;
+constexpr int WF_PREFETCH = 8;  // column loads in flight per thread
 
+// Trace column pointers in the parameter block (CAP of them) or, for CAP == 1, in a
+// device table.
+template <int CAP>
 struct WideFibParams {
-    const uint32_t *trace[WF_MAX_COLS];
+    const uint32_t *trace[CAP];
+    const uint32_t *const *trace_dev;
     uint32_t *out[4];
     const uint32_t *den_inv;
     const qm31 *powers_dev;  // device powers
@@ -58,41 +63,52 @@ __device__ __forceinline__ uint32_t reduce64_wf(uint64_t x) {
 }
 
 // Powers on the device: plain QM31 (the reference ABI) or, when DOUBLED, with every
-// coordinate already doubled for m31_mul2.
-template <bool DOUBLED>
-__global__ void __launch_bounds__(256) wide_fib_kernel(const __grid_constant__ WideFibParams p) {
+// coordinate already doubled for m31_mul2. Four rows per thread; the column loop
+// issues WF_PREFETCH loads before it consumes them, so each thread keeps several
+// DRAM requests in flight instead of one.
+template <bool DOUBLED, int CAP>
+__global__ void __launch_bounds__(256) wide_fib_kernel(const __grid_constant__ WideFibParams<CAP> p) {
     const uint64_t n = 1ull << p.log_size;
     const uint64_t quads = (n + 3) / 4;
+    auto colp = [&](uint32_t c) { return CAP == 1 ? p.trace_dev[c] : p.trace[c]; };
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < quads; k += (uint64_t)gridDim.x * blockDim.x) {
         const bool full = 4 * k + 3 < n;
-        uint64_t acc[4][4] = {};
-        uint32_t c0[4], c1[4];
         auto load = [&](uint32_t col, uint32_t *v) {
+            const uint32_t *c = colp(col);
             if (full) {
-                uint4 t = __ldg(reinterpret_cast<const uint4 *>(p.trace[col]) + k);
+                uint4 t = __ldg(reinterpret_cast<const uint4 *>(c) + k);
                 v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
             } else {
-                for (int r = 0; r < 4; r++) v[r] = (4 * k + r < n) ? p.trace[col][4 * k + r] : 0u;
+                for (int r = 0; r < 4; r++) v[r] = (4 * k + r < n) ? c[4 * k + r] : 0u;
             }
         };
+        uint64_t acc[4][4] = {};
+        uint32_t c0[4], c1[4];
         load(0, c0);
         load(1, c1);
         uint32_t s0[4], s1[4];
         for (int r = 0; r < 4; r++) { s0[r] = m31_sqr(c0[r]); s1[r] = m31_sqr(c1[r]); }
-        for (uint32_t i = 0; i + 2 < p.n_cols; i++) {
-            uint32_t c2[4];
-            load(i + 2, c2);
-            qm31 w2 = p.powers_dev[p.n_cols - 3 - i];
-            if (!DOUBLED) w2 = {{w2.a.a << 1, w2.a.b << 1}, {w2.b.a << 1, w2.b.b << 1}};
+        for (uint32_t base = 2; base < p.n_cols; base += WF_PREFETCH) {
+            uint32_t buf[WF_PREFETCH][4];
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                uint32_t cons = m31_sub(m31_add(s0[r], s1[r]), c2[r]);
-                acc[r][0] += mul_lazy_wf(cons, w2.a.a);
-                acc[r][1] += mul_lazy_wf(cons, w2.a.b);
-                acc[r][2] += mul_lazy_wf(cons, w2.b.a);
-                acc[r][3] += mul_lazy_wf(cons, w2.b.b);
-                s0[r] = s1[r];
-                s1[r] = m31_sqr(c2[r]);
+            for (int u = 0; u < WF_PREFETCH; u++)
+                if (base + u < p.n_cols) load(base + u, buf[u]);
+#pragma unroll
+            for (int u = 0; u < WF_PREFETCH; u++) {
+                const uint32_t col = base + u;
+                if (col >= p.n_cols) break;
+                qm31 w2 = p.powers_dev[p.n_cols - 1 - col];  // constraint col - 2 takes powers[N-3-(col-2)]
+                if (!DOUBLED) w2 = {{w2.a.a << 1, w2.a.b << 1}, {w2.b.a << 1, w2.b.b << 1}};
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    uint32_t cons = m31_sub(m31_add(s0[r], s1[r]), buf[u][r]);
+                    acc[r][0] += mul_lazy_wf(cons, w2.a.a);
+                    acc[r][1] += mul_lazy_wf(cons, w2.a.b);
+                    acc[r][2] += mul_lazy_wf(cons, w2.b.a);
+                    acc[r][3] += mul_lazy_wf(cons, w2.b.b);
+                    s0[r] = s1[r];
+                    s1[r] = m31_sqr(buf[u][r]);
+                }
             }
         }
         uint32_t o[4][4];
@@ -108,6 +124,62 @@ __global__ void __launch_bounds__(256) wide_fib_kernel(const __grid_constant__ W
                     if (4 * k + r < n) p.out[c][4 * k + r] = o[c][r];
         }
     }
+}
+
+template <bool DOUBLED, int CAP>
+void launch_wf(const WideFibParams<CAP> &p, uint64_t quads, cudaStream_t st) {
+    // Small domains: 64-thread CTAs so that more SMs share the rows.
+    const uint32_t threads = quads < (uint64_t)device_sm_count() * 256 ? 64 : 256;
+    uint64_t blocks = (quads + threads - 1) / threads, cap = (uint64_t)device_sm_count() * 32;
+    if (blocks > cap) blocks = cap;
+    wide_fib_kernel<DOUBLED, CAP><<<(unsigned)blocks, threads, 0, st>>>(p);
+}
+
+template <int CAP>
+int wide_fib_launch(const uint32_t *const *trace, const uint32_t *const *trace_dev, uint32_t n_cols, uint32_t log_size,
+                    const stwo_qm31 *powers_host, const uint32_t *powers_dev, const uint32_t *den_inv,
+                    uint32_t *const *out4, cudaStream_t st) {
+    auto p = std::make_unique<WideFibParams<CAP>>();
+    if (CAP > 1)
+        for (uint32_t i = 0; i < n_cols; i++) {
+            p->trace[i] = trace[i];
+            STWO_REQUIRE(((uintptr_t)trace[i] & 15) == 0, STWO_ERR_INVALID_ARGUMENT,
+                         "trace columns must be 16-byte aligned");
+        }
+    p->trace_dev = trace_dev;
+    for (int c = 0; c < 4; c++) p->out[c] = out4[c];
+    p->den_inv = den_inv;
+    p->n_cols = n_cols;
+    p->log_size = log_size;
+    p->powers_dev = reinterpret_cast<const qm31 *>(powers_dev);
+    const uint64_t n = 1ull << log_size, quads = (n + 3) / 4;
+    if (powers_dev) {
+        launch_wf<false>(*p, quads, st);
+        STWO_LAUNCH_CHECK("wide_fib_kernel");
+        return STWO_OK;
+    }
+    // Host powers: staged, doubled, into a stream-ordered buffer private to this call,
+    // so concurrent calls on other streams never see each other's powers.
+    std::unique_ptr<qm31[]> w2(new qm31[n_cols - 2]);
+    for (uint32_t i = 0; i + 2 < n_cols; i++) {
+        stwo_qm31 v = powers_host[i];
+        w2[i] = {{v.a << 1, v.b << 1}, {v.c << 1, v.d << 1}};
+    }
+    void *buf = nullptr;
+    {
+        int arc = pool_alloc(&buf, sizeof(qm31) * (n_cols - 2), st);
+        if (arc) return arc;
+    }
+    cudaError_t e = cudaMemcpyAsync(buf, w2.get(), sizeof(qm31) * (n_cols - 2), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        p->powers_dev = static_cast<const qm31 *>(buf);
+        launch_wf<true>(*p, quads, st);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(buf, st);
+    if (e != cudaSuccess) return set_error(STWO_ERR_CUDA, "wide_fib_kernel: %s", cudaGetErrorString(e));
+    return STWO_OK;
 }
 
 }  // namespace
@@ -134,51 +206,24 @@ int wide_fib_async(const uint32_t *const *trace, uint32_t n_cols, uint32_t log_s
     STWO_REQUIRE(n_cols >= 2 && n_cols <= (uint32_t)WF_MAX_COLS, STWO_ERR_UNSUPPORTED_SIZE,
                  "wide-Fibonacci composition over %u columns", n_cols);
     STWO_REQUIRE(log_size <= 31, STWO_ERR_UNSUPPORTED_SIZE, "domain log size %u", log_size);
-    auto p = std::make_unique<WideFibParams>();
-    for (uint32_t i = 0; i < n_cols; i++) {
-        p->trace[i] = trace[i];
-        STWO_REQUIRE(((uintptr_t)trace[i] & 15) == 0, STWO_ERR_INVALID_ARGUMENT, "trace columns must be 16-byte aligned");
-    }
-    for (int c = 0; c < 4; c++) p->out[c] = out4[c];
-    p->den_inv = den_inv;
-    p->n_cols = n_cols;
-    p->log_size = log_size;
-    p->powers_dev = reinterpret_cast<const qm31 *>(powers_dev);
-    uint64_t n = 1ull << log_size, quads = (n + 3) / 4;
-    uint64_t blocks = (quads + 255) / 256, cap = (uint64_t)device_sm_count() * 8;
-    if (blocks > cap) blocks = cap;
     if (n_cols < 3) {
         // No constraints: the composition is zero.
-        for (int c = 0; c < 4; c++) STWO_CUDA_TRY(cudaMemsetAsync(out4[c], 0, n * 4, st));
+        for (int c = 0; c < 4; c++) STWO_CUDA_TRY(cudaMemsetAsync(out4[c], 0, 4ull << log_size, st));
         return STWO_OK;
     }
-    if (powers_dev) {
-        wide_fib_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(*p);
-        STWO_LAUNCH_CHECK("wide_fib_kernel");
-        return STWO_OK;
-    }
-    // Host powers: staged, doubled, into a stream-ordered buffer private to this call,
-    // so concurrent calls on other streams never see each other's powers.
-    std::unique_ptr<qm31[]> w2(new qm31[n_cols - 2]);
-    for (uint32_t i = 0; i + 2 < n_cols; i++) {
-        stwo_qm31 v = powers_host[i];
-        w2[i] = {{v.a << 1, v.b << 1}, {v.c << 1, v.d << 1}};
-    }
-    void *buf = nullptr;
-    {
-        int arc = pool_alloc(&buf, sizeof(qm31) * (n_cols - 2), st);
-        if (arc) return arc;
-    }
-    cudaError_t e = cudaMemcpyAsync(buf, w2.get(), sizeof(qm31) * (n_cols - 2), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) {
-        p->powers_dev = static_cast<const qm31 *>(buf);
-        wide_fib_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(*p);
-        count_launch();
-        e = cudaGetLastError();
-    }
-    cudaFreeAsync(buf, st);
-    if (e != cudaSuccess) return set_error(STWO_ERR_CUDA, "wide_fib_kernel: %s", cudaGetErrorString(e));
-    return STWO_OK;
+    if (n_cols <= 64)
+        return wide_fib_launch<64>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, out4, st);
+    if (n_cols <= 256)
+        return wide_fib_launch<256>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, out4, st);
+    return wide_fib_launch<WF_MAX_COLS>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, out4, st);
+}
+
+// Same, with the trace column pointers in a device table and the powers on the device.
+int wide_fib_dev_async(const uint32_t *const *trace_dev, uint32_t n_cols, uint32_t log_size, const uint32_t *powers_dev,
+                       const uint32_t *den_inv, uint32_t *const *out4, cudaStream_t st) {
+    STWO_REQUIRE(n_cols >= 3 && log_size <= 31 && powers_dev, STWO_ERR_UNSUPPORTED_SIZE,
+                 "wide-Fibonacci composition over %u columns", n_cols);
+    return wide_fib_launch<1>(nullptr, trace_dev, n_cols, log_size, nullptr, powers_dev, den_inv, out4, st);
 }
 
 }  // namespace stwo

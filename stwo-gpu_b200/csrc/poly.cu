@@ -114,15 +114,13 @@ __device__ __forceinline__ qm31 shfl_xor_q(qm31 v, int m) {
     return v;
 }
 
-__global__ void __launch_bounds__(EAP_THREADS) eval_at_point_kernel(const __grid_constant__ EapParams p) {
+// One CTA's share of polynomial `poly`: chunk `chunk` of its 2^L coefficients c with
+// factors f; its CTAs are blk_first .. blk_first + nblk - 1 (partials indexed by CTA).
+__device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t L, const qm31 *f, const uint32_t *c,
+                                         uint32_t blk_first, uint32_t nblk, qm31 *partials, uint32_t *tickets,
+                                         qm31 *results) {
     __shared__ qm31 warp_vals[EAP_THREADS / 32];
     __shared__ bool is_last;
-    uint32_t poly = 0;
-    while (poly + 1 < p.n_polys && blockIdx.x >= p.block_start[poly + 1]) poly++;
-    const uint32_t chunk = blockIdx.x - p.block_start[poly];
-    const uint32_t L = p.log_size[poly];
-    const qm31 *f = p.factors[poly];
-    const uint32_t *c = p.coeffs[poly];
     const uint32_t tid = threadIdx.x;
     const uint64_t n = 1ull << L;
     const uint64_t base = ((uint64_t)chunk << EAP_CHUNK_LOG) + ((uint64_t)tid << EAP_PER_THREAD_LOG);
@@ -167,26 +165,80 @@ __global__ void __launch_bounds__(EAP_THREADS) eval_at_point_kernel(const __grid
         // Chunk index bits -> factors 11.. .
         for (uint32_t b = 0; EAP_CHUNK_LOG + b < L; b++)
             if ((chunk >> b) & 1u) s = qm31_mul(s, f[EAP_CHUNK_LOG + b]);
-        p.partials[blockIdx.x] = s;
+        partials[blockIdx.x] = s;
         __threadfence();
-        uint32_t nblk = p.block_start[poly + 1] - p.block_start[poly];
-        uint32_t t = atomicAdd(&p.tickets[poly], 1u);
+        uint32_t t = atomicAdd(&tickets[poly], 1u);
         is_last = (t == nblk - 1);
     }
     __syncthreads();
-    if (is_last && tid == 0) {
+    if (is_last) {
+        // The whole last CTA sums the partials: strided per thread, then across lanes
+        // and warps (field addition, so the order does not change the sum).
         __threadfence();
         qm31 s = qm31_zero();
-        for (uint32_t b = p.block_start[poly]; b < p.block_start[poly + 1]; b++) {
+        for (uint32_t b = blk_first + tid; b < blk_first + nblk; b += EAP_THREADS) {
             qm31 v;
-            const volatile uint32_t *pv = reinterpret_cast<const volatile uint32_t *>(&p.partials[b]);
+            const volatile uint32_t *pv = reinterpret_cast<const volatile uint32_t *>(&partials[b]);
             v.a.a = pv[0]; v.a.b = pv[1]; v.b.a = pv[2]; v.b.b = pv[3];
             s = qm31_add(s, v);
         }
-        p.results[poly] = s;
-        p.tickets[poly] = 0;  // ready for the next launch
+#pragma unroll
+        for (int m = 16; m >= 1; m >>= 1) s = qm31_add(s, shfl_xor_q(s, m));
+        if (lane == 0) warp_vals[tid >> 5] = s;
+        __syncthreads();
+        if (tid == 0) {
+            qm31 t = qm31_zero();
+            for (int i = 0; i < EAP_THREADS / 32; i++) t = qm31_add(t, warp_vals[i]);
+            results[poly] = t;
+            tickets[poly] = 0;  // ready for the next launch
+        }
     }
 }
+
+__global__ void __launch_bounds__(EAP_THREADS) eval_at_point_kernel(const __grid_constant__ EapParams p) {
+    uint32_t poly = 0;
+    while (poly + 1 < p.n_polys && blockIdx.x >= p.block_start[poly + 1]) poly++;
+    eap_body(poly, blockIdx.x - p.block_start[poly], p.log_size[poly], p.factors[poly], p.coeffs[poly],
+             p.block_start[poly], p.block_start[poly + 1] - p.block_start[poly], p.partials, p.tickets, p.results);
+}
+
+// Polynomials described in device memory, all evaluated at one point also in device
+// memory (x then y); each CTA derives its polynomial's factors itself.
+struct EapDevPoly {
+    const uint32_t *coeffs;
+    uint32_t log_size;
+    uint32_t block_start;  // first CTA of the polynomial
+};
+
+__global__ void __launch_bounds__(EAP_THREADS) eval_at_point_dev_kernel(const EapDevPoly *__restrict__ polys,
+                                                                        uint32_t n_polys, const qm31 *point,
+                                                                        qm31 *partials, uint32_t *tickets,
+                                                                        qm31 *results) {
+    __shared__ qm31 f[32];
+    // the last polynomial whose first CTA is <= blockIdx.x
+    uint32_t lo = 0, hi = n_polys - 1;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) / 2;
+        if (polys[mid].block_start <= blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const EapDevPoly d = polys[lo];
+    const uint32_t next = lo + 1 < n_polys ? polys[lo + 1].block_start : gridDim.x;
+    if (threadIdx.x == 0) {
+        // f_0 = y, f_1 = x, f_b = pi^(b-1)(x)
+        f[0] = point[1];
+        qm31 x = point[0];
+        for (uint32_t b = 1; b < 32; b++) {
+            f[b] = x;
+            qm31 sq = qm31_mul(x, x);
+            x = qm31_sub(qm31_add(sq, sq), qm31_one());
+        }
+    }
+    __syncthreads();
+    eap_body(lo, blockIdx.x - d.block_start, d.log_size, f, d.coeffs, d.block_start, next - d.block_start, partials,
+             tickets, results);
+}
+
 
 inline qm31 to_q(stwo_qm31 v) { return {{v.a, v.b}, {v.c, v.d}}; }
 inline stwo_qm31 from_q(qm31 v) { return {v.a.a, v.a.b, v.b.a, v.b.b}; }
@@ -253,6 +305,21 @@ int eval_at_points_async(const uint32_t *const *coeffs, const uint32_t *log_size
     }
     return STWO_OK;
 }
+
+// eval_at_point for polynomials described in device memory (polys_dev: n_polys
+// EapDevPoly), at the device point point_dev (QM31 x then y). partials: total_blocks
+// QM31; tickets: n_polys zeroed words (left zeroed).
+int eval_at_points_dev_async(const void *polys_dev, uint32_t n_polys, uint32_t total_blocks, const void *point_dev,
+                             void *results, void *partials, uint32_t *tickets, cudaStream_t st) {
+    STWO_REQUIRE(n_polys >= 1 && total_blocks >= n_polys, STWO_ERR_INVALID_ARGUMENT, "eval_at_point descriptors");
+    eval_at_point_dev_kernel<<<total_blocks, EAP_THREADS, 0, st>>>(
+        static_cast<const EapDevPoly *>(polys_dev), n_polys, static_cast<const qm31 *>(point_dev),
+        static_cast<qm31 *>(partials), tickets, static_cast<qm31 *>(results));
+    STWO_LAUNCH_CHECK("eval_at_point_dev_kernel");
+    return STWO_OK;
+}
+
+uint32_t eval_at_point_blocks(uint32_t log_size) { return eap_blocks(log_size); }
 
 int extend_evaluate_async(const uint32_t *const *coeffs, const uint32_t *coeff_logs, uint32_t *const *outs,
                           uint32_t log_blowup, uint32_t n, const uint32_t *tw, uint64_t tree_size, cudaStream_t st) {

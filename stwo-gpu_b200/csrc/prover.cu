@@ -1,5 +1,6 @@
 // Wide-Fibonacci STARK prover: stwo's prove() for the wide-Fibonacci AIR, driven on
-// the host in C++ over this library's kernels.
+// the host in C++ over this library's kernels, with the Fiat-Shamir channel on the
+// device.
 //
 // The protocol is stwo's (stwo-prover @ ce5b975, as the reference drives it in
 // stwo_gpu_backend/src/examples/wide_fibonacci.rs:205-250 with PcsConfig::default()
@@ -20,11 +21,13 @@
 //   5. proof of work (least nonce with pow_bits trailing zeros), query positions,
 //      Merkle and FRI decommitments, gathered from device memory in one launch.
 //
-// Everything that touches column data runs on the GPU; the channel, the query
-// positions and the decommitted words live on the host. Each job runs on one stream
-// and synchronises only where the channel needs a device result (tree roots, sampled
-// values, the last FRI layer, the nonce, the gathered decommitment words), so jobs on
-// other streams fill the device meanwhile.
+// Steps 1-5 up to the query positions are one asynchronous sequence of launches on the
+// job's stream: the channel (channel.cuh) runs in single-thread kernels between the
+// data kernels and leaves every challenge in device memory, where the next kernel
+// reads it. The host synchronises twice per proof: to read the channel's record (roots,
+// sampled values, last layer, nonce, query words) and to read the decommitted words.
+// All of a job's buffers, column-pointer tables and kernel parameters that depend on
+// the channel live in one slab from the library's memory pool.
 //
 // The proof bytes are the CommitmentSchemeProof fields in declaration order, little
 // endian, vectors prefixed with a u64 length, hashes as 32 raw bytes, field elements as
@@ -32,7 +35,6 @@
 //   commitments, sampled_values, decommitments, queried_values, proof_of_work,
 //   fri_proof{first_layer, inner_layers, last_layer_poly{coeffs, log_size}}.
 #include <algorithm>
-#include <array>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
@@ -42,55 +44,72 @@
 #include <vector>
 
 #include "blake2s.cuh"
-#include "blake2s_host.h"
+#include "channel.cuh"
 #include "common.cuh"
+#include "quotients.cuh"
 
 namespace stwo {
 
 int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
                 const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st);
-int merkle_layer_async(uint32_t log_size, const uint32_t *prev, const uint32_t *const *cols, uint32_t n_cols,
-                       bool cols_on_device, uint32_t *out, cudaStream_t st);
-int merkle_top_async(uint32_t prev_log, uint32_t *const *layers, cudaStream_t st);
-int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, const uint32_t *const *cols,
-                    uint32_t n_cols, bool cols_on_device, stwo_qm31 rc_c, const stwo_spoint *pts, const uint32_t *bsz,
-                    const uint32_t *cidx, const stwo_qm31 *vals, uint32_t n_batches, uint32_t *const *out4,
-                    cudaStream_t st);
+int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_cols, const uint32_t *level_ncols,
+                          uint32_t *const *layers, cudaStream_t st);
 int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const uint32_t *itw, uint64_t off,
-               uint32_t *const *dst4, bool circle, cudaStream_t st);
-int wide_fib_async(const uint32_t *const *trace, uint32_t n_cols, uint32_t log_size, const stwo_qm31 *powers_host,
-                   const uint32_t *powers_dev, const uint32_t *den_inv, uint32_t *const *out4, cudaStream_t st);
+               uint32_t *const *dst4, bool circle, cudaStream_t st, const void *alpha_dev);
+int wide_fib_dev_async(const uint32_t *const *trace_dev, uint32_t n_cols, uint32_t log_size, const uint32_t *powers_dev,
+                       const uint32_t *den_inv, uint32_t *const *out4, cudaStream_t st);
 int batch_inverse_m31_async(const uint32_t *src, uint32_t *dst, uint64_t n, cudaStream_t st);
-size_t eval_at_points_scratch_bytes(const uint32_t *log_sizes, uint32_t n_polys);
-int eval_at_points_async(const uint32_t *const *coeffs, const uint32_t *log_sizes, uint32_t n_polys,
-                         const stwo_spoint *points, stwo_qm31 *results, void *scratch, size_t scratch_bytes,
-                         bool tickets_zeroed, cudaStream_t st);
+int eval_at_points_dev_async(const void *polys_dev, uint32_t n_polys, uint32_t total_blocks, const void *point_dev,
+                             void *results, void *partials, uint32_t *tickets, cudaStream_t st);
+uint32_t eval_at_point_blocks(uint32_t log_size);
 
 namespace {
 
 constexpr uint32_t WF_MAX_TRACE_COLS = 1024;
 constexpr uint32_t MAX_DOMAIN_LOG = 27;  // largest committed domain CanonicCoset(L+1+B)
+constexpr uint32_t MAX_LAYERS = 32;      // FRI inner layers
+constexpr uint32_t MAX_QUERIES = 1024;
+
+// ------------------------------------------------------------------ device state
+
+// What the device channel records for the host: the tree roots in commitment order
+// (trace, composition, FRI first layer, FRI inner layers), the challenges, the last
+// layer, the nonce and the raw query words. The sampled values follow it in memory.
+struct ProofState {
+    fs::DevChannel ch;
+    uint32_t error;
+    uint32_t pad;
+    unsigned long long nonce;  // least valid proof-of-work nonce (all ones: none yet)
+    qm31 rc, qrc, last_coeff;
+    qm31 oods[2];  // x, y
+    qm31 alphas[MAX_LAYERS + 1];
+    uint32_t roots[MAX_LAYERS + 3][8];
+    uint32_t query_words[MAX_QUERIES];
+};
+
+// The polynomial descriptors of the OODS evaluation (eval_at_points_dev_async).
+struct EapDevPoly {
+    const uint32_t *coeffs;
+    uint32_t log_size;
+    uint32_t block_start;
+};
 
 // ------------------------------------------------------------------ device kernels
 
 // Trace rows (write_trace_row, wide_fibonacci.rs:196-203): a_0 = a0[r], a_1 = a1[r],
 // a_{j+2} = a_j^2 + a_{j+1}^2. Row r is position r of every column, the bit-reversed
-// storage order of the trace evaluations.
-struct TraceCols {
-    uint32_t *c[WF_MAX_TRACE_COLS];
-};
-
+// storage order of the trace evaluations. Column pointers come from a device table.
 __global__ void __launch_bounds__(256) wide_fib_trace_kernel(const uint32_t *__restrict__ a0,
                                                              const uint32_t *__restrict__ a1,
-                                                             const __grid_constant__ TraceCols t, uint32_t n_cols,
+                                                             uint32_t *const *__restrict__ cols, uint32_t n_cols,
                                                              uint64_t rows) {
     for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t x = a0[r], y = a1[r];
-        t.c[0][r] = x;
-        t.c[1][r] = y;
+        cols[0][r] = x;
+        cols[1][r] = y;
         for (uint32_t j = 2; j < n_cols; j++) {
             uint32_t z = m31_add(m31_sqr(x), m31_sqr(y));
-            t.c[j][r] = z;
+            cols[j][r] = z;
             x = y;
             y = z;
         }
@@ -127,6 +146,167 @@ __global__ void __launch_bounds__(256) vanishing_kernel(uint32_t *__restrict__ o
     }
 }
 
+// Channel step after the trace tree: mix its root, draw the composition coefficient r,
+// and write powers[k] = r^k (k < n_powers; lane l computes k = l, l + 32, ...).
+__global__ void fs_trace_kernel(ProofState *s, const uint32_t *root, qm31 *powers, uint32_t n_powers) {
+    __shared__ qm31 rc;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 8; i++) s->roots[0][i] = root[i];
+        fs::ch_mix_root(s->ch, root);
+        rc = fs::ch_draw_felt(s->ch, s->error);
+        s->rc = rc;
+    }
+    __syncthreads();
+    const qm31 r = rc;
+    qm31 p = qm31_pow(r, threadIdx.x);
+    const qm31 step = qm31_pow(r, blockDim.x);
+    for (uint32_t k = threadIdx.x; k < n_powers; k += blockDim.x) {
+        powers[k] = p;
+        p = qm31_mul(p, step);
+    }
+}
+
+// Channel step after the composition tree: mix its root, draw t and take the OODS
+// point (CirclePoint::get_random_point): x = (1 - t^2) / (1 + t^2), y = 2t / (1 + t^2).
+__global__ void fs_comp_kernel(ProofState *s, const uint32_t *root) {
+    for (int i = 0; i < 8; i++) s->roots[1][i] = root[i];
+    fs::ch_mix_root(s->ch, root);
+    const qm31 t = fs::ch_draw_felt(s->ch, s->error), t2 = qm31_mul(t, t);
+    const qm31 inv = qm31_inv(qm31_add(t2, qm31_one()));
+    s->oods[0] = qm31_mul(qm31_sub(qm31_one(), t2), inv);
+    s->oods[1] = qm31_mul(qm31_add(t, t), inv);
+}
+
+// -initial + step/2 of CanonicCoset(log).coset (initial index 2^(30-log), step 2^(31-log)).
+__host__ __device__ inline cpoint vanishing_shift(uint32_t log) {
+    cpoint init = index_to_point(1u << (30 - log));
+    cpoint half_step = index_to_point(1u << (30 - log));
+    return point_mul(point_conj(init), half_step);
+}
+
+// Channel step after the OODS evaluation: mix the sampled values (N trace values, then
+// the composition's 4 coordinates), check the composition against the constraints at
+// the OODS point, draw the quotient coefficient and fill the quotient kernels'
+// sample-dependent parameters of both column groups.
+__global__ void fs_oods_kernel(ProofState *s, const qm31 *sampled, uint32_t N, uint32_t L, QuotParamsDev *q_comp,
+                               QuotParamsDev *q_trace) {
+    fs::ch_mix_felts(s->ch, sampled, N + 4);
+    // composition value: from_partial_evals over the basis 1, i, u, iu
+    const qm31 basis[4] = {{{1, 0}, {0, 0}}, {{0, 1}, {0, 0}}, {{0, 0}, {1, 0}}, {{0, 0}, {0, 1}}};
+    qm31 comp = qm31_zero();
+    for (int k = 0; k < 4; k++) comp = qm31_add(comp, qm31_mul(sampled[N + k], basis[k]));
+    // constraints: sum_i r^(N-3-i) (c_i^2 + c_{i+1}^2 - c_{i+2}) / coset_vanishing(oods)
+    const cpoint sh = vanishing_shift(L);
+    const qm31 ox = s->oods[0], oy = s->oods[1];
+    qm31 x = qm31_sub(qm31_scale(ox, sh.x), qm31_scale(oy, sh.y));
+    for (uint32_t d = 0; d + 1 < L; d++) {
+        qm31 q = qm31_mul(x, x);
+        x = qm31_sub(qm31_add(q, q), qm31_one());
+    }
+    qm31 acc = qm31_zero();
+    for (uint32_t i = 0; i + 2 < N; i++) {
+        qm31 cons = qm31_sub(qm31_add(qm31_mul(sampled[i], sampled[i]), qm31_mul(sampled[i + 1], sampled[i + 1])),
+                             sampled[i + 2]);
+        acc = qm31_add(qm31_mul(acc, s->rc), cons);
+    }
+    if (!qm31_eq(qm31_mul(acc, qm31_inv(x)), comp)) s->error |= fs::ERR_CONSTRAINTS;
+    const qm31 qrc = fs::ch_draw_felt(s->ch, s->error);
+    s->qrc = qrc;
+    quot_fill_batch(*q_comp, 0, qrc, ox, oy, sampled + N, 4, 0);
+    quot_fill_batch(*q_trace, 0, qrc, ox, oy, sampled, N, 0);
+}
+
+// Channel step after an FRI tree: mix its root, draw the folding alpha.
+__global__ void fs_layer_kernel(ProofState *s, const uint32_t *root, uint32_t root_slot, uint32_t alpha_slot) {
+    for (int i = 0; i < 8; i++) s->roots[root_slot][i] = root[i];
+    fs::ch_mix_root(s->ch, root);
+    s->alphas[alpha_slot] = fs::ch_draw_felt(s->ch, s->error);
+}
+
+// Last FRI layer: 2^log values (bit-reversed) over the line domain
+// Coset(2^(29-log), 2^(31-log)) interpolated (LineEvaluation::interpolate); every
+// coefficient but the constant must vanish (degree bound 1); the constant is mixed.
+struct Cols4c {
+    const uint32_t *c[4];
+};
+
+__global__ void fs_last_kernel(ProofState *s, const __grid_constant__ Cols4c cur, uint32_t log) {
+    const uint32_t n = 1u << log;  // log <= 4
+    qm31 v[16];
+    for (uint32_t i = 0; i < n; i++)
+        v[bit_reverse_bits(i, log)] = {{cur.c[0][i], cur.c[1][i]}, {cur.c[2][i], cur.c[3][i]}};
+    uint32_t di = 1u << (29 - log), ds = 1u << (31 - log);
+    for (uint32_t size = n; size > 1; size >>= 1) {
+        for (uint32_t c = 0; c < n; c += size)
+            for (uint32_t i = 0; i < size / 2; i++) {
+                const uint32_t xi = m31_inv(index_to_point((di + ds * i) & 0x7fffffffu).x);
+                const qm31 a = v[c + i], b = v[c + i + size / 2];
+                v[c + i] = qm31_add(a, b);
+                v[c + i + size / 2] = qm31_scale(qm31_sub(a, b), xi);
+            }
+        di = (di * 2) & 0x7fffffffu;
+        ds = (ds * 2) & 0x7fffffffu;
+    }
+    const uint32_t ninv = m31_inv(n);
+    for (uint32_t i = 1; i < n; i++)  // any non-constant coefficient (storage order is irrelevant here)
+        if (!qm31_eq(v[i], qm31_zero())) s->error |= fs::ERR_LAST_LAYER;
+    const qm31 c0 = qm31_scale(v[0], ninv);
+    s->last_coeff = c0;
+    fs::ch_mix_felts(s->ch, &c0, 1);
+}
+
+// Proof-of-work search (GrindOps::grind): nonce k is valid when the digest mixed with k
+// (one compression of the digest with message [lo(k), hi(k), 0...]) has at least
+// pow_bits trailing zero bits as a little-endian u128. Thread t tries t, t + G, t + 2G ...
+// (G = grid size) and stops once its next nonce is not below the least valid nonce
+// found so far, so the result is the least valid nonce below max_k * G.
+__device__ __forceinline__ uint32_t ctz128(const uint32_t w[4]) {
+    if (w[0]) return __ffs(w[0]) - 1;
+    if (w[1]) return 32 + __ffs(w[1]) - 1;
+    if (w[2]) return 64 + __ffs(w[2]) - 1;
+    if (w[3]) return 96 + __ffs(w[3]) - 1;
+    return 128;
+}
+
+__global__ void __launch_bounds__(256) grind_kernel(ProofState *s, uint32_t pow_bits, uint64_t max_k) {
+    const uint32_t one = 1;
+    uint32_t d[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) d[i] = s->ch.digest[i];
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    volatile unsigned long long *best = &s->nonce;
+    for (uint64_t k = 0; k < max_k; k++) {
+        const uint64_t nonce = t + k * stride;
+        if (nonce >= *best) return;
+        uint32_t h[8], m[16] = {0};
+#pragma unroll
+        for (int i = 0; i < 8; i++) h[i] = d[i];
+        m[0] = (uint32_t)nonce;
+        m[1] = (uint32_t)(nonce >> 32);
+        blake::compress(h, m, one);
+        if (ctz128(h) >= pow_bits) {
+            atomicMin(&s->nonce, (unsigned long long)nonce);
+            return;
+        }
+    }
+}
+
+// After the search: mix the nonce and draw the raw query words (Queries::generate takes
+// each u32 masked to the largest domain's log size).
+__global__ void fs_finish_kernel(ProofState *s, uint32_t n_queries) {
+    if (s->nonce == ~0ull) {
+        s->error |= fs::ERR_GRIND;
+        return;
+    }
+    fs::ch_mix_nonce(s->ch, s->nonce);
+    for (uint32_t q = 0; q < n_queries; q += 8) {
+        uint32_t w[8];
+        fs::ch_draw_words(s->ch, w);
+        for (uint32_t i = 0; i < 8 && q + i < n_queries; i++) s->query_words[q + i] = w[i];
+    }
+}
+
 // Reads of single words from device buffers (decommitment values and witnesses).
 struct GatherReq {
     const uint32_t *ptr;
@@ -138,66 +318,48 @@ __global__ void gather_kernel(const GatherReq *__restrict__ req, uint32_t n, uin
     if (i < n) out[i] = req[i].ptr[req[i].idx];
 }
 
-// Proof-of-work search (GrindOps::grind): nonce k is valid when the channel digest
-// mixed with k (one BLAKE2s compression of the digest with message [lo(k), hi(k), 0...])
-// has at least pow_bits trailing zero bits as a little-endian u128. Thread t tries the
-// nonces base + t + k * (grid size), k < per_thread, and records the least valid one.
-struct GrindParams {
-    uint32_t h[8];
-    uint32_t pow_bits;
-};
-
-__device__ __forceinline__ uint32_t ctz128(const uint32_t w[4]) {
-    if (w[0]) return __ffs(w[0]) - 1;
-    if (w[1]) return 32 + __ffs(w[1]) - 1;
-    if (w[2]) return 64 + __ffs(w[2]) - 1;
-    if (w[3]) return 96 + __ffs(w[3]) - 1;
-    return 128;
-}
-
-__global__ void __launch_bounds__(256) grind_kernel(const GrindParams p, uint64_t base, uint32_t per_thread,
-                                                    unsigned long long *__restrict__ best) {
-    const uint32_t one = 1;
-    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint32_t k = 0; k < per_thread; k++) {
-        const uint64_t nonce = base + t + k * stride;
-        uint32_t h[8], m[16] = {0};
-#pragma unroll
-        for (int i = 0; i < 8; i++) h[i] = p.h[i];
-        m[0] = (uint32_t)nonce;
-        m[1] = (uint32_t)(nonce >> 32);
-        blake::compress(h, m, one);
-        if (ctz128(h) >= p.pow_bits) {
-            atomicMin(best, (unsigned long long)nonce);
-            return;
-        }
-    }
-}
-
 // ------------------------------------------------------------------ host plumbing
 
 double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-// Stream-ordered device allocations of one job, all released when the job ends.
+// Stream-ordered device memory of one job: one slab from the library pool, sized by
+// the job's bound and carved with a bump pointer (256-byte aligned), so a proof costs
+// one pool allocation and one free; anything past the slab gets its own allocation.
+// All of it is released, stream-ordered, when the job ends.
 struct Arena {
     cudaStream_t st;
-    std::vector<void *> ptrs;
+    uint8_t *slab = nullptr;
+    uint64_t cap = 0, used = 0;
+    std::vector<void *> extra;
     uint64_t bytes = 0;
     explicit Arena(cudaStream_t s) : st(s) {}
     ~Arena() {
-        for (void *p : ptrs) cudaFreeAsync(p, st);
+        if (slab) cudaFreeAsync(slab, st);
+        for (void *p : extra) cudaFreeAsync(p, st);
+    }
+    int reserve(uint64_t b) {
+        void *p = nullptr;
+        int rc = pool_alloc(&p, b, st);
+        if (rc) return rc;
+        slab = static_cast<uint8_t *>(p);
+        cap = b;
+        return STWO_OK;
     }
     template <typename T = uint32_t>
     T *alloc(size_t count) {
-        void *p = nullptr;
         size_t b = std::max<size_t>(count * sizeof(T), 16);
         b = (b + 255) & ~size_t(255);
-        if (pool_alloc(&p, b, st) != STWO_OK) return nullptr;
-        ptrs.push_back(p);
         bytes += b;
+        if (slab && used + b <= cap) {
+            void *p = slab + used;
+            used += b;
+            return static_cast<T *>(p);
+        }
+        void *p = nullptr;
+        if (pool_alloc(&p, b, st) != STWO_OK) return nullptr;
+        extra.push_back(p);
         return static_cast<T *>(p);
     }
 };
@@ -212,125 +374,56 @@ struct Arena {
         if (_rc) return _rc;      \
     } while (0)
 
-inline qm31 to_q(stwo_qm31 v) { return {{v.a, v.b}, {v.c, v.d}}; }
-inline stwo_qm31 from_q(qm31 v) { return {v.a.a, v.a.b, v.b.a, v.b.b}; }
-
 // Half coset {initial index, step index} of CanonicCoset(log).circle_domain().
 inline uint32_t half_coset_init(uint32_t log) { return 1u << (30 - log); }
 inline uint32_t half_coset_step(uint32_t log) { return (uint32_t)((1ull << (32 - log)) & 0x7fffffffu); }
 
-// Blake2sChannel (stwo core/channel/blake2s.rs): a 32-byte digest, the number of
-// digest updates and the number of draws since the last update.
-struct Channel {
-    uint8_t digest[32] = {0};
-    uint64_t n_challenges = 0, n_sent = 0;
-
-    void update(const uint8_t d[32]) {
-        memcpy(digest, d, 32);
-        n_challenges++;
-        n_sent = 0;
+// Host image of device data uploaded in one copy: blobs appended at 256-byte aligned
+// offsets of a device region whose address is known once the image is complete.
+struct Upload {
+    std::vector<uint8_t> host;
+    size_t add(const void *p, size_t n) {
+        size_t off = (host.size() + 255) & ~size_t(255);
+        host.resize(off + n);
+        if (p) memcpy(host.data() + off, p, n);
+        else memset(host.data() + off, 0, n);
+        return off;
     }
-    // Blake2sMerkleChannel::mix_root: digest = H(digest || root).
-    void mix_root(const uint8_t root[32]) {
-        uint8_t buf[64], out[32];
-        memcpy(buf, digest, 32);
-        memcpy(buf + 32, root, 32);
-        host_blake2s::hash(buf, 64, out);
-        update(out);
-    }
-    // digest = H(digest || felts as u32 LE words).
-    void mix_felts(const std::vector<qm31> &f) {
-        std::vector<uint8_t> buf(32 + 16 * f.size());
-        memcpy(buf.data(), digest, 32);
-        for (size_t i = 0; i < f.size(); i++) {
-            uint32_t w[4] = {f[i].a.a, f[i].a.b, f[i].b.a, f[i].b.b};
-            memcpy(buf.data() + 32 + 16 * i, w, 16);
-        }
-        uint8_t out[32];
-        host_blake2s::hash(buf.data(), buf.size(), out);
-        update(out);
-    }
-    // digest = compress(digest as chaining state, [lo, hi, 0, ...]) with zero counter and flags.
-    void mix_nonce(uint64_t nonce) {
-        uint32_t h[8], m[16] = {0};
-        memcpy(h, digest, 32);
-        m[0] = (uint32_t)nonce;
-        m[1] = (uint32_t)(nonce >> 32);
-        host_blake2s::compress(h, m, 0, 0);
-        uint8_t out[32];
-        memcpy(out, h, 32);
-        update(out);
-    }
-    // H(digest || n_sent as u64 LE, zero-padded to 32 bytes).
-    void draw_random_bytes(uint8_t out[32]) {
-        uint8_t buf[64] = {0};
-        memcpy(buf, digest, 32);
-        memcpy(buf + 32, &n_sent, 8);
-        n_sent++;
-        host_blake2s::hash(buf, 64, out);
-    }
-    // Eight base field elements; redrawn until every u32 is below 2P.
-    void draw_base_felts(uint32_t f[8]) {
-        for (;;) {
-            uint8_t b[32];
-            draw_random_bytes(b);
-            uint32_t u[8];
-            memcpy(u, b, 32);
-            bool ok = true;
-            for (int i = 0; i < 8; i++) ok = ok && u[i] < 2 * P;
-            if (!ok) continue;
-            for (int i = 0; i < 8; i++) f[i] = u[i] >= P ? u[i] - P : u[i];
-            return;
-        }
-    }
-    qm31 draw_felt() {
-        uint32_t f[8];
-        draw_base_felts(f);
-        return {{f[0], f[1]}, {f[2], f[3]}};
+    template <class T>
+    T *at(size_t off) {
+        return reinterpret_cast<T *>(host.data() + off);
     }
 };
 
-// Merkle tree of columns of power-of-two sizes (MerkleProver::commit): the columns in
-// decreasing size order (stable); layer l hashes the children (below the top) and the
-// columns of size 2^l. All layers stay on the device for decommitment.
+// A Merkle tree whose columns are given per layer: the host keeps the layer buffers,
+// the columns (for decommitment) and the device tables the tree kernel reads.
 struct MerkleTree {
     std::vector<uint32_t *> layers;  // layers[l]: 2^l nodes of 8 words
-    std::vector<std::pair<uint32_t, const uint32_t *>> cols;
+    std::vector<std::pair<uint32_t, const uint32_t *>> cols;  // (log size, column), decreasing size, stable
+    std::vector<const uint32_t *const *> level_tables;        // device column table per layer
+    std::vector<uint32_t> level_n;
+    std::vector<std::pair<size_t, uint32_t>> table_offsets;   // (image offset, layer) of each table
     uint32_t max_log = 0;
-    uint8_t root[32];
 };
 
-// Layers of at most 2^MERKLE_TOP_LOG nodes that hash children only are hashed by one
-// single-CTA launch.
-constexpr uint32_t MERKLE_TOP_LOG = 10;
-
-int commit_tree(MerkleTree &t, std::vector<std::pair<uint32_t, const uint32_t *>> cols, Arena &ar,
-                cudaStream_t st) {
+int plan_tree(MerkleTree &t, std::vector<std::pair<uint32_t, const uint32_t *>> cols, Arena &ar, Upload &up) {
     std::stable_sort(cols.begin(), cols.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
     t.cols = cols;
     t.max_log = cols[0].first;
-    const uint32_t min_col_log = cols.back().first;
     t.layers.assign(t.max_log + 1, nullptr);
+    t.level_tables.assign(t.max_log + 1, nullptr);
+    t.level_n.assign(t.max_log + 1, 0);
     for (int l = (int)t.max_log; l >= 0; l--) {
         PV_ALLOC(layer, uint32_t, (size_t)8 << l);
         t.layers[l] = layer;
-    }
-    for (int l = (int)t.max_log; l >= 0; l--) {
-        if ((uint32_t)l < min_col_log && (uint32_t)l <= MERKLE_TOP_LOG) {
-            PV_TRY(merkle_top_async((uint32_t)l + 1, t.layers.data(), st));  // layers l .. 0
-            break;
-        }
         std::vector<const uint32_t *> lc;
         for (auto &c : cols)
             if (c.first == (uint32_t)l) lc.push_back(c.second);
-        const uint32_t *prev = l < (int)t.max_log ? t.layers[l + 1] : nullptr;
-        PV_TRY(merkle_layer_async((uint32_t)l, prev, lc.data(), (uint32_t)lc.size(), false, t.layers[l], st));
+        if (!lc.empty()) {
+            t.table_offsets.push_back({up.add(lc.data(), lc.size() * sizeof(void *)), (uint32_t)l});
+            t.level_n[l] = (uint32_t)lc.size();
+        }
     }
-    void *stage = nullptr;
-    PV_TRY(host_stage(32, &stage));
-    STWO_CUDA_TRY(cudaMemcpyAsync(stage, t.layers[0], 32, cudaMemcpyDeviceToHost, st));
-    PV_TRY(wait_stream(st));
-    memcpy(t.root, stage, 32);
     return STWO_OK;
 }
 
@@ -411,7 +504,7 @@ struct Writer {
     std::vector<uint8_t> b;
     void u32(uint32_t v) { b.insert(b.end(), (uint8_t *)&v, (uint8_t *)&v + 4); }
     void u64(uint64_t v) { b.insert(b.end(), (uint8_t *)&v, (uint8_t *)&v + 8); }
-    void bytes(const uint8_t *p, size_t n) { b.insert(b.end(), p, p + n); }
+    void bytes(const void *p, size_t n) { b.insert(b.end(), (const uint8_t *)p, (const uint8_t *)p + n); }
     void q(qm31 v) {
         u32(v.a.a);
         u32(v.a.b);
@@ -457,46 +550,6 @@ void fri_positions(const std::vector<uint64_t> &queries, std::vector<uint64_t> &
     }
 }
 
-// LineEvaluation::interpolate of the last FRI layer (2^log values in bit-reversed order
-// over the line domain Coset(init, step, log)); coefficients in natural order.
-std::vector<qm31> interpolate_line(const std::vector<qm31> &evals, uint32_t init, uint32_t step, uint32_t log) {
-    const size_t n = evals.size();
-    std::vector<qm31> v(n);
-    for (size_t i = 0; i < n; i++) v[bit_reverse_bits((uint32_t)i, log)] = evals[i];
-    uint32_t di = init, ds = step;
-    for (size_t size = n; size > 1; size >>= 1) {
-        for (size_t c = 0; c < n; c += size)
-            for (size_t i = 0; i < size / 2; i++) {
-                const uint32_t x = index_to_point((uint32_t)((di + (uint64_t)ds * i) & 0x7fffffffu)).x;
-                const uint32_t xi = m31_inv(x);
-                qm31 a = v[c + i], b = v[c + i + size / 2];
-                v[c + i] = qm31_add(a, b);
-                v[c + i + size / 2] = qm31_scale(qm31_sub(a, b), xi);
-            }
-        di = (di * 2) & 0x7fffffffu;
-        ds = (ds * 2) & 0x7fffffffu;
-    }
-    const uint32_t ninv = m31_inv((uint32_t)n);
-    std::vector<qm31> coeffs(n);  // bit-reversed (LinePoly storage) -> natural order
-    for (size_t i = 0; i < n; i++) coeffs[bit_reverse_bits((uint32_t)i, log)] = qm31_scale(v[i], ninv);
-    return coeffs;
-}
-
-// Circle point over QM31 and its group operation with a base-field point.
-struct qpoint {
-    qm31 x, y;
-};
-inline qpoint qpoint_mul_base(qpoint p, cpoint s) {
-    return {qm31_sub(qm31_scale(p.x, s.x), qm31_scale(p.y, s.y)), qm31_add(qm31_scale(p.x, s.y), qm31_scale(p.y, s.x))};
-}
-
-// -initial + step/2 of CanonicCoset(log).coset (initial index 2^(30-log), step 2^(31-log)).
-cpoint vanishing_shift(uint32_t log) {
-    cpoint init = index_to_point(1u << (30 - log));
-    cpoint half_step = index_to_point(1u << (30 - log));
-    return point_mul(point_conj(init), half_step);
-}
-
 struct Job {
     uint32_t L, N, B, n_queries, pow_bits;
 };
@@ -507,7 +560,7 @@ int validate(const Job &j) {
     STWO_REQUIRE(j.B >= 1 && j.B <= 4, STWO_ERR_UNSUPPORTED_SIZE, "log blowup %u unsupported (1..4)", j.B);
     STWO_REQUIRE(j.L >= 2 && j.L + 1 + j.B <= MAX_DOMAIN_LOG, STWO_ERR_UNSUPPORTED_SIZE,
                  "trace log size %u with log blowup %u unsupported", j.L, j.B);
-    STWO_REQUIRE(j.n_queries >= 1 && j.n_queries <= 1024, STWO_ERR_UNSUPPORTED_SIZE, "%u queries unsupported",
+    STWO_REQUIRE(j.n_queries >= 1 && j.n_queries <= MAX_QUERIES, STWO_ERR_UNSUPPORTED_SIZE, "%u queries unsupported",
                  j.n_queries);
     STWO_REQUIRE(j.pow_bits <= 40, STWO_ERR_UNSUPPORTED_SIZE, "pow_bits %u unsupported (0..40)", j.pow_bits);
     return STWO_OK;
@@ -529,63 +582,198 @@ uint64_t job_device_bytes(const Job &j, bool own_twiddles) {
     if (j.B > 1) b += j.N * r(4 * ne);                    // trace on the composition domain
     b += tree(j.L + j.B) + tree(j.L + 1 + j.B);           // trace and composition trees
     b += 2 * r(4 * ne) + 4 * r(4 * ne) + 4 * r(4 * neb);  // denominators, composition, its evaluations
-    b += r(16 * (j.N - 2));                               // coefficient powers
-    b += r(1 << 20);                                      // eval_at_point scratch and results (bound)
+    b += r(16 * j.N);                                     // coefficient powers
+    const uint64_t eap_blocks = (uint64_t)j.N * eval_at_point_blocks(j.L) + 4 * eval_at_point_blocks(j.L + 1);
+    b += r(16 * eap_blocks);                              // eval_at_point partials
     b += 4 * r(4 * neb) + 4 * r(4 * nb);                  // quotients
     b += tree(j.L + 1 + j.B);                             // FRI first layer tree
     for (uint32_t l = j.B; l <= j.L + j.B; l++) b += 4 * r(4ull << l) + tree(l);  // FRI layers
-    b += r(64);                                           // nonce
+    // the uploaded image: state and sampled values, tickets, quotient parameters, tables
+    b += r(sizeof(ProofState) + 16 * (j.N + 4)) + r(4 * (j.N + 4)) + 2 * r(sizeof(QuotParamsDev));
+    b += 2 * r(8 * j.N) + r(sizeof(EapDevPoly) * (j.N + 4)) + (2 * (j.L + j.B) + 8) * r(64) + r(8 * j.N);
     const uint64_t words = (uint64_t)j.n_queries * ((j.L + 2 + j.B) * 8 * 3 * 8 + 2 * (j.N + 16));
     b += r(words * sizeof(GatherReq)) + r(words * 4);     // decommitment gather
     return b;
 }
 
+// Timing events of one thread's proofs (reused; created on first use per device).
+struct PhaseEvents {
+    cudaEvent_t ev[5] = {};
+    int device = -1;
+    ~PhaseEvents() {
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+    int ensure() {
+        int dev = 0;
+        STWO_CUDA_TRY(cudaGetDevice(&dev));
+        if (device == dev) return STWO_OK;
+        for (auto &e : ev) {
+            if (e) cudaEventDestroy(e);
+            e = nullptr;
+            STWO_CUDA_TRY(cudaEventCreate(&e));
+        }
+        device = dev;
+        return STWO_OK;
+    }
+};
+thread_local PhaseEvents t_phase;
+
 int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const uint32_t *tw_in,
                const uint32_t *itw_in, uint64_t tsz_in, std::vector<uint8_t> &proof, cudaStream_t st,
                stwo_prove_stats *stats) {
     PV_TRY(validate(j));
-    const uint32_t L = j.L, N = j.N, B = j.B, E = L + 1;
+    const uint32_t L = j.L, N = j.N, B = j.B, E = L + 1, D = E + B;
     const uint64_t rows = 1ull << L;
     const double t0 = now_ms();
     const uint64_t launches0 = t_kernel_launches;
+    if (stats) PV_TRY(t_phase.ensure());
+    cudaEvent_t *ev = t_phase.ev;
     Arena ar(st);
-    Channel ch;
+    PV_TRY(ar.reserve(job_device_bytes(j, !(tw_in || itw_in))));
+    if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[0], st));
 
-    // Twiddles: the caller's tree, or one for CanonicCoset(L + 1 + B).half_coset
-    // (wide_fibonacci.rs:216-220). Any canonic tree at least that large serves.
+    // ---- buffers (all of the job's device memory, before the first launch)
     const uint32_t *tw = tw_in, *itw = itw_in;
     uint64_t tsz = tsz_in;
+    uint32_t *own_tw = nullptr, *own_itw = nullptr;
     if (tw_in || itw_in) {
         STWO_REQUIRE(tw_in && itw_in && is_pow2(tsz_in) && tsz_in >= (1ull << (L + B)), STWO_ERR_INVALID_ARGUMENT,
-                     "twiddle tree of %llu entries does not cover domain log size %u", (unsigned long long)tsz_in,
-                     L + 1 + B);
+                     "twiddle tree of %llu entries does not cover domain log size %u", (unsigned long long)tsz_in, D);
     } else {
-        const uint32_t D = L + 1 + B;
         tsz = 1ull << (L + B);
-        PV_ALLOC(t, uint32_t, tsz);
-        PV_ALLOC(it, uint32_t, tsz);
-        PV_TRY(stwo_precompute_twiddles(half_coset_init(D), half_coset_step(D), L + B, t, it, st));
-        tw = t;
-        itw = it;
+        own_tw = ar.alloc<uint32_t>(tsz);
+        own_itw = ar.alloc<uint32_t>(tsz);
+        STWO_REQUIRE(own_tw && own_itw, STWO_ERR_OUT_OF_MEMORY, "twiddle allocation failed");
+        tw = own_tw;
+        itw = own_itw;
     }
-
-    // ---- 1. trace: generation, interpolation, evaluation on CanonicCoset(L + B), tree
     PV_ALLOC(a0, uint32_t, rows);
     PV_ALLOC(a1, uint32_t, rows);
-    STWO_CUDA_TRY(cudaMemcpyAsync(a0, a0_in, rows * 4, cudaMemcpyDefault, st));
-    STWO_CUDA_TRY(cudaMemcpyAsync(a1, a1_in, rows * 4, cudaMemcpyDefault, st));
-    std::vector<uint32_t *> tpoly(N), tev(N);
-    auto tc = std::make_unique<TraceCols>();
+    std::vector<uint32_t *> tpoly(N), tev(N), text(N);
     for (uint32_t c = 0; c < N; c++) {
         PV_ALLOC(p, uint32_t, rows);
         PV_ALLOC(e, uint32_t, rows << B);
         tpoly[c] = p;
         tev[c] = e;
-        tc->c[c] = p;
+        if (B == 1) {
+            text[c] = e;  // the committed evaluations are already on CanonicCoset(L + 1)
+        } else {
+            PV_ALLOC(x, uint32_t, 1ull << E);
+            text[c] = x;
+        }
     }
+    PV_ALLOC(den, uint32_t, 1ull << E);
+    PV_ALLOC(den_inv, uint32_t, 1ull << E);
+    PV_ALLOC(powers, qm31, N);
+    std::vector<uint32_t *> comp(4), cev(4), qc(4), qt(4);
+    for (int k = 0; k < 4; k++) {
+        PV_ALLOC(c, uint32_t, 1ull << E);
+        PV_ALLOC(e, uint32_t, 1ull << D);
+        PV_ALLOC(a, uint32_t, 1ull << D);
+        PV_ALLOC(b, uint32_t, 1ull << (L + B));
+        comp[k] = c;
+        cev[k] = e;
+        qc[k] = a;
+        qt[k] = b;
+    }
+    // FRI layers: inner logs D-1 .. B+1, then the last layer (log B)
+    const uint32_t n_layers = D - 1 - B;
+    STWO_REQUIRE(n_layers <= MAX_LAYERS && L + B - 1 > B, STWO_ERR_UNSUPPORTED_SIZE, "FRI layer count unsupported");
+    std::vector<std::vector<uint32_t *>> lay(n_layers + 1, std::vector<uint32_t *>(4));
+    for (uint32_t li = 0; li <= n_layers; li++)
+        for (int k = 0; k < 4; k++) {
+            PV_ALLOC(c, uint32_t, 1ull << (D - 1 - li));
+            lay[li][k] = c;
+        }
+    const uint32_t eap_n = N + 4;
+    uint32_t eap_total = 0;
+    std::vector<EapDevPoly> eap(eap_n);
+    for (uint32_t i = 0; i < eap_n; i++) {
+        const uint32_t lg = i < N ? L : E;
+        eap[i] = {i < N ? tpoly[i] : comp[i - N], lg, eap_total};
+        eap_total += eval_at_point_blocks(lg);
+    }
+    PV_ALLOC(eap_partials, qm31, eap_total);
+
+    // ---- the uploaded image: state (+ sampled values), tickets, quotient parameters, tables
+    Upload up;
+    const size_t off_state = up.add(nullptr, sizeof(ProofState) + sizeof(qm31) * eap_n);
+    up.at<ProofState>(off_state)->nonce = ~0ull;
+    const size_t off_tickets = up.add(nullptr, 4 * eap_n);
+    auto qpc = std::make_unique<QuotParamsDev>();
+    auto qpt = std::make_unique<QuotParamsDev>();
+    memset(qpc.get(), 0, sizeof(QuotParamsDev));
+    memset(qpt.get(), 0, sizeof(QuotParamsDev));
+    quot_init_static(*qpc, half_coset_init(D), half_coset_step(D), D, qc.data());
+    quot_init_static(*qpt, half_coset_init(L + B), half_coset_step(L + B), L + B, qt.data());
+    qpc->n_batches = qpt->n_batches = 1;
+    qpc->batch_end[0] = 4;
+    qpt->batch_end[0] = N;
+    for (int k = 0; k < 4; k++) {
+        qpc->cols[k] = cev[k];
+        qpc->col_idx[k] = (uint16_t)k;
+    }
+    for (uint32_t c = 0; c < N; c++) {
+        qpt->cols[c] = tev[c];
+        qpt->col_idx[c] = (uint16_t)c;
+    }
+    const size_t off_qc = up.add(qpc.get(), sizeof(QuotParamsDev));
+    const size_t off_qt = up.add(qpt.get(), sizeof(QuotParamsDev));
+    const size_t off_tpoly = up.add(tpoly.data(), sizeof(void *) * N);
+    const size_t off_text = up.add(text.data(), sizeof(void *) * N);
+    const size_t off_eap = up.add(eap.data(), sizeof(EapDevPoly) * eap_n);
+    MerkleTree t_trace, t_comp, t_fri0;
+    std::vector<MerkleTree> t_lay(n_layers);
     {
-        const uint64_t blocks = std::min<uint64_t>((rows + 255) / 256, (uint64_t)device_sm_count() * 8);
-        wide_fib_trace_kernel<<<(unsigned)blocks, 256, 0, st>>>(a0, a1, *tc, N, rows);
+        std::vector<std::pair<uint32_t, const uint32_t *>> cols;
+        for (uint32_t c = 0; c < N; c++) cols.push_back({L + B, tev[c]});
+        PV_TRY(plan_tree(t_trace, cols, ar, up));
+        cols.clear();
+        for (int k = 0; k < 4; k++) cols.push_back({D, cev[k]});
+        PV_TRY(plan_tree(t_comp, cols, ar, up));
+        cols.clear();
+        for (int k = 0; k < 4; k++) cols.push_back({D, qc[k]});
+        for (int k = 0; k < 4; k++) cols.push_back({L + B, qt[k]});
+        PV_TRY(plan_tree(t_fri0, cols, ar, up));
+        for (uint32_t li = 0; li < n_layers; li++) {
+            cols.clear();
+            for (int k = 0; k < 4; k++) cols.push_back({D - 1 - li, lay[li][k]});
+            PV_TRY(plan_tree(t_lay[li], cols, ar, up));
+        }
+    }
+    PV_ALLOC(dev_img, uint8_t, up.host.size());
+    auto dev_at = [&](size_t off) { return dev_img + off; };
+    auto fix_tables = [&](MerkleTree &t) {
+        for (auto &f : t.table_offsets)
+            t.level_tables[f.second] = reinterpret_cast<const uint32_t *const *>(dev_at(f.first));
+    };
+    fix_tables(t_trace);
+    fix_tables(t_comp);
+    fix_tables(t_fri0);
+    for (auto &t : t_lay) fix_tables(t);
+    ProofState *dstate = reinterpret_cast<ProofState *>(dev_at(off_state));
+    qm31 *dsampled = reinterpret_cast<qm31 *>(dev_at(off_state) + sizeof(ProofState));
+    uint32_t *dtickets = reinterpret_cast<uint32_t *>(dev_at(off_tickets));
+    QuotParamsDev *dqc = reinterpret_cast<QuotParamsDev *>(dev_at(off_qc));
+    QuotParamsDev *dqt = reinterpret_cast<QuotParamsDev *>(dev_at(off_qt));
+    {
+        // staged through pinned memory; the stage's next use comes after a wait on st
+        void *stage = nullptr;
+        PV_TRY(host_stage(up.host.size(), &stage));
+        memcpy(stage, up.host.data(), up.host.size());
+        STWO_CUDA_TRY(cudaMemcpyAsync(dev_img, stage, up.host.size(), cudaMemcpyHostToDevice, st));
+    }
+
+    // ---- 1. trace: twiddles, generation, interpolation, evaluation, tree
+    if (own_tw) PV_TRY(stwo_precompute_twiddles(half_coset_init(D), half_coset_step(D), L + B, own_tw, own_itw, st));
+    STWO_CUDA_TRY(cudaMemcpyAsync(a0, a0_in, rows * 4, cudaMemcpyDefault, st));
+    STWO_CUDA_TRY(cudaMemcpyAsync(a1, a1_in, rows * 4, cudaMemcpyDefault, st));
+    {
+        const uint32_t threads = rows < (uint64_t)device_sm_count() * 256 ? 64 : 256;
+        const uint64_t blocks = std::min<uint64_t>((rows + threads - 1) / threads, (uint64_t)device_sm_count() * 16);
+        wide_fib_trace_kernel<<<(unsigned)blocks, threads, 0, st>>>(
+            a0, a1, reinterpret_cast<uint32_t *const *>(dev_at(off_tpoly)), N, rows);
         STWO_LAUNCH_CHECK("wide_fib_trace_kernel");
     }
     // The trace columns are interpolated in place: they become the coefficient columns.
@@ -594,32 +782,19 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         std::vector<const uint32_t *> src(tpoly.begin(), tpoly.end());
         PV_TRY(fft_columns(src.data(), tev.data(), N, L + B, L, tw, tsz, false, st));
     }
-    MerkleTree t_trace;
-    {
-        std::vector<std::pair<uint32_t, const uint32_t *>> cols;
-        for (uint32_t c = 0; c < N; c++) cols.push_back({L + B, tev[c]});
-        PV_TRY(commit_tree(t_trace, cols, ar, st));
-    }
-    ch.mix_root(t_trace.root);
-    const double t1 = now_ms();
+    auto commit = [&](MerkleTree &t) {
+        return merkle_tree_dev_async(t.max_log, t.level_tables.data(), t.level_n.data(), t.layers.data(), st);
+    };
+    PV_TRY(commit(t_trace));
+    fs_trace_kernel<<<1, 32, 0, st>>>(dstate, t_trace.layers[0], powers, N - 2);
+    STWO_LAUNCH_CHECK("fs_trace_kernel");
+    if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[1], st));
 
-    // ---- 2. composition polynomial on CanonicCoset(L + 1), committed on CanonicCoset(L + 1 + B)
-    const qm31 rc = ch.draw_felt();
-    std::vector<const uint32_t *> text(N);
-    if (B == 1) {
-        for (uint32_t c = 0; c < N; c++) text[c] = tev[c];  // already on CanonicCoset(L + 1)
-    } else {
-        std::vector<uint32_t *> dst(N);
-        for (uint32_t c = 0; c < N; c++) {
-            PV_ALLOC(e, uint32_t, 1ull << E);
-            dst[c] = e;
-            text[c] = e;
-        }
+    // ---- 2. composition on CanonicCoset(L + 1), committed on CanonicCoset(L + 1 + B)
+    if (B > 1) {
         std::vector<const uint32_t *> src(tpoly.begin(), tpoly.end());
-        PV_TRY(fft_columns(src.data(), dst.data(), N, E, L, tw, tsz, false, st));
+        PV_TRY(fft_columns(src.data(), text.data(), N, E, L, tw, tsz, false, st));
     }
-    PV_ALLOC(den, uint32_t, 1ull << E);
-    PV_ALLOC(den_inv, uint32_t, 1ull << E);
     {
         VanishingParams vp{};
         cpoint g = {CIRCLE_GEN_X, CIRCLE_GEN_Y};
@@ -637,251 +812,97 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         STWO_LAUNCH_CHECK("vanishing_kernel");
     }
     PV_TRY(batch_inverse_m31_async(den, den_inv, 1ull << E, st));
-    // DomainEvaluationAccumulator: powers [1, r, ..., r^(N-3)]; constraint i takes r^(N-3-i).
-    std::vector<stwo_qm31> powers(N - 2);
-    {
-        qm31 p = qm31_one();
-        for (uint32_t k = 0; k + 2 < N; k++) {
-            powers[k] = from_q(p);
-            p = qm31_mul(p, rc);
-        }
-    }
-    PV_ALLOC(powers_dev, stwo_qm31, N - 2);
-    {
-        // staged through pinned memory; the stage's next reuse is after a wait on this stream
-        void *stage = nullptr;
-        PV_TRY(host_stage(sizeof(stwo_qm31) * (N - 2), &stage));
-        memcpy(stage, powers.data(), sizeof(stwo_qm31) * (N - 2));
-        STWO_CUDA_TRY(cudaMemcpyAsync(powers_dev, stage, sizeof(stwo_qm31) * (N - 2), cudaMemcpyHostToDevice, st));
-    }
-    std::vector<uint32_t *> comp(4), cev(4);
-    for (int k = 0; k < 4; k++) {
-        PV_ALLOC(c, uint32_t, 1ull << E);
-        PV_ALLOC(e, uint32_t, 1ull << (E + B));
-        comp[k] = c;
-        cev[k] = e;
-    }
-    PV_TRY(wide_fib_async(text.data(), N, E, nullptr, reinterpret_cast<const uint32_t *>(powers_dev), den_inv,
-                          comp.data(), st));
+    PV_TRY(wide_fib_dev_async(reinterpret_cast<const uint32_t *const *>(dev_at(off_text)), N, E,
+                              reinterpret_cast<const uint32_t *>(powers), den_inv, comp.data(), st));
     PV_TRY(fft_columns(comp.data(), comp.data(), 4, E, E, itw, tsz, true, st));  // in place -> coefficients
     {
         std::vector<const uint32_t *> src(comp.begin(), comp.end());
-        PV_TRY(fft_columns(src.data(), cev.data(), 4, E + B, E, tw, tsz, false, st));
+        PV_TRY(fft_columns(src.data(), cev.data(), 4, D, E, tw, tsz, false, st));
     }
-    MerkleTree t_comp;
-    {
-        std::vector<std::pair<uint32_t, const uint32_t *>> cols;
-        for (int k = 0; k < 4; k++) cols.push_back({E + B, cev[k]});
-        PV_TRY(commit_tree(t_comp, cols, ar, st));
-    }
-    ch.mix_root(t_comp.root);
-    const double t2 = now_ms();
+    PV_TRY(commit(t_comp));
+    fs_comp_kernel<<<1, 1, 0, st>>>(dstate, t_comp.layers[0]);
+    STWO_LAUNCH_CHECK("fs_comp_kernel");
+    if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[2], st));
 
-    // ---- 3. out-of-domain sampling (CirclePoint::get_random_point)
-    qpoint oods;
-    {
-        const qm31 t = ch.draw_felt(), t2q = qm31_mul(t, t);
-        const qm31 inv = qm31_inv(qm31_add(t2q, qm31_one()));
-        oods = {qm31_mul(qm31_sub(qm31_one(), t2q), inv), qm31_mul(qm31_add(t, t), inv)};
-    }
-    std::vector<qm31> sampled(N + 4);
-    {
-        std::vector<const uint32_t *> polys;
-        std::vector<uint32_t> logs;
-        for (uint32_t c = 0; c < N; c++) {
-            polys.push_back(tpoly[c]);
-            logs.push_back(L);
-        }
-        for (int k = 0; k < 4; k++) {
-            polys.push_back(comp[k]);
-            logs.push_back(E);
-        }
-        std::vector<stwo_spoint> pts(polys.size(), stwo_spoint{from_q(oods.x), from_q(oods.y)});
-        const size_t sb = eval_at_points_scratch_bytes(logs.data(), (uint32_t)polys.size());
-        PV_ALLOC(scratch, uint8_t, sb);
-        PV_ALLOC(res, stwo_qm31, polys.size());
-        PV_TRY(eval_at_points_async(polys.data(), logs.data(), (uint32_t)polys.size(), pts.data(), res, scratch, sb,
-                                    false, st));
-        void *stage = nullptr;
-        PV_TRY(host_stage(polys.size() * sizeof(stwo_qm31), &stage));
-        STWO_CUDA_TRY(cudaMemcpyAsync(stage, res, polys.size() * sizeof(stwo_qm31), cudaMemcpyDeviceToHost, st));
-        PV_TRY(wait_stream(st));
-        const stwo_qm31 *hv = static_cast<const stwo_qm31 *>(stage);
-        for (size_t i = 0; i < polys.size(); i++) sampled[i] = to_q(hv[i]);
-    }
-    ch.mix_felts(sampled);
-    {
-        // The composition's sampled value (from_partial_evals over the basis 1, i, u, iu)
-        // must equal the constraints evaluated on the sampled trace values.
-        const qm31 basis[4] = {{{1, 0}, {0, 0}}, {{0, 1}, {0, 0}}, {{0, 0}, {1, 0}}, {{0, 0}, {0, 1}}};
-        qm31 comp_val = qm31_zero();
-        for (int k = 0; k < 4; k++) comp_val = qm31_add(comp_val, qm31_mul(sampled[N + k], basis[k]));
-        qm31 x = qpoint_mul_base(oods, vanishing_shift(L)).x;
-        for (uint32_t d = 0; d + 1 < L; d++) {
-            qm31 s = qm31_mul(x, x);
-            x = qm31_sub(qm31_add(s, s), qm31_one());
-        }
-        qm31 acc = qm31_zero();
-        for (uint32_t i = 0; i + 2 < N; i++) {
-            qm31 cons = qm31_sub(qm31_add(qm31_mul(sampled[i], sampled[i]), qm31_mul(sampled[i + 1], sampled[i + 1])),
-                                 sampled[i + 2]);
-            acc = qm31_add(qm31_mul(acc, rc), cons);
-        }
-        acc = qm31_mul(acc, qm31_inv(x));
-        STWO_REQUIRE(qm31_eq(acc, comp_val), STWO_ERR_INVALID_ARGUMENT,
-                     "constraints not satisfied at the out-of-domain point");
-    }
-    const double t3 = now_ms();
+    // ---- 3. out-of-domain sampling
+    PV_TRY(eval_at_points_dev_async(dev_at(off_eap), eap_n, eap_total, dstate->oods, dsampled, eap_partials, dtickets,
+                                    st));
+    fs_oods_kernel<<<1, 1, 0, st>>>(dstate, dsampled, N, L, dqc, dqt);
+    STWO_LAUNCH_CHECK("fs_oods_kernel");
+    if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[3], st));
 
     // ---- 4. DEEP quotients (largest columns first) and the FRI commitment
-    const qm31 qrc = ch.draw_felt();
-    std::vector<uint32_t *> qc(4), qt(4);
-    for (int k = 0; k < 4; k++) {
-        PV_ALLOC(a, uint32_t, 1ull << (E + B));
-        PV_ALLOC(b, uint32_t, 1ull << (L + B));
-        qc[k] = a;
-        qt[k] = b;
-    }
-    {
-        const stwo_spoint sp = {from_q(oods.x), from_q(oods.y)};
-        std::vector<uint32_t> idx4 = {0, 1, 2, 3}, sz4 = {4};
-        std::vector<stwo_qm31> v4;
-        for (int k = 0; k < 4; k++) v4.push_back(from_q(sampled[N + k]));
-        std::vector<const uint32_t *> cc(cev.begin(), cev.end());
-        PV_TRY(quotients_async(half_coset_init(E + B), half_coset_step(E + B), E + B, cc.data(), 4, false, from_q(qrc),
-                               &sp, sz4.data(), idx4.data(), v4.data(), 1, qc.data(), st));
-        std::vector<uint32_t> idxn(N), szn = {N};
-        std::vector<stwo_qm31> vn(N);
-        for (uint32_t c = 0; c < N; c++) {
-            idxn[c] = c;
-            vn[c] = from_q(sampled[c]);
-        }
-        std::vector<const uint32_t *> tcols(tev.begin(), tev.end());
-        PV_TRY(quotients_async(half_coset_init(L + B), half_coset_step(L + B), L + B, tcols.data(), N, false,
-                               from_q(qrc), &sp, szn.data(), idxn.data(), vn.data(), 1, qt.data(), st));
-    }
-    MerkleTree t_fri0;
-    {
-        std::vector<std::pair<uint32_t, const uint32_t *>> cols;
-        for (int k = 0; k < 4; k++) cols.push_back({E + B, qc[k]});
-        for (int k = 0; k < 4; k++) cols.push_back({L + B, qt[k]});
-        PV_TRY(commit_tree(t_fri0, cols, ar, st));
-    }
-    ch.mix_root(t_fri0.root);
-    struct Layer {
-        uint32_t log;
-        std::vector<uint32_t *> v;
-        MerkleTree tree;
-    };
-    std::vector<Layer> layers;
-    uint32_t cur_log = E + B - 1;  // LineDomain(Coset::half_odds(E + B - 1))
-    std::vector<uint32_t *> cur(4);
-    for (int k = 0; k < 4; k++) {
-        PV_ALLOC(c, uint32_t, 1ull << cur_log);
-        cur[k] = c;
-        STWO_CUDA_TRY(cudaMemsetAsync(c, 0, 4ull << cur_log, st));
-    }
-    qm31 alpha = ch.draw_felt();
+    PV_TRY(quotients_dev_async(dqc, D, st));
+    PV_TRY(quotients_dev_async(dqt, L + B, st));
+    PV_TRY(commit(t_fri0));
+    fs_layer_kernel<<<1, 1, 0, st>>>(dstate, t_fri0.layers[0], 2, 0);
+    STWO_LAUNCH_CHECK("fs_layer_kernel");
+    for (int k = 0; k < 4; k++) STWO_CUDA_TRY(cudaMemsetAsync(lay[0][k], 0, 4ull << (D - 1), st));
     {
         std::vector<const uint32_t *> s(qc.begin(), qc.end());
-        PV_TRY(fold_async(s.data(), 1ull << (E + B), from_q(alpha), itw, tsz - (1ull << cur_log), cur.data(), true, st));
+        PV_TRY(fold_async(s.data(), 1ull << D, stwo_qm31{}, itw, tsz - (1ull << (D - 1)), lay[0].data(), true, st,
+                          &dstate->alphas[0]));
     }
-    bool trace_folded = false;
-    while (cur_log > B) {  // last layer domain: 2^(log_last_layer_degree_bound + log_blowup) = 2^B
-        if (!trace_folded && cur_log == L + B - 1) {
+    for (uint32_t li = 0; li < n_layers; li++) {
+        const uint32_t lg = D - 1 - li;
+        if (lg == L + B - 1) {
             // The trace quotient folds into this layer with the previous layer's alpha.
             std::vector<const uint32_t *> s(qt.begin(), qt.end());
-            PV_TRY(fold_async(s.data(), 1ull << (L + B), from_q(alpha), itw, tsz - (1ull << cur_log), cur.data(), true,
-                              st));
-            trace_folded = true;
+            PV_TRY(fold_async(s.data(), 1ull << (L + B), stwo_qm31{}, itw, tsz - (1ull << lg), lay[li].data(), true, st,
+                              &dstate->alphas[li]));
         }
-        Layer lay;
-        lay.log = cur_log;
-        lay.v = cur;
-        std::vector<std::pair<uint32_t, const uint32_t *>> cols;
-        for (int k = 0; k < 4; k++) cols.push_back({cur_log, cur[k]});
-        PV_TRY(commit_tree(lay.tree, cols, ar, st));
-        ch.mix_root(lay.tree.root);
-        alpha = ch.draw_felt();
-        std::vector<uint32_t *> nxt(4);
-        for (int k = 0; k < 4; k++) {
-            PV_ALLOC(c, uint32_t, 1ull << (cur_log - 1));
-            nxt[k] = c;
-        }
-        std::vector<const uint32_t *> s(cur.begin(), cur.end());
-        PV_TRY(fold_async(s.data(), 1ull << cur_log, from_q(alpha), itw, tsz - (1ull << cur_log), nxt.data(), false, st));
-        layers.push_back(std::move(lay));
-        cur = nxt;
-        cur_log--;
+        PV_TRY(commit(t_lay[li]));
+        fs_layer_kernel<<<1, 1, 0, st>>>(dstate, t_lay[li].layers[0], 3 + li, li + 1);
+        STWO_LAUNCH_CHECK("fs_layer_kernel");
+        std::vector<const uint32_t *> s(lay[li].begin(), lay[li].end());
+        PV_TRY(fold_async(s.data(), 1ull << lg, stwo_qm31{}, itw, tsz - (1ull << lg), lay[li + 1].data(), false, st,
+                          &dstate->alphas[li + 1]));
     }
-    STWO_REQUIRE(trace_folded, STWO_ERR_UNSUPPORTED_SIZE, "trace quotient not folded (trace too small)");
-    // Last layer: 2^B evaluations over Coset(2^(29-B), 2^(31-B)) -> line polynomial of degree bound 1.
-    qm31 last_coeff;
     {
-        const size_t n = 1ull << B;
-        void *stage = nullptr;
-        PV_TRY(host_stage(16 * n, &stage));
-        uint32_t *hv = static_cast<uint32_t *>(stage);
-        for (int k = 0; k < 4; k++)
-            STWO_CUDA_TRY(cudaMemcpyAsync(hv + k * n, cur[k], 4 * n, cudaMemcpyDeviceToHost, st));
+        Cols4c last{{lay[n_layers][0], lay[n_layers][1], lay[n_layers][2], lay[n_layers][3]}};
+        fs_last_kernel<<<1, 1, 0, st>>>(dstate, last, B);
+        STWO_LAUNCH_CHECK("fs_last_kernel");
+    }
+    if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[4], st));
+
+    // ---- 5. proof of work and query words, then the channel's record to the host
+    {
+        const uint64_t want = 1ull << std::min<uint32_t>(j.pow_bits + 2, 24);  // a few times the expected tries
+        const uint64_t threads = std::max<uint64_t>(256, std::min<uint64_t>(want, (uint64_t)device_sm_count() * 1024));
+        const uint64_t blocks = (threads + 255) / 256, grid = blocks * 256;
+        const uint64_t max_k = ((1ull << (j.pow_bits + 8)) + grid - 1) / grid + 1;  // gives up after 2^(pow_bits+8)
+        grind_kernel<<<(unsigned)blocks, 256, 0, st>>>(dstate, j.pow_bits, max_k);
+        STWO_LAUNCH_CHECK("grind_kernel");
+        fs_finish_kernel<<<1, 1, 0, st>>>(dstate, j.n_queries);
+        STWO_LAUNCH_CHECK("fs_finish_kernel");
+    }
+    const size_t rec_bytes = sizeof(ProofState) + sizeof(qm31) * eap_n;
+    std::vector<uint8_t> rec(rec_bytes);
+    {
+        void *rec_stage = nullptr;
+        PV_TRY(host_stage(rec_bytes, &rec_stage));
+        STWO_CUDA_TRY(cudaMemcpyAsync(rec_stage, dstate, rec_bytes, cudaMemcpyDeviceToHost, st));
         PV_TRY(wait_stream(st));
-        std::vector<qm31> ev(n);
-        for (size_t i = 0; i < n; i++) ev[i] = {{hv[i], hv[n + i]}, {hv[2 * n + i], hv[3 * n + i]}};
-        std::vector<qm31> coeffs = interpolate_line(ev, 1u << (29 - B), 1u << (31 - B), B);
-        for (size_t i = 1; i < n; i++)
-            STWO_REQUIRE(qm31_eq(coeffs[i], qm31_zero()), STWO_ERR_INVALID_ARGUMENT,
-                         "FRI last layer exceeds its degree bound");
-        last_coeff = coeffs[0];
-        ch.mix_felts({last_coeff});
+        memcpy(rec.data(), rec_stage, rec_bytes);
     }
-    const double t4 = now_ms();
+    const ProofState &ps = *reinterpret_cast<const ProofState *>(rec.data());
+    const qm31 *sampled = reinterpret_cast<const qm31 *>(rec.data() + sizeof(ProofState));
+    STWO_REQUIRE(!(ps.error & fs::ERR_DRAW), STWO_ERR_CUDA, "channel draw exceeded its retry bound");
+    STWO_REQUIRE(!(ps.error & fs::ERR_CONSTRAINTS), STWO_ERR_INVALID_ARGUMENT,
+                 "constraints not satisfied at the out-of-domain point");
+    STWO_REQUIRE(!(ps.error & fs::ERR_LAST_LAYER), STWO_ERR_INVALID_ARGUMENT, "FRI last layer exceeds its degree bound");
+    STWO_REQUIRE(!(ps.error & fs::ERR_GRIND), STWO_ERR_INVALID_ARGUMENT, "no proof-of-work nonce within 2^%u tries",
+                 j.pow_bits + 8);
 
-    // ---- 5. proof of work, queries, decommitments
-    uint64_t nonce = 0;
-    {
-        PV_ALLOC(best, unsigned long long, 1);
-        GrindParams gp{};
-        memcpy(gp.h, ch.digest, 32);
-        gp.pow_bits = j.pow_bits;
-        const uint32_t blocks = (uint32_t)device_sm_count() * 4, threads = 256, per_thread = 16;
-        const uint64_t chunk = (uint64_t)blocks * threads * per_thread;
-        unsigned long long found = ~0ull;
-        // Expected work 2^pow_bits tries; the search gives up after 2^(pow_bits + 8).
-        const uint64_t limit = std::max<uint64_t>(1ull << (j.pow_bits + 8), chunk);
-        for (uint64_t base = 0; found == ~0ull && base < limit; base += chunk) {
-            STWO_CUDA_TRY(cudaMemsetAsync(best, 0xff, 8, st));
-            grind_kernel<<<blocks, threads, 0, st>>>(gp, base, per_thread, best);
-            STWO_LAUNCH_CHECK("grind_kernel");
-            void *stage = nullptr;
-            PV_TRY(host_stage(8, &stage));
-            STWO_CUDA_TRY(cudaMemcpyAsync(stage, best, 8, cudaMemcpyDeviceToHost, st));
-            PV_TRY(wait_stream(st));
-            memcpy(&found, stage, 8);
-        }
-        STWO_REQUIRE(found != ~0ull, STWO_ERR_INVALID_ARGUMENT, "no proof-of-work nonce found");
-        nonce = found;
-    }
-    ch.mix_nonce(nonce);
-
-    // Queries::generate over the largest quotient domain (log E + B).
+    // Queries::generate over the largest quotient domain (log D).
     std::vector<uint64_t> queries;
     {
         std::set<uint64_t> qs;
-        uint32_t cnt = 0;
-        const uint32_t mask = (uint32_t)((1ull << (E + B)) - 1);
-        while (cnt < j.n_queries) {
-            uint8_t b[32];
-            ch.draw_random_bytes(b);
-            for (int i = 0; i < 8 && cnt < j.n_queries; i++, cnt++) {
-                uint32_t u;
-                memcpy(&u, b + 4 * i, 4);
-                qs.insert(u & mask);
-            }
-        }
+        const uint32_t mask = (uint32_t)((1ull << D) - 1);
+        for (uint32_t i = 0; i < j.n_queries; i++) qs.insert(ps.query_words[i] & mask);
         queries.assign(qs.begin(), qs.end());
     }
-    const std::map<uint32_t, std::vector<uint64_t>> tree_queries = {{E + B, queries},
-                                                                     {L + B, fold_queries(queries, 1)}};
+    const std::map<uint32_t, std::vector<uint64_t>> tree_queries = {{D, queries}, {L + B, fold_queries(queries, 1)}};
 
     Gatherer g;
     TreeDecommit d_trace = plan_decommit(t_trace, tree_queries, g);
@@ -892,26 +913,26 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     {
         std::map<uint32_t, std::vector<uint64_t>> pos;
         for (int grp = 0; grp < 2; grp++) {
-            const uint32_t lg = grp == 0 ? E + B : L + B;
+            const uint32_t lg = grp == 0 ? D : L + B;
             const std::vector<uint32_t *> &col = grp == 0 ? qc : qt;
             std::vector<uint64_t> p, wv;
-            fri_positions(fold_queries(queries, E + B - lg), p, wv);
+            fri_positions(fold_queries(queries, D - lg), p, wv);
             pos[lg] = p;
             for (uint64_t x : wv)
                 for (int k = 0; k < 4; k++) w_first.push_back(g.add(col[k], x));
         }
         d_fri0 = plan_decommit(t_fri0, pos, g);
     }
-    std::vector<std::vector<size_t>> w_inner(layers.size());
-    std::vector<TreeDecommit> d_inner(layers.size());
+    std::vector<std::vector<size_t>> w_inner(n_layers);
+    std::vector<TreeDecommit> d_inner(n_layers);
     {
         std::vector<uint64_t> lq = fold_queries(queries, 1);
-        for (size_t li = 0; li < layers.size(); li++) {
+        for (uint32_t li = 0; li < n_layers; li++) {
             std::vector<uint64_t> p, wv;
             fri_positions(lq, p, wv);
             for (uint64_t x : wv)
-                for (int k = 0; k < 4; k++) w_inner[li].push_back(g.add(layers[li].v[k], x));
-            d_inner[li] = plan_decommit(layers[li].tree, {{layers[li].log, p}}, g);
+                for (int k = 0; k < 4; k++) w_inner[li].push_back(g.add(lay[li][k], x));
+            d_inner[li] = plan_decommit(t_lay[li], {{D - 1 - li, p}}, g);
             lq = fold_queries(lq, 1);
         }
     }
@@ -921,8 +942,8 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     // ---- serialisation
     Writer w;
     w.u64(2);  // commitments
-    w.bytes(t_trace.root, 32);
-    w.bytes(t_comp.root, 32);
+    w.bytes(ps.roots[0], 32);
+    w.bytes(ps.roots[1], 32);
     w.u64(2);  // sampled_values
     w.u64(N);
     for (uint32_t c = 0; c < N; c++) {
@@ -945,29 +966,31 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
             for (size_t gi : col) w.u32(vals[gi]);
         }
     }
-    w.u64(nonce);  // proof_of_work
-    auto write_fri_layer = [&](const std::vector<size_t> &wit, const TreeDecommit &d, const uint8_t root[32]) {
+    w.u64(ps.nonce);  // proof_of_work
+    auto write_fri_layer = [&](const std::vector<size_t> &wit, const TreeDecommit &d, const uint32_t root[8]) {
         w.u64(wit.size() / 4);
         for (size_t gi : wit) w.u32(vals[gi]);
         write_decommitment(w, d, vals);
         w.bytes(root, 32);
     };
-    write_fri_layer(w_first, d_fri0, t_fri0.root);
-    w.u64(layers.size());
-    for (size_t li = 0; li < layers.size(); li++) write_fri_layer(w_inner[li], d_inner[li], layers[li].tree.root);
+    write_fri_layer(w_first, d_fri0, ps.roots[2]);
+    w.u64(n_layers);
+    for (uint32_t li = 0; li < n_layers; li++) write_fri_layer(w_inner[li], d_inner[li], ps.roots[3 + li]);
     w.u64(1);  // last_layer_poly.coeffs
-    w.q(last_coeff);
+    w.q(ps.last_coeff);
     w.u32(0);  // last_layer_poly.log_size
     proof = std::move(w.b);
     const double t5 = now_ms();
 
     if (stats) {
-        stats->trace_ms = t1 - t0;
-        stats->composition_ms = t2 - t1;
-        stats->oods_ms = t3 - t2;
-        stats->fri_ms = t4 - t3;
-        stats->decommit_ms = t5 - t4;
+        float ms[4];
+        for (int p = 0; p < 4; p++) STWO_CUDA_TRY(cudaEventElapsedTime(&ms[p], ev[p], ev[p + 1]));
+        stats->trace_ms = ms[0];
+        stats->composition_ms = ms[1];
+        stats->oods_ms = ms[2];
+        stats->fri_ms = ms[3];
         stats->total_ms = t5 - t0;
+        stats->decommit_ms = std::max(0.0, stats->total_ms - (ms[0] + ms[1] + ms[2] + ms[3]));
         stats->device_bytes = ar.bytes;
         stats->kernel_launches = t_kernel_launches - launches0;
         stats->proof_bytes = proof.size();

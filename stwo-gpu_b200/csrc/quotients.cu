@@ -20,26 +20,23 @@
 #include <vector>
 
 #include "common.cuh"
+#include "quotients.cuh"
 
 namespace stwo {
 namespace {
 
-constexpr int QUOT_MAX_COLS = 512;
-constexpr int QUOT_MAX_SAMPLES = 512;
-constexpr int QUOT_MAX_BATCHES = 16;
+using QuotParams = QuotParamsT<QUOT_MAX_COLS, QUOT_MAX_SAMPLES>;
+constexpr int QUOT_PREFETCH = 8;  // column loads in flight per thread
 
-struct QuotParams {
-    const uint32_t *cols[QUOT_MAX_COLS];
-    qm31 c2[QUOT_MAX_SAMPLES];            // c_j with every coordinate doubled (for m31_mul2)
-    uint16_t col_idx[QUOT_MAX_SAMPLES];
-    qm31 a_sum[QUOT_MAX_BATCHES], b_sum[QUOT_MAX_BATCHES], batch_coeff[QUOT_MAX_BATCHES];
-    cm31 prx[QUOT_MAX_BATCHES], pry[QUOT_MAX_BATCHES], pix[QUOT_MAX_BATCHES], piy[QUOT_MAX_BATCHES];
-    uint32_t batch_end[QUOT_MAX_BATCHES];  // cumulative sample counts
-    uint32_t n_batches;
-    uint32_t half_init, half_step;        // half coset indices
-    uint32_t log_size;                    // domain log size
-    uint32_t *out[4];
-    cpoint gen_pows[31];                  // GEN^(2^b), so the kernel shares no state between calls
+// The kernel reads its parameters through get(): by value from the parameter block,
+// or from a device-resident block (the prover's, filled by the device channel).
+struct QuotByValue {
+    QuotParams p;
+    __device__ const QuotParams &get() const { return p; }
+};
+struct QuotByRef {
+    const QuotParamsDev *p;
+    __device__ const QuotParamsDev &get() const { return *p; }
 };
 
 __device__ __forceinline__ cpoint point_at_index(const cpoint *gen_pows, uint32_t idx) {
@@ -62,9 +59,10 @@ __device__ __forceinline__ uint32_t reduce64(uint64_t x) {
     return reduce_once((uint32_t)s);
 }
 
-template <bool COLS_ON_DEVICE>
-__global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ QuotParams p,
+template <bool COLS_ON_DEVICE, class PR>
+__global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ PR pr,
                                                         const uint32_t *const *__restrict__ dev_cols) {
+    const auto &p = pr.get();
     const uint64_t n_pairs = 1ull << (p.log_size - 1);
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_pairs;
          k += (uint64_t)gridDim.x * blockDim.x) {
@@ -98,14 +96,27 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
         for (uint32_t b = 0; b < p.n_batches; b++) {
             uint64_t s0[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
             const uint32_t j1 = p.batch_end[b];
-            for (uint32_t j = j0; j < j1; j++) {
-                const uint32_t *col = COLS_ON_DEVICE ? dev_cols[p.col_idx[j]] : p.cols[p.col_idx[j]];
-                uint2 v = __ldg(reinterpret_cast<const uint2 *>(col) + k);
-                qm31 c2 = p.c2[j];
-                s0[0][0] += mul_lazy(v.x, c2.a.a); s0[0][1] += mul_lazy(v.x, c2.a.b);
-                s0[0][2] += mul_lazy(v.x, c2.b.a); s0[0][3] += mul_lazy(v.x, c2.b.b);
-                s0[1][0] += mul_lazy(v.y, c2.a.a); s0[1][1] += mul_lazy(v.y, c2.a.b);
-                s0[1][2] += mul_lazy(v.y, c2.b.a); s0[1][3] += mul_lazy(v.y, c2.b.b);
+            // Column loads are issued QUOT_PREFETCH at a time before they are consumed,
+            // so each thread keeps several DRAM requests in flight.
+            for (uint32_t jb = j0; jb < j1; jb += QUOT_PREFETCH) {
+                uint2 v[QUOT_PREFETCH];
+#pragma unroll
+                for (int u = 0; u < QUOT_PREFETCH; u++) {
+                    const uint32_t j = jb + u;
+                    if (j < j1) {
+                        const uint32_t *col = COLS_ON_DEVICE ? dev_cols[p.col_idx[j]] : p.cols[p.col_idx[j]];
+                        v[u] = __ldg(reinterpret_cast<const uint2 *>(col) + k);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < QUOT_PREFETCH; u++) {
+                    if (jb + u >= j1) break;
+                    const qm31 c2 = p.c2[jb + u];
+                    s0[0][0] += mul_lazy(v[u].x, c2.a.a); s0[0][1] += mul_lazy(v[u].x, c2.a.b);
+                    s0[0][2] += mul_lazy(v[u].x, c2.b.a); s0[0][3] += mul_lazy(v[u].x, c2.b.b);
+                    s0[1][0] += mul_lazy(v[u].y, c2.a.a); s0[1][1] += mul_lazy(v[u].y, c2.a.b);
+                    s0[1][2] += mul_lazy(v[u].y, c2.b.a); s0[1][3] += mul_lazy(v[u].y, c2.b.b);
+                }
             }
             j0 = j1;
             for (int s = 0; s < 2; s++) {
@@ -136,52 +147,26 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
                  QUOT_MAX_BATCHES);
     STWO_REQUIRE(cols_on_device || n_cols <= (uint32_t)QUOT_MAX_COLS, STWO_ERR_UNSUPPORTED_SIZE,
                  "at most %d columns", QUOT_MAX_COLS);
-    QuotParams *p = new QuotParams();
-    std::unique_ptr<QuotParams> guard(p);
-    {
-        cpoint g = {CIRCLE_GEN_X, CIRCLE_GEN_Y};
-        for (int b = 0; b < 31; b++) {
-            p->gen_pows[b] = g;
-            g = point_mul(g, g);
-        }
-    }
+    auto holder = std::make_unique<QuotByValue>();
+    QuotParams *p = &holder->p;
+    quot_init_static(*p, half_init, half_step, log_size, out4);
     p->n_batches = n_batches;
-    p->half_init = half_init;
-    p->half_step = half_step;
-    p->log_size = log_size;
-    for (int c = 0; c < 4; c++) p->out[c] = out4[c];
     if (!cols_on_device)
         for (uint32_t i = 0; i < n_cols; i++) p->cols[i] = cols[i];
     qm31 rcq = to_q(rc_c);
     uint32_t off = 0;
+    std::vector<qm31> v;
     for (uint32_t b = 0; b < n_batches; b++) {
         STWO_REQUIRE(off + bsz[b] <= (uint32_t)QUOT_MAX_SAMPLES, STWO_ERR_UNSUPPORTED_SIZE, "at most %d samples",
                      QUOT_MAX_SAMPLES);
-        qm31 px = to_q(pts[b].x), py = to_q(pts[b].y);
-        p->prx[b] = px.a;
-        p->pix[b] = px.b;
-        p->pry[b] = py.a;
-        p->piy[b] = py.b;
-        p->batch_coeff[b] = qm31_pow(rcq, bsz[b]);
-        qm31 alpha = qm31_one(), as = qm31_zero(), bs = qm31_zero();
+        v.resize(bsz[b]);
         for (uint32_t j = 0; j < bsz[b]; j++) {
-            alpha = qm31_mul(alpha, rcq);
-            qm31 v = to_q(vals[off + j]);
-            qm31 a = qm31_sub(qm31_conj(v), v);
-            qm31 c = qm31_sub(qm31_conj(py), py);
-            qm31 bb = qm31_sub(qm31_mul(v, c), qm31_mul(a, py));
-            a = qm31_mul(alpha, a);
-            bb = qm31_mul(alpha, bb);
-            c = qm31_mul(alpha, c);
-            as = qm31_add(as, a);
-            bs = qm31_add(bs, bb);
-            p->c2[off + j] = {{c.a.a << 1, c.a.b << 1}, {c.b.a << 1, c.b.b << 1}};
+            v[j] = to_q(vals[off + j]);
             STWO_REQUIRE(cidx[off + j] < n_cols, STWO_ERR_INVALID_ARGUMENT, "sample column index %u out of range",
                          cidx[off + j]);
             p->col_idx[off + j] = (uint16_t)cidx[off + j];
         }
-        p->a_sum[b] = as;
-        p->b_sum[b] = bs;
+        quot_fill_batch(*p, b, rcq, to_q(pts[b].x), to_q(pts[b].y), v.data(), bsz[b], off);
         off += bsz[b];
         p->batch_end[b] = off;
     }
@@ -189,8 +174,19 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    if (cols_on_device) quotients_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(*p, cols);
-    else quotients_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(*p, nullptr);
+    if (cols_on_device) quotients_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(*holder, cols);
+    else quotients_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(*holder, nullptr);
+    STWO_LAUNCH_CHECK("quotients_kernel");
+    return STWO_OK;
+}
+
+int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, cudaStream_t st) {
+    STWO_REQUIRE(log_size >= 1 && log_size <= 31, STWO_ERR_UNSUPPORTED_SIZE, "domain log size %u", log_size);
+    uint64_t pairs = 1ull << (log_size - 1);
+    uint64_t blocks = (pairs + 255) / 256;
+    uint64_t cap = (uint64_t)device_sm_count() * 8;
+    if (blocks > cap) blocks = cap;
+    quotients_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(QuotByRef{p_dev}, nullptr);
     STWO_LAUNCH_CHECK("quotients_kernel");
     return STWO_OK;
 }

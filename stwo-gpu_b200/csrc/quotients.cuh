@@ -1,0 +1,80 @@
+// DEEP-quotient parameters shared by the quotient kernel (quotients.cu), its host
+// entry points and the prover's device channel, which fills the sample-dependent
+// fields on the device.
+#pragma once
+#include <cstdint>
+
+#include "field.cuh"
+
+namespace stwo {
+
+constexpr int QUOT_MAX_COLS = 512;
+constexpr int QUOT_MAX_SAMPLES = 512;
+constexpr int QUOT_MAX_BATCHES = 16;
+
+template <int MAXC, int MAXS>
+struct QuotParamsT {
+    const uint32_t *cols[MAXC];
+    qm31 c2[MAXS];                        // c_j with every coordinate doubled (for m31_mul2)
+    uint16_t col_idx[MAXS];
+    qm31 a_sum[QUOT_MAX_BATCHES], b_sum[QUOT_MAX_BATCHES], batch_coeff[QUOT_MAX_BATCHES];
+    cm31 prx[QUOT_MAX_BATCHES], pry[QUOT_MAX_BATCHES], pix[QUOT_MAX_BATCHES], piy[QUOT_MAX_BATCHES];
+    uint32_t batch_end[QUOT_MAX_BATCHES];  // cumulative sample counts
+    uint32_t n_batches;
+    uint32_t half_init, half_step;        // half coset indices
+    uint32_t log_size;                    // domain log size
+    uint32_t *out[4];
+    cpoint gen_pows[31];                  // GEN^(2^b), so the kernel shares no state between calls
+};
+
+// The prover's device-resident parameters: up to 1024 columns and samples.
+using QuotParamsDev = QuotParamsT<1024, 1024>;
+
+// Sample-dependent fields of batch b (samples off .. off+count-1 at point (px, py)):
+// the batch coefficient rc^count and, per sample j with alpha = rc^(j+1),
+// (a, b, c) = alpha * (conj(v) - v, v*c0 - a*py, c0), c0 = conj(py) - py
+// (complex_conjugate_line_coeffs); a and b summed per batch, c stored doubled.
+template <class QP>
+__host__ __device__ inline void quot_fill_batch(QP &p, uint32_t b, qm31 rc, qm31 px, qm31 py, const qm31 *vals,
+                                                uint32_t count, uint32_t off) {
+    p.prx[b] = px.a;
+    p.pix[b] = px.b;
+    p.pry[b] = py.a;
+    p.piy[b] = py.b;
+    p.batch_coeff[b] = qm31_pow(rc, count);
+    const qm31 c0 = qm31_sub(qm31_conj(py), py);
+    qm31 alpha = qm31_one(), as = qm31_zero(), bs = qm31_zero();
+    for (uint32_t j = 0; j < count; j++) {
+        alpha = qm31_mul(alpha, rc);
+        const qm31 v = vals[j];
+        qm31 a = qm31_sub(qm31_conj(v), v);
+        qm31 bb = qm31_sub(qm31_mul(v, c0), qm31_mul(a, py));
+        a = qm31_mul(alpha, a);
+        bb = qm31_mul(alpha, bb);
+        const qm31 c = qm31_mul(alpha, c0);
+        as = qm31_add(as, a);
+        bs = qm31_add(bs, bb);
+        p.c2[off + j] = {{c.a.a << 1, c.a.b << 1}, {c.b.a << 1, c.b.b << 1}};
+    }
+    p.a_sum[b] = as;
+    p.b_sum[b] = bs;
+}
+
+// The column-independent fields: domain, outputs, generator table.
+template <class QP>
+inline void quot_init_static(QP &p, uint32_t half_init, uint32_t half_step, uint32_t log_size, uint32_t *const *out4) {
+    cpoint g = {CIRCLE_GEN_X, CIRCLE_GEN_Y};
+    for (int b = 0; b < 31; b++) {
+        p.gen_pows[b] = g;
+        g = point_mul(g, g);
+    }
+    p.half_init = half_init;
+    p.half_step = half_step;
+    p.log_size = log_size;
+    for (int c = 0; c < 4; c++) p.out[c] = out4[c];
+}
+
+// Launches the quotient kernel on parameters resident in device memory.
+int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, cudaStream_t st);
+
+}  // namespace stwo

@@ -89,6 +89,10 @@ int library_pool(cudaMemPool_t *pool) {
         STWO_CUDA_TRY(cudaMemPoolCreate(&p, &props));
         uint64_t threshold = ~0ull;
         STWO_CUDA_TRY(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &threshold));
+        // A stream may reuse memory another stream freed only once that free has
+        // completed: the pool must not make one job's stream wait on another's.
+        int no = 0;
+        STWO_CUDA_TRY(cudaMemPoolSetAttribute(p, cudaMemPoolReuseAllowInternalDependencies, &no));
         g_pools[dev] = p;
     }
     *pool = g_pools[dev];
@@ -105,6 +109,26 @@ int pool_alloc(void **p, size_t bytes, cudaStream_t st) {
         *p = nullptr;
         return set_error(e == cudaErrorMemoryAllocation ? STWO_ERR_OUT_OF_MEMORY : STWO_ERR_CUDA,
                          "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    return STWO_OK;
+}
+
+int reserve_pool(uint64_t bytes) {
+    if (bytes == 0) return STWO_OK;
+    cudaMemPool_t pool;
+    int rc = library_pool(&pool);
+    if (rc) return rc;
+    cudaStream_t s = nullptr;
+    STWO_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    void *p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, s);
+    if (e == cudaSuccess) e = cudaFreeAsync(p, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(e == cudaErrorMemoryAllocation ? STWO_ERR_OUT_OF_MEMORY : STWO_ERR_CUDA,
+                         "reserving %llu pool bytes failed: %s", (unsigned long long)bytes, cudaGetErrorString(e));
     }
     return STWO_OK;
 }
@@ -168,6 +192,8 @@ const char *stwo_last_error(void) { return g_last_error; }
 void stwo_clear_last_error(void) { clear_error(); }
 
 uint64_t stwo_kernel_launches(void) { return g_kernel_launches.load(std::memory_order_relaxed); }
+
+int stwo_reserve_device_memory(uint64_t bytes) { return reserve_pool(bytes); }
 
 int stwo_stream_synchronize(void *stream) {
     cudaError_t e = cudaStreamSynchronize(as_stream(stream));

@@ -10,6 +10,7 @@
 // thread waits on the channel. All jobs share one twiddle tree, built at creation for
 // the largest domain the server accepts. A job's proof bytes do not depend on what
 // else is running: each job's arithmetic is confined to its own buffers and stream.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstdlib>
@@ -35,9 +36,10 @@ double steady_ms() {
 }
 
 struct PendingJob {
-    uint64_t id;
-    stwo_wide_fib_job job;
-    std::vector<uint32_t> a0, a1;
+    uint64_t id = 0;
+    stwo_wide_fib_job job{};
+    std::vector<uint32_t> a0, a1;           // host copies, or
+    const uint32_t *a0_dev = nullptr, *a1_dev = nullptr;  // caller-owned device inputs
     uint64_t bytes;
     double submit_ms;
 };
@@ -82,10 +84,11 @@ struct stwo_prover_server {
         cudaError_t se = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
         for (;;) {
             PendingJob j;
+            bool got = false;
             {
                 std::unique_lock<std::mutex> lock(mu);
-                cv_work.wait(lock, [&] { return stopping || (!pending.empty() && take(j)); });
-                if (stopping && j.a0.empty()) break;
+                cv_work.wait(lock, [&] { return stopping || (!pending.empty() && (got = take(j))); });
+                if (!got) break;  // stopping, nothing taken
                 running++;
             }
             stwo_server_result r{};
@@ -97,7 +100,8 @@ struct stwo_prover_server {
                 r.status = set_error(STWO_ERR_CUDA, "worker stream creation failed: %s", cudaGetErrorString(se));
             } else {
                 clear_error();
-                r.status = wide_fib_prove(&j.job, j.a0.data(), j.a1.data(), tw, itw, tree_size, proof, &r.stats, st);
+                const uint32_t *a0 = j.a0_dev ? j.a0_dev : j.a0.data(), *a1 = j.a1_dev ? j.a1_dev : j.a1.data();
+                r.status = wide_fib_prove(&j.job, a0, a1, tw, itw, tree_size, proof, &r.stats, st);
             }
             if (r.status == STWO_OK) {
                 r.proof = static_cast<uint8_t *>(malloc(proof.size()));
@@ -161,26 +165,27 @@ stwo_prover_server *stwo_server_create(uint32_t n_workers, uint64_t device_budge
         delete s;
         return nullptr;
     }
+    // Map the budget into the library's pool now (bounded by the free memory), so
+    // admitted jobs never wait on the driver to back new allocations.
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        const uint64_t margin = 2ull << 30;
+        const uint64_t want = std::min<uint64_t>(device_budget_bytes, free_b > margin ? free_b - margin : 0);
+        if (reserve_pool(want) != STWO_OK) clear_error();  // a smaller pool only costs speed
+    }
     for (uint32_t i = 0; i < n_workers; i++) s->workers.emplace_back([s] { s->worker(); });
     return s;
 }
 
-int stwo_server_submit(stwo_prover_server *s, uint64_t job_id, const stwo_wide_fib_job *job, const uint32_t *a0,
-                       const uint32_t *a1) {
-    STWO_REQUIRE(s && job && a0 && a1, STWO_ERR_INVALID_ARGUMENT, "null argument");
-    const uint64_t bytes = wide_fib_job_device_bytes(job, false);
+namespace {
+int submit_job(stwo_prover_server *s, PendingJob &&j) {
+    const uint64_t bytes = wide_fib_job_device_bytes(&j.job, false);
     STWO_REQUIRE(bytes, STWO_ERR_UNSUPPORTED_SIZE, "job parameters unsupported");
-    STWO_REQUIRE(job->log_n_rows + 1 + job->log_blowup <= s->max_domain_log, STWO_ERR_UNSUPPORTED_SIZE,
-                 "job domain log size %u exceeds the server's %u", job->log_n_rows + 1 + job->log_blowup,
+    STWO_REQUIRE(j.job.log_n_rows + 1 + j.job.log_blowup <= s->max_domain_log, STWO_ERR_UNSUPPORTED_SIZE,
+                 "job domain log size %u exceeds the server's %u", j.job.log_n_rows + 1 + j.job.log_blowup,
                  s->max_domain_log);
     STWO_REQUIRE(bytes <= s->budget, STWO_ERR_OUT_OF_MEMORY, "job needs %llu device bytes, budget is %llu",
                  (unsigned long long)bytes, (unsigned long long)s->budget);
-    PendingJob j;
-    j.id = job_id;
-    j.job = *job;
-    const size_t rows = 1ull << job->log_n_rows;
-    j.a0.assign(a0, a0 + rows);
-    j.a1.assign(a1, a1 + rows);
     j.bytes = bytes;
     j.submit_ms = steady_ms();
     {
@@ -190,6 +195,31 @@ int stwo_server_submit(stwo_prover_server *s, uint64_t job_id, const stwo_wide_f
     }
     s->cv_work.notify_one();
     return STWO_OK;
+}
+}  // namespace
+
+int stwo_server_submit(stwo_prover_server *s, uint64_t job_id, const stwo_wide_fib_job *job, const uint32_t *a0,
+                       const uint32_t *a1) {
+    STWO_REQUIRE(s && job && a0 && a1, STWO_ERR_INVALID_ARGUMENT, "null argument");
+    STWO_REQUIRE(job->log_n_rows <= 30, STWO_ERR_UNSUPPORTED_SIZE, "job parameters unsupported");
+    PendingJob j;
+    j.id = job_id;
+    j.job = *job;
+    const size_t rows = 1ull << job->log_n_rows;
+    j.a0.assign(a0, a0 + rows);
+    j.a1.assign(a1, a1 + rows);
+    return submit_job(s, std::move(j));
+}
+
+int stwo_server_submit_device(stwo_prover_server *s, uint64_t job_id, const stwo_wide_fib_job *job,
+                              const uint32_t *a0_dev, const uint32_t *a1_dev) {
+    STWO_REQUIRE(s && job && a0_dev && a1_dev, STWO_ERR_INVALID_ARGUMENT, "null argument");
+    PendingJob j;
+    j.id = job_id;
+    j.job = *job;
+    j.a0_dev = a0_dev;
+    j.a1_dev = a1_dev;
+    return submit_job(s, std::move(j));
 }
 
 uint32_t stwo_server_poll(stwo_prover_server *s, stwo_server_result *out, uint32_t max_results, int32_t timeout_ms) {

@@ -108,6 +108,12 @@ class ProofServer:
         L.clear_error()
         L.check(L.lib().stwo_server_submit(self._s, job_id, C.byref(job.c()), a0.ctypes.data, a1.ctypes.data))
 
+    def submit_device(self, job_id, job, a0_dev, a1_dev):
+        """Queues a job whose inputs are device pointers (ints); they must stay valid
+        until the job's result has been polled."""
+        L.clear_error()
+        L.check(L.lib().stwo_server_submit_device(self._s, job_id, C.byref(job.c()), a0_dev, a1_dev))
+
     def poll(self, max_results=64, timeout_ms=-1):
         """Finished jobs as dicts: job_id, status, error, proof, submit/start/done ms, stats."""
         buf = (L.ServerResult * max_results)()
