@@ -481,7 +481,7 @@ def fft_roofline(stwo, dev, rank, args):
     traffic = None
     tf = os.path.join(ROOT, "profiles", "fft_traffic.json")
     if os.path.exists(tf):
-        traffic = json.load(open(tf)).get("dram_bytes_per_launch")
+        traffic = json.load(open(tf)).get("dram_bytes_per_step")
     ref_gpu = None
     if rank == 0 and not args.no_suite:
         ns = argparse.Namespace(**vars(args))
@@ -699,6 +699,73 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_profile(args):
+    """One workload between cudaProfilerStart/Stop for ncu (--profile-from-start off),
+    after warm-up: `fft[:LOG]` (8 columns at LOG, interpolate + blowup-4 evaluate, two
+    steps), `proof:L,N` (one wide-Fibonacci proof, log_blowup 1, 3 queries, pow_bits 5)
+    or `merkle` (the 64 x 2^22 tree of the kernel sweep)."""
+    import numpy as np
+    import torch
+    stwo = load_package()
+    L = stwo._lib
+    lib = L.lib()
+    dev = torch.device("cuda", 0)
+    what = args.profile
+    if what.startswith("fft"):
+        lg = int(what.split(":")[1]) if ":" in what else 24
+        ncols, lb = 8, 2
+        N = lg + lb
+        sptr = torch.cuda.current_stream(dev).cuda_stream
+        hc = stwo.CanonicCoset(N).half_coset()
+        tsz = 1 << hc.log_size
+        tw = torch.empty(tsz, dtype=torch.int32, device=dev)
+        itw = torch.empty(tsz, dtype=torch.int32, device=dev)
+        L.check(lib.stwo_precompute_twiddles(hc.initial_index, hc.step_size, hc.log_size, tw.data_ptr(),
+                                             itw.data_ptr(), sptr))
+        evals = [torch.randint(0, P, (1 << lg,), dtype=torch.int64, device=dev).to(torch.int32) for _ in range(ncols)]
+        outs = [torch.empty(1 << N, dtype=torch.int32, device=dev) for _ in range(ncols)]
+        ev_p, out_p, logs = L.ptr_array([t.data_ptr() for t in evals]), L.ptr_array([t.data_ptr() for t in outs]), \
+            L.u32_array([lg] * ncols)
+
+        def work():
+            L.check(lib.stwo_interpolate_columns(ev_p, logs, ncols, itw.data_ptr(), tsz, sptr))
+            L.check(lib.stwo_extend_evaluate_columns(ev_p, logs, out_p, lb, ncols, tw.data_ptr(), tsz, sptr))
+        reps = 2
+    elif what.startswith("proof:"):
+        lg, nc = (int(x) for x in what.split(":")[1].split(","))
+        job = stwo.WideFibJob(lg, nc, 1, 3, 5)
+        a0, a1 = stwo.wide_fib_inputs(lg, 7)
+
+        def work():
+            stwo.prove_wide_fib(job, a0, a1)
+        reps = 1
+    elif what == "merkle":
+        lg, nc = 22, 64
+        sptr = torch.cuda.current_stream(dev).cuda_stream
+        cols = [torch.randint(0, P, (1 << lg,), dtype=torch.int64, device=dev).to(torch.int32) for _ in range(nc)]
+        layers = [torch.empty(8 << l, dtype=torch.int32, device=dev) for l in range(lg + 1)]
+        cptr = L.ptr_array([c.data_ptr() for c in cols])
+
+        def work():
+            L.check(lib.stwo_merkle_commit_layer(lg, None, cptr, nc, layers[lg].data_ptr(), sptr))
+            for l in range(lg - 1, -1, -1):
+                L.check(lib.stwo_merkle_commit_layer(l, layers[l + 1].data_ptr(), None, 0, layers[l].data_ptr(), sptr))
+        reps = 1
+    else:
+        raise SystemExit(f"unknown --profile {what}")
+    for _ in range(3):
+        work()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        work()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profile": what, "reps": reps, "wall_ms": (time.perf_counter() - t0) * 1e3}), flush=True)
+    del np
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -711,7 +778,12 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds of oracle work per CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-suite", action="store_true", help="skip the config-1 per-kernel sweep")
+    ap.add_argument("--profile", default=None,
+                    help="run one workload for ncu instead: fft[:LOG] | proof:L,N | merkle")
     args = ap.parse_args()
+    if args.profile:
+        run_profile(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -8,9 +8,9 @@
 //   out = den_inv * sum_{i < N-2} (c_i^2 + c_{i+1}^2 - c_{i+2}) * powers[N-3-i].
 // The reference launches it with grid and block swapped and clones the column
 // pointer array with the wrong length (.cu:48,54); here the pointers travel in the
-// parameter block, each thread does four consecutive rows (16-byte loads per
-// column), and each QM31 coordinate of the sum accumulates unreduced partial
-// products in 64 bits, reduced once per row.
+// parameter block or a device table, each thread does two consecutive rows (8-byte
+// loads per column), and each QM31 coordinate of the sum accumulates unreduced
+// partial products in 64 bits, reduced once per row.
 #include <memory>
 
 #include "common.cuh"
@@ -63,33 +63,36 @@ __device__ __forceinline__ uint32_t reduce64_wf(uint64_t x) {
 }
 
 // Powers on the device: plain QM31 (the reference ABI) or, when DOUBLED, with every
-// coordinate already doubled for m31_mul2. Four rows per thread; the column loop
-// issues WF_PREFETCH loads before it consumes them, so each thread keeps several
-// DRAM requests in flight instead of one.
+// coordinate already doubled for m31_mul2. Two rows per thread (8-byte loads); the
+// column loop issues WF_PREFETCH loads before it consumes them, and the small
+// per-thread state (about 64 registers) keeps four CTAs of 256 threads per SM, so
+// enough loads are in flight to cover DRAM latency.
 template <bool DOUBLED, int CAP>
-__global__ void __launch_bounds__(256) wide_fib_kernel(const __grid_constant__ WideFibParams<CAP> p) {
+__global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant__ WideFibParams<CAP> p) {
     const uint64_t n = 1ull << p.log_size;
-    const uint64_t quads = (n + 3) / 4;
+    const uint64_t pairs = (n + 1) / 2;
     auto colp = [&](uint32_t c) { return CAP == 1 ? p.trace_dev[c] : p.trace[c]; };
-    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < quads; k += (uint64_t)gridDim.x * blockDim.x) {
-        const bool full = 4 * k + 3 < n;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < pairs; k += (uint64_t)gridDim.x * blockDim.x) {
+        const bool full = 2 * k + 1 < n;
         auto load = [&](uint32_t col, uint32_t *v) {
             const uint32_t *c = colp(col);
             if (full) {
-                uint4 t = __ldg(reinterpret_cast<const uint4 *>(c) + k);
-                v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+                uint2 t = __ldg(reinterpret_cast<const uint2 *>(c) + k);
+                v[0] = t.x;
+                v[1] = t.y;
             } else {
-                for (int r = 0; r < 4; r++) v[r] = (4 * k + r < n) ? c[4 * k + r] : 0u;
+                v[0] = c[2 * k];
+                v[1] = 0u;
             }
         };
-        uint64_t acc[4][4] = {};
-        uint32_t c0[4], c1[4];
+        uint64_t acc[2][4] = {};
+        uint32_t c0[2], c1[2];
         load(0, c0);
         load(1, c1);
-        uint32_t s0[4], s1[4];
-        for (int r = 0; r < 4; r++) { s0[r] = m31_sqr(c0[r]); s1[r] = m31_sqr(c1[r]); }
+        uint32_t s0[2], s1[2];
+        for (int r = 0; r < 2; r++) { s0[r] = m31_sqr(c0[r]); s1[r] = m31_sqr(c1[r]); }
         for (uint32_t base = 2; base < p.n_cols; base += WF_PREFETCH) {
-            uint32_t buf[WF_PREFETCH][4];
+            uint32_t buf[WF_PREFETCH][2];
 #pragma unroll
             for (int u = 0; u < WF_PREFETCH; u++)
                 if (base + u < p.n_cols) load(base + u, buf[u]);
@@ -100,7 +103,7 @@ __global__ void __launch_bounds__(256) wide_fib_kernel(const __grid_constant__ W
                 qm31 w2 = p.powers_dev[p.n_cols - 1 - col];  // constraint col - 2 takes powers[N-3-(col-2)]
                 if (!DOUBLED) w2 = {{w2.a.a << 1, w2.a.b << 1}, {w2.b.a << 1, w2.b.b << 1}};
 #pragma unroll
-                for (int r = 0; r < 4; r++) {
+                for (int r = 0; r < 2; r++) {
                     uint32_t cons = m31_sub(m31_add(s0[r], s1[r]), buf[u][r]);
                     acc[r][0] += mul_lazy_wf(cons, w2.a.a);
                     acc[r][1] += mul_lazy_wf(cons, w2.a.b);
@@ -111,26 +114,24 @@ __global__ void __launch_bounds__(256) wide_fib_kernel(const __grid_constant__ W
                 }
             }
         }
-        uint32_t o[4][4];
-        for (int r = 0; r < 4; r++) {
-            uint32_t d = (4 * k + r < n) ? __ldg(p.den_inv + 4 * k + r) : 0u;
+        uint32_t o[4][2];
+        for (int r = 0; r < 2; r++) {
+            uint32_t d = (2 * k + r < n) ? __ldg(p.den_inv + 2 * k + r) : 0u;
             uint32_t d2 = d << 1;
             for (int c = 0; c < 4; c++) o[c][r] = m31_mul2(reduce64_wf(acc[r][c]), d2);
         }
         for (int c = 0; c < 4; c++) {
-            if (full) reinterpret_cast<uint4 *>(p.out[c])[k] = make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
-            else
-                for (int r = 0; r < 4; r++)
-                    if (4 * k + r < n) p.out[c][4 * k + r] = o[c][r];
+            if (full) reinterpret_cast<uint2 *>(p.out[c])[k] = make_uint2(o[c][0], o[c][1]);
+            else p.out[c][2 * k] = o[c][0];
         }
     }
 }
 
 template <bool DOUBLED, int CAP>
-void launch_wf(const WideFibParams<CAP> &p, uint64_t quads, cudaStream_t st) {
+void launch_wf(const WideFibParams<CAP> &p, uint64_t pairs, cudaStream_t st) {
     // Small domains: 64-thread CTAs so that more SMs share the rows.
-    const uint32_t threads = quads < (uint64_t)device_sm_count() * 256 ? 64 : 256;
-    uint64_t blocks = (quads + threads - 1) / threads, cap = (uint64_t)device_sm_count() * 32;
+    const uint32_t threads = pairs < (uint64_t)device_sm_count() * 256 ? 64 : 256;
+    uint64_t blocks = (pairs + threads - 1) / threads, cap = (uint64_t)device_sm_count() * 32;
     if (blocks > cap) blocks = cap;
     wide_fib_kernel<DOUBLED, CAP><<<(unsigned)blocks, threads, 0, st>>>(p);
 }
@@ -152,9 +153,9 @@ int wide_fib_launch(const uint32_t *const *trace, const uint32_t *const *trace_d
     p->n_cols = n_cols;
     p->log_size = log_size;
     p->powers_dev = reinterpret_cast<const qm31 *>(powers_dev);
-    const uint64_t n = 1ull << log_size, quads = (n + 3) / 4;
+    const uint64_t n = 1ull << log_size, pairs = (n + 1) / 2;
     if (powers_dev) {
-        launch_wf<false>(*p, quads, st);
+        launch_wf<false>(*p, pairs, st);
         STWO_LAUNCH_CHECK("wide_fib_kernel");
         return STWO_OK;
     }
@@ -173,7 +174,7 @@ int wide_fib_launch(const uint32_t *const *trace, const uint32_t *const *trace_d
     cudaError_t e = cudaMemcpyAsync(buf, w2.get(), sizeof(qm31) * (n_cols - 2), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         p->powers_dev = static_cast<const qm31 *>(buf);
-        launch_wf<true>(*p, quads, st);
+        launch_wf<true>(*p, pairs, st);
         count_launch();
         e = cudaGetLastError();
     }

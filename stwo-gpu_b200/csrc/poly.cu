@@ -87,12 +87,19 @@ __global__ void canonic_to_bitrev_kernel(const uint32_t *__restrict__ src, uint3
 
 // ------------------------------------------------------------------ eval_at_point
 // p(P) = sum_i c_i prod_{bit b of i} f_b with f_0 = y, f_1 = x, f_b = pi^(b-1)(x),
-// pi(x) = 2x^2 - 1 (eval_at_point.cu:99-109). Each CTA folds a chunk of 2^CHUNK_LOG
-// coefficients (bits 0..CHUNK_LOG-1) and multiplies by the factors of its chunk
-// index; the last CTA of each polynomial (atomic ticket) adds the partials.
+// pi(x) = 2x^2 - 1 (eval_at_point.cu:99-109). A CTA folds a chunk of 2^15
+// coefficients as 4 groups of 8192: a thread takes 32 consecutive coefficients (bits
+// 0..4) and forms sum_i c_i F_i against the CTA's table F_i = prod_{b in i} f_b, an
+// M31-by-QM31 dot product accumulated unreduced in 64 bits; the lanes fold bits 5..9
+// and the warps bits 10..12. Group partials are weighted by their group index's
+// factors (bits 13..14) before the lane fold, which is linear, so one fold serves the
+// whole chunk. The chunk partial takes the factors of its chunk index; the last CTA
+// of each polynomial (atomic ticket) adds the partials.
 constexpr int EAP_THREADS = 256;
-constexpr int EAP_PER_THREAD_LOG = 3;
-constexpr int EAP_CHUNK_LOG = 11;  // 256 threads x 8 coefficients
+constexpr int EAP_PER_THREAD_LOG = 5;                    // 32 coefficients per thread
+constexpr int EAP_GROUP_LOG = EAP_PER_THREAD_LOG + 8;    // x 256 threads
+constexpr int EAP_ITER_LOG = 2;                          // groups per CTA: 4
+constexpr int EAP_CHUNK_LOG = EAP_GROUP_LOG + EAP_ITER_LOG;
 constexpr int EAP_MAX_POLYS = 32;
 
 struct EapParams {
@@ -114,35 +121,73 @@ __device__ __forceinline__ qm31 shfl_xor_q(qm31 v, int m) {
     return v;
 }
 
+// Unreduced product of a in [0, P) and b2 = 2b: a value congruent to a*b in [0, 2^32).
+__device__ __forceinline__ uint32_t mul_lazy_e(uint32_t a, uint32_t b2) {
+    const uint64_t w = (uint64_t)a * b2;
+    return (uint32_t)(w >> 32) + ((uint32_t)w >> 1);
+}
+__device__ __forceinline__ uint32_t reduce64_e(uint64_t x) {
+    uint64_t s = (x & P) + (x >> 31);
+    s = (s & P) + (s >> 31);
+    return reduce_once((uint32_t)s);
+}
+
 // One CTA's share of polynomial `poly`: chunk `chunk` of its 2^L coefficients c with
 // factors f; its CTAs are blk_first .. blk_first + nblk - 1 (partials indexed by CTA).
 __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t L, const qm31 *f, const uint32_t *c,
                                          uint32_t blk_first, uint32_t nblk, qm31 *partials, uint32_t *tickets,
                                          qm31 *results) {
     __shared__ qm31 warp_vals[EAP_THREADS / 32];
+    __shared__ qm31 g[1 << EAP_ITER_LOG];
+    __shared__ qm31 F2[1 << EAP_PER_THREAD_LOG];  // F_i with coordinates doubled (for mul_lazy)
     __shared__ bool is_last;
     const uint32_t tid = threadIdx.x;
     const uint64_t n = 1ull << L;
-    const uint64_t base = ((uint64_t)chunk << EAP_CHUNK_LOG) + ((uint64_t)tid << EAP_PER_THREAD_LOG);
-
-    // Per-thread fold of 8 coefficients (bits 0..2); bits beyond L read as absent.
-    qm31 acc = qm31_zero();
-    if (base < n) {
-        uint32_t v[8];
-        const uint32_t cnt = (n - base) < 8 ? (uint32_t)(n - base) : 8u;
-        for (uint32_t i = 0; i < 8; i++) v[i] = i < cnt ? __ldg(c + base + i) : 0u;
-        qm31 lvl[4];
-        for (int i = 0; i < 4; i++) {
-            // v[2i] + v[2i+1] * f0
-            qm31 t = qm31_scale(f[0], v[2 * i + 1]);
-            t.a.a = m31_add(t.a.a, v[2 * i]);
-            lvl[i] = t;
-        }
-        lvl[0] = qm31_add(lvl[0], qm31_mul(lvl[1], f[1]));
-        lvl[2] = qm31_add(lvl[2], qm31_mul(lvl[3], f[1]));
-        acc = qm31_add(lvl[0], qm31_mul(lvl[2], f[2]));
+    if (tid < (1u << EAP_PER_THREAD_LOG)) {
+        qm31 w = qm31_one();
+        for (int b = 0; b < EAP_PER_THREAD_LOG; b++)
+            if ((tid >> b) & 1u) w = qm31_mul(w, f[b]);
+        F2[tid] = {{w.a.a << 1, w.a.b << 1}, {w.b.a << 1, w.b.b << 1}};
+    } else if (tid < (1u << EAP_PER_THREAD_LOG) + (1u << EAP_ITER_LOG)) {
+        // group weights: products of f_{13+b} over the set bits b of the group index
+        const uint32_t it = tid - (1u << EAP_PER_THREAD_LOG);
+        qm31 w = qm31_one();
+        for (int b = 0; b < EAP_ITER_LOG; b++)
+            if ((it >> b) & 1u) w = qm31_mul(w, f[EAP_GROUP_LOG + b]);
+        g[it] = w;
     }
-    // Across lanes: bits 3..7 (lane bit j <-> factor 3 + j).
+    __syncthreads();
+
+    qm31 acc = qm31_zero();
+    for (uint32_t it = 0; it < (1u << EAP_ITER_LOG); it++) {
+        const uint64_t base = ((uint64_t)chunk << EAP_CHUNK_LOG) + ((uint64_t)it << EAP_GROUP_LOG) +
+                              ((uint64_t)tid << EAP_PER_THREAD_LOG);
+        if (base >= n) break;
+        uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        auto term = [&](uint32_t v, uint32_t i) {
+            const qm31 w = F2[i];
+            s0 += mul_lazy_e(v, w.a.a);
+            s1 += mul_lazy_e(v, w.a.b);
+            s2 += mul_lazy_e(v, w.b.a);
+            s3 += mul_lazy_e(v, w.b.b);
+        };
+        if (base + 32 <= n) {
+            const uint4 *q = reinterpret_cast<const uint4 *>(c + base);
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const uint4 x = __ldg(q + u);
+                term(x.x, 4 * u);
+                term(x.y, 4 * u + 1);
+                term(x.z, 4 * u + 2);
+                term(x.w, 4 * u + 3);
+            }
+        } else {
+            for (uint32_t i = 0; base + i < n && i < 32; i++) term(__ldg(c + base + i), i);
+        }
+        const qm31 part = {{reduce64_e(s0), reduce64_e(s1)}, {reduce64_e(s2), reduce64_e(s3)}};
+        acc = qm31_add(acc, it == 0 ? part : qm31_mul(part, g[it]));
+    }
+    // Across lanes: bits 5..9 (lane bit j <-> factor 5 + j).
     const uint32_t lane = tid & 31u;
 #pragma unroll
     for (int j = 0; j < 5; j++) {
@@ -150,19 +195,19 @@ __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t
         // lane with bit j clear keeps lo + hi * f; the other result is discarded.
         qm31 lo = (lane >> j) & 1u ? other : acc;
         qm31 hi = (lane >> j) & 1u ? acc : other;
-        acc = qm31_add(lo, qm31_mul(hi, f[3 + j]));
+        acc = qm31_add(lo, qm31_mul(hi, f[EAP_PER_THREAD_LOG + j]));
     }
     if (lane == 0) warp_vals[tid >> 5] = acc;
     __syncthreads();
     if (tid == 0) {
-        // Warps: bits 8..10.
+        // Warps: bits 10..12.
         qm31 w[8];
         for (int i = 0; i < 8; i++) w[i] = warp_vals[i];
         for (int lvl = 0; lvl < 3; lvl++)
             for (int i = 0; i < (8 >> (lvl + 1)); i++)
-                w[i] = qm31_add(w[2 * i], qm31_mul(w[2 * i + 1], f[8 + lvl]));
+                w[i] = qm31_add(w[2 * i], qm31_mul(w[2 * i + 1], f[EAP_PER_THREAD_LOG + 5 + lvl]));
         qm31 s = w[0];
-        // Chunk index bits -> factors 11.. .
+        // Chunk index bits -> factors 15.. .
         for (uint32_t b = 0; EAP_CHUNK_LOG + b < L; b++)
             if ((chunk >> b) & 1u) s = qm31_mul(s, f[EAP_CHUNK_LOG + b]);
         partials[blockIdx.x] = s;

@@ -184,36 +184,47 @@ __host__ __device__ inline cpoint vanishing_shift(uint32_t log) {
     return point_mul(point_conj(init), half_step);
 }
 
-// Channel step after the OODS evaluation: mix the sampled values (N trace values, then
-// the composition's 4 coordinates), check the composition against the constraints at
-// the OODS point, draw the quotient coefficient and fill the quotient kernels'
-// sample-dependent parameters of both column groups.
-__global__ void fs_oods_kernel(ProofState *s, const qm31 *sampled, uint32_t N, uint32_t L, QuotParamsDev *q_comp,
-                               QuotParamsDev *q_trace) {
-    fs::ch_mix_felts(s->ch, sampled, N + 4);
-    // composition value: from_partial_evals over the basis 1, i, u, iu
-    const qm31 basis[4] = {{{1, 0}, {0, 0}}, {{0, 1}, {0, 0}}, {{0, 0}, {1, 0}}, {{0, 0}, {0, 1}}};
-    qm31 comp = qm31_zero();
-    for (int k = 0; k < 4; k++) comp = qm31_add(comp, qm31_mul(sampled[N + k], basis[k]));
-    // constraints: sum_i r^(N-3-i) (c_i^2 + c_{i+1}^2 - c_{i+2}) / coset_vanishing(oods)
-    const cpoint sh = vanishing_shift(L);
+// Channel step after the OODS evaluation, by one CTA: the constraint sum
+// sum_i r^(N-3-i) (c_i^2 + c_{i+1}^2 - c_{i+2}) over the sampled trace values (powers
+// from fs_trace_kernel), checked against the composition's sampled value times the
+// vanishing polynomial at the OODS point; thread 0 mixes the sampled values (N trace
+// values, then the composition's 4 coordinates) and draws the quotient coefficient;
+// then the quotient kernels' sample-dependent parameters of both column groups.
+__global__ void __launch_bounds__(256) fs_oods_kernel(ProofState *s, const qm31 *sampled, const qm31 *powers,
+                                                      uint32_t N, uint32_t L, QuotParamsDev *q_comp,
+                                                      QuotParamsDev *q_trace) {
+    __shared__ qm31 sh[32];
+    __shared__ qm31 qrc_sh;
+    qm31 part = qm31_zero();
+    for (uint32_t i = threadIdx.x; i + 2 < N; i += blockDim.x) {
+        const qm31 cons = qm31_sub(
+            qm31_add(qm31_mul(sampled[i], sampled[i]), qm31_mul(sampled[i + 1], sampled[i + 1])), sampled[i + 2]);
+        part = qm31_add(part, qm31_mul(cons, powers[N - 3 - i]));
+    }
+    const qm31 acc = block_sum_qm31(part, sh);
     const qm31 ox = s->oods[0], oy = s->oods[1];
-    qm31 x = qm31_sub(qm31_scale(ox, sh.x), qm31_scale(oy, sh.y));
-    for (uint32_t d = 0; d + 1 < L; d++) {
-        qm31 q = qm31_mul(x, x);
-        x = qm31_sub(qm31_add(q, q), qm31_one());
+    if (threadIdx.x == 0) {
+        // composition value: from_partial_evals over the basis 1, i, u, iu
+        const qm31 basis[4] = {{{1, 0}, {0, 0}}, {{0, 1}, {0, 0}}, {{0, 0}, {1, 0}}, {{0, 0}, {0, 1}}};
+        qm31 comp = qm31_zero();
+        for (int k = 0; k < 4; k++) comp = qm31_add(comp, qm31_mul(sampled[N + k], basis[k]));
+        // coset_vanishing(CanonicCoset(L).coset, oods)
+        const cpoint sh_pt = vanishing_shift(L);
+        qm31 x = qm31_sub(qm31_scale(ox, sh_pt.x), qm31_scale(oy, sh_pt.y));
+        for (uint32_t d = 0; d + 1 < L; d++) {
+            qm31 q = qm31_mul(x, x);
+            x = qm31_sub(qm31_add(q, q), qm31_one());
+        }
+        if (!qm31_eq(qm31_mul(acc, qm31_inv(x)), comp)) s->error |= fs::ERR_CONSTRAINTS;
+        fs::ch_mix_felts(s->ch, sampled, N + 4);
+        const qm31 qrc = fs::ch_draw_felt(s->ch, s->error);
+        s->qrc = qrc;
+        qrc_sh = qrc;
     }
-    qm31 acc = qm31_zero();
-    for (uint32_t i = 0; i + 2 < N; i++) {
-        qm31 cons = qm31_sub(qm31_add(qm31_mul(sampled[i], sampled[i]), qm31_mul(sampled[i + 1], sampled[i + 1])),
-                             sampled[i + 2]);
-        acc = qm31_add(qm31_mul(acc, s->rc), cons);
-    }
-    if (!qm31_eq(qm31_mul(acc, qm31_inv(x)), comp)) s->error |= fs::ERR_CONSTRAINTS;
-    const qm31 qrc = fs::ch_draw_felt(s->ch, s->error);
-    s->qrc = qrc;
-    quot_fill_batch(*q_comp, 0, qrc, ox, oy, sampled + N, 4, 0);
-    quot_fill_batch(*q_trace, 0, qrc, ox, oy, sampled, N, 0);
+    __syncthreads();
+    const qm31 qrc = qrc_sh;
+    quot_fill_batch_block(*q_comp, 0, qrc, ox, oy, sampled + N, 4, 0, sh);
+    quot_fill_batch_block(*q_trace, 0, qrc, ox, oy, sampled, N, 0, sh);
 }
 
 // Channel step after an FRI tree: mix its root, draw the folding alpha.
@@ -827,13 +838,13 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     // ---- 3. out-of-domain sampling
     PV_TRY(eval_at_points_dev_async(dev_at(off_eap), eap_n, eap_total, dstate->oods, dsampled, eap_partials, dtickets,
                                     st));
-    fs_oods_kernel<<<1, 1, 0, st>>>(dstate, dsampled, N, L, dqc, dqt);
+    fs_oods_kernel<<<1, 256, 0, st>>>(dstate, dsampled, powers, N, L, dqc, dqt);
     STWO_LAUNCH_CHECK("fs_oods_kernel");
     if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[3], st));
 
     // ---- 4. DEEP quotients (largest columns first) and the FRI commitment
-    PV_TRY(quotients_dev_async(dqc, D, st));
-    PV_TRY(quotients_dev_async(dqt, L + B, st));
+    PV_TRY(quotients_dev_async(dqc, D, 4, st));
+    PV_TRY(quotients_dev_async(dqt, L + B, N, st));
     PV_TRY(commit(t_fri0));
     fs_layer_kernel<<<1, 1, 0, st>>>(dstate, t_fri0.layers[0], 2, 0);
     STWO_LAUNCH_CHECK("fs_layer_kernel");

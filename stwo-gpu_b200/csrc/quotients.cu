@@ -59,10 +59,24 @@ __device__ __forceinline__ uint32_t reduce64(uint64_t x) {
     return reduce_once((uint32_t)s);
 }
 
-template <bool COLS_ON_DEVICE, class PR>
+// STAGE: the CTA first copies every sample's column pointer and doubled coefficient
+// into shared memory (n_stage samples), so the column loop reads them there instead
+// of chasing col_idx -> cols through global memory (device-resident parameters).
+template <bool COLS_ON_DEVICE, bool STAGE, class PR>
 __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ PR pr,
-                                                        const uint32_t *const *__restrict__ dev_cols) {
+                                                        const uint32_t *const *__restrict__ dev_cols,
+                                                        uint32_t n_stage) {
     const auto &p = pr.get();
+    extern __shared__ uint4 q_smem[];
+    qm31 *s_c2 = reinterpret_cast<qm31 *>(q_smem);
+    const uint32_t **s_cols = reinterpret_cast<const uint32_t **>(s_c2 + (STAGE ? n_stage : 0));
+    if (STAGE) {
+        for (uint32_t j = threadIdx.x; j < n_stage; j += blockDim.x) {
+            s_c2[j] = p.c2[j];
+            s_cols[j] = COLS_ON_DEVICE ? dev_cols[p.col_idx[j]] : p.cols[p.col_idx[j]];
+        }
+        __syncthreads();
+    }
     const uint64_t n_pairs = 1ull << (p.log_size - 1);
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_pairs;
          k += (uint64_t)gridDim.x * blockDim.x) {
@@ -104,14 +118,15 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                 for (int u = 0; u < QUOT_PREFETCH; u++) {
                     const uint32_t j = jb + u;
                     if (j < j1) {
-                        const uint32_t *col = COLS_ON_DEVICE ? dev_cols[p.col_idx[j]] : p.cols[p.col_idx[j]];
+                        const uint32_t *col = STAGE ? s_cols[j]
+                                                    : (COLS_ON_DEVICE ? dev_cols[p.col_idx[j]] : p.cols[p.col_idx[j]]);
                         v[u] = __ldg(reinterpret_cast<const uint2 *>(col) + k);
                     }
                 }
 #pragma unroll
                 for (int u = 0; u < QUOT_PREFETCH; u++) {
                     if (jb + u >= j1) break;
-                    const qm31 c2 = p.c2[jb + u];
+                    const qm31 c2 = STAGE ? s_c2[jb + u] : p.c2[jb + u];
                     s0[0][0] += mul_lazy(v[u].x, c2.a.a); s0[0][1] += mul_lazy(v[u].x, c2.a.b);
                     s0[0][2] += mul_lazy(v[u].x, c2.b.a); s0[0][3] += mul_lazy(v[u].x, c2.b.b);
                     s0[1][0] += mul_lazy(v[u].y, c2.a.a); s0[1][1] += mul_lazy(v[u].y, c2.a.b);
@@ -174,19 +189,21 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    if (cols_on_device) quotients_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(*holder, cols);
-    else quotients_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(*holder, nullptr);
+    if (cols_on_device) quotients_kernel<true, false><<<(unsigned)blocks, 256, 0, st>>>(*holder, cols, 0u);
+    else quotients_kernel<false, false><<<(unsigned)blocks, 256, 0, st>>>(*holder, nullptr, 0u);
     STWO_LAUNCH_CHECK("quotients_kernel");
     return STWO_OK;
 }
 
-int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, cudaStream_t st) {
+int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t n_samples, cudaStream_t st) {
     STWO_REQUIRE(log_size >= 1 && log_size <= 31, STWO_ERR_UNSUPPORTED_SIZE, "domain log size %u", log_size);
+    STWO_REQUIRE(n_samples >= 1 && n_samples <= 1024, STWO_ERR_UNSUPPORTED_SIZE, "%u samples", n_samples);
+    const size_t smem = (size_t)n_samples * (sizeof(qm31) + sizeof(void *));
     uint64_t pairs = 1ull << (log_size - 1);
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    quotients_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(QuotByRef{p_dev}, nullptr);
+    quotients_kernel<false, true><<<(unsigned)blocks, 256, smem, st>>>(QuotByRef{p_dev}, nullptr, n_samples);
     STWO_LAUNCH_CHECK("quotients_kernel");
     return STWO_OK;
 }

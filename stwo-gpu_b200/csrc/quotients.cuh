@@ -60,6 +60,57 @@ __host__ __device__ inline void quot_fill_batch(QP &p, uint32_t b, qm31 rc, qm31
     p.b_sum[b] = bs;
 }
 
+// Sum of one QM31 per thread over a CTA of blockDim.x <= 1024 threads; every thread
+// gets the sum. sh: 32 QM31 of shared memory.
+__device__ inline qm31 block_sum_qm31(qm31 v, qm31 *sh) {
+    for (int m = 16; m >= 1; m >>= 1) {
+        v.a.a = m31_add(v.a.a, __shfl_xor_sync(0xffffffffu, v.a.a, m));
+        v.a.b = m31_add(v.a.b, __shfl_xor_sync(0xffffffffu, v.a.b, m));
+        v.b.a = m31_add(v.b.a, __shfl_xor_sync(0xffffffffu, v.b.a, m));
+        v.b.b = m31_add(v.b.b, __shfl_xor_sync(0xffffffffu, v.b.b, m));
+    }
+    __syncthreads();  // sh may hold a previous call's values
+    if ((threadIdx.x & 31u) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    qm31 s = qm31_zero();
+    for (uint32_t w = 0; w < (blockDim.x + 31) / 32; w++) s = qm31_add(s, sh[w]);
+    return s;
+}
+
+// quot_fill_batch by a whole CTA: thread t takes samples t, t + T, ... with
+// alpha = rc^(j+1), and the a / b sums are reduced across the CTA.
+template <class QP>
+__device__ inline void quot_fill_batch_block(QP &p, uint32_t b, qm31 rc, qm31 px, qm31 py, const qm31 *vals,
+                                             uint32_t count, uint32_t off, qm31 *sh) {
+    const uint32_t T = blockDim.x;
+    const qm31 c0 = qm31_sub(qm31_conj(py), py);
+    const qm31 step = qm31_pow(rc, T);
+    qm31 alpha = qm31_pow(rc, threadIdx.x + 1), as = qm31_zero(), bs = qm31_zero();
+    for (uint32_t j = threadIdx.x; j < count; j += T) {
+        const qm31 v = vals[j];
+        qm31 a = qm31_sub(qm31_conj(v), v);
+        qm31 bb = qm31_sub(qm31_mul(v, c0), qm31_mul(a, py));
+        a = qm31_mul(alpha, a);
+        bb = qm31_mul(alpha, bb);
+        const qm31 c = qm31_mul(alpha, c0);
+        as = qm31_add(as, a);
+        bs = qm31_add(bs, bb);
+        p.c2[off + j] = {{c.a.a << 1, c.a.b << 1}, {c.b.a << 1, c.b.b << 1}};
+        alpha = qm31_mul(alpha, step);
+    }
+    as = block_sum_qm31(as, sh);
+    bs = block_sum_qm31(bs, sh);
+    if (threadIdx.x == 0) {
+        p.prx[b] = px.a;
+        p.pix[b] = px.b;
+        p.pry[b] = py.a;
+        p.piy[b] = py.b;
+        p.batch_coeff[b] = qm31_pow(rc, count);
+        p.a_sum[b] = as;
+        p.b_sum[b] = bs;
+    }
+}
+
 // The column-independent fields: domain, outputs, generator table.
 template <class QP>
 inline void quot_init_static(QP &p, uint32_t half_init, uint32_t half_step, uint32_t log_size, uint32_t *const *out4) {
@@ -74,7 +125,8 @@ inline void quot_init_static(QP &p, uint32_t half_init, uint32_t half_step, uint
     for (int c = 0; c < 4; c++) p.out[c] = out4[c];
 }
 
-// Launches the quotient kernel on parameters resident in device memory.
-int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, cudaStream_t st);
+// Launches the quotient kernel on parameters resident in device memory (n_samples:
+// the total sample count, batch_end of the last batch).
+int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t n_samples, cudaStream_t st);
 
 }  // namespace stwo
