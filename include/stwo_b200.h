@@ -249,7 +249,7 @@ int stwo_wide_fib_composition(const uint32_t *const *trace, uint32_t n_columns, 
  * PcsConfig{pow_bits, FriConfig{log_last_layer_degree_bound = 0, log_blowup, n_queries}}
  * and a Blake2s channel starting from the zero digest. Limits: 3 <= n_columns <= 1024,
  * 1 <= log_blowup <= 4, 2 <= log_n_rows, log_n_rows + 1 + log_blowup <= 27,
- * 1 <= n_queries <= 1024, pow_bits <= 40. */
+ * 1 <= n_queries <= 1024, pow_bits <= 32 (the search gives up after 2^(pow_bits+6) nonces). */
 typedef struct {
     uint32_t log_n_rows;
     uint32_t n_columns;

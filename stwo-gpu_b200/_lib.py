@@ -7,7 +7,8 @@ import ctypes as C
 import os
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "lib", "libstwo_b200.so")
+# STWO_B200_LIB selects another build of the library (for A/B measurements).
+LIB_PATH = os.environ.get("STWO_B200_LIB") or os.path.join(PKG, "lib", "libstwo_b200.so")
 
 u32 = C.c_uint32
 u64 = C.c_uint64

@@ -573,7 +573,7 @@ int validate(const Job &j) {
                  "trace log size %u with log blowup %u unsupported", j.L, j.B);
     STWO_REQUIRE(j.n_queries >= 1 && j.n_queries <= MAX_QUERIES, STWO_ERR_UNSUPPORTED_SIZE, "%u queries unsupported",
                  j.n_queries);
-    STWO_REQUIRE(j.pow_bits <= 40, STWO_ERR_UNSUPPORTED_SIZE, "pow_bits %u unsupported (0..40)", j.pow_bits);
+    STWO_REQUIRE(j.pow_bits <= 32, STWO_ERR_UNSUPPORTED_SIZE, "pow_bits %u unsupported (0..32)", j.pow_bits);
     return STWO_OK;
 }
 
@@ -881,7 +881,7 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         const uint64_t want = 1ull << std::min<uint32_t>(j.pow_bits + 2, 24);  // a few times the expected tries
         const uint64_t threads = std::max<uint64_t>(256, std::min<uint64_t>(want, (uint64_t)device_sm_count() * 1024));
         const uint64_t blocks = (threads + 255) / 256, grid = blocks * 256;
-        const uint64_t max_k = ((1ull << (j.pow_bits + 8)) + grid - 1) / grid + 1;  // gives up after 2^(pow_bits+8)
+        const uint64_t max_k = ((1ull << (j.pow_bits + 6)) + grid - 1) / grid + 1;  // gives up after 2^(pow_bits+6)
         grind_kernel<<<(unsigned)blocks, 256, 0, st>>>(dstate, j.pow_bits, max_k);
         STWO_LAUNCH_CHECK("grind_kernel");
         fs_finish_kernel<<<1, 1, 0, st>>>(dstate, j.n_queries);
@@ -903,7 +903,7 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
                  "constraints not satisfied at the out-of-domain point");
     STWO_REQUIRE(!(ps.error & fs::ERR_LAST_LAYER), STWO_ERR_INVALID_ARGUMENT, "FRI last layer exceeds its degree bound");
     STWO_REQUIRE(!(ps.error & fs::ERR_GRIND), STWO_ERR_INVALID_ARGUMENT, "no proof-of-work nonce within 2^%u tries",
-                 j.pow_bits + 8);
+                 j.pow_bits + 6);
 
     // Queries::generate over the largest quotient domain (log D).
     std::vector<uint64_t> queries;

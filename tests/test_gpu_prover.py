@@ -72,7 +72,7 @@ def test_gpu_prover_accepts_device_inputs():
 
 
 @pytest.mark.parametrize("bad", [(2, 2, 1, 3, 5), (1, 8, 1, 3, 5), (4, 8, 0, 3, 5), (4, 8, 5, 3, 5),
-                                 (4, 8, 1, 0, 5), (4, 2000, 1, 3, 5), (26, 8, 1, 3, 5)])
+                                 (4, 8, 1, 0, 5), (4, 2000, 1, 3, 5), (26, 8, 1, 3, 5), (4, 8, 1, 3, 33)])
 def test_gpu_prover_rejects_unsupported_jobs(bad):
     stwo = load_package()
     n = 1 << min(bad[0], 4)
