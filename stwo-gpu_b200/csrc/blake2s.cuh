@@ -10,6 +10,25 @@ namespace blake {
 
 __device__ __forceinline__ uint32_t rotr(uint32_t x, uint32_t c) { return __funnelshift_r(x, x, c); }
 
+#ifndef STWO_B2S_PRMT
+#define STWO_B2S_PRMT 1
+#endif
+// Byte-aligned rotations as byte permutes.
+__device__ __forceinline__ uint32_t rotr16(uint32_t x) {
+#if STWO_B2S_PRMT
+    return __byte_perm(x, 0, 0x1032);
+#else
+    return rotr(x, 16);
+#endif
+}
+__device__ __forceinline__ uint32_t rotr8(uint32_t x) {
+#if STWO_B2S_PRMT
+    return __byte_perm(x, 0, 0x0321);
+#else
+    return rotr(x, 8);
+#endif
+}
+
 __device__ constexpr uint32_t IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
                             0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
 
@@ -24,11 +43,11 @@ __device__ __forceinline__ uint32_t add_on_fma(uint32_t c, uint32_t d, uint32_t 
 
 #define STWO_G(a, b, c, d, x, y)    \
     a = a + b + (x);                \
-    d = rotr(d ^ a, 16);            \
+    d = rotr16(d ^ a);              \
     c = add_on_fma(c, d, one);      \
     b = rotr(b ^ c, 12);            \
     a = a + b + (y);                \
-    d = rotr(d ^ a, 8);             \
+    d = rotr8(d ^ a);               \
     c = add_on_fma(c, d, one);      \
     b = rotr(b ^ c, 7);
 

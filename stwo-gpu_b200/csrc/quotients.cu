@@ -26,7 +26,10 @@ namespace stwo {
 namespace {
 
 using QuotParams = QuotParamsT<QUOT_MAX_COLS, QUOT_MAX_SAMPLES>;
-constexpr int QUOT_PREFETCH = 8;  // column loads in flight per thread
+#ifndef QUOT_PREFETCH_N
+#define QUOT_PREFETCH_N 4
+#endif
+constexpr int QUOT_PREFETCH = QUOT_PREFETCH_N;  // column loads per group (two groups in flight)
 
 // The kernel reads its parameters through get(): by value from the parameter block,
 // or from a device-resident block (the prover's, filled by the device channel).
@@ -110,10 +113,9 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
         for (uint32_t b = 0; b < p.n_batches; b++) {
             uint64_t s0[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
             const uint32_t j1 = p.batch_end[b];
-            // Column loads are issued QUOT_PREFETCH at a time before they are consumed,
-            // so each thread keeps several DRAM requests in flight.
-            for (uint32_t jb = j0; jb < j1; jb += QUOT_PREFETCH) {
-                uint2 v[QUOT_PREFETCH];
+            // Column loads in groups of QUOT_PREFETCH, double-buffered: the next group's
+            // loads are in flight while this group is accumulated.
+            auto load_group = [&](uint32_t jb, uint2 (&v)[QUOT_PREFETCH]) {
 #pragma unroll
                 for (int u = 0; u < QUOT_PREFETCH; u++) {
                     const uint32_t j = jb + u;
@@ -123,6 +125,8 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                         v[u] = __ldg(reinterpret_cast<const uint2 *>(col) + k);
                     }
                 }
+            };
+            auto consume = [&](uint32_t jb, const uint2 (&v)[QUOT_PREFETCH]) {
 #pragma unroll
                 for (int u = 0; u < QUOT_PREFETCH; u++) {
                     if (jb + u >= j1) break;
@@ -132,6 +136,14 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                     s0[1][0] += mul_lazy(v[u].y, c2.a.a); s0[1][1] += mul_lazy(v[u].y, c2.a.b);
                     s0[1][2] += mul_lazy(v[u].y, c2.b.a); s0[1][3] += mul_lazy(v[u].y, c2.b.b);
                 }
+            };
+            uint2 va[QUOT_PREFETCH], vb[QUOT_PREFETCH];
+            if (j0 < j1) load_group(j0, va);
+            for (uint32_t jb = j0; jb < j1; jb += 2 * QUOT_PREFETCH) {
+                if (jb + QUOT_PREFETCH < j1) load_group(jb + QUOT_PREFETCH, vb);
+                consume(jb, va);
+                if (jb + 2 * QUOT_PREFETCH < j1) load_group(jb + 2 * QUOT_PREFETCH, va);
+                if (jb + QUOT_PREFETCH < j1) consume(jb + QUOT_PREFETCH, vb);
             }
             j0 = j1;
             for (int s = 0; s < 2; s++) {

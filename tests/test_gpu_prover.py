@@ -151,3 +151,44 @@ def test_server_respects_the_memory_budget():
             big = (11, 64, 1, 3, 5)
             a0, a1 = stwo.wide_fib_inputs(11, 0)
             srv.submit(99, job_of(big), a0, a1)
+
+
+def test_concurrent_prove_calls_on_separate_streams_match():
+    """prove_wide_fib from several host threads, each on its own stream, gives each
+    job the same bytes as proving it alone."""
+    import threading
+    import torch
+    stwo = load_package()
+    jobs = [(7 + i % 5, 8 + 3 * i, 1 + (i % 2), 3, i % 6) for i in range(8)]
+    alone = []
+    for i, t in enumerate(jobs):
+        a0, a1 = stwo.wide_fib_inputs(t[0], 300 + i)
+        alone.append(stwo.prove_wide_fib(job_of(t), a0, a1)[0])
+    got = [None] * len(jobs)
+
+    def run(i):
+        torch.cuda.set_device(0)
+        s = torch.cuda.Stream()
+        a0, a1 = stwo.wide_fib_inputs(jobs[i][0], 300 + i)
+        for _ in range(2):
+            got[i] = stwo.prove_wide_fib(job_of(jobs[i]), a0, a1, stream=s.cuda_stream)[0]
+
+    th = [threading.Thread(target=run, args=(i,)) for i in range(len(jobs))]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    assert got == alone
+
+
+def test_server_shutdown_with_queued_jobs_is_clean():
+    stwo = load_package()
+    srv = stwo.ProofServer(n_workers=2, device_budget_bytes=4 << 30, max_domain_log=16)
+    for i in range(12):
+        a0, a1 = stwo.wide_fib_inputs(12, i)
+        srv.submit(i, job_of((12, 32, 1, 3, 5)), a0, a1)
+    srv.close()  # drops queued jobs, waits for running ones
+    # the library stays usable
+    a0, a1 = stwo.wide_fib_inputs(5, 2)
+    proof, _ = stwo.prove_wide_fib(job_of((5, 6, 1, 3, 5)), a0, a1)
+    assert stwo.verify(proof, 5, 6, 1, 3, 5)
