@@ -58,6 +58,21 @@ __host__ __device__ __forceinline__ uint32_t m31_mul2(uint32_t a, uint32_t b2) {
 
 __host__ __device__ __forceinline__ uint32_t m31_mul(uint32_t a, uint32_t b) { return m31_mul2(a, b << 1); }
 
+// Unreduced dot products: acc += a * b for canonical a, b (< P), one 32x32->64-bit
+// multiply-add per term. Each product is below 2^62, and a folded accumulator below
+// 2^34, so three terms fit between folds.
+__host__ __device__ __forceinline__ uint64_t mac64(uint64_t acc, uint32_t a, uint32_t b) {
+    return acc + (uint64_t)a * b;
+}
+// A value congruent to acc mod P, below 2^34.
+__host__ __device__ __forceinline__ uint64_t fold64(uint64_t acc) { return (acc & P) + (acc >> 31); }
+// acc mod P, canonical.
+__host__ __device__ __forceinline__ uint32_t reduce64_p(uint64_t acc) {
+    uint64_t s = (acc & P) + (acc >> 31);
+    s = (s & P) + (s >> 31);
+    return reduce_once((uint32_t)s);
+}
+
 __host__ __device__ __forceinline__ uint32_t m31_sqr(uint32_t a) { return m31_mul(a, a); }
 
 __host__ __device__ inline uint32_t m31_pow(uint32_t a, uint64_t e) {

@@ -37,7 +37,7 @@ __global__ void accumulate_kernel(const __grid_constant__ Acc4 p, uint64_t n4, u
 }
 
 constexpr int WF_MAX_COLS = 2048;
-constexpr int WF_PREFETCH = 8;  // column loads in flight per thread
+constexpr int WF_PREFETCH = 6;  // column loads in flight per thread (a multiple of the fold period 3)
 
 // Trace column pointers in the parameter block (CAP of them) or, for CAP == 1, in a
 // device table.
@@ -52,22 +52,12 @@ struct WideFibParams {
     uint32_t log_size;
 };
 
-__device__ __forceinline__ uint32_t mul_lazy_wf(uint32_t a, uint32_t b2) {
-    uint64_t w = (uint64_t)a * b2;
-    return (uint32_t)(w >> 32) + ((uint32_t)w >> 1);
-}
-__device__ __forceinline__ uint32_t reduce64_wf(uint64_t x) {
-    uint64_t s = (x & P) + (x >> 31);
-    s = (s & P) + (s >> 31);
-    return reduce_once((uint32_t)s);
-}
-
-// Powers on the device: plain QM31 (the reference ABI) or, when DOUBLED, with every
-// coordinate already doubled for m31_mul2. Two rows per thread (8-byte loads); the
-// column loop issues WF_PREFETCH loads before it consumes them, and the small
-// per-thread state (about 64 registers) keeps four CTAs of 256 threads per SM, so
-// enough loads are in flight to cover DRAM latency.
-template <bool DOUBLED, int CAP>
+// Powers on the device (plain QM31). Two rows per thread (8-byte loads); the column
+// loop issues WF_PREFETCH loads before it consumes them, and the small per-thread
+// state keeps four CTAs of 256 threads per SM, so enough loads are in flight to cover
+// DRAM latency. Each coordinate of the sum is a 64-bit multiply-accumulate of
+// canonical values, folded after every third column.
+template <int CAP>
 __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant__ WideFibParams<CAP> p) {
     const uint64_t n = 1ull << p.log_size;
     const uint64_t pairs = (n + 1) / 2;
@@ -100,15 +90,16 @@ __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant_
             for (int u = 0; u < WF_PREFETCH; u++) {
                 const uint32_t col = base + u;
                 if (col >= p.n_cols) break;
-                qm31 w2 = p.powers_dev[p.n_cols - 1 - col];  // constraint col - 2 takes powers[N-3-(col-2)]
-                if (!DOUBLED) w2 = {{w2.a.a << 1, w2.a.b << 1}, {w2.b.a << 1, w2.b.b << 1}};
+                const qm31 w = p.powers_dev[p.n_cols - 1 - col];  // constraint col - 2 takes powers[N-3-(col-2)]
 #pragma unroll
                 for (int r = 0; r < 2; r++) {
-                    uint32_t cons = m31_sub(m31_add(s0[r], s1[r]), buf[u][r]);
-                    acc[r][0] += mul_lazy_wf(cons, w2.a.a);
-                    acc[r][1] += mul_lazy_wf(cons, w2.a.b);
-                    acc[r][2] += mul_lazy_wf(cons, w2.b.a);
-                    acc[r][3] += mul_lazy_wf(cons, w2.b.b);
+                    const uint32_t cons = m31_sub(m31_add(s0[r], s1[r]), buf[u][r]);
+                    acc[r][0] = mac64(acc[r][0], cons, w.a.a);
+                    acc[r][1] = mac64(acc[r][1], cons, w.a.b);
+                    acc[r][2] = mac64(acc[r][2], cons, w.b.a);
+                    acc[r][3] = mac64(acc[r][3], cons, w.b.b);
+                    if (u % 3 == 2)
+                        for (int c = 0; c < 4; c++) acc[r][c] = fold64(acc[r][c]);
                     s0[r] = s1[r];
                     s1[r] = m31_sqr(buf[u][r]);
                 }
@@ -118,7 +109,7 @@ __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant_
         for (int r = 0; r < 2; r++) {
             uint32_t d = (2 * k + r < n) ? __ldg(p.den_inv + 2 * k + r) : 0u;
             uint32_t d2 = d << 1;
-            for (int c = 0; c < 4; c++) o[c][r] = m31_mul2(reduce64_wf(acc[r][c]), d2);
+            for (int c = 0; c < 4; c++) o[c][r] = m31_mul2(reduce64_p(acc[r][c]), d2);
         }
         for (int c = 0; c < 4; c++) {
             if (full) reinterpret_cast<uint2 *>(p.out[c])[k] = make_uint2(o[c][0], o[c][1]);
@@ -127,13 +118,13 @@ __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant_
     }
 }
 
-template <bool DOUBLED, int CAP>
+template <int CAP>
 void launch_wf(const WideFibParams<CAP> &p, uint64_t pairs, cudaStream_t st) {
     // Small domains: 64-thread CTAs so that more SMs share the rows.
     const uint32_t threads = pairs < (uint64_t)device_sm_count() * 256 ? 64 : 256;
     uint64_t blocks = (pairs + threads - 1) / threads, cap = (uint64_t)device_sm_count() * 32;
     if (blocks > cap) blocks = cap;
-    wide_fib_kernel<DOUBLED, CAP><<<(unsigned)blocks, threads, 0, st>>>(p);
+    wide_fib_kernel<CAP><<<(unsigned)blocks, threads, 0, st>>>(p);
 }
 
 template <int CAP>
@@ -155,16 +146,16 @@ int wide_fib_launch(const uint32_t *const *trace, const uint32_t *const *trace_d
     p->powers_dev = reinterpret_cast<const qm31 *>(powers_dev);
     const uint64_t n = 1ull << log_size, pairs = (n + 1) / 2;
     if (powers_dev) {
-        launch_wf<false>(*p, pairs, st);
+        launch_wf(*p, pairs, st);
         STWO_LAUNCH_CHECK("wide_fib_kernel");
         return STWO_OK;
     }
-    // Host powers: staged, doubled, into a stream-ordered buffer private to this call,
-    // so concurrent calls on other streams never see each other's powers.
+    // Host powers: staged into a stream-ordered buffer private to this call, so
+    // concurrent calls on other streams never see each other's powers.
     std::unique_ptr<qm31[]> w2(new qm31[n_cols - 2]);
     for (uint32_t i = 0; i + 2 < n_cols; i++) {
         stwo_qm31 v = powers_host[i];
-        w2[i] = {{v.a << 1, v.b << 1}, {v.c << 1, v.d << 1}};
+        w2[i] = {{v.a, v.b}, {v.c, v.d}};
     }
     void *buf = nullptr;
     {
@@ -174,7 +165,7 @@ int wide_fib_launch(const uint32_t *const *trace, const uint32_t *const *trace_d
     cudaError_t e = cudaMemcpyAsync(buf, w2.get(), sizeof(qm31) * (n_cols - 2), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         p->powers_dev = static_cast<const qm31 *>(buf);
-        launch_wf<true>(*p, pairs, st);
+        launch_wf(*p, pairs, st);
         count_launch();
         e = cudaGetLastError();
     }

@@ -90,7 +90,7 @@ __global__ void canonic_to_bitrev_kernel(const uint32_t *__restrict__ src, uint3
 // pi(x) = 2x^2 - 1 (eval_at_point.cu:99-109). A CTA folds a chunk of 2^15
 // coefficients as 4 groups of 8192: a thread takes 32 consecutive coefficients (bits
 // 0..4) and forms sum_i c_i F_i against the CTA's table F_i = prod_{b in i} f_b, an
-// M31-by-QM31 dot product accumulated unreduced in 64 bits; the lanes fold bits 5..9
+// M31-by-QM31 dot product of 64-bit multiply-accumulates; the lanes fold bits 5..9
 // and the warps bits 10..12. Group partials are weighted by their group index's
 // factors (bits 13..14) before the lane fold, which is linear, so one fold serves the
 // whole chunk. The chunk partial takes the factors of its chunk index; the last CTA
@@ -121,17 +121,6 @@ __device__ __forceinline__ qm31 shfl_xor_q(qm31 v, int m) {
     return v;
 }
 
-// Unreduced product of a in [0, P) and b2 = 2b: a value congruent to a*b in [0, 2^32).
-__device__ __forceinline__ uint32_t mul_lazy_e(uint32_t a, uint32_t b2) {
-    const uint64_t w = (uint64_t)a * b2;
-    return (uint32_t)(w >> 32) + ((uint32_t)w >> 1);
-}
-__device__ __forceinline__ uint32_t reduce64_e(uint64_t x) {
-    uint64_t s = (x & P) + (x >> 31);
-    s = (s & P) + (s >> 31);
-    return reduce_once((uint32_t)s);
-}
-
 // One CTA's share of polynomial `poly`: chunk `chunk` of its 2^L coefficients c with
 // factors f; its CTAs are blk_first .. blk_first + nblk - 1 (partials indexed by CTA).
 __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t L, const qm31 *f, const uint32_t *c,
@@ -139,7 +128,7 @@ __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t
                                          qm31 *results) {
     __shared__ qm31 warp_vals[EAP_THREADS / 32];
     __shared__ qm31 g[1 << EAP_ITER_LOG];
-    __shared__ qm31 F2[1 << EAP_PER_THREAD_LOG];  // F_i with coordinates doubled (for mul_lazy)
+    __shared__ qm31 F2[1 << EAP_PER_THREAD_LOG];  // F_i
     __shared__ bool is_last;
     const uint32_t tid = threadIdx.x;
     const uint64_t n = 1ull << L;
@@ -147,7 +136,7 @@ __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t
         qm31 w = qm31_one();
         for (int b = 0; b < EAP_PER_THREAD_LOG; b++)
             if ((tid >> b) & 1u) w = qm31_mul(w, f[b]);
-        F2[tid] = {{w.a.a << 1, w.a.b << 1}, {w.b.a << 1, w.b.b << 1}};
+        F2[tid] = w;
     } else if (tid < (1u << EAP_PER_THREAD_LOG) + (1u << EAP_ITER_LOG)) {
         // group weights: products of f_{13+b} over the set bits b of the group index
         const uint32_t it = tid - (1u << EAP_PER_THREAD_LOG);
@@ -164,12 +153,19 @@ __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t
                               ((uint64_t)tid << EAP_PER_THREAD_LOG);
         if (base >= n) break;
         uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        // 64-bit multiply-accumulates of canonical values, folded after every third term
         auto term = [&](uint32_t v, uint32_t i) {
             const qm31 w = F2[i];
-            s0 += mul_lazy_e(v, w.a.a);
-            s1 += mul_lazy_e(v, w.a.b);
-            s2 += mul_lazy_e(v, w.b.a);
-            s3 += mul_lazy_e(v, w.b.b);
+            s0 = mac64(s0, v, w.a.a);
+            s1 = mac64(s1, v, w.a.b);
+            s2 = mac64(s2, v, w.b.a);
+            s3 = mac64(s3, v, w.b.b);
+            if (i % 3 == 2) {
+                s0 = fold64(s0);
+                s1 = fold64(s1);
+                s2 = fold64(s2);
+                s3 = fold64(s3);
+            }
         };
         if (base + 32 <= n) {
             const uint4 *q = reinterpret_cast<const uint4 *>(c + base);
@@ -184,7 +180,7 @@ __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t
         } else {
             for (uint32_t i = 0; base + i < n && i < 32; i++) term(__ldg(c + base + i), i);
         }
-        const qm31 part = {{reduce64_e(s0), reduce64_e(s1)}, {reduce64_e(s2), reduce64_e(s3)}};
+        const qm31 part = {{reduce64_p(s0), reduce64_p(s1)}, {reduce64_p(s2), reduce64_p(s3)}};
         acc = qm31_add(acc, it == 0 ? part : qm31_mul(part, g[it]));
     }
     // Across lanes: bits 5..9 (lane bit j <-> factor 5 + j).

@@ -51,10 +51,6 @@ __device__ __forceinline__ cpoint point_at_index(const cpoint *gen_pows, uint32_
 }
 
 // Unreduced product: value congruent to a*b, in [0, 2p].
-__device__ __forceinline__ uint32_t mul_lazy(uint32_t a, uint32_t b2) {
-    uint64_t w = (uint64_t)a * b2;
-    return (uint32_t)(w >> 32) + ((uint32_t)w >> 1);
-}
 __device__ __forceinline__ uint32_t reduce64(uint64_t x) {
     // x < 2^62: fold twice
     uint64_t s = (x & P) + (x >> 31);
@@ -126,15 +122,21 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                     }
                 }
             };
+            // 64-bit multiply-accumulates of canonical values (products below 2^62),
+            // folded after every second column: a folded sum (below 2^34) plus two
+            // products stays below 2^64.
             auto consume = [&](uint32_t jb, const uint2 (&v)[QUOT_PREFETCH]) {
 #pragma unroll
                 for (int u = 0; u < QUOT_PREFETCH; u++) {
                     if (jb + u >= j1) break;
-                    const qm31 c2 = STAGE ? s_c2[jb + u] : p.c2[jb + u];
-                    s0[0][0] += mul_lazy(v[u].x, c2.a.a); s0[0][1] += mul_lazy(v[u].x, c2.a.b);
-                    s0[0][2] += mul_lazy(v[u].x, c2.b.a); s0[0][3] += mul_lazy(v[u].x, c2.b.b);
-                    s0[1][0] += mul_lazy(v[u].y, c2.a.a); s0[1][1] += mul_lazy(v[u].y, c2.a.b);
-                    s0[1][2] += mul_lazy(v[u].y, c2.b.a); s0[1][3] += mul_lazy(v[u].y, c2.b.b);
+                    const qm31 c = STAGE ? s_c2[jb + u] : p.c2[jb + u];
+                    s0[0][0] = mac64(s0[0][0], v[u].x, c.a.a); s0[0][1] = mac64(s0[0][1], v[u].x, c.a.b);
+                    s0[0][2] = mac64(s0[0][2], v[u].x, c.b.a); s0[0][3] = mac64(s0[0][3], v[u].x, c.b.b);
+                    s0[1][0] = mac64(s0[1][0], v[u].y, c.a.a); s0[1][1] = mac64(s0[1][1], v[u].y, c.a.b);
+                    s0[1][2] = mac64(s0[1][2], v[u].y, c.b.a); s0[1][3] = mac64(s0[1][3], v[u].y, c.b.b);
+                    if (u & 1)
+                        for (int s = 0; s < 2; s++)
+                            for (int t = 0; t < 4; t++) s0[s][t] = fold64(s0[s][t]);
                 }
             };
             uint2 va[QUOT_PREFETCH], vb[QUOT_PREFETCH];

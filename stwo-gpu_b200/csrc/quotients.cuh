@@ -15,7 +15,7 @@ constexpr int QUOT_MAX_BATCHES = 16;
 template <int MAXC, int MAXS>
 struct QuotParamsT {
     const uint32_t *cols[MAXC];
-    qm31 c2[MAXS];                        // c_j with every coordinate doubled (for m31_mul2)
+    qm31 c2[MAXS];                        // c_j (canonical)
     uint16_t col_idx[MAXS];
     qm31 a_sum[QUOT_MAX_BATCHES], b_sum[QUOT_MAX_BATCHES], batch_coeff[QUOT_MAX_BATCHES];
     cm31 prx[QUOT_MAX_BATCHES], pry[QUOT_MAX_BATCHES], pix[QUOT_MAX_BATCHES], piy[QUOT_MAX_BATCHES];
@@ -33,7 +33,7 @@ using QuotParamsDev = QuotParamsT<1024, 1024>;
 // Sample-dependent fields of batch b (samples off .. off+count-1 at point (px, py)):
 // the batch coefficient rc^count and, per sample j with alpha = rc^(j+1),
 // (a, b, c) = alpha * (conj(v) - v, v*c0 - a*py, c0), c0 = conj(py) - py
-// (complex_conjugate_line_coeffs); a and b summed per batch, c stored doubled.
+// (complex_conjugate_line_coeffs); a and b summed per batch, c stored per sample.
 template <class QP>
 __host__ __device__ inline void quot_fill_batch(QP &p, uint32_t b, qm31 rc, qm31 px, qm31 py, const qm31 *vals,
                                                 uint32_t count, uint32_t off) {
@@ -54,7 +54,7 @@ __host__ __device__ inline void quot_fill_batch(QP &p, uint32_t b, qm31 rc, qm31
         const qm31 c = qm31_mul(alpha, c0);
         as = qm31_add(as, a);
         bs = qm31_add(bs, bb);
-        p.c2[off + j] = {{c.a.a << 1, c.a.b << 1}, {c.b.a << 1, c.b.b << 1}};
+        p.c2[off + j] = c;
     }
     p.a_sum[b] = as;
     p.b_sum[b] = bs;
@@ -95,7 +95,7 @@ __device__ inline void quot_fill_batch_block(QP &p, uint32_t b, qm31 rc, qm31 px
         const qm31 c = qm31_mul(alpha, c0);
         as = qm31_add(as, a);
         bs = qm31_add(bs, bb);
-        p.c2[off + j] = {{c.a.a << 1, c.a.b << 1}, {c.b.a << 1, c.b.b << 1}};
+        p.c2[off + j] = c;
         alpha = qm31_mul(alpha, step);
     }
     as = block_sum_qm31(as, sh);
