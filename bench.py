@@ -550,6 +550,67 @@ def percentiles(xs):
             "p999_ms": float(np.percentile(a, 99.9)), "mean_ms": float(a.mean())}
 
 
+def batch48(stwo, dev, args, O=None):
+    """The batched-uneven-sizes case: 48 seeded jobs, log_n_rows uniform in {10..20},
+    columns uniform in {16, 32, 64, 128}, admitted at once to the proof server, each
+    proof compared with the same job proved alone; and one Merkle tree mixing
+    columns of log sizes 12..22 (4 per size), its root compared with the oracle's."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(4848)
+    jobs = [(int(rng.integers(10, 21)), int(rng.choice([16, 32, 64, 128])), int(rng.integers(0, 1 << 62)))
+            for _ in range(48)]
+    ins = []
+    for t in jobs:
+        a0, a1 = stwo.wide_fib_inputs(t[0], t[2])
+        ins.append((a0, a1, torch.from_numpy(a0.view(np.int32)).to(dev), torch.from_numpy(a1.view(np.int32)).to(dev)))
+    batched, single = StreamRunner(stwo, args.workers), StreamRunner(stwo, 1)
+    batched.run(jobs[:8], ins[:8], resident=True)
+    single.run(jobs[:2], ins[:2], resident=True)
+    res_b, ms_b = batched.run(jobs, ins, resident=True)
+    res_s, ms_s = single.run(jobs, ins, resident=True)
+    batched.close()
+    single.close()
+    identical = all(res_b[i]["proof"] == res_s[i]["proof"] for i in range(len(jobs)))
+    # mixed-size tree: layer l hashes its children and the 4 columns of size 2^l (12 <= l <= 22)
+    L = stwo._lib
+    lib = L.lib()
+    sptr = torch.cuda.current_stream(dev).cuda_stream
+    top = 22
+    cols = {l: [torch.randint(0, P, (1 << l,), dtype=torch.int64, device=dev).to(torch.int32) for _ in range(4)]
+            for l in range(12, top + 1)}
+    layers = [torch.empty(8 << l, dtype=torch.int32, device=dev) for l in range(top + 1)]
+
+    def tree():
+        for l in range(top, -1, -1):
+            cs = cols.get(l, [])
+            L.check(lib.stwo_merkle_commit_layer(l, layers[l + 1].data_ptr() if l < top else None,
+                                                 L.ptr_array([c.data_ptr() for c in cs]), len(cs),
+                                                 layers[l].data_ptr(), sptr))
+    tree()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(torch.cuda.current_stream(dev))
+    for _ in range(3):
+        tree()
+    e.record(torch.cuda.current_stream(dev))
+    torch.cuda.synchronize()
+    tree_ms = s.elapsed_time(e) / 3
+    root_equal = None
+    if O is not None:
+        O.set_threads(os.cpu_count() or 1)
+        prev = None
+        for l in range(top, -1, -1):
+            prev = O.merkle_commit_on_layer(l, prev, [c.cpu().numpy().view(np.uint32) for c in cols.get(l, [])])
+        O.set_threads(1)
+        root_equal = bool((prev.reshape(-1) == layers[0].cpu().numpy().view(np.uint32)).all())
+    return {"jobs": 48, "workload": "log_n_rows U{10..20}, columns U{16,32,64,128}, log_blowup 1, 3 queries, "
+                                    "pow_bits 5, all 48 admitted at once",
+            "proofs_per_s": len(jobs) / (ms_b / 1e3), "per_job_proofs_per_s": len(jobs) / (ms_s / 1e3),
+            "batched_vs_per_job": ms_s / ms_b, "bit_identical": identical,
+            "mixed_tree": {"columns": "4 per log size 12..22", "ms": tree_ms, "root_equal_to_oracle": root_equal}}
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -557,6 +618,10 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     stwo = load_package()
+    import ctypes as C
+    tune_buf = C.create_string_buffer(4096)
+    stwo._lib.check(stwo._lib.lib().stwo_autotune(tune_buf, 4096))
+    autotune = json.loads(tune_buf.value.decode())
 
     def barrier():
         if world > 1:
@@ -640,7 +705,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- single proofs, FFT roofline, kernel sweep, CPU baseline (rank 0, 1 GPU)
     roof, fft = fft_roofline(stwo, dev, rank, args)
-    singles, kernels, cpu, verified = None, None, None, None
+    singles, kernels, cpu, verified, batch = None, None, None, None, None
     if rank == 0:
         O = load_oracle() if not args.no_cpu_baseline else None
         singles = {}
@@ -668,6 +733,7 @@ def run_ours(args, rank, world, local_rank):
                        for i in range(min(2, args.jobs)))
         if world == 1 and not args.no_suite:
             kernels = kernel_suite(stwo)
+            batch = batch48(stwo, dev, args, O)
         if O is not None and world == 1:
             threads = os.cpu_count() or 1
             n, dt, desc = cpu_stream_sample(O, stwo, steps[0], args.cpu_budget, threads)
@@ -687,12 +753,14 @@ def run_ours(args, rank, world, local_rank):
                         "bit_identical": identical, "proofs_compared": compared, "verified_sample": verified,
                         "latency": latency, "latency_jobs": args.latency_jobs},
             "single_proofs": singles,
+            "batch48": batch,
             "roofline": roof,
             "fft": fft,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_step},
             "kernels": kernels,
+            "autotune": autotune,
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }

@@ -117,6 +117,8 @@ SIGNATURES = [
     ("stwo_wide_fib_composition", C.c_int, [vp, u32, u32, vp, vp, vp, vp]),
     ("stwo_kernel_launches", u64, []),
     ("stwo_reserve_device_memory", C.c_int, [u64]),
+    ("stwo_autotune", C.c_int, [C.c_char_p, sz]),
+    ("stwo_set_tunable", C.c_int, [C.c_char_p, C.c_int]),
     # prover tier
     ("stwo_wide_fib_prove_device_bytes", u64, [C.POINTER(WideFibJob), C.c_int]),
     ("stwo_wide_fib_prove", C.c_int, [C.POINTER(WideFibJob), vp, vp, vp, vp, u64, C.POINTER(C.POINTER(C.c_uint8)),

@@ -96,6 +96,18 @@ int wait_stream(cudaStream_t st);
 // buffer across threads. Valid until the thread's next host_stage call.
 int host_stage(size_t bytes, void **out);
 
+// Launch parameters that stwo_autotune measures and stwo_set_tunable sets
+// (process-wide; every value of a tunable computes the same results).
+enum Tunable {
+    TUNE_FFT_EPT_CONTIG_SMALL,  // log2 elements per thread, contiguous passes, domains <= 2^20
+    TUNE_FFT_EPT_CONTIG_LARGE,  // same, larger domains
+    TUNE_FFT_EPT_STRIDED,       // same, strided passes
+    TUNE_MERKLE_SUB_THREADS,    // CTA size of the multi-layer Merkle kernel (log2 + 1 layers per launch)
+    TUNE_COUNT
+};
+int tunable(Tunable t);
+void set_tunable(Tunable t, int v);
+
 // Stream handle conversion for the C ABI.
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 

@@ -481,20 +481,21 @@ int launchT_e(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
     return STWO_OK;
 }
 
-// Elements per thread: 2^6 (256 threads per CTA, 16 warps per SM at two CTAs) by
-// default, measured faster on B200 than 2^5 (512 threads, 32 warps, 64 registers:
-// 2222 vs 2125 log-24 columns/s); STWO_FFT_EPT_LOG=5 selects the latter.
-inline int fft_ept_log() {
-    static int v = [] {
+// Elements per thread, 2^6 (256 threads per CTA) or 2^5 (512 threads): a tunable per
+// pass kind and domain size (stwo_autotune); 2^6 by default, measured faster at log 24
+// (2222 vs 2125 columns/s). STWO_FFT_EPT_LOG=5 sets every pass kind to 2^5.
+inline int fft_ept_log(bool contiguous, uint32_t N) {
+    static const int forced = [] {
         const char *e = getenv("STWO_FFT_EPT_LOG");
-        return (e && atoi(e) == 5) ? 5 : 6;
+        return e ? atoi(e) : 0;
     }();
-    return v;
+    if (forced == 5 || forced == 6) return forced;
+    return tunable(!contiguous ? TUNE_FFT_EPT_STRIDED : N <= 20 ? TUNE_FFT_EPT_CONTIG_SMALL : TUNE_FFT_EPT_CONTIG_LARGE);
 }
 
 template <int G, int C, bool INV>
 int launchT_t(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
-    return fft_ept_log() == 6 ? launchT_e<G, C, INV, 6>(p, n_cols, st) : launchT_e<G, C, INV, 5>(p, n_cols, st);
+    return fft_ept_log(C == 0, p.N) == 5 ? launchT_e<G, C, INV, 5>(p, n_cols, st) : launchT_e<G, C, INV, 6>(p, n_cols, st);
 }
 
 // Dispatch over (G, C): contiguous passes G = 11..14 (C = 0), strided passes

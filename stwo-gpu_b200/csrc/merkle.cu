@@ -72,25 +72,24 @@ __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, co
     }
 }
 
-// Up to 9 layers in one launch. CTA c owns nodes [c*256 >> j, (c+1)*256 >> j) of level
-// j (layer top_log - j): exactly the parents of the nodes it owned one level up, which
-// it wrote itself before the barrier. Level j hashes the children (absent on the leaf
+// Up to log2(THREADS) + 1 layers in one launch. CTA c owns nodes
+// [c*THREADS >> j, (c+1)*THREADS >> j) of level j (layer top_log - j): exactly the
+// parents of the nodes it owned one level up, which it wrote itself before the barrier. Level j hashes the children (absent on the leaf
 // layer) and the layer's columns (device pointer tables, one per level).
-constexpr int MERKLE_SUB_THREADS = 256;
-constexpr int MERKLE_SUB_LEVELS = 9;  // 256 nodes -> 1 node
+constexpr int MERKLE_SUB_MAX_LEVELS = 10;  // a CTA of 512 threads: 512 nodes -> 1 node
 
 struct SubtreeParams {
     uint4 *layer[32];                                   // layer[l]: 2^l nodes
-    const uint32_t *const *cols[MERKLE_SUB_LEVELS];     // device column tables per level
-    uint32_t n_cols[MERKLE_SUB_LEVELS];
+    const uint32_t *const *cols[MERKLE_SUB_MAX_LEVELS];  // device column tables per level
+    uint32_t n_cols[MERKLE_SUB_MAX_LEVELS];
     uint32_t top_log, levels, has_prev;
 };
 
-__global__ void __launch_bounds__(MERKLE_SUB_THREADS) merkle_subtree_kernel(const __grid_constant__ SubtreeParams p,
-                                                                           uint32_t one) {
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) merkle_subtree_kernel(const __grid_constant__ SubtreeParams p, uint32_t one) {
     for (uint32_t j = 0; j < p.levels; j++) {
         const uint32_t l = p.top_log - j;
-        const uint64_t per_cta = (uint64_t)MERKLE_SUB_THREADS >> j;
+        const uint64_t per_cta = (uint64_t)THREADS >> j;
         const uint64_t first = blockIdx.x * per_cta, n_l = 1ull << l;
         const uint4 *prev = (j > 0 || p.has_prev) ? p.layer[l + 1] : nullptr;
         const uint32_t *const *ct = p.cols[j];
@@ -118,7 +117,7 @@ void launch_layer(uint32_t log_size, const uint32_t *prev, const uint32_t *const
 
 // A whole tree whose per-layer columns are device pointer tables: level_cols[l],
 // level_ncols[l] for layer l (table may be null when the count is 0); layers[l] the
-// 2^l-node outputs. ceil((max_log + 1) / 9) launches.
+// 2^l-node outputs. ceil((max_log + 1) / (log2(CTA size) + 1)) launches.
 int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_cols, const uint32_t *level_ncols,
                           uint32_t *const *layers, cudaStream_t st) {
     STWO_REQUIRE(max_log <= 30, STWO_ERR_UNSUPPORTED_SIZE, "merkle tree of log size %u", max_log);
@@ -127,9 +126,12 @@ int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_
         p.layer[l] = reinterpret_cast<uint4 *>(layers[l]);
         STWO_REQUIRE(((uintptr_t)layers[l] & 15) == 0, STWO_ERR_INVALID_ARGUMENT, "hash buffers must be 16-byte aligned");
     }
+    // CTA size (tunable): 128, 256 or 512 threads, i.e. 8, 9 or 10 layers per launch.
+    const int threads = tunable(TUNE_MERKLE_SUB_THREADS);
+    const int max_levels = threads == 512 ? 10 : threads == 128 ? 8 : 9;
     int top = (int)max_log;
     while (top >= 0) {
-        const uint32_t levels = (uint32_t)std::min(top + 1, MERKLE_SUB_LEVELS);
+        const uint32_t levels = (uint32_t)std::min(top + 1, max_levels);
         p.top_log = (uint32_t)top;
         p.levels = levels;
         p.has_prev = top < (int)max_log;
@@ -138,10 +140,11 @@ int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_
             p.n_cols[j] = level_ncols[top - j];
         }
         const uint64_t nodes = 1ull << top;
-        const uint64_t blocks = nodes > (uint64_t)MERKLE_SUB_THREADS ? nodes / MERKLE_SUB_THREADS : 1;
-        STWO_REQUIRE(levels == (uint32_t)MERKLE_SUB_LEVELS || blocks == 1, STWO_ERR_UNSUPPORTED_SIZE,
-                     "merkle subtree partition");
-        merkle_subtree_kernel<<<(unsigned)blocks, MERKLE_SUB_THREADS, 0, st>>>(p, 1u);
+        const uint64_t blocks = nodes > (uint64_t)threads ? nodes / threads : 1;
+        STWO_REQUIRE(levels == (uint32_t)max_levels || blocks == 1, STWO_ERR_UNSUPPORTED_SIZE, "merkle subtree partition");
+        if (threads == 512) merkle_subtree_kernel<512><<<(unsigned)blocks, 512, 0, st>>>(p, 1u);
+        else if (threads == 128) merkle_subtree_kernel<128><<<(unsigned)blocks, 128, 0, st>>>(p, 1u);
+        else merkle_subtree_kernel<256><<<(unsigned)blocks, 256, 0, st>>>(p, 1u);
         STWO_LAUNCH_CHECK("merkle_subtree_kernel");
         top -= (int)levels;
     }
