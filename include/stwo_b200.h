@@ -152,13 +152,15 @@ void stwo_clear_last_error(void);
  * `bytes`, so allocations up to that total map no new memory later. */
 int stwo_reserve_device_memory(uint64_t bytes);
 /* Measures the library's launch-parameter variants on the current device (FFT elements
- * per thread per pass kind and size, Merkle layers per launch) and keeps the fastest
+ * per thread per pass kind and size, Merkle layers per launch and bottom-level nodes
+ * per thread) and keeps the fastest
  * for this process; every variant computes the same values. Writes a JSON summary of
  * the timings and choices into report (NUL-terminated, at most report_cap bytes) if
  * it is not NULL. Takes well under a second. */
 int stwo_autotune(char *report, size_t report_cap);
 /* Sets one tunable by name: fft_ept_contig_small / fft_ept_contig_large /
- * fft_ept_strided (5 or 6), merkle_sub_threads (128, 256 or 512). */
+ * fft_ept_strided (5 or 6), merkle_sub_threads (128, 256 or 512), merkle_sub_spread
+ * (0..5: log2 of the bottom-level nodes each thread hashes). */
 int stwo_set_tunable(const char *name, int value);
 /* Number of kernel launches the library has made in this process (all threads). */
 uint64_t stwo_kernel_launches(void);

@@ -5,7 +5,9 @@
 //   up to 2^20, contiguous passes on larger domains, and strided passes; measured on 8
 //   columns interpolated at 2^18 / 2^22 and evaluated at blowup 4;
 //   Merkle layers per launch (CTA of 128, 256 or 512 threads); measured on a tree of
-//   64 columns x 2^19 leaves.
+//   64 columns x 2^19 leaves;
+//   Merkle bottom-level nodes per thread (2^1 .. 2^5); measured on a tree of 4
+//   columns x 2^20 leaves.
 //
 // Each candidate runs once to warm up, then three times; the least time wins. Every
 // variant computes the same values, so tuning changes speed only. Device memory for
@@ -94,6 +96,11 @@ int stwo_set_tunable(const char *name, int value) {
         STWO_REQUIRE(value == 128 || value == 256 || value == 512, STWO_ERR_INVALID_ARGUMENT,
                      "merkle_sub_threads must be 128, 256 or 512");
         set_tunable(TUNE_MERKLE_SUB_THREADS, value);
+        return STWO_OK;
+    }
+    if (n == "merkle_sub_spread") {
+        STWO_REQUIRE(value >= 0 && value <= 5, STWO_ERR_INVALID_ARGUMENT, "merkle_sub_spread must be 0..5");
+        set_tunable(TUNE_MERKLE_SUB_SPREAD, value);
         return STWO_OK;
     }
     return set_error(STWO_ERR_INVALID_ARGUMENT, "unknown tunable %s", name);
@@ -189,6 +196,41 @@ int stwo_autotune(char *report, size_t report_cap) {
             }
             set_tunable(TUNE_MERKLE_SUB_THREADS, best);
             snprintf(part, sizeof(part), ", \"merkle_sub_threads\": {\"chosen\": %d, \"ms\": {", best);
+            rep += std::string(part) + times + "}}";
+        }
+        // ---- Merkle nodes per thread: 4 columns x 2^20 leaves (one compression per
+        // leaf, the shape of the composition and FRI trees), the whole tree
+        if (rc == STWO_OK) {
+            const uint32_t LOG = 20, NC = 4;
+            std::vector<const uint32_t *> cols(in.begin(), in.begin() + NC);
+            uint32_t *table = buf.get(NC * 2);
+            std::vector<uint32_t *> layers(LOG + 1);
+            for (uint32_t l = 0; l <= LOG; l++) layers[l] = buf.get(8ull << l);
+            STWO_REQUIRE(table && layers[LOG], STWO_ERR_OUT_OF_MEMORY, "autotune allocation failed");
+            STWO_CUDA_TRY(cudaMemcpyAsync(table, cols.data(), NC * sizeof(void *), cudaMemcpyHostToDevice, st));
+            std::vector<const uint32_t *const *> lt(LOG + 1, nullptr);
+            std::vector<uint32_t> ln(LOG + 1, 0);
+            lt[LOG] = reinterpret_cast<const uint32_t *const *>(table);
+            ln[LOG] = NC;
+            float best_ms = 1e30f;
+            int best = tunable(TUNE_MERKLE_SUB_SPREAD);
+            std::string times;
+            char part[128];
+            for (int v : {3, 1, 2, 4, 5}) {
+                set_tunable(TUNE_MERKLE_SUB_SPREAD, v);
+                float ms = 0;
+                rc = time_best(st, [&] { return merkle_tree_dev_async(LOG, lt.data(), ln.data(), layers.data(), st); },
+                               &ms);
+                if (rc) break;
+                snprintf(part, sizeof(part), "%s\"%d\": %.4f", times.empty() ? "" : ", ", v, ms);
+                times += part;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = v;
+                }
+            }
+            set_tunable(TUNE_MERKLE_SUB_SPREAD, best);
+            snprintf(part, sizeof(part), ", \"merkle_sub_spread\": {\"chosen\": %d, \"ms\": {", best);
             rep += std::string(part) + times + "}}";
         }
     }

@@ -44,7 +44,13 @@ __device__ __forceinline__ void merkle_node(uint64_t i, const uint4 *prev, ColAt
         }
         compress(h, m, one);
     }
-    for (uint32_t c0 = 0; c0 < n_cols; c0 += 16) {
+    uint32_t c0 = 0;
+    for (; c0 + 16 <= n_cols; c0 += 16) {  // full chunks: no per-word bound checks
+#pragma unroll
+        for (int j = 0; j < 16; j++) m[j] = __ldg(col_at(c0 + j) + i);
+        compress(h, m, one);
+    }
+    if (c0 < n_cols) {  // the zero-padded last chunk
 #pragma unroll
         for (int j = 0; j < 16; j++) {
             uint32_t cj = c0 + j;
@@ -72,24 +78,27 @@ __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, co
     }
 }
 
-// Up to log2(THREADS) + 1 layers in one launch. CTA c owns nodes
-// [c*THREADS >> j, (c+1)*THREADS >> j) of level j (layer top_log - j): exactly the
-// parents of the nodes it owned one level up, which it wrote itself before the barrier. Level j hashes the children (absent on the leaf
-// layer) and the layer's columns (device pointer tables, one per level).
-constexpr int MERKLE_SUB_MAX_LEVELS = 10;  // a CTA of 512 threads: 512 nodes -> 1 node
+// Up to log2(THREADS) + 1 + spread layers in one launch. CTA c owns the
+// (THREADS << spread) >> j nodes of level j (layer top_log - j) that start at
+// c * ((THREADS << spread) >> j): exactly the parents of the nodes it owned one level
+// down, which it wrote itself before the barrier. Level j hashes the children (absent
+// on the leaf layer) and the layer's columns (device pointer tables, one per level).
+// With spread s a thread hashes 2^s nodes of the bottom level, so the CTA stays dense
+// for s + 1 levels before its upper levels thin out.
+constexpr int MERKLE_SUB_MAX_LEVELS = 15;  // 512 threads, spread 5: 16384 nodes -> 1 node
 
 struct SubtreeParams {
     uint4 *layer[32];                                   // layer[l]: 2^l nodes
     const uint32_t *const *cols[MERKLE_SUB_MAX_LEVELS];  // device column tables per level
     uint32_t n_cols[MERKLE_SUB_MAX_LEVELS];
-    uint32_t top_log, levels, has_prev;
+    uint32_t top_log, levels, has_prev, spread;
 };
 
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) merkle_subtree_kernel(const __grid_constant__ SubtreeParams p, uint32_t one) {
     for (uint32_t j = 0; j < p.levels; j++) {
         const uint32_t l = p.top_log - j;
-        const uint64_t per_cta = (uint64_t)THREADS >> j;
+        const uint64_t per_cta = ((uint64_t)THREADS << p.spread) >> j;
         const uint64_t first = blockIdx.x * per_cta, n_l = 1ull << l;
         const uint4 *prev = (j > 0 || p.has_prev) ? p.layer[l + 1] : nullptr;
         const uint32_t *const *ct = p.cols[j];
@@ -126,21 +135,29 @@ int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_
         p.layer[l] = reinterpret_cast<uint4 *>(layers[l]);
         STWO_REQUIRE(((uintptr_t)layers[l] & 15) == 0, STWO_ERR_INVALID_ARGUMENT, "hash buffers must be 16-byte aligned");
     }
-    // CTA size (tunable): 128, 256 or 512 threads, i.e. 8, 9 or 10 layers per launch.
+    // CTA size (tunable): 128, 256 or 512 threads, i.e. 8, 9 or 10 layers per launch,
+    // plus `spread` more (tunable, 0..5) while the launch still fills every SM with
+    // 2048 threads.
     const int threads = tunable(TUNE_MERKLE_SUB_THREADS);
-    const int max_levels = threads == 512 ? 10 : threads == 128 ? 8 : 9;
+    const int tlog = threads == 512 ? 9 : threads == 128 ? 7 : 8;
+    const int max_spread = tunable(TUNE_MERKLE_SUB_SPREAD);
+    const uint64_t min_blocks = (uint64_t)device_sm_count() * 2048 / threads;
     int top = (int)max_log;
     while (top >= 0) {
+        int spread = max_spread;
+        while (spread > 0 && (top < tlog + spread || ((1ull << top) >> (tlog + spread)) < min_blocks)) spread--;
+        const int max_levels = tlog + 1 + spread;
         const uint32_t levels = (uint32_t)std::min(top + 1, max_levels);
         p.top_log = (uint32_t)top;
         p.levels = levels;
         p.has_prev = top < (int)max_log;
+        p.spread = (uint32_t)spread;
         for (uint32_t j = 0; j < levels; j++) {
             p.cols[j] = level_cols[top - j];
             p.n_cols[j] = level_ncols[top - j];
         }
-        const uint64_t nodes = 1ull << top;
-        const uint64_t blocks = nodes > (uint64_t)threads ? nodes / threads : 1;
+        const uint64_t nodes = 1ull << top, per_cta = (uint64_t)threads << spread;
+        const uint64_t blocks = nodes > per_cta ? nodes / per_cta : 1;
         STWO_REQUIRE(levels == (uint32_t)max_levels || blocks == 1, STWO_ERR_UNSUPPORTED_SIZE, "merkle subtree partition");
         if (threads == 512) merkle_subtree_kernel<512><<<(unsigned)blocks, 512, 0, st>>>(p, 1u);
         else if (threads == 128) merkle_subtree_kernel<128><<<(unsigned)blocks, 128, 0, st>>>(p, 1u);

@@ -57,6 +57,7 @@ struct stwo_prover_server {
     uint64_t tree_size = 0;
     bool stopping = false;
     bool blocking_wait = true;  // workers yield their core while waiting on the device
+    bool use_priorities = true; // per-job stream priority by job size
     uint32_t running = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -77,11 +78,32 @@ struct stwo_prover_server {
         return false;
     }
 
+    // Stream priority of a job: smaller jobs get higher priority, so that the short
+    // kernel chains of small jobs take free SM slots ahead of the queued CTAs of large
+    // transforms instead of waiting behind them. Class 0 (the highest) holds jobs of up
+    // to 2^16 trace cells; each further class doubles the bound twice.
+    static uint32_t priority_class(const stwo_wide_fib_job &j, uint32_t n_classes) {
+        uint32_t ln = 0;
+        while ((1u << ln) < j.n_columns) ln++;
+        const uint32_t w = j.log_n_rows + ln;
+        const uint32_t c = w <= 16 ? 0 : (w - 15) / 2;
+        return std::min(c, n_classes - 1);
+    }
+
     void worker() {
         cudaSetDevice(device);
         t_blocking_wait = blocking_wait;
-        cudaStream_t st = nullptr;
-        cudaError_t se = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        // One stream per priority level, greatest priority first.
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (!use_priorities) greatest = least;
+        std::vector<cudaStream_t> streams;
+        cudaError_t se = cudaSuccess;
+        for (int pr = greatest; pr <= least && se == cudaSuccess; pr++) {
+            cudaStream_t s = nullptr;
+            se = cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, pr);
+            if (se == cudaSuccess) streams.push_back(s);
+        }
         for (;;) {
             PendingJob j;
             bool got = false;
@@ -101,6 +123,7 @@ struct stwo_prover_server {
             } else {
                 clear_error();
                 const uint32_t *a0 = j.a0_dev ? j.a0_dev : j.a0.data(), *a1 = j.a1_dev ? j.a1_dev : j.a1.data();
+                cudaStream_t st = streams[priority_class(j.job, (uint32_t)streams.size())];
                 r.status = wide_fib_prove(&j.job, a0, a1, tw, itw, tree_size, proof, &r.stats, st);
             }
             if (r.status == STWO_OK) {
@@ -124,7 +147,7 @@ struct stwo_prover_server {
             cv_work.notify_all();  // freed budget may admit waiting jobs
             cv_done.notify_all();
         }
-        if (st) cudaStreamDestroy(st);
+        for (cudaStream_t s : streams) cudaStreamDestroy(s);
     }
 };
 
@@ -146,6 +169,7 @@ stwo_prover_server *stwo_server_create(uint32_t n_workers, uint64_t device_budge
     }
     s->budget = device_budget_bytes;
     if (const char *w = getenv("STWO_SERVER_WAIT")) s->blocking_wait = strcmp(w, "spin") != 0;
+    if (const char *w = getenv("STWO_SERVER_PRIORITY")) s->use_priorities = strcmp(w, "0") != 0;
     s->max_domain_log = max_domain_log;
     // One twiddle tree for CanonicCoset(max_domain_log).half_coset serves every smaller
     // canonic domain: its doublings are the smaller domains' half cosets.

@@ -195,8 +195,9 @@ def test_server_shutdown_with_queued_jobs_is_clean():
 
 
 def test_tunables_change_speed_not_results():
-    """Every FFT elements-per-thread and Merkle layers-per-launch setting gives the same
-    proof bytes; stwo_autotune reports its choices as JSON."""
+    """Every FFT elements-per-thread, Merkle layers-per-launch and Merkle
+    nodes-per-thread setting gives the same proof bytes; stwo_autotune reports its
+    choices as JSON."""
     import ctypes as C
     import json
     stwo = load_package()
@@ -204,20 +205,30 @@ def test_tunables_change_speed_not_results():
     t = (16, 40, 2, 3, 5)
     a0, a1 = stwo.wide_fib_inputs(16, 77)
     base, _ = stwo.prove_wide_fib(job_of(t), a0, a1)
+    # trees of 2^20 and 2^21 leaves, large enough for several nodes per thread
+    tb = (19, 24, 1, 3, 5)
+    b0, b1 = stwo.wide_fib_inputs(19, 78)
+    base_b, _ = stwo.prove_wide_fib(job_of(tb), b0, b1)
     settings = [("fft_ept_contig_small", 5), ("fft_ept_contig_large", 5), ("fft_ept_strided", 5),
-                ("merkle_sub_threads", 128), ("merkle_sub_threads", 512)]
+                ("merkle_sub_threads", 128), ("merkle_sub_threads", 512), ("merkle_sub_spread", 0),
+                ("merkle_sub_spread", 5)]
     try:
         for name, value in settings:
             stwo._lib.check(lib.stwo_set_tunable(name.encode(), value))
             assert stwo.prove_wide_fib(job_of(t), a0, a1)[0] == base, (name, value)
+            assert stwo.prove_wide_fib(job_of(tb), b0, b1)[0] == base_b, (name, value)
         with pytest.raises(stwo._lib.StwoError):
             stwo._lib.check(lib.stwo_set_tunable(b"merkle_sub_threads", 100))
+        with pytest.raises(stwo._lib.StwoError):
+            stwo._lib.check(lib.stwo_set_tunable(b"merkle_sub_spread", 6))
         buf = C.create_string_buffer(4096)
         stwo._lib.check(lib.stwo_autotune(buf, 4096))
         rep = json.loads(buf.value.decode())
-        assert set(rep) == {"fft_ept_contig_small", "fft_ept_contig_large", "fft_ept_strided", "merkle_sub_threads"}
+        assert set(rep) == {"fft_ept_contig_small", "fft_ept_contig_large", "fft_ept_strided", "merkle_sub_threads",
+                            "merkle_sub_spread"}
         assert stwo.prove_wide_fib(job_of(t), a0, a1)[0] == base
+        assert stwo.prove_wide_fib(job_of(tb), b0, b1)[0] == base_b
     finally:
         for name, value in [("fft_ept_contig_small", 6), ("fft_ept_contig_large", 6), ("fft_ept_strided", 6),
-                            ("merkle_sub_threads", 256)]:
+                            ("merkle_sub_threads", 256), ("merkle_sub_spread", 3)]:
             lib.stwo_set_tunable(name.encode(), value)
