@@ -46,8 +46,9 @@ struct WideFibParams {
     const uint32_t *trace[CAP];
     const uint32_t *const *trace_dev;
     uint32_t *out[4];
-    const uint32_t *den_inv;
-    const qm31 *powers_dev;  // device powers
+    const uint32_t *den_inv;  // per-row denominator inverses, or null:
+    uint32_t den_half[2];     // the inverses on the first and second half of the (bit-reversed) rows
+    const qm31 *powers_dev;   // device powers
     uint32_t n_cols;
     uint32_t log_size;
 };
@@ -107,7 +108,8 @@ __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant_
         }
         uint32_t o[4][2];
         for (int r = 0; r < 2; r++) {
-            uint32_t d = (2 * k + r < n) ? __ldg(p.den_inv + 2 * k + r) : 0u;
+            const uint64_t row = 2 * k + r;
+            uint32_t d = row >= n ? 0u : p.den_inv ? __ldg(p.den_inv + row) : p.den_half[row >> (p.log_size - 1)];
             uint32_t d2 = d << 1;
             for (int c = 0; c < 4; c++) o[c][r] = m31_mul2(reduce64_p(acc[r][c]), d2);
         }
@@ -130,7 +132,7 @@ void launch_wf(const WideFibParams<CAP> &p, uint64_t pairs, cudaStream_t st) {
 template <int CAP>
 int wide_fib_launch(const uint32_t *const *trace, const uint32_t *const *trace_dev, uint32_t n_cols, uint32_t log_size,
                     const stwo_qm31 *powers_host, const uint32_t *powers_dev, const uint32_t *den_inv,
-                    uint32_t *const *out4, cudaStream_t st) {
+                    const uint32_t *den_half, uint32_t *const *out4, cudaStream_t st) {
     auto p = std::make_unique<WideFibParams<CAP>>();
     if (CAP > 1)
         for (uint32_t i = 0; i < n_cols; i++) {
@@ -141,6 +143,10 @@ int wide_fib_launch(const uint32_t *const *trace, const uint32_t *const *trace_d
     p->trace_dev = trace_dev;
     for (int c = 0; c < 4; c++) p->out[c] = out4[c];
     p->den_inv = den_inv;
+    if (den_half) {
+        p->den_half[0] = den_half[0];
+        p->den_half[1] = den_half[1];
+    }
     p->n_cols = n_cols;
     p->log_size = log_size;
     p->powers_dev = reinterpret_cast<const qm31 *>(powers_dev);
@@ -204,18 +210,24 @@ int wide_fib_async(const uint32_t *const *trace, uint32_t n_cols, uint32_t log_s
         return STWO_OK;
     }
     if (n_cols <= 64)
-        return wide_fib_launch<64>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, out4, st);
+        return wide_fib_launch<64>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, nullptr, out4,
+                                   st);
     if (n_cols <= 256)
-        return wide_fib_launch<256>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, out4, st);
-    return wide_fib_launch<WF_MAX_COLS>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, out4, st);
+        return wide_fib_launch<256>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, nullptr, out4,
+                                    st);
+    return wide_fib_launch<WF_MAX_COLS>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, nullptr,
+                                        out4, st);
 }
 
-// Same, with the trace column pointers in a device table and the powers on the device.
+// Same, with the trace column pointers in a device table and the powers on the device;
+// the denominator inverse of a row is den_half[0] on the first half of the rows and
+// den_half[1] on the second (the vanishing polynomial of a canonic coset takes one
+// value on each half of its blowup-2 domain in bit-reversed order).
 int wide_fib_dev_async(const uint32_t *const *trace_dev, uint32_t n_cols, uint32_t log_size, const uint32_t *powers_dev,
-                       const uint32_t *den_inv, uint32_t *const *out4, cudaStream_t st) {
-    STWO_REQUIRE(n_cols >= 3 && log_size <= 31 && powers_dev, STWO_ERR_UNSUPPORTED_SIZE,
+                       const uint32_t den_half[2], uint32_t *const *out4, cudaStream_t st) {
+    STWO_REQUIRE(n_cols >= 3 && log_size >= 1 && log_size <= 31 && powers_dev, STWO_ERR_UNSUPPORTED_SIZE,
                  "wide-Fibonacci composition over %u columns", n_cols);
-    return wide_fib_launch<1>(nullptr, trace_dev, n_cols, log_size, nullptr, powers_dev, den_inv, out4, st);
+    return wide_fib_launch<1>(nullptr, trace_dev, n_cols, log_size, nullptr, powers_dev, nullptr, den_half, out4, st);
 }
 
 }  // namespace stwo

@@ -57,8 +57,7 @@ int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_
 int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const uint32_t *itw, uint64_t off,
                uint32_t *const *dst4, bool circle, cudaStream_t st, const void *alpha_dev);
 int wide_fib_dev_async(const uint32_t *const *trace_dev, uint32_t n_cols, uint32_t log_size, const uint32_t *powers_dev,
-                       const uint32_t *den_inv, uint32_t *const *out4, cudaStream_t st);
-int batch_inverse_m31_async(const uint32_t *src, uint32_t *dst, uint64_t n, cudaStream_t st);
+                       const uint32_t den_half[2], uint32_t *const *out4, cudaStream_t st);
 int eval_at_points_dev_async(const void *polys_dev, uint32_t n_polys, uint32_t total_blocks, const void *point_dev,
                              void *results, void *partials, uint32_t *tickets, cudaStream_t st);
 uint32_t eval_at_point_blocks(uint32_t log_size);
@@ -116,33 +115,32 @@ __global__ void __launch_bounds__(256) wide_fib_trace_kernel(const uint32_t *__r
     }
 }
 
-// Vanishing polynomial of CanonicCoset(L).coset at every point of the circle domain
-// CanonicCoset(E) in bit-reversed order (coset_vanishing as wide_fibonacci.rs:99-117
-// calls it): p -> p - initial + step/2, then the x coordinate doubled L-1 times.
-struct VanishingParams {
-    cpoint gen_pows[31];  // GEN^(2^b)
-    cpoint shift;         // -initial + step/2 of the vanishing coset
-    uint32_t half_init, half_step, ext_log, doublings;
-};
+// Half coset {initial index, step index} of CanonicCoset(log).circle_domain():
+// 2^(30-log) and 2^(32-log).
+inline uint32_t half_coset_init(uint32_t log) { return 1u << (30 - log); }
+inline uint32_t half_coset_step(uint32_t log) { return (uint32_t)((1ull << (32 - log)) & 0x7fffffffu); }
 
-__global__ void __launch_bounds__(256) vanishing_kernel(uint32_t *__restrict__ out,
-                                                        const __grid_constant__ VanishingParams p) {
-    const uint64_t n = 1ull << p.ext_log, half = n >> 1;
-    for (uint64_t pos = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; pos < n; pos += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t i = bit_reverse_bits((uint32_t)pos, p.ext_log);
-        uint32_t idx = p.half_init + p.half_step * (uint32_t)(i < half ? i : i - half);
-        if (i >= half) idx = 0x80000000u - (idx & 0x7fffffffu);  // the conjugate half
-        cpoint r = {1, 0};
-#pragma unroll 1
-        for (int b = 0; b < 31; b++)
-            if ((idx >> b) & 1u) r = point_mul(r, p.gen_pows[b]);
-        r = point_mul(r, p.shift);
-        uint32_t x = r.x;
-        for (uint32_t d = 0; d < p.doublings; d++) {
-            uint32_t s = m31_sqr(x);
-            x = m31_sub(m31_add(s, s), 1);
-        }
-        out[pos] = x;
+// -initial + step/2 of CanonicCoset(log).coset (initial index 2^(30-log), step 2^(31-log)).
+__host__ __device__ inline cpoint vanishing_shift(uint32_t log) {
+    cpoint init = index_to_point(1u << (30 - log));
+    cpoint half_step = index_to_point(1u << (30 - log));
+    return point_mul(point_conj(init), half_step);
+}
+
+// Vanishing polynomial of CanonicCoset(L).coset on the circle domain CanonicCoset(L + 1)
+// in bit-reversed order (coset_vanishing as wide_fibonacci.rs:99-117 calls it: p ->
+// p - initial + step/2, then the x coordinate doubled L - 1 times). After L - 1
+// doublings the 2^(L+1) domain points land on two values, one for each half of the
+// bit-reversed order, so the composition needs only their two inverses: the values
+// at bit-reversed positions 0 and 2^L, i.e. the half-coset points of indices 0 and 1.
+inline void vanishing_inverses(uint32_t L, uint32_t out[2]) {
+    const uint32_t E = L + 1;
+    const uint32_t idx[2] = {half_coset_init(E), half_coset_init(E) + half_coset_step(E)};
+    const cpoint sh = vanishing_shift(L);
+    for (int h = 0; h < 2; h++) {
+        uint32_t x = point_mul(index_to_point(idx[h] & 0x7fffffffu), sh).x;
+        for (uint32_t d = 0; d + 1 < L; d++) x = m31_sub(m31_add(m31_sqr(x), m31_sqr(x)), 1);
+        out[h] = m31_inv(x);
     }
 }
 
@@ -177,12 +175,6 @@ __global__ void fs_comp_kernel(ProofState *s, const uint32_t *root) {
     s->oods[1] = qm31_mul(qm31_add(t, t), inv);
 }
 
-// -initial + step/2 of CanonicCoset(log).coset (initial index 2^(30-log), step 2^(31-log)).
-__host__ __device__ inline cpoint vanishing_shift(uint32_t log) {
-    cpoint init = index_to_point(1u << (30 - log));
-    cpoint half_step = index_to_point(1u << (30 - log));
-    return point_mul(point_conj(init), half_step);
-}
 
 // Channel step after the OODS evaluation, by one CTA: the constraint sum
 // sum_i r^(N-3-i) (c_i^2 + c_{i+1}^2 - c_{i+2}) over the sampled trace values (powers
@@ -384,10 +376,6 @@ struct Arena {
         int _rc = (expr);         \
         if (_rc) return _rc;      \
     } while (0)
-
-// Half coset {initial index, step index} of CanonicCoset(log).circle_domain().
-inline uint32_t half_coset_init(uint32_t log) { return 1u << (30 - log); }
-inline uint32_t half_coset_step(uint32_t log) { return (uint32_t)((1ull << (32 - log)) & 0x7fffffffu); }
 
 // Host image of device data uploaded in one copy: blobs appended at 256-byte aligned
 // offsets of a device region whose address is known once the image is complete.
@@ -592,7 +580,7 @@ uint64_t job_device_bytes(const Job &j, bool own_twiddles) {
     b += j.N * (r(4 * n) + r(4 * nb));                    // trace coefficients, trace evaluations
     if (j.B > 1) b += j.N * r(4 * ne);                    // trace on the composition domain
     b += tree(j.L + j.B) + tree(j.L + 1 + j.B);           // trace and composition trees
-    b += 2 * r(4 * ne) + 4 * r(4 * ne) + 4 * r(4 * neb);  // denominators, composition, its evaluations
+    b += 4 * r(4 * ne) + 4 * r(4 * neb);                  // composition, its evaluations
     b += r(16 * j.N);                                     // coefficient powers
     const uint64_t eap_blocks = (uint64_t)j.N * eval_at_point_blocks(j.L) + 4 * eval_at_point_blocks(j.L + 1);
     b += r(16 * eap_blocks);                              // eval_at_point partials
@@ -674,8 +662,6 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
             text[c] = x;
         }
     }
-    PV_ALLOC(den, uint32_t, 1ull << E);
-    PV_ALLOC(den_inv, uint32_t, 1ull << E);
     PV_ALLOC(powers, qm31, N);
     std::vector<uint32_t *> comp(4), cev(4), qc(4), qt(4);
     for (int k = 0; k < 4; k++) {
@@ -716,8 +702,10 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     auto qpt = std::make_unique<QuotParamsDev>();
     memset(qpc.get(), 0, sizeof(QuotParamsDev));
     memset(qpt.get(), 0, sizeof(QuotParamsDev));
-    quot_init_static(*qpc, half_coset_init(D), half_coset_step(D), D, qc.data());
-    quot_init_static(*qpt, half_coset_init(L + B), half_coset_step(L + B), L + B, qt.data());
+    const cpoint *circle_tab = nullptr;
+    PV_TRY(circle_point_table(&circle_tab));
+    quot_init_static(*qpc, half_coset_init(D), half_coset_step(D), D, qc.data(), circle_tab);
+    quot_init_static(*qpt, half_coset_init(L + B), half_coset_step(L + B), L + B, qt.data(), circle_tab);
     qpc->n_batches = qpt->n_batches = 1;
     qpc->batch_end[0] = 4;
     qpt->batch_end[0] = N;
@@ -806,25 +794,10 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         std::vector<const uint32_t *> src(tpoly.begin(), tpoly.end());
         PV_TRY(fft_columns(src.data(), text.data(), N, E, L, tw, tsz, false, st));
     }
-    {
-        VanishingParams vp{};
-        cpoint g = {CIRCLE_GEN_X, CIRCLE_GEN_Y};
-        for (int b = 0; b < 31; b++) {
-            vp.gen_pows[b] = g;
-            g = point_mul(g, g);
-        }
-        vp.shift = vanishing_shift(L);
-        vp.half_init = half_coset_init(E);
-        vp.half_step = half_coset_step(E);
-        vp.ext_log = E;
-        vp.doublings = L - 1;
-        const uint64_t blocks = std::min<uint64_t>(((1ull << E) + 255) / 256, (uint64_t)device_sm_count() * 8);
-        vanishing_kernel<<<(unsigned)blocks, 256, 0, st>>>(den, vp);
-        STWO_LAUNCH_CHECK("vanishing_kernel");
-    }
-    PV_TRY(batch_inverse_m31_async(den, den_inv, 1ull << E, st));
+    uint32_t den_half[2];
+    vanishing_inverses(L, den_half);
     PV_TRY(wide_fib_dev_async(reinterpret_cast<const uint32_t *const *>(dev_at(off_text)), N, E,
-                              reinterpret_cast<const uint32_t *>(powers), den_inv, comp.data(), st));
+                              reinterpret_cast<const uint32_t *>(powers), den_half, comp.data(), st));
     PV_TRY(fft_columns(comp.data(), comp.data(), 4, E, E, itw, tsz, true, st));  // in place -> coefficients
     {
         std::vector<const uint32_t *> src(comp.begin(), comp.end());

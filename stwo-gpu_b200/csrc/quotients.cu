@@ -16,7 +16,9 @@
 // denominators of the thread are inverted with one field inversion (Montgomery's
 // trick). The column terms accumulate unreduced 33-bit partial products in 64-bit
 // registers and reduce once per batch.
+#include <atomic>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -42,12 +44,14 @@ struct QuotByRef {
     __device__ const QuotParamsDev &get() const { return *p; }
 };
 
-__device__ __forceinline__ cpoint point_at_index(const cpoint *gen_pows, uint32_t idx) {
-    cpoint r = {1, 0};
-#pragma unroll 1
-    for (int b = 0; b < 31; b++)
-        if ((idx >> b) & 1u) r = point_mul(r, gen_pows[b]);
-    return r;
+// G^idx for a 31-bit circle-group index: the product of three table entries,
+// G^(idx mod 2^11), G^(2^11 * (idx >> 11 mod 2^11)) and G^(2^22 * (idx >> 22)).
+__device__ __forceinline__ cpoint point_from_tables(const cpoint *__restrict__ tab, uint32_t idx) {
+    const uint2 *t = reinterpret_cast<const uint2 *>(tab);
+    const uint2 a = __ldg(t + (idx & 2047u));
+    const uint2 b = __ldg(t + CIRCLE_TAB_LO + ((idx >> 11) & 2047u));
+    const uint2 c = __ldg(t + 2 * CIRCLE_TAB_LO + (idx >> 22));
+    return point_mul(point_mul({a.x, a.y}, {b.x, b.y}), {c.x, c.y});
 }
 
 // Unreduced product: value congruent to a*b, in [0, 2p].
@@ -58,10 +62,21 @@ __device__ __forceinline__ uint32_t reduce64(uint64_t x) {
     return reduce_once((uint32_t)s);
 }
 
+// den_b(p) of batch b at a domain point with x coordinate px and y coordinate py.
+template <class QP>
+__device__ __forceinline__ cm31 quot_den(const QP &p, uint32_t b, uint32_t px, uint32_t py) {
+    const cm31 t1 = {m31_sub(p.prx[b].a, px), p.prx[b].b};
+    const cm31 t2 = {m31_sub(p.pry[b].a, py), p.pry[b].b};
+    return cm31_sub(cm31_mul(t1, p.piy[b]), cm31_mul(t2, p.pix[b]));
+}
+
 // STAGE: the CTA first copies every sample's column pointer and doubled coefficient
 // into shared memory (n_stage samples), so the column loop reads them there instead
 // of chasing col_idx -> cols through global memory (device-resident parameters).
-template <bool COLS_ON_DEVICE, bool STAGE, class PR>
+// ONE_BATCH: exactly one sample batch (the prover's two quotient groups each have
+// one: every column sampled at the OODS point), so the per-row state stays in
+// registers and the two rows' denominators share one inversion.
+template <bool COLS_ON_DEVICE, bool STAGE, bool ONE_BATCH, class PR>
 __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ PR pr,
                                                         const uint32_t *const *__restrict__ dev_cols,
                                                         uint32_t n_stage) {
@@ -77,36 +92,44 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
         __syncthreads();
     }
     const uint64_t n_pairs = 1ull << (p.log_size - 1);
+    const uint32_t n_batches = ONE_BATCH ? 1u : p.n_batches;
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_pairs;
          k += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t hidx = bit_reverse_bits((uint32_t)k, p.log_size - 1);
-        cpoint pt = point_at_index(p.gen_pows, p.half_init + p.half_step * hidx);
-        // Denominators for both rows (y and -y), then one shared inversion.
-        cm31 den[2][QUOT_MAX_BATCHES];
-        cm31 prefix = {1, 0};
-        cm31 pre[2][QUOT_MAX_BATCHES];
+        // Rows 2k and 2k+1 are the domain point and its conjugate.
+        const uint32_t hidx = bit_reverse_bits((uint32_t)k, p.log_size - 1);
+        const cpoint pt = point_from_tables(p.tab, (p.half_init + p.half_step * hidx) & 0x7fffffffu);
         const uint32_t ys[2] = {pt.y, m31_neg(pt.y)};
-        for (uint32_t b = 0; b < p.n_batches; b++) {
-            for (int s = 0; s < 2; s++) {
-                cm31 t1 = {m31_sub(p.prx[b].a, pt.x), p.prx[b].b};
-                cm31 t2 = {m31_sub(p.pry[b].a, ys[s]), p.pry[b].b};
-                den[s][b] = cm31_sub(cm31_mul(t1, p.piy[b]), cm31_mul(t2, p.pix[b]));
-                prefix = cm31_mul(prefix, den[s][b]);
-                pre[s][b] = prefix;
+        // Denominator inverses of both rows, all batches: one inversion (Montgomery's trick).
+        cm31 den1[2];
+        cm31 den[2][ONE_BATCH ? 1 : QUOT_MAX_BATCHES];
+        if constexpr (ONE_BATCH) {
+            const cm31 d0 = quot_den(p, 0, pt.x, ys[0]), d1 = quot_den(p, 0, pt.x, ys[1]);
+            const cm31 inv = cm31_inv(cm31_mul(d0, d1));
+            den1[0] = cm31_mul(inv, d1);
+            den1[1] = cm31_mul(inv, d0);
+        } else {
+            cm31 prefix = {1, 0};
+            cm31 pre[2][QUOT_MAX_BATCHES];
+            for (uint32_t b = 0; b < n_batches; b++) {
+                for (int s = 0; s < 2; s++) {
+                    den[s][b] = quot_den(p, b, pt.x, ys[s]);
+                    prefix = cm31_mul(prefix, den[s][b]);
+                    pre[s][b] = prefix;
+                }
             }
-        }
-        cm31 inv = cm31_inv(prefix);
-        for (int b = (int)p.n_batches - 1; b >= 0; b--) {
-            for (int s = 1; s >= 0; s--) {
-                cm31 prev = (s == 1) ? pre[0][b] : (b > 0 ? pre[1][b - 1] : cm31{1, 0});
-                cm31 d = den[s][b];
-                den[s][b] = cm31_mul(inv, prev);  // inverse of d
-                inv = cm31_mul(inv, d);
+            cm31 inv = cm31_inv(prefix);
+            for (int b = (int)n_batches - 1; b >= 0; b--) {
+                for (int s = 1; s >= 0; s--) {
+                    cm31 prev = (s == 1) ? pre[0][b] : (b > 0 ? pre[1][b - 1] : cm31{1, 0});
+                    cm31 d = den[s][b];
+                    den[s][b] = cm31_mul(inv, prev);  // inverse of d
+                    inv = cm31_mul(inv, d);
+                }
             }
         }
         qm31 acc[2] = {qm31_zero(), qm31_zero()};
         uint32_t j0 = 0;
-        for (uint32_t b = 0; b < p.n_batches; b++) {
+        for (uint32_t b = 0; b < n_batches; b++) {
             uint64_t s0[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
             const uint32_t j1 = p.batch_end[b];
             // Column loads in groups of QUOT_PREFETCH, double-buffered: the next group's
@@ -152,7 +175,9 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                 qm31 num = {{reduce64(s0[s][0]), reduce64(s0[s][1])}, {reduce64(s0[s][2]), reduce64(s0[s][3])}};
                 qm31 lin = qm31_add(qm31_scale(p.a_sum[b], ys[s]), p.b_sum[b]);
                 num = qm31_sub(num, lin);
-                acc[s] = qm31_add(qm31_mul(acc[s], p.batch_coeff[b]), qm31_mul_cm31(num, den[s][b]));
+                const cm31 dinv = ONE_BATCH ? den1[s] : den[s][b];
+                acc[s] = ONE_BATCH ? qm31_mul_cm31(num, dinv)
+                                   : qm31_add(qm31_mul(acc[s], p.batch_coeff[b]), qm31_mul_cm31(num, dinv));
             }
         }
         reinterpret_cast<uint2 *>(p.out[0])[k] = make_uint2(acc[0].a.a, acc[1].a.a);
@@ -161,6 +186,42 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
         reinterpret_cast<uint2 *>(p.out[3])[k] = make_uint2(acc[0].b.b, acc[1].b.b);
     }
 }
+
+// The circle-group tables of point_from_tables on the current device: G^i for
+// i < 2^11, G^(2^11 i) for i < 2^11, G^(2^22 i) for i < 2^9 (36 KiB), computed on the
+// host and copied once per device.
+__device__ cpoint g_circle_tab[CIRCLE_TAB_SIZE];
+
+}  // namespace
+
+int circle_point_table(const cpoint **out) {
+    static std::atomic<uint64_t> done{0};
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    int rc = once_per_device(done, [] {
+        std::vector<cpoint> t(CIRCLE_TAB_SIZE);
+        cpoint step[3] = {index_to_point(1), index_to_point(1u << 11), index_to_point(1u << 22)};
+        const uint32_t len[3] = {CIRCLE_TAB_LO, CIRCLE_TAB_LO, CIRCLE_TAB_SIZE - 2 * CIRCLE_TAB_LO};
+        uint32_t off = 0;
+        for (int s = 0; s < 3; s++) {
+            cpoint r = {1, 0};
+            for (uint32_t i = 0; i < len[s]; i++) {
+                t[off + i] = r;
+                r = point_mul(r, step[s]);
+            }
+            off += len[s];
+        }
+        STWO_CUDA_TRY(cudaMemcpyToSymbol(g_circle_tab, t.data(), sizeof(cpoint) * CIRCLE_TAB_SIZE));
+        return (int)STWO_OK;
+    });
+    if (rc) return rc;
+    void *addr = nullptr;
+    STWO_CUDA_TRY(cudaGetSymbolAddress(&addr, g_circle_tab));
+    *out = static_cast<const cpoint *>(addr);
+    return STWO_OK;
+}
+
+namespace {
 
 inline qm31 to_q(stwo_qm31 v) { return {{v.a, v.b}, {v.c, v.d}}; }
 
@@ -178,7 +239,10 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
                  "at most %d columns", QUOT_MAX_COLS);
     auto holder = std::make_unique<QuotByValue>();
     QuotParams *p = &holder->p;
-    quot_init_static(*p, half_init, half_step, log_size, out4);
+    const cpoint *tab = nullptr;
+    int trc = circle_point_table(&tab);
+    if (trc) return trc;
+    quot_init_static(*p, half_init, half_step, log_size, out4, tab);
     p->n_batches = n_batches;
     if (!cols_on_device)
         for (uint32_t i = 0; i < n_cols; i++) p->cols[i] = cols[i];
@@ -203,8 +267,13 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    if (cols_on_device) quotients_kernel<true, false><<<(unsigned)blocks, 256, 0, st>>>(*holder, cols, 0u);
-    else quotients_kernel<false, false><<<(unsigned)blocks, 256, 0, st>>>(*holder, nullptr, 0u);
+    if (n_batches == 1) {
+        if (cols_on_device) quotients_kernel<true, false, true><<<(unsigned)blocks, 256, 0, st>>>(*holder, cols, 0u);
+        else quotients_kernel<false, false, true><<<(unsigned)blocks, 256, 0, st>>>(*holder, nullptr, 0u);
+    } else {
+        if (cols_on_device) quotients_kernel<true, false, false><<<(unsigned)blocks, 256, 0, st>>>(*holder, cols, 0u);
+        else quotients_kernel<false, false, false><<<(unsigned)blocks, 256, 0, st>>>(*holder, nullptr, 0u);
+    }
     STWO_LAUNCH_CHECK("quotients_kernel");
     return STWO_OK;
 }
@@ -217,7 +286,7 @@ int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t 
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    quotients_kernel<false, true><<<(unsigned)blocks, 256, smem, st>>>(QuotByRef{p_dev}, nullptr, n_samples);
+    quotients_kernel<false, true, true><<<(unsigned)blocks, 256, smem, st>>>(QuotByRef{p_dev}, nullptr, n_samples);
     STWO_LAUNCH_CHECK("quotients_kernel");
     return STWO_OK;
 }

@@ -12,6 +12,13 @@ constexpr int QUOT_MAX_COLS = 512;
 constexpr int QUOT_MAX_SAMPLES = 512;
 constexpr int QUOT_MAX_BATCHES = 16;
 
+// Circle-group point tables (quotients.cu): G^i for i < 2^11, G^(2^11 i) for i < 2^11
+// and G^(2^22 i) for i < 2^9, consecutive.
+constexpr uint32_t CIRCLE_TAB_LO = 2048;
+constexpr uint32_t CIRCLE_TAB_SIZE = 2 * CIRCLE_TAB_LO + 512;
+// Device address of the tables on the current device (filled on first use).
+int circle_point_table(const cpoint **out);
+
 template <int MAXC, int MAXS>
 struct QuotParamsT {
     const uint32_t *cols[MAXC];
@@ -24,7 +31,7 @@ struct QuotParamsT {
     uint32_t half_init, half_step;        // half coset indices
     uint32_t log_size;                    // domain log size
     uint32_t *out[4];
-    cpoint gen_pows[31];                  // GEN^(2^b), so the kernel shares no state between calls
+    const cpoint *tab;                    // circle_point_table() of the launching device
 };
 
 // The prover's device-resident parameters: up to 1024 columns and samples.
@@ -111,14 +118,11 @@ __device__ inline void quot_fill_batch_block(QP &p, uint32_t b, qm31 rc, qm31 px
     }
 }
 
-// The column-independent fields: domain, outputs, generator table.
+// The column-independent fields: domain, outputs, point tables.
 template <class QP>
-inline void quot_init_static(QP &p, uint32_t half_init, uint32_t half_step, uint32_t log_size, uint32_t *const *out4) {
-    cpoint g = {CIRCLE_GEN_X, CIRCLE_GEN_Y};
-    for (int b = 0; b < 31; b++) {
-        p.gen_pows[b] = g;
-        g = point_mul(g, g);
-    }
+inline void quot_init_static(QP &p, uint32_t half_init, uint32_t half_step, uint32_t log_size, uint32_t *const *out4,
+                             const cpoint *tab) {
+    p.tab = tab;
     p.half_init = half_init;
     p.half_step = half_step;
     p.log_size = log_size;
