@@ -17,6 +17,7 @@
 // trick). The column terms accumulate unreduced 33-bit partial products in 64-bit
 // registers and reduce once per batch.
 #include <atomic>
+#include <type_traits>
 #include <memory>
 #include <mutex>
 #include <vector>
@@ -73,10 +74,11 @@ __device__ __forceinline__ cm31 quot_den(const QP &p, uint32_t b, uint32_t px, u
 // STAGE: the CTA first copies every sample's column pointer and doubled coefficient
 // into shared memory (n_stage samples), so the column loop reads them there instead
 // of chasing col_idx -> cols through global memory (device-resident parameters).
-// ONE_BATCH: exactly one sample batch (the prover's two quotient groups each have
-// one: every column sampled at the OODS point), so the per-row state stays in
-// registers and the two rows' denominators share one inversion.
-template <bool COLS_ON_DEVICE, bool STAGE, bool ONE_BATCH, class PR>
+// NB > 0: exactly NB sample batches, known at compile time, so the per-row
+// denominators stay in registers (the prover's two quotient groups have one batch
+// each: every column sampled at the OODS point); NB == 0: any count up to
+// QUOT_MAX_BATCHES.
+template <bool COLS_ON_DEVICE, bool STAGE, int NB, class PR>
 __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ PR pr,
                                                         const uint32_t *const *__restrict__ dev_cols,
                                                         uint32_t n_stage) {
@@ -91,8 +93,9 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
         }
         __syncthreads();
     }
+    constexpr int MAXB = NB > 0 ? NB : QUOT_MAX_BATCHES;
     const uint64_t n_pairs = 1ull << (p.log_size - 1);
-    const uint32_t n_batches = ONE_BATCH ? 1u : p.n_batches;
+    const uint32_t n_batches = NB > 0 ? (uint32_t)NB : p.n_batches;
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_pairs;
          k += (uint64_t)gridDim.x * blockDim.x) {
         // Rows 2k and 2k+1 are the domain point and its conjugate.
@@ -100,17 +103,14 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
         const cpoint pt = point_from_tables(p.tab, (p.half_init + p.half_step * hidx) & 0x7fffffffu);
         const uint32_t ys[2] = {pt.y, m31_neg(pt.y)};
         // Denominator inverses of both rows, all batches: one inversion (Montgomery's trick).
-        cm31 den1[2];
-        cm31 den[2][ONE_BATCH ? 1 : QUOT_MAX_BATCHES];
-        if constexpr (ONE_BATCH) {
-            const cm31 d0 = quot_den(p, 0, pt.x, ys[0]), d1 = quot_den(p, 0, pt.x, ys[1]);
-            const cm31 inv = cm31_inv(cm31_mul(d0, d1));
-            den1[0] = cm31_mul(inv, d1);
-            den1[1] = cm31_mul(inv, d0);
-        } else {
+        cm31 den[2][MAXB];
+        {
             cm31 prefix = {1, 0};
-            cm31 pre[2][QUOT_MAX_BATCHES];
-            for (uint32_t b = 0; b < n_batches; b++) {
+            cm31 pre[2][MAXB];
+#pragma unroll
+            for (int b = 0; b < MAXB; b++) {
+                if (NB == 0 && b >= (int)n_batches) break;
+#pragma unroll
                 for (int s = 0; s < 2; s++) {
                     den[s][b] = quot_den(p, b, pt.x, ys[s]);
                     prefix = cm31_mul(prefix, den[s][b]);
@@ -118,10 +118,13 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                 }
             }
             cm31 inv = cm31_inv(prefix);
-            for (int b = (int)n_batches - 1; b >= 0; b--) {
+#pragma unroll
+            for (int b = MAXB - 1; b >= 0; b--) {
+                if (NB == 0 && b >= (int)n_batches) continue;
+#pragma unroll
                 for (int s = 1; s >= 0; s--) {
-                    cm31 prev = (s == 1) ? pre[0][b] : (b > 0 ? pre[1][b - 1] : cm31{1, 0});
-                    cm31 d = den[s][b];
+                    const cm31 prev = (s == 1) ? pre[0][b] : (b > 0 ? pre[1][b - 1] : cm31{1, 0});
+                    const cm31 d = den[s][b];
                     den[s][b] = cm31_mul(inv, prev);  // inverse of d
                     inv = cm31_mul(inv, d);
                 }
@@ -129,7 +132,9 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
         }
         qm31 acc[2] = {qm31_zero(), qm31_zero()};
         uint32_t j0 = 0;
-        for (uint32_t b = 0; b < n_batches; b++) {
+#pragma unroll
+        for (int b = 0; b < MAXB; b++) {
+            if (NB == 0 && b >= (int)n_batches) break;
             uint64_t s0[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
             const uint32_t j1 = p.batch_end[b];
             // Column loads in groups of QUOT_PREFETCH, double-buffered: the next group's
@@ -175,9 +180,8 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                 qm31 num = {{reduce64(s0[s][0]), reduce64(s0[s][1])}, {reduce64(s0[s][2]), reduce64(s0[s][3])}};
                 qm31 lin = qm31_add(qm31_scale(p.a_sum[b], ys[s]), p.b_sum[b]);
                 num = qm31_sub(num, lin);
-                const cm31 dinv = ONE_BATCH ? den1[s] : den[s][b];
-                acc[s] = ONE_BATCH ? qm31_mul_cm31(num, dinv)
-                                   : qm31_add(qm31_mul(acc[s], p.batch_coeff[b]), qm31_mul_cm31(num, dinv));
+                acc[s] = b == 0 ? qm31_mul_cm31(num, den[s][b])
+                                : qm31_add(qm31_mul(acc[s], p.batch_coeff[b]), qm31_mul_cm31(num, den[s][b]));
             }
         }
         reinterpret_cast<uint2 *>(p.out[0])[k] = make_uint2(acc[0].a.a, acc[1].a.a);
@@ -267,12 +271,19 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    if (n_batches == 1) {
-        if (cols_on_device) quotients_kernel<true, false, true><<<(unsigned)blocks, 256, 0, st>>>(*holder, cols, 0u);
-        else quotients_kernel<false, false, true><<<(unsigned)blocks, 256, 0, st>>>(*holder, nullptr, 0u);
-    } else {
-        if (cols_on_device) quotients_kernel<true, false, false><<<(unsigned)blocks, 256, 0, st>>>(*holder, cols, 0u);
-        else quotients_kernel<false, false, false><<<(unsigned)blocks, 256, 0, st>>>(*holder, nullptr, 0u);
+    auto launch = [&](auto nb) {
+        constexpr int NBV = decltype(nb)::value;
+        if (cols_on_device)
+            quotients_kernel<true, false, NBV><<<(unsigned)blocks, 256, 0, st>>>(*holder, cols, 0u);
+        else
+            quotients_kernel<false, false, NBV><<<(unsigned)blocks, 256, 0, st>>>(*holder, nullptr, 0u);
+    };
+    switch (n_batches) {
+    case 1: launch(std::integral_constant<int, 1>{}); break;
+    case 2: launch(std::integral_constant<int, 2>{}); break;
+    case 3: launch(std::integral_constant<int, 3>{}); break;
+    case 4: launch(std::integral_constant<int, 4>{}); break;
+    default: launch(std::integral_constant<int, 0>{}); break;
     }
     STWO_LAUNCH_CHECK("quotients_kernel");
     return STWO_OK;
@@ -286,7 +297,7 @@ int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t 
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    quotients_kernel<false, true, true><<<(unsigned)blocks, 256, smem, st>>>(QuotByRef{p_dev}, nullptr, n_samples);
+    quotients_kernel<false, true, 1><<<(unsigned)blocks, 256, smem, st>>>(QuotByRef{p_dev}, nullptr, n_samples);
     STWO_LAUNCH_CHECK("quotients_kernel");
     return STWO_OK;
 }
