@@ -8,6 +8,7 @@
 // Each thread folds two adjacent outputs, reading one 16-byte vector per input
 // coordinate column and writing one 8-byte vector per output column.
 #include "common.cuh"
+#include "fri.cuh"
 
 namespace stwo {
 
@@ -18,19 +19,6 @@ namespace {
 
 struct Cols4 { const uint32_t *c[4]; };
 struct MutCols4 { uint32_t *c[4]; };
-
-__device__ __forceinline__ uint32_t circle_itw(const uint32_t *__restrict__ lt0, uint64_t h) {
-    uint64_t q = h >> 2;
-    uint32_t r = (uint32_t)(h & 3u);
-    uint32_t v = __ldg(lt0 + 2 * q + ((r >> 1) ^ 1u));
-    return (r == 1u || r == 2u) ? m31_neg(v) : v;
-}
-
-__device__ __forceinline__ qm31 fold_pair(qm31 a, qm31 b, uint32_t t, qm31 alpha) {
-    qm31 s = qm31_add(a, b);
-    qm31 d = qm31_scale(qm31_sub(a, b), t);
-    return qm31_add(s, qm31_mul(alpha, d));
-}
 
 // alpha_dev: when set, alpha is read from device memory (a challenge the device
 // channel drew) instead of the by-value argument.

@@ -46,6 +46,7 @@
 #include "blake2s.cuh"
 #include "channel.cuh"
 #include "common.cuh"
+#include "fri.cuh"
 #include "quotients.cuh"
 
 namespace stwo {
@@ -229,23 +230,19 @@ __global__ void fs_layer_kernel(ProofState *s, const uint32_t *root, uint32_t ro
 // Last FRI layer: 2^log values (bit-reversed) over the line domain
 // Coset(2^(29-log), 2^(31-log)) interpolated (LineEvaluation::interpolate); every
 // coefficient but the constant must vanish (degree bound 1); the constant is mixed.
-struct Cols4c {
-    const uint32_t *c[4];
-};
 
-__global__ void fs_last_kernel(ProofState *s, const __grid_constant__ Cols4c cur, uint32_t log) {
+__device__ void fs_last(ProofState *s, const uint32_t *const c[4], uint32_t log) {
     const uint32_t n = 1u << log;  // log <= 4
     qm31 v[16];
-    for (uint32_t i = 0; i < n; i++)
-        v[bit_reverse_bits(i, log)] = {{cur.c[0][i], cur.c[1][i]}, {cur.c[2][i], cur.c[3][i]}};
+    for (uint32_t i = 0; i < n; i++) v[bit_reverse_bits(i, log)] = {{c[0][i], c[1][i]}, {c[2][i], c[3][i]}};
     uint32_t di = 1u << (29 - log), ds = 1u << (31 - log);
     for (uint32_t size = n; size > 1; size >>= 1) {
-        for (uint32_t c = 0; c < n; c += size)
+        for (uint32_t c0 = 0; c0 < n; c0 += size)
             for (uint32_t i = 0; i < size / 2; i++) {
                 const uint32_t xi = m31_inv(index_to_point((di + ds * i) & 0x7fffffffu).x);
-                const qm31 a = v[c + i], b = v[c + i + size / 2];
-                v[c + i] = qm31_add(a, b);
-                v[c + i + size / 2] = qm31_scale(qm31_sub(a, b), xi);
+                const qm31 a = v[c0 + i], b = v[c0 + i + size / 2];
+                v[c0 + i] = qm31_add(a, b);
+                v[c0 + i + size / 2] = qm31_scale(qm31_sub(a, b), xi);
             }
         di = (di * 2) & 0x7fffffffu;
         ds = (ds * 2) & 0x7fffffffu;
@@ -256,6 +253,143 @@ __global__ void fs_last_kernel(ProofState *s, const __grid_constant__ Cols4c cur
     const qm31 c0 = qm31_scale(v[0], ninv);
     s->last_coeff = c0;
     fs::ch_mix_felts(s->ch, &c0, 1);
+}
+
+// The FRI tail in one launch: one CTA of 1024 threads runs every inner layer of log
+// size <= TAIL_MAX_LOG in order, then the last layer, exactly as the per-layer
+// launches do:
+//   [the trace quotient's circle fold into the layer, with the previous alpha]
+//   -> the layer's Merkle tree over its 4 coordinate columns (leaves: one compression
+//      of the 4 values; nodes: one compression of the two children), every level
+//      written to its global buffer for the decommitment and kept in shared memory
+//      for the next level
+//   -> thread 0: mix the root, draw the layer's alpha
+//   -> fold_line into the next layer.
+// Values this kernel wrote are read back with plain (coherent) loads after a
+// barrier; nothing is read through the non-coherent path except the trace quotient
+// and the twiddles.
+constexpr uint32_t TAIL_MAX_LOG = 10;
+constexpr uint32_t TAIL_MAX = TAIL_MAX_LOG;  // inner layers of log size 2 .. TAIL_MAX_LOG
+constexpr uint32_t TAIL_THREADS = 1024;
+constexpr size_t TAIL_SMEM = (32ull << TAIL_MAX_LOG) + (32ull << (TAIL_MAX_LOG - 1));
+
+struct TailParams {
+    uint32_t li0, n_tail, lg0, last_log;
+    uint32_t circle_t;                            // tail index of the layer the trace quotient folds into, or ~0
+    const uint32_t *qt[4];                        // trace quotient (2 * 2^lg values at circle_t)
+    const uint32_t *circle_tw;                    // inverse-twiddle suffix of that fold
+    uint32_t *lay[TAIL_MAX + 1][4];               // tail layers, then the last layer
+    uint4 *nodes[TAIL_MAX][TAIL_MAX_LOG + 1];     // tree layers of each tail layer
+    const uint32_t *line_tw[TAIL_MAX];            // inverse-twiddle suffix of each layer's line fold
+};
+
+__global__ void __launch_bounds__(TAIL_THREADS) fri_tail_kernel(ProofState *s, const TailParams *__restrict__ tp,
+                                                                 uint32_t one) {
+    extern __shared__ uint4 t_buf[];
+    uint4 *buf[2] = {t_buf, t_buf + (2u << TAIL_MAX_LOG)};
+    __shared__ qm31 alpha_sh;
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t t = 0; t < tp->n_tail; t++) {
+        const uint32_t li = tp->li0 + t, lg = tp->lg0 - t, n = 1u << lg;
+        uint32_t *const *cur = tp->lay[t];
+        if (t == tp->circle_t) {
+            const qm31 a = s->alphas[li], a2 = qm31_mul(a, a);
+            for (uint32_t i = tid; i < n; i += TAIL_THREADS) {
+                const qm31 f0 = {{__ldg(tp->qt[0] + 2 * i), __ldg(tp->qt[1] + 2 * i)},
+                                 {__ldg(tp->qt[2] + 2 * i), __ldg(tp->qt[3] + 2 * i)}};
+                const qm31 f1 = {{__ldg(tp->qt[0] + 2 * i + 1), __ldg(tp->qt[1] + 2 * i + 1)},
+                                 {__ldg(tp->qt[2] + 2 * i + 1), __ldg(tp->qt[3] + 2 * i + 1)}};
+                const qm31 f = fold_pair(f0, f1, circle_itw(tp->circle_tw, i), a);
+                const qm31 p = {{cur[0][i], cur[1][i]}, {cur[2][i], cur[3][i]}};
+                const qm31 r = qm31_add(qm31_mul(p, a2), f);
+                cur[0][i] = r.a.a;
+                cur[1][i] = r.a.b;
+                cur[2][i] = r.b.a;
+                cur[3][i] = r.b.b;
+            }
+            __syncthreads();
+        }
+        // Leaves: one compression of the layer's 4 values.
+        for (uint32_t i = tid; i < n; i += TAIL_THREADS) {
+            uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            uint32_t m[16] = {cur[0][i], cur[1][i], cur[2][i], cur[3][i], 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+            blake::compress(h, m, one);
+            const uint4 lo = make_uint4(h[0], h[1], h[2], h[3]), hi = make_uint4(h[4], h[5], h[6], h[7]);
+            tp->nodes[t][lg][2 * i] = lo;
+            tp->nodes[t][lg][2 * i + 1] = hi;
+            buf[0][2 * i] = lo;
+            buf[0][2 * i + 1] = hi;
+        }
+        __syncthreads();
+        // Nodes, level by level: children from one shared buffer, parents into the other.
+        // Levels of at most 32 nodes are left to the first warp, which synchronises
+        // with itself only.
+        auto node = [&](uint32_t l, uint32_t k, uint32_t src) {
+            uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            uint32_t m[16];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint4 v = buf[src][4 * k + q];
+                m[4 * q] = v.x; m[4 * q + 1] = v.y; m[4 * q + 2] = v.z; m[4 * q + 3] = v.w;
+            }
+            blake::compress(h, m, one);
+            const uint4 lo = make_uint4(h[0], h[1], h[2], h[3]), hi = make_uint4(h[4], h[5], h[6], h[7]);
+            tp->nodes[t][l][2 * k] = lo;
+            tp->nodes[t][l][2 * k + 1] = hi;
+            buf[src ^ 1][2 * k] = lo;
+            buf[src ^ 1][2 * k + 1] = hi;
+        };
+        uint32_t src = 0;
+        int l = (int)lg - 1;
+        for (; l >= 0 && (1u << l) > 32u; l--) {
+            for (uint32_t k = tid; k < (1u << l); k += TAIL_THREADS) node((uint32_t)l, k, src);
+            src ^= 1;
+            __syncthreads();
+        }
+        if (tid < 32) {  // src is only read by thread 0 below
+            for (; l >= 0; l--) {
+                if (tid < (1u << l)) node((uint32_t)l, tid, src);
+                src ^= 1;
+                __syncwarp();
+            }
+        }
+        if (tid == 0) {
+            const uint4 lo = buf[src][0], hi = buf[src][1];
+            const uint32_t root[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+            for (int i = 0; i < 8; i++) s->roots[3 + li][i] = root[i];
+            fs::ch_mix_root(s->ch, root);
+            const qm31 a = fs::ch_draw_felt(s->ch, s->error);
+            s->alphas[li + 1] = a;
+            alpha_sh = a;
+        }
+        __syncthreads();
+        // fold_line into the next layer.
+        const qm31 alpha = alpha_sh;
+        uint32_t *const *nxt = tp->lay[t + 1];
+        for (uint32_t i = tid; i < n / 2; i += TAIL_THREADS) {
+            const qm31 f0 = {{cur[0][2 * i], cur[1][2 * i]}, {cur[2][2 * i], cur[3][2 * i]}};
+            const qm31 f1 = {{cur[0][2 * i + 1], cur[1][2 * i + 1]}, {cur[2][2 * i + 1], cur[3][2 * i + 1]}};
+            const qm31 r = fold_pair(f0, f1, __ldg(tp->line_tw[t] + i), alpha);
+            nxt[0][i] = r.a.a;
+            nxt[1][i] = r.a.b;
+            nxt[2][i] = r.b.a;
+            nxt[3][i] = r.b.b;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) fs_last(s, tp->lay[tp->n_tail], tp->last_log);
+}
+
+int launch_fri_tail(ProofState *s, const TailParams *tp, cudaStream_t st) {
+    static std::atomic<uint64_t> attr_set{0};
+    int rc = once_per_device(attr_set, [] {
+        STWO_CUDA_TRY(cudaFuncSetAttribute(fri_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM));
+        return (int)STWO_OK;
+    });
+    if (rc) return rc;
+    fri_tail_kernel<<<1, TAIL_THREADS, TAIL_SMEM, st>>>(s, tp, 1u);
+    STWO_LAUNCH_CHECK("fri_tail_kernel");
+    return STWO_OK;
 }
 
 // Proof-of-work search (GrindOps::grind): nonce k is valid when the digest mixed with k
@@ -590,6 +724,7 @@ uint64_t job_device_bytes(const Job &j, bool own_twiddles) {
     // the uploaded image: state and sampled values, tickets, quotient parameters, tables
     b += r(sizeof(ProofState) + 16 * (j.N + 4)) + r(4 * (j.N + 4)) + 2 * r(sizeof(QuotParamsDev));
     b += 2 * r(8 * j.N) + r(sizeof(EapDevPoly) * (j.N + 4)) + (2 * (j.L + j.B) + 8) * r(64) + r(8 * j.N);
+    b += r(sizeof(TailParams));
     const uint64_t words = (uint64_t)j.n_queries * ((j.L + 2 + j.B) * 8 * 3 * 8 + 2 * (j.N + 16));
     b += r(words * sizeof(GatherReq)) + r(words * 4);     // decommitment gather
     return b;
@@ -741,6 +876,30 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
             PV_TRY(plan_tree(t_lay[li], cols, ar, up));
         }
     }
+    // The FRI tail: inner layers of log size <= TAIL_MAX_LOG (from li0 on) and the last
+    // layer run in one launch. The trace quotient folds into layer 1 (log L + B - 1).
+    const uint32_t li0 = D - 1 > TAIL_MAX_LOG ? D - 1 - TAIL_MAX_LOG : 0;
+    const uint32_t li_circle = D - (L + B);
+    size_t off_tail = 0;
+    {
+        auto tp = std::make_unique<TailParams>();
+        memset(tp.get(), 0, sizeof(TailParams));
+        tp->li0 = li0;
+        tp->n_tail = n_layers - li0;
+        tp->lg0 = D - 1 - li0;
+        tp->last_log = B;
+        tp->circle_t = li_circle >= li0 ? li_circle - li0 : ~0u;
+        for (int k = 0; k < 4; k++) tp->qt[k] = qt[k];
+        tp->circle_tw = itw + (tsz - (1ull << (L + B - 1)));
+        for (uint32_t t = 0; t <= tp->n_tail; t++)
+            for (int k = 0; k < 4; k++) tp->lay[t][k] = lay[li0 + t][k];
+        for (uint32_t t = 0; t < tp->n_tail; t++) {
+            const uint32_t lg = tp->lg0 - t;
+            for (uint32_t l = 0; l <= lg; l++) tp->nodes[t][l] = reinterpret_cast<uint4 *>(t_lay[li0 + t].layers[l]);
+            tp->line_tw[t] = itw + (tsz - (1ull << lg));
+        }
+        off_tail = up.add(tp.get(), sizeof(TailParams));
+    }
     PV_ALLOC(dev_img, uint8_t, up.host.size());
     auto dev_at = [&](size_t off) { return dev_img + off; };
     auto fix_tables = [&](MerkleTree &t) {
@@ -827,9 +986,9 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         PV_TRY(fold_async(s.data(), 1ull << D, stwo_qm31{}, itw, tsz - (1ull << (D - 1)), lay[0].data(), true, st,
                           &dstate->alphas[0]));
     }
-    for (uint32_t li = 0; li < n_layers; li++) {
+    for (uint32_t li = 0; li < li0; li++) {
         const uint32_t lg = D - 1 - li;
-        if (lg == L + B - 1) {
+        if (li == li_circle) {
             // The trace quotient folds into this layer with the previous layer's alpha.
             std::vector<const uint32_t *> s(qt.begin(), qt.end());
             PV_TRY(fold_async(s.data(), 1ull << (L + B), stwo_qm31{}, itw, tsz - (1ull << lg), lay[li].data(), true, st,
@@ -842,11 +1001,7 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         PV_TRY(fold_async(s.data(), 1ull << lg, stwo_qm31{}, itw, tsz - (1ull << lg), lay[li + 1].data(), false, st,
                           &dstate->alphas[li + 1]));
     }
-    {
-        Cols4c last{{lay[n_layers][0], lay[n_layers][1], lay[n_layers][2], lay[n_layers][3]}};
-        fs_last_kernel<<<1, 1, 0, st>>>(dstate, last, B);
-        STWO_LAUNCH_CHECK("fs_last_kernel");
-    }
+    PV_TRY(launch_fri_tail(dstate, reinterpret_cast<const TailParams *>(dev_at(off_tail)), st));
     if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[4], st));
 
     // ---- 5. proof of work and query words, then the channel's record to the host
