@@ -30,9 +30,10 @@ namespace {
 
 using QuotParams = QuotParamsT<QUOT_MAX_COLS, QUOT_MAX_SAMPLES>;
 #ifndef QUOT_PREFETCH_N
-#define QUOT_PREFETCH_N 4
+#define QUOT_PREFETCH_N 6
 #endif
 constexpr int QUOT_PREFETCH = QUOT_PREFETCH_N;  // column loads per group (two groups in flight)
+static_assert(QUOT_PREFETCH % 3 == 0, "the fold cadence needs groups of a multiple of 3 columns");
 
 // The kernel reads its parameters through get(): by value from the parameter block,
 // or from a device-resident block (the prover's, filled by the device channel).
@@ -151,8 +152,8 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                 }
             };
             // 64-bit multiply-accumulates of canonical values (products below 2^62),
-            // folded after every second column: a folded sum (below 2^34) plus two
-            // products stays below 2^64.
+            // folded after every third column: a folded sum (below 2^34) plus three
+            // products stays below 2^64. The group size is a multiple of 3.
             auto consume = [&](uint32_t jb, const uint2 (&v)[QUOT_PREFETCH]) {
 #pragma unroll
                 for (int u = 0; u < QUOT_PREFETCH; u++) {
@@ -162,7 +163,7 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                     s0[0][2] = mac64(s0[0][2], v[u].x, c.b.a); s0[0][3] = mac64(s0[0][3], v[u].x, c.b.b);
                     s0[1][0] = mac64(s0[1][0], v[u].y, c.a.a); s0[1][1] = mac64(s0[1][1], v[u].y, c.a.b);
                     s0[1][2] = mac64(s0[1][2], v[u].y, c.b.a); s0[1][3] = mac64(s0[1][3], v[u].y, c.b.b);
-                    if (u & 1)
+                    if (u % 3 == 2)
                         for (int s = 0; s < 2; s++)
                             for (int t = 0; t < 4; t++) s0[s][t] = fold64(s0[s][t]);
                 }

@@ -18,6 +18,7 @@ JOBS = [
     (3, 20, 3, 9, 2),
     (7, 33, 4, 20, 8),
     (9, 17, 1, 7, 11),
+    (10, 20, 1, 3, 5),   # first FRI layer of log size 11: the fused tail starts at layer 1
     (10, 100, 2, 3, 5),
     (11, 64, 1, 30, 1),
     (12, 64, 1, 3, 5),   # 64 columns, 2^12 rows: the reference CpuBackend's single proof
