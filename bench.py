@@ -771,7 +771,8 @@ def run_profile(args):
     """One workload between cudaProfilerStart/Stop for ncu (--profile-from-start off),
     after warm-up: `fft[:LOG]` (8 columns at LOG, interpolate + blowup-4 evaluate, two
     steps), `proof:L,N` (one wide-Fibonacci proof, log_blowup 1, 3 queries, pow_bits 5)
-    or `merkle` (the 64 x 2^22 tree of the kernel sweep)."""
+    `merkle` (the 64 x 2^22 tree of the kernel sweep) or `quotients` (the sweep's 32
+    columns x 2^22 with 4 sample points)."""
     import numpy as np
     import torch
     stwo = load_package()
@@ -819,6 +820,29 @@ def run_profile(args):
             for l in range(lg - 1, -1, -1):
                 L.check(lib.stwo_merkle_commit_layer(l, layers[l + 1].data_ptr(), None, 0, layers[l].data_ptr(), sptr))
         reps = 1
+    elif what == "quotients":
+        import ctypes as C
+        import random
+        lg, nc, nb = 22, 32, 4
+        sptr = torch.cuda.current_stream(dev).cuda_stream
+        dom = stwo.CanonicCoset(lg).circle_domain()
+        cols = [torch.randint(0, P, (1 << lg,), dtype=torch.int64, device=dev).to(torch.int32) for _ in range(nc)]
+        outq = [torch.empty(1 << lg, dtype=torch.int32, device=dev) for _ in range(4)]
+        rr = random.Random(5)
+
+        def rq():
+            return L.QM31(*[rr.randrange(P) for _ in range(4)])
+        sp = (L.SPoint * nb)(*[L.SPoint(rq(), rq()) for _ in range(nb)])
+        sizes = (C.c_uint32 * nb)(*([nc] * nb))
+        idx = (C.c_uint32 * (nc * nb))(*(list(range(nc)) * nb))
+        vals = (L.QM31 * (nc * nb))(*[rq() for _ in range(nc * nb)])
+        rcoef = rq()
+        cp, op = L.ptr_array([c.data_ptr() for c in cols]), L.ptr_array([c.data_ptr() for c in outq])
+
+        def work():
+            L.check(lib.stwo_accumulate_quotients(dom.half_coset.initial_index, dom.half_coset.step_size, lg, cp, nc,
+                                                  rcoef, sp, sizes, idx, vals, nb, op, sptr))
+        reps = 1
     else:
         raise SystemExit(f"unknown --profile {what}")
     for _ in range(3):
@@ -847,7 +871,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-suite", action="store_true", help="skip the config-1 per-kernel sweep")
     ap.add_argument("--profile", default=None,
-                    help="run one workload for ncu instead: fft[:LOG] | proof:L,N | merkle")
+                    help="run one workload for ncu instead: fft[:LOG] | proof:L,N | merkle | quotients")
     args = ap.parse_args()
     if args.profile:
         run_profile(args)

@@ -272,12 +272,17 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
+    // Every sample's coefficient and column pointer staged in shared memory (at most
+    // QUOT_MAX_SAMPLES x 24 bytes = 12 KiB): the column loop then reads them there
+    // instead of indexing the parameter block at run time.
+    const uint32_t n_samples = off;
+    const size_t smem = (size_t)n_samples * (sizeof(qm31) + sizeof(void *));
     auto launch = [&](auto nb) {
         constexpr int NBV = decltype(nb)::value;
         if (cols_on_device)
-            quotients_kernel<true, false, NBV><<<(unsigned)blocks, 256, 0, st>>>(*holder, cols, 0u);
+            quotients_kernel<true, true, NBV><<<(unsigned)blocks, 256, smem, st>>>(*holder, cols, n_samples);
         else
-            quotients_kernel<false, false, NBV><<<(unsigned)blocks, 256, 0, st>>>(*holder, nullptr, 0u);
+            quotients_kernel<false, true, NBV><<<(unsigned)blocks, 256, smem, st>>>(*holder, nullptr, n_samples);
     };
     switch (n_batches) {
     case 1: launch(std::integral_constant<int, 1>{}); break;

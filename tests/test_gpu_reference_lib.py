@@ -121,8 +121,9 @@ def test_folds_match_reference(stwo, R):
     d1 = stwo.LineEvaluation(line, stwo.SecureColumnByCoords.from_numpy(dst0))
     B.fold_circle_into_line(d1, stwo.SecureEvaluation(circle, stwo.SecureColumnByCoords.from_numpy(cols)), alpha, ctree)
     d2 = stwo.SecureColumnByCoords.from_numpy(dst0)
-    R.fold_circle_into_line(ctree.itwiddles.device_ptr, ctree.root_coset.size() - line.size(), n,
-                            stwo.SecureColumnByCoords.from_numpy(cols).ptrs(), reflib.QM31(*alpha), d2.ptrs())
+    src2 = stwo.SecureColumnByCoords.from_numpy(cols)  # kept alive until the reference call returns
+    R.fold_circle_into_line(ctree.itwiddles.device_ptr, ctree.root_coset.size() - line.size(), n, src2.ptrs(),
+                            reflib.QM31(*alpha), d2.ptrs())
     for a, b in zip(d1.values.to_numpy(), d2.to_numpy()):
         assert (a == b).all()
 
@@ -155,7 +156,8 @@ def test_accumulate_and_quotients_match_reference(stwo, R):
     a = stwo.SecureColumnByCoords.from_numpy(l0)
     B.accumulate(a, stwo.SecureColumnByCoords.from_numpy(r0))
     b = stwo.SecureColumnByCoords.from_numpy(l0)
-    R.accumulate(n, b.ptrs(), stwo.SecureColumnByCoords.from_numpy(r0).ptrs())
+    rb = stwo.SecureColumnByCoords.from_numpy(r0)  # kept alive until the reference call returns
+    R.accumulate(n, b.ptrs(), rb.ptrs())
     for x, y in zip(a.to_numpy(), b.to_numpy()):
         assert (x == y).all()
     # quotients: equal batch sizes (the reference mis-indexes line coefficients otherwise)
