@@ -107,7 +107,11 @@ def _mixed_jobs(n, seed):
     return jobs
 
 
-def test_server_proofs_equal_single_job_proofs():
+@pytest.mark.parametrize("priorities", ["1", "0"])
+def test_server_proofs_equal_single_job_proofs(priorities, monkeypatch):
+    """Every proof of a concurrent mix equals the same job proved alone, with per-job
+    stream priorities (the default) and without (STWO_SERVER_PRIORITY=0)."""
+    monkeypatch.setenv("STWO_SERVER_PRIORITY", priorities)
     stwo = load_package()
     jobs = _mixed_jobs(24, 3)
     alone = {}
