@@ -243,7 +243,13 @@ def kernel_suite(stwo, reps=5):
     nodes = (1 << (lg + 1)) - 1
     b = nc * (1 << lg) * 4 + nodes * 32 + ((1 << lg) - 1) * 64
     comp = (1 << lg) * (nc // 16) + ((1 << lg) - 1)
+    # The compression's own ALU-pipe bound: the xors and rotations of its 80 G functions
+    # (640 instructions) at 64 ALU lanes per SM per clock, at the maximum SM clock.
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    alu_bound = sms * 64 * 1965e6 / 640
     rec = {"ms": t, "gbs": b / t / 1e6, "frac_hbm": b / t / 1e6 / peak, "compressions_per_s": comp / (t / 1e3),
+           "alu_bound_compressions_per_s": alu_bound, "frac_alu_bound": comp / (t / 1e3) / alu_bound,
+           "alu_bound_basis": f"{sms} SMs x 64 ALU lanes x 1965 MHz / 640 ALU instructions per compression",
            "workload": "64 cols x 2^22, full tree"}
     if R is not None:
         dcols = R.copy_device_pointer_vec_from_host_to_device(cptr, nc)
