@@ -448,11 +448,12 @@ __device__ __forceinline__ void roundsT(uint32_t *sm, const GeoT &geo, std::inte
         ...);
 }
 
-// Three CTAs per SM (at most 80 registers a thread, 192 KB of shared memory): measured
-// 2292 vs 2231 columns/s at log 24 against two CTAs per SM with 112-128 registers, and
-// 2132 with four CTAs per SM (64 registers).
+// 2^6 elements a thread: three CTAs per SM (at most 80 registers a thread, 192 KB of
+// shared memory), measured 2292 vs 2231 columns/s at log 24 against two CTAs per SM
+// with 112-128 registers, and 2132 with four CTAs per SM (64 registers). 2^5 elements
+// a thread (512 threads): two CTAs per SM (64 registers; at three it spills).
 template <int G, int C, bool INV, int E>
-__global__ void __launch_bounds__(1 << (TT - E), 3) fftT_kernel(const __grid_constant__ FftLaunch p, uint32_t n_cols) {
+__global__ void __launch_bounds__(1 << (TT - E), E == 6 ? 3 : 2) fftT_kernel(const __grid_constant__ FftLaunch p, uint32_t n_cols) {
     extern __shared__ uint32_t sm[];
     GeoT geo;
     geo.p = &p;
