@@ -321,16 +321,21 @@ stwo_prover_server *stwo_server_create(uint32_t n_workers, uint64_t device_budge
  * the job is unsupported or can never fit the budget. */
 int stwo_server_submit(stwo_prover_server *server, uint64_t job_id, const stwo_wide_fib_job *job, const uint32_t *a0,
                        const uint32_t *a1);
-/* Moves up to max_results finished jobs into out and returns their number. Waits up to
- * timeout_ms for one (negative: until one finishes or nothing is queued or running). */
 /* Queues a job whose inputs are already in device memory; the caller keeps a0_dev and
  * a1_dev valid until the job's result has been polled. */
 int stwo_server_submit_device(stwo_prover_server *server, uint64_t job_id, const stwo_wide_fib_job *job,
                               const uint32_t *a0_dev, const uint32_t *a1_dev);
+/* Moves up to max_results finished jobs into out and returns their number. Waits up to
+ * timeout_ms for one (negative: until one finishes or nothing is queued or running). */
 uint32_t stwo_server_poll(stwo_prover_server *server, stwo_server_result *out, uint32_t max_results,
                           int32_t timeout_ms);
 void stwo_server_stats(stwo_prover_server *server, uint32_t *pending, uint32_t *running,
                        uint64_t *device_bytes_in_use);
+/* Same-shape reuse so far: proofs that ran on a worker's retained slab (a queued job
+ * with the shape of the worker's previous job takes its place at once), and of those
+ * the proofs that replayed the captured launch sequence as one CUDA graph (all but
+ * the first reuse of a slab). Off with STWO_SERVER_GRAPHS=0 at creation. */
+void stwo_server_graph_stats(stwo_prover_server *server, uint64_t *slab_reuses, uint64_t *graph_replays);
 double stwo_server_now_ms(void);
 /* Drops queued jobs, waits for running ones, frees everything (including unpolled proofs). */
 void stwo_server_destroy(stwo_prover_server *server);

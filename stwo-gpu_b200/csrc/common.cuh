@@ -20,9 +20,9 @@ void clear_error();
 // Counts of kernel launches made by the library: process-wide and per host thread.
 extern std::atomic<uint64_t> g_kernel_launches;
 extern thread_local uint64_t t_kernel_launches;
-inline void count_launch() {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    t_kernel_launches++;
+inline void count_launch(uint64_t n = 1) {
+    g_kernel_launches.fetch_add(n, std::memory_order_relaxed);
+    t_kernel_launches += n;
 }
 
 #define STWO_CUDA_TRY(expr)                                                               \
@@ -84,10 +84,13 @@ int reserve_pool(uint64_t bytes);
 // cudaMallocFromPoolAsync from the library pool (free with cudaFreeAsync).
 int pool_alloc(void **p, size_t bytes, cudaStream_t st);
 
-// Waits for all work on `st`. A thread that sets t_blocking_wait yields its CPU core
-// while it waits (a blocking-sync event) instead of spinning; the proof server's
-// workers do, so many in-flight jobs do not compete for host cores.
+// Waits for all work on `st`. A thread that sets t_blocking_wait first polls for up to
+// t_spin_us microseconds (a wake-up from a blocking wait costs a few hundred
+// microseconds, more than a small proof's remaining device work), then yields its CPU
+// core on a blocking-sync event; the proof server's workers do, so many in-flight large
+// jobs do not compete for host cores. Other threads spin (cudaStreamSynchronize).
 extern thread_local bool t_blocking_wait;
+extern thread_local uint32_t t_spin_us;
 int wait_stream(cudaStream_t st);
 
 // Pinned host memory of at least `bytes`, owned by the calling thread and reused by its

@@ -47,6 +47,7 @@
 #include "channel.cuh"
 #include "common.cuh"
 #include "fri.cuh"
+#include "prover.cuh"
 #include "quotients.cuh"
 
 namespace stwo {
@@ -471,10 +472,16 @@ struct Arena {
     uint64_t cap = 0, used = 0;
     std::vector<void *> extra;
     uint64_t bytes = 0;
+    bool retain = false;  // the slab belongs to a ProveCache: not freed here
     explicit Arena(cudaStream_t s) : st(s) {}
     ~Arena() {
-        if (slab) cudaFreeAsync(slab, st);
+        if (slab && !retain) cudaFreeAsync(slab, st);
         for (void *p : extra) cudaFreeAsync(p, st);
+    }
+    void adopt(uint8_t *s, uint64_t c) {
+        slab = s;
+        cap = c;
+        retain = true;
     }
     int reserve(uint64_t b) {
         void *p = nullptr;
@@ -753,19 +760,46 @@ struct PhaseEvents {
 };
 thread_local PhaseEvents t_phase;
 
+}  // namespace
+
+void prove_cache_release(ProveCache *c, cudaStream_t st) {
+    if (!c) return;
+    if (c->exec) cudaGraphExecDestroy(c->exec);
+    if (c->slab) cudaFreeAsync(c->slab, st);
+    *c = ProveCache{};
+}
+
+namespace {
+
 int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const uint32_t *tw_in,
                const uint32_t *itw_in, uint64_t tsz_in, std::vector<uint8_t> &proof, cudaStream_t st,
-               stwo_prove_stats *stats) {
+               stwo_prove_stats *stats, ProveCache *cache) {
     PV_TRY(validate(j));
     const uint32_t L = j.L, N = j.N, B = j.B, E = L + 1, D = E + B;
     const uint64_t rows = 1ull << L;
     const double t0 = now_ms();
     const uint64_t launches0 = t_kernel_launches;
-    if (stats) PV_TRY(t_phase.ensure());
+    // A cache (a server worker's) keeps the job's slab after the proof, so that the next
+    // proof of the same shape finds every buffer, table and parameter block at the same
+    // address: its launch sequence is captured as a CUDA graph on that second proof
+    // and replayed from the third on. Only for jobs with a caller's twiddle tree and
+    // log_n_rows >= 3 (a 4-point transform reads a twiddle back to the host).
+    int dev = 0;
+    STWO_CUDA_TRY(cudaGetDevice(&dev));
+    const bool cacheable = cache && tw_in && itw_in && L >= 3;
+    const uint32_t key[5] = {j.L, j.N, j.B, j.n_queries, j.pow_bits};
+    const bool hit = cacheable && cache->valid && cache->device == dev && cache->tw == tw_in &&
+                     cache->itw == itw_in && cache->tsz == tsz_in && memcmp(cache->key, key, sizeof(key)) == 0;
+    if (cache && cache->valid && !hit) prove_cache_release(cache, st);
+    // Phase events are recorded whenever the launch sequence may be captured, so that a
+    // graph always carries them.
+    const bool timing = stats || cacheable;
+    if (timing) PV_TRY(t_phase.ensure());
     cudaEvent_t *ev = t_phase.ev;
     Arena ar(st);
-    PV_TRY(ar.reserve(job_device_bytes(j, !(tw_in || itw_in))));
-    if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[0], st));
+    if (hit) ar.adopt(cache->slab, cache->cap);
+    else PV_TRY(ar.reserve(job_device_bytes(j, !(tw_in || itw_in))));
+    if (timing) STWO_CUDA_TRY(cudaEventRecord(ev[0], st));
 
     // ---- buffers (all of the job's device memory, before the first launch)
     const uint32_t *tw = tw_in, *itw = itw_in;
@@ -923,10 +957,20 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         STWO_CUDA_TRY(cudaMemcpyAsync(dev_img, stage, up.host.size(), cudaMemcpyHostToDevice, st));
     }
 
-    // ---- 1. trace: twiddles, generation, interpolation, evaluation, tree
-    if (own_tw) PV_TRY(stwo_precompute_twiddles(half_coset_init(D), half_coset_step(D), L + B, own_tw, own_itw, st));
     STWO_CUDA_TRY(cudaMemcpyAsync(a0, a0_in, rows * 4, cudaMemcpyDefault, st));
     STWO_CUDA_TRY(cudaMemcpyAsync(a1, a1_in, rows * 4, cudaMemcpyDefault, st));
+
+    // The launch sequence from the trace to the query words: device work only, no host
+    // wait, every address inside the slab or the caller's twiddle tree.
+    auto record = [&](int k, bool capturing) -> int {
+        if (!timing) return STWO_OK;
+        STWO_CUDA_TRY(capturing ? cudaEventRecordWithFlags(ev[k], st, cudaEventRecordExternal)
+                                : cudaEventRecord(ev[k], st));
+        return STWO_OK;
+    };
+    auto launch_all = [&](bool capturing) -> int {
+    // ---- 1. trace: twiddles, generation, interpolation, evaluation, tree
+    if (own_tw) PV_TRY(stwo_precompute_twiddles(half_coset_init(D), half_coset_step(D), L + B, own_tw, own_itw, st));
     {
         const uint32_t threads = rows < (uint64_t)device_sm_count() * 256 ? 64 : 256;
         const uint64_t blocks = std::min<uint64_t>((rows + threads - 1) / threads, (uint64_t)device_sm_count() * 16);
@@ -946,7 +990,7 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     PV_TRY(commit(t_trace));
     fs_trace_kernel<<<1, 32, 0, st>>>(dstate, t_trace.layers[0], powers, N - 2);
     STWO_LAUNCH_CHECK("fs_trace_kernel");
-    if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[1], st));
+    PV_TRY(record(1, capturing));
 
     // ---- 2. composition on CanonicCoset(L + 1), committed on CanonicCoset(L + 1 + B)
     if (B > 1) {
@@ -965,14 +1009,14 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     PV_TRY(commit(t_comp));
     fs_comp_kernel<<<1, 1, 0, st>>>(dstate, t_comp.layers[0]);
     STWO_LAUNCH_CHECK("fs_comp_kernel");
-    if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[2], st));
+    PV_TRY(record(2, capturing));
 
     // ---- 3. out-of-domain sampling
     PV_TRY(eval_at_points_dev_async(dev_at(off_eap), eap_n, eap_total, dstate->oods, dsampled, eap_partials, dtickets,
                                     st));
     fs_oods_kernel<<<1, 256, 0, st>>>(dstate, dsampled, powers, N, L, dqc, dqt);
     STWO_LAUNCH_CHECK("fs_oods_kernel");
-    if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[3], st));
+    PV_TRY(record(3, capturing));
 
     // ---- 4. DEEP quotients (largest columns first) and the FRI commitment
     PV_TRY(quotients_dev_async(dqc, D, 4, st));
@@ -1002,7 +1046,7 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
                           &dstate->alphas[li + 1]));
     }
     PV_TRY(launch_fri_tail(dstate, reinterpret_cast<const TailParams *>(dev_at(off_tail)), st));
-    if (stats) STWO_CUDA_TRY(cudaEventRecord(ev[4], st));
+    PV_TRY(record(4, capturing));
 
     // ---- 5. proof of work and query words, then the channel's record to the host
     {
@@ -1014,6 +1058,40 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         STWO_LAUNCH_CHECK("grind_kernel");
         fs_finish_kernel<<<1, 1, 0, st>>>(dstate, j.n_queries);
         STWO_LAUNCH_CHECK("fs_finish_kernel");
+    }
+    return STWO_OK;
+    };
+
+    const bool cache_ok = cacheable && ar.extra.empty();
+    if (cache_ok && hit && cache->exec) {
+        STWO_CUDA_TRY(cudaGraphLaunch(cache->exec, st));
+        count_launch(cache->launches);
+        cache->replays++;
+    } else if (cache_ok && hit && !cache->no_graph) {
+        const uint64_t l0 = t_kernel_launches;
+        STWO_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int rc_cap = launch_all(true);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+        cudaGraphExec_t exec = nullptr;
+        cudaError_t ei = cudaSuccess;
+        if (rc_cap == STWO_OK && ec == cudaSuccess) ei = cudaGraphInstantiate(&exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (rc_cap == STWO_OK && ec == cudaSuccess && ei == cudaSuccess) {
+            cache->exec = exec;
+            cache->launches = t_kernel_launches - l0;  // counted at capture, run now
+            STWO_CUDA_TRY(cudaGraphLaunch(exec, st));
+        } else {
+            // The sequence did not capture: run it directly, now and for this shape.
+            cudaGetLastError();
+            clear_error();
+            cache->no_graph = true;
+            g_kernel_launches.fetch_sub(t_kernel_launches - l0, std::memory_order_relaxed);  // nothing ran
+            t_kernel_launches = l0;
+            PV_TRY(launch_all(false));
+        }
+    } else {
+        PV_TRY(launch_all(false));
     }
     const size_t rec_bytes = sizeof(ProofState) + sizeof(qm31) * eap_n;
     std::vector<uint8_t> rec(rec_bytes);
@@ -1121,6 +1199,21 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     proof = std::move(w.b);
     const double t5 = now_ms();
 
+    if (cacheable) {
+        if (cache_ok && !hit) {
+            cache->valid = true;
+            memcpy(cache->key, key, sizeof(key));
+            cache->tw = tw_in;
+            cache->itw = itw_in;
+            cache->tsz = tsz_in;
+            cache->device = dev;
+            cache->slab = ar.slab;
+            cache->cap = ar.cap;
+            ar.retain = true;
+        } else if (!cache_ok && hit) {
+            prove_cache_release(cache, st);  // the slab it holds was adopted: freed once, here
+        }
+    }
     if (stats) {
         float ms[4];
         for (int p = 0; p < 4; p++) STWO_CUDA_TRY(cudaEventElapsedTime(&ms[p], ev[p], ev[p + 1]));
@@ -1142,10 +1235,10 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
 // Shared with the batch server.
 int wide_fib_prove(const stwo_wide_fib_job *job, const uint32_t *a0, const uint32_t *a1, const uint32_t *tw,
                    const uint32_t *itw, uint64_t tree_size, std::vector<uint8_t> &proof, stwo_prove_stats *stats,
-                   cudaStream_t st) {
+                   cudaStream_t st, ProveCache *cache) {
     STWO_REQUIRE(job && a0 && a1, STWO_ERR_INVALID_ARGUMENT, "null argument");
     Job j{job->log_n_rows, job->n_columns, job->log_blowup, job->n_queries, job->pow_bits};
-    int rc = prove_impl(j, a0, a1, tw, itw, tree_size, proof, st, stats);
+    int rc = prove_impl(j, a0, a1, tw, itw, tree_size, proof, st, stats, cache);
     if (rc) cudaStreamSynchronize(st);  // the arena's frees are queued; leave the stream idle
     return rc;
 }

@@ -4,6 +4,7 @@
 // print CUDA failures and carry on. Here every failure is recorded per thread and
 // returned as a status by the native API; the reference-compatible entry points keep
 // their void / pointer signatures and return NULL on failure.
+#include <chrono>
 #include <cstdarg>
 #include <mutex>
 
@@ -80,6 +81,7 @@ int host_stage(size_t bytes, void **out) {
 }
 
 thread_local bool t_blocking_wait = false;
+thread_local uint32_t t_spin_us = 0;
 
 int library_pool(cudaMemPool_t *pool) {
     int dev = 0;
@@ -153,6 +155,15 @@ int wait_stream(cudaStream_t st) {
         t_event.device = dev;
     }
     STWO_CUDA_TRY(cudaEventRecord(t_event.ev, st));
+    if (t_spin_us) {
+        const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(t_spin_us);
+        for (;;) {
+            const cudaError_t q = cudaEventQuery(t_event.ev);
+            if (q == cudaSuccess) return STWO_OK;
+            if (q != cudaErrorNotReady) STWO_CUDA_TRY(q);
+            if (std::chrono::steady_clock::now() >= until) break;
+        }
+    }
     STWO_CUDA_TRY(cudaEventSynchronize(t_event.ev));
     return STWO_OK;
 }

@@ -11,6 +11,7 @@
 // the largest domain the server accepts. A job's proof bytes do not depend on what
 // else is running: each job's arithmetic is confined to its own buffers and stream.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstdlib>
@@ -21,13 +22,9 @@
 #include <vector>
 
 #include "common.cuh"
+#include "prover.cuh"
 
 namespace stwo {
-
-int wide_fib_prove(const stwo_wide_fib_job *job, const uint32_t *a0, const uint32_t *a1, const uint32_t *tw,
-                   const uint32_t *itw, uint64_t tree_size, std::vector<uint8_t> &proof, stwo_prove_stats *stats,
-                   cudaStream_t st);
-uint64_t wide_fib_job_device_bytes(const stwo_wide_fib_job *job, bool own_twiddles);
 
 namespace {
 
@@ -56,8 +53,11 @@ struct stwo_prover_server {
     uint32_t *tw = nullptr, *itw = nullptr;
     uint64_t tree_size = 0;
     bool stopping = false;
-    bool blocking_wait = true;  // workers yield their core while waiting on the device
+    bool blocking_wait = true;  // workers yield their core while waiting on the device...
+    uint32_t spin_us = 2000;    // ...after polling this long
     bool use_priorities = true; // per-job stream priority by job size
+    bool use_graphs = true;     // same-shape jobs reuse a worker's slab and proof graph
+    std::atomic<uint64_t> slab_reuses{0}, graph_replays{0};
     uint32_t running = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -82,6 +82,11 @@ struct stwo_prover_server {
     // kernel chains of small jobs take free SM slots ahead of the queued CTAs of large
     // transforms instead of waiting behind them. Class 0 (the highest) holds jobs of up
     // to 2^16 trace cells; each further class doubles the bound twice.
+    static bool same_shape(const stwo_wide_fib_job &a, const stwo_wide_fib_job &b) {
+        return a.log_n_rows == b.log_n_rows && a.n_columns == b.n_columns && a.log_blowup == b.log_blowup &&
+               a.n_queries == b.n_queries && a.pow_bits == b.pow_bits;
+    }
+
     static uint32_t priority_class(const stwo_wide_fib_job &j, uint32_t n_classes) {
         uint32_t ln = 0;
         while ((1u << ln) < j.n_columns) ln++;
@@ -93,6 +98,7 @@ struct stwo_prover_server {
     void worker() {
         cudaSetDevice(device);
         t_blocking_wait = blocking_wait;
+        t_spin_us = spin_us;
         // One stream per priority level, greatest priority first.
         int least = 0, greatest = 0;
         cudaDeviceGetStreamPriorityRange(&least, &greatest);
@@ -104,15 +110,22 @@ struct stwo_prover_server {
             se = cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, pr);
             if (se == cudaSuccess) streams.push_back(s);
         }
+        // The slab of this worker's last proof, kept while the next job it takes has the
+        // same shape: that job reuses every buffer at the same address and, from the
+        // second reuse on, replays the proof's launch sequence as one CUDA graph.
+        ProveCache cache;
+        cudaStream_t cache_st = nullptr;
+        PendingJob j;
+        bool have_next = false;
         for (;;) {
-            PendingJob j;
-            bool got = false;
-            {
+            if (!have_next) {
+                bool got = false;
                 std::unique_lock<std::mutex> lock(mu);
                 cv_work.wait(lock, [&] { return stopping || (!pending.empty() && (got = take(j))); });
                 if (!got) break;  // stopping, nothing taken
                 running++;
             }
+            have_next = false;
             stwo_server_result r{};
             r.job_id = j.id;
             r.submit_ms = j.submit_ms;
@@ -124,7 +137,15 @@ struct stwo_prover_server {
                 clear_error();
                 const uint32_t *a0 = j.a0_dev ? j.a0_dev : j.a0.data(), *a1 = j.a1_dev ? j.a1_dev : j.a1.data();
                 cudaStream_t st = streams[priority_class(j.job, (uint32_t)streams.size())];
-                r.status = wide_fib_prove(&j.job, a0, a1, tw, itw, tree_size, proof, &r.stats, st);
+                const bool reuse = cache.valid;  // set only while this job has the cached shape
+                const uint64_t replays0 = cache.replays;
+                r.status = wide_fib_prove(&j.job, a0, a1, tw, itw, tree_size, proof, &r.stats, st,
+                                          use_graphs ? &cache : nullptr);
+                cache_st = st;
+                if (reuse && r.status == STWO_OK) {
+                    slab_reuses++;
+                    if (cache.replays > replays0) graph_replays++;
+                }
             }
             if (r.status == STWO_OK) {
                 r.proof = static_cast<uint8_t *>(malloc(proof.size()));
@@ -138,15 +159,35 @@ struct stwo_prover_server {
                 strncpy(r.error, stwo_last_error(), sizeof(r.error) - 1);
             }
             r.done_ms = steady_ms();
+            // A queued job of the same shape takes this one's place (and budget) at once.
+            PendingJob next;
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                done.push_back(r);
+                if (cache.valid && !stopping)
+                    for (auto it = pending.begin(); it != pending.end(); ++it)
+                        if (same_shape(it->job, j.job) && it->bytes == j.bytes) {
+                            next = std::move(*it);
+                            pending.erase(it);
+                            have_next = true;
+                            break;
+                        }
+            }
+            cv_done.notify_all();
+            if (have_next) {
+                j = std::move(next);
+                continue;
+            }
+            // Free the retained slab before its bytes go back to the budget.
+            if (cache.valid) prove_cache_release(&cache, cache_st);
             {
                 std::lock_guard<std::mutex> lock(mu);
                 in_use -= j.bytes;
                 running--;
-                done.push_back(r);
             }
             cv_work.notify_all();  // freed budget may admit waiting jobs
-            cv_done.notify_all();
         }
+        if (cache.valid) prove_cache_release(&cache, cache_st);
         for (cudaStream_t s : streams) cudaStreamDestroy(s);
     }
 };
@@ -169,7 +210,9 @@ stwo_prover_server *stwo_server_create(uint32_t n_workers, uint64_t device_budge
     }
     s->budget = device_budget_bytes;
     if (const char *w = getenv("STWO_SERVER_WAIT")) s->blocking_wait = strcmp(w, "spin") != 0;
+    if (const char *w = getenv("STWO_SERVER_SPIN_US")) s->spin_us = (uint32_t)strtoul(w, nullptr, 10);
     if (const char *w = getenv("STWO_SERVER_PRIORITY")) s->use_priorities = strcmp(w, "0") != 0;
+    if (const char *w = getenv("STWO_SERVER_GRAPHS")) s->use_graphs = strcmp(w, "0") != 0;
     s->max_domain_log = max_domain_log;
     // One twiddle tree for CanonicCoset(max_domain_log).half_coset serves every smaller
     // canonic domain: its doublings are the smaller domains' half cosets.
@@ -266,6 +309,12 @@ void stwo_server_stats(stwo_prover_server *s, uint32_t *pending, uint32_t *runni
     if (pending) *pending = (uint32_t)s->pending.size();
     if (running) *running = s->running;
     if (device_bytes_in_use) *device_bytes_in_use = s->in_use;
+}
+
+void stwo_server_graph_stats(stwo_prover_server *s, uint64_t *slab_reuses, uint64_t *graph_replays) {
+    if (!s) return;
+    if (slab_reuses) *slab_reuses = s->slab_reuses.load();
+    if (graph_replays) *graph_replays = s->graph_replays.load();
 }
 
 void stwo_server_destroy(stwo_prover_server *s) {

@@ -133,6 +133,13 @@ class ProofServer:
         L.lib().stwo_server_stats(self._s, C.byref(p), C.byref(r), C.byref(b))
         return {"pending": p.value, "running": r.value, "device_bytes_in_use": b.value}
 
+    def graph_stats(self):
+        """Proofs that reused a worker's retained slab, and those that replayed the
+        proof's CUDA graph (same-shape jobs in a row on one worker)."""
+        a, b = C.c_uint64(), C.c_uint64()
+        L.lib().stwo_server_graph_stats(self._s, C.byref(a), C.byref(b))
+        return {"slab_reuses": a.value, "graph_replays": b.value}
+
     @staticmethod
     def now_ms():
         return L.lib().stwo_server_now_ms()

@@ -134,6 +134,48 @@ def test_server_proofs_equal_single_job_proofs(priorities, monkeypatch):
         assert r["submit_ms"] <= r["start_ms"] <= r["done_ms"]
 
 
+@pytest.mark.parametrize("graphs", ["1", "0"])
+@pytest.mark.parametrize("workers", [1, 3])
+def test_server_same_shape_runs_replay_equal_proofs(graphs, workers, monkeypatch):
+    """Runs of same-shape jobs: a worker keeps its slab for the next job of the same
+    shape, captures the proof's launch sequence as a CUDA graph on the second and
+    replays it from the third. Every proof (each job with its own inputs) equals the
+    same job proved alone; STWO_SERVER_GRAPHS=0 turns the reuse off."""
+    monkeypatch.setenv("STWO_SERVER_GRAPHS", graphs)
+    stwo = load_package()
+    shapes = [(9, 24, 1, 3, 5), (11, 16, 2, 4, 3), (3, 5, 1, 2, 1), (2, 3, 1, 1, 0)]
+    jobs = []
+    for k in range(28):
+        t = shapes[0] if k < 10 else shapes[1] if k < 19 else shapes[2] if k < 25 else shapes[3]
+        jobs.append((k, t, 700 + k))
+    alone = {}
+    for jid, t, seed in jobs:
+        a0, a1 = stwo.wide_fib_inputs(t[0], seed)
+        alone[jid] = stwo.prove_wide_fib(job_of(t), a0, a1)[0]
+    with stwo.ProofServer(n_workers=workers, device_budget_bytes=8 << 30, max_domain_log=16) as srv:
+        for jid, t, seed in jobs:
+            a0, a1 = stwo.wide_fib_inputs(t[0], seed)
+            srv.submit(jid, job_of(t), a0, a1)
+        got = {}
+        while len(got) < len(jobs):
+            for r in srv.poll(timeout_ms=-1):
+                assert r["status"] == 0, r["error"]
+                got[r["job_id"]] = r
+        assert srv.stats()["running"] == 0 and srv.stats()["device_bytes_in_use"] == 0
+        gs = srv.graph_stats()
+    for jid, t, _ in jobs:
+        assert got[jid]["proof"] == alone[jid], (jid, t)
+        assert got[jid]["stats"]["kernel_launches"] > 0
+    if graphs == "0":
+        assert gs == {"slab_reuses": 0, "graph_replays": 0}
+    elif workers == 1:
+        # runs of 10, 9 and 6 jobs of cacheable shapes (log_n_rows >= 3): every job but a
+        # run's first reuses the slab; every job but a run's first two replays the graph
+        assert gs == {"slab_reuses": 9 + 8 + 5, "graph_replays": 8 + 7 + 4}
+    else:
+        assert gs["slab_reuses"] > 0 and gs["graph_replays"] > 0
+
+
 def test_server_respects_the_memory_budget():
     stwo = load_package()
     t = (10, 32, 1, 3, 5)
