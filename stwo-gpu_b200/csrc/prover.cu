@@ -969,97 +969,100 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         return STWO_OK;
     };
     auto launch_all = [&](bool capturing) -> int {
-    // ---- 1. trace: twiddles, generation, interpolation, evaluation, tree
-    if (own_tw) PV_TRY(stwo_precompute_twiddles(half_coset_init(D), half_coset_step(D), L + B, own_tw, own_itw, st));
-    {
-        const uint32_t threads = rows < (uint64_t)device_sm_count() * 256 ? 64 : 256;
-        const uint64_t blocks = std::min<uint64_t>((rows + threads - 1) / threads, (uint64_t)device_sm_count() * 16);
-        wide_fib_trace_kernel<<<(unsigned)blocks, threads, 0, st>>>(
-            a0, a1, reinterpret_cast<uint32_t *const *>(dev_at(off_tpoly)), N, rows);
-        STWO_LAUNCH_CHECK("wide_fib_trace_kernel");
-    }
-    // The trace columns are interpolated in place: they become the coefficient columns.
-    PV_TRY(fft_columns(tpoly.data(), tpoly.data(), N, L, L, itw, tsz, true, st));
-    {
-        std::vector<const uint32_t *> src(tpoly.begin(), tpoly.end());
-        PV_TRY(fft_columns(src.data(), tev.data(), N, L + B, L, tw, tsz, false, st));
-    }
-    auto commit = [&](MerkleTree &t) {
-        return merkle_tree_dev_async(t.max_log, t.level_tables.data(), t.level_n.data(), t.layers.data(), st);
-    };
-    PV_TRY(commit(t_trace));
-    fs_trace_kernel<<<1, 32, 0, st>>>(dstate, t_trace.layers[0], powers, N - 2);
-    STWO_LAUNCH_CHECK("fs_trace_kernel");
-    PV_TRY(record(1, capturing));
-
-    // ---- 2. composition on CanonicCoset(L + 1), committed on CanonicCoset(L + 1 + B)
-    if (B > 1) {
-        std::vector<const uint32_t *> src(tpoly.begin(), tpoly.end());
-        PV_TRY(fft_columns(src.data(), text.data(), N, E, L, tw, tsz, false, st));
-    }
-    uint32_t den_half[2];
-    vanishing_inverses(L, den_half);
-    PV_TRY(wide_fib_dev_async(reinterpret_cast<const uint32_t *const *>(dev_at(off_text)), N, E,
-                              reinterpret_cast<const uint32_t *>(powers), den_half, comp.data(), st));
-    PV_TRY(fft_columns(comp.data(), comp.data(), 4, E, E, itw, tsz, true, st));  // in place -> coefficients
-    {
-        std::vector<const uint32_t *> src(comp.begin(), comp.end());
-        PV_TRY(fft_columns(src.data(), cev.data(), 4, D, E, tw, tsz, false, st));
-    }
-    PV_TRY(commit(t_comp));
-    fs_comp_kernel<<<1, 1, 0, st>>>(dstate, t_comp.layers[0]);
-    STWO_LAUNCH_CHECK("fs_comp_kernel");
-    PV_TRY(record(2, capturing));
-
-    // ---- 3. out-of-domain sampling
-    PV_TRY(eval_at_points_dev_async(dev_at(off_eap), eap_n, eap_total, dstate->oods, dsampled, eap_partials, dtickets,
-                                    st));
-    fs_oods_kernel<<<1, 256, 0, st>>>(dstate, dsampled, powers, N, L, dqc, dqt);
-    STWO_LAUNCH_CHECK("fs_oods_kernel");
-    PV_TRY(record(3, capturing));
-
-    // ---- 4. DEEP quotients (largest columns first) and the FRI commitment
-    PV_TRY(quotients_dev_async(dqc, D, 4, st));
-    PV_TRY(quotients_dev_async(dqt, L + B, N, st));
-    PV_TRY(commit(t_fri0));
-    fs_layer_kernel<<<1, 1, 0, st>>>(dstate, t_fri0.layers[0], 2, 0);
-    STWO_LAUNCH_CHECK("fs_layer_kernel");
-    for (int k = 0; k < 4; k++) STWO_CUDA_TRY(cudaMemsetAsync(lay[0][k], 0, 4ull << (D - 1), st));
-    {
-        std::vector<const uint32_t *> s(qc.begin(), qc.end());
-        PV_TRY(fold_async(s.data(), 1ull << D, stwo_qm31{}, itw, tsz - (1ull << (D - 1)), lay[0].data(), true, st,
-                          &dstate->alphas[0]));
-    }
-    for (uint32_t li = 0; li < li0; li++) {
-        const uint32_t lg = D - 1 - li;
-        if (li == li_circle) {
-            // The trace quotient folds into this layer with the previous layer's alpha.
-            std::vector<const uint32_t *> s(qt.begin(), qt.end());
-            PV_TRY(fold_async(s.data(), 1ull << (L + B), stwo_qm31{}, itw, tsz - (1ull << lg), lay[li].data(), true, st,
-                              &dstate->alphas[li]));
+        // ---- 1. trace: twiddles, generation, interpolation, evaluation, tree
+        if (own_tw)
+            PV_TRY(stwo_precompute_twiddles(half_coset_init(D), half_coset_step(D), L + B, own_tw, own_itw, st));
+        {
+            const uint32_t threads = rows < (uint64_t)device_sm_count() * 256 ? 64 : 256;
+            const uint64_t blocks =
+                std::min<uint64_t>((rows + threads - 1) / threads, (uint64_t)device_sm_count() * 16);
+            wide_fib_trace_kernel<<<(unsigned)blocks, threads, 0, st>>>(
+                a0, a1, reinterpret_cast<uint32_t *const *>(dev_at(off_tpoly)), N, rows);
+            STWO_LAUNCH_CHECK("wide_fib_trace_kernel");
         }
-        PV_TRY(commit(t_lay[li]));
-        fs_layer_kernel<<<1, 1, 0, st>>>(dstate, t_lay[li].layers[0], 3 + li, li + 1);
-        STWO_LAUNCH_CHECK("fs_layer_kernel");
-        std::vector<const uint32_t *> s(lay[li].begin(), lay[li].end());
-        PV_TRY(fold_async(s.data(), 1ull << lg, stwo_qm31{}, itw, tsz - (1ull << lg), lay[li + 1].data(), false, st,
-                          &dstate->alphas[li + 1]));
-    }
-    PV_TRY(launch_fri_tail(dstate, reinterpret_cast<const TailParams *>(dev_at(off_tail)), st));
-    PV_TRY(record(4, capturing));
+        // The trace columns are interpolated in place: they become the coefficient columns.
+        PV_TRY(fft_columns(tpoly.data(), tpoly.data(), N, L, L, itw, tsz, true, st));
+        {
+            std::vector<const uint32_t *> src(tpoly.begin(), tpoly.end());
+            PV_TRY(fft_columns(src.data(), tev.data(), N, L + B, L, tw, tsz, false, st));
+        }
+        auto commit = [&](MerkleTree &t) {
+            return merkle_tree_dev_async(t.max_log, t.level_tables.data(), t.level_n.data(), t.layers.data(), st);
+        };
+        PV_TRY(commit(t_trace));
+        fs_trace_kernel<<<1, 32, 0, st>>>(dstate, t_trace.layers[0], powers, N - 2);
+        STWO_LAUNCH_CHECK("fs_trace_kernel");
+        PV_TRY(record(1, capturing));
 
-    // ---- 5. proof of work and query words, then the channel's record to the host
-    {
-        const uint64_t want = 1ull << std::min<uint32_t>(j.pow_bits + 2, 24);  // a few times the expected tries
-        const uint64_t threads = std::max<uint64_t>(256, std::min<uint64_t>(want, (uint64_t)device_sm_count() * 1024));
-        const uint64_t blocks = (threads + 255) / 256, grid = blocks * 256;
-        const uint64_t max_k = ((1ull << (j.pow_bits + 6)) + grid - 1) / grid + 1;  // gives up after 2^(pow_bits+6)
-        grind_kernel<<<(unsigned)blocks, 256, 0, st>>>(dstate, j.pow_bits, max_k);
-        STWO_LAUNCH_CHECK("grind_kernel");
-        fs_finish_kernel<<<1, 1, 0, st>>>(dstate, j.n_queries);
-        STWO_LAUNCH_CHECK("fs_finish_kernel");
-    }
-    return STWO_OK;
+        // ---- 2. composition on CanonicCoset(L + 1), committed on CanonicCoset(L + 1 + B)
+        if (B > 1) {
+            std::vector<const uint32_t *> src(tpoly.begin(), tpoly.end());
+            PV_TRY(fft_columns(src.data(), text.data(), N, E, L, tw, tsz, false, st));
+        }
+        uint32_t den_half[2];
+        vanishing_inverses(L, den_half);
+        PV_TRY(wide_fib_dev_async(reinterpret_cast<const uint32_t *const *>(dev_at(off_text)), N, E,
+                                  reinterpret_cast<const uint32_t *>(powers), den_half, comp.data(), st));
+        PV_TRY(fft_columns(comp.data(), comp.data(), 4, E, E, itw, tsz, true, st));  // in place -> coefficients
+        {
+            std::vector<const uint32_t *> src(comp.begin(), comp.end());
+            PV_TRY(fft_columns(src.data(), cev.data(), 4, D, E, tw, tsz, false, st));
+        }
+        PV_TRY(commit(t_comp));
+        fs_comp_kernel<<<1, 1, 0, st>>>(dstate, t_comp.layers[0]);
+        STWO_LAUNCH_CHECK("fs_comp_kernel");
+        PV_TRY(record(2, capturing));
+
+        // ---- 3. out-of-domain sampling
+        PV_TRY(eval_at_points_dev_async(dev_at(off_eap), eap_n, eap_total, dstate->oods, dsampled, eap_partials,
+                                        dtickets, st));
+        fs_oods_kernel<<<1, 256, 0, st>>>(dstate, dsampled, powers, N, L, dqc, dqt);
+        STWO_LAUNCH_CHECK("fs_oods_kernel");
+        PV_TRY(record(3, capturing));
+
+        // ---- 4. DEEP quotients (largest columns first) and the FRI commitment
+        PV_TRY(quotients_dev_async(dqc, D, 4, st));
+        PV_TRY(quotients_dev_async(dqt, L + B, N, st));
+        PV_TRY(commit(t_fri0));
+        fs_layer_kernel<<<1, 1, 0, st>>>(dstate, t_fri0.layers[0], 2, 0);
+        STWO_LAUNCH_CHECK("fs_layer_kernel");
+        for (int k = 0; k < 4; k++) STWO_CUDA_TRY(cudaMemsetAsync(lay[0][k], 0, 4ull << (D - 1), st));
+        {
+            std::vector<const uint32_t *> s(qc.begin(), qc.end());
+            PV_TRY(fold_async(s.data(), 1ull << D, stwo_qm31{}, itw, tsz - (1ull << (D - 1)), lay[0].data(), true, st,
+                              &dstate->alphas[0]));
+        }
+        for (uint32_t li = 0; li < li0; li++) {
+            const uint32_t lg = D - 1 - li;
+            if (li == li_circle) {
+                // The trace quotient folds into this layer with the previous layer's alpha.
+                std::vector<const uint32_t *> s(qt.begin(), qt.end());
+                PV_TRY(fold_async(s.data(), 1ull << (L + B), stwo_qm31{}, itw, tsz - (1ull << lg), lay[li].data(), true,
+                                  st, &dstate->alphas[li]));
+            }
+            PV_TRY(commit(t_lay[li]));
+            fs_layer_kernel<<<1, 1, 0, st>>>(dstate, t_lay[li].layers[0], 3 + li, li + 1);
+            STWO_LAUNCH_CHECK("fs_layer_kernel");
+            std::vector<const uint32_t *> s(lay[li].begin(), lay[li].end());
+            PV_TRY(fold_async(s.data(), 1ull << lg, stwo_qm31{}, itw, tsz - (1ull << lg), lay[li + 1].data(), false, st,
+                              &dstate->alphas[li + 1]));
+        }
+        PV_TRY(launch_fri_tail(dstate, reinterpret_cast<const TailParams *>(dev_at(off_tail)), st));
+        PV_TRY(record(4, capturing));
+
+        // ---- 5. proof of work and query words, then the channel's record to the host
+        {
+            const uint64_t want = 1ull << std::min<uint32_t>(j.pow_bits + 2, 24);  // a few times the expected tries
+            const uint64_t threads =
+                std::max<uint64_t>(256, std::min<uint64_t>(want, (uint64_t)device_sm_count() * 1024));
+            const uint64_t blocks = (threads + 255) / 256, grid = blocks * 256;
+            const uint64_t max_k = ((1ull << (j.pow_bits + 6)) + grid - 1) / grid + 1;  // gives up after 2^(pow_bits+6)
+            grind_kernel<<<(unsigned)blocks, 256, 0, st>>>(dstate, j.pow_bits, max_k);
+            STWO_LAUNCH_CHECK("grind_kernel");
+            fs_finish_kernel<<<1, 1, 0, st>>>(dstate, j.n_queries);
+            STWO_LAUNCH_CHECK("fs_finish_kernel");
+        }
+        return STWO_OK;
     };
 
     const bool cache_ok = cacheable && ar.extra.empty();
