@@ -903,7 +903,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--jobs", type=int, default=48, help="jobs per step")
     ap.add_argument("--workers", type=int, default=8, help="proof server jobs in flight")
-    ap.add_argument("--latency-jobs", type=int, default=200, help="jobs per Poisson load level")
+    ap.add_argument("--latency-jobs", type=int, default=2000, help="jobs per Poisson load level")
     ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds of oracle work per CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-suite", action="store_true", help="skip the config-1 per-kernel sweep")
