@@ -300,6 +300,25 @@ int stwo_wide_fib_prove(const stwo_wide_fib_job *job, const uint32_t *a0, const 
                         uint64_t *proof_len, stwo_prove_stats *stats, void *stream);
 void stwo_free_proof(uint8_t *proof);
 
+/* Repeated proofs of one job shape (no counterpart in the reference). A cache keeps
+ * the device memory of its last proof; the next stwo_wide_fib_prove_cached call with
+ * the same shape, twiddle tree and device reuses it, every buffer at the same address,
+ * so the proof's launch sequence (trace to query words) is captured as a CUDA graph on
+ * that second call and replayed with one launch from the third on. A call with a
+ * different shape frees the memory first. Needs the caller's twiddle tree; jobs with
+ * log_n_rows < 3 are proved without reuse, and on the legacy default stream (NULL) the
+ * memory is reused but no graph is captured. A cache serves one thread and one stream
+ * at a time; it holds up to stwo_wide_fib_prove_device_bytes(job, 0) bytes between
+ * calls (stwo_prove_cache_stats). destroy frees them, stream-ordered on `stream`. */
+typedef struct stwo_prove_cache stwo_prove_cache;
+stwo_prove_cache *stwo_prove_cache_create(void);
+int stwo_wide_fib_prove_cached(stwo_prove_cache *cache, const stwo_wide_fib_job *job, const uint32_t *a0,
+                               const uint32_t *a1, const uint32_t *twiddles, const uint32_t *itwiddles,
+                               uint64_t tree_size, uint8_t **proof, uint64_t *proof_len, stwo_prove_stats *stats,
+                               void *stream);
+void stwo_prove_cache_stats(const stwo_prove_cache *cache, uint64_t *device_bytes, uint64_t *graph_replays);
+void stwo_prove_cache_destroy(stwo_prove_cache *cache, void *stream);
+
 /* Proof server on the current device: n_workers jobs in flight at most, admitted in
  * arrival order while their device bound fits device_budget_bytes (smaller later jobs
  * pass a job that does not fit), each on its own stream; one shared twiddle tree for

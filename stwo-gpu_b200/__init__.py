@@ -11,5 +11,5 @@ from .backend import (  # noqa: F401
     Coset, CudaBackend, LineDomain, LineEvaluation, SecureColumnByCoords, SecureEvaluation, SecureFieldVec,
     TwiddleTree, index_to_point,
 )
-from .prover import ProofServer, WideFibJob, kernel_launches, prove_wide_fib, wide_fib_inputs  # noqa: F401
+from .prover import ProofServer, ProveCache, WideFibJob, kernel_launches, prove_wide_fib, wide_fib_inputs  # noqa: F401
 from .verifier import VerificationError, verify  # noqa: F401

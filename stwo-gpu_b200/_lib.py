@@ -124,6 +124,12 @@ SIGNATURES = [
     ("stwo_wide_fib_prove", C.c_int, [C.POINTER(WideFibJob), vp, vp, vp, vp, u64, C.POINTER(C.POINTER(C.c_uint8)),
                                       C.POINTER(u64), C.POINTER(ProveStats), vp]),
     ("stwo_free_proof", None, [vp]),
+    ("stwo_prove_cache_create", vp, []),
+    ("stwo_wide_fib_prove_cached", C.c_int, [vp, C.POINTER(WideFibJob), vp, vp, vp, vp, u64,
+                                             C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(u64),
+                                             C.POINTER(ProveStats), vp]),
+    ("stwo_prove_cache_stats", None, [vp, C.POINTER(u64), C.POINTER(u64)]),
+    ("stwo_prove_cache_destroy", None, [vp, vp]),
     ("stwo_server_create", vp, [u32, u64, u32]),
     ("stwo_server_submit", C.c_int, [vp, u64, C.POINTER(WideFibJob), vp, vp]),
     ("stwo_server_submit_device", C.c_int, [vp, u64, C.POINTER(WideFibJob), vp, vp]),

@@ -40,6 +40,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <new>
 #include <set>
 #include <vector>
 
@@ -766,7 +767,9 @@ void prove_cache_release(ProveCache *c, cudaStream_t st) {
     if (!c) return;
     if (c->exec) cudaGraphExecDestroy(c->exec);
     if (c->slab) cudaFreeAsync(c->slab, st);
+    const uint64_t replays = c->replays;  // a running count over the cache's life
     *c = ProveCache{};
+    c->replays = replays;
 }
 
 namespace {
@@ -1072,10 +1075,11 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         cache->replays++;
     } else if (cache_ok && hit && !cache->no_graph) {
         const uint64_t l0 = t_kernel_launches;
-        STWO_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        const int rc_cap = launch_all(true);
+        // (the legacy default stream cannot be captured: the sequence then runs directly)
+        const cudaError_t eb = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        const int rc_cap = eb == cudaSuccess ? launch_all(true) : (int)STWO_ERR_CUDA;
         cudaGraph_t graph = nullptr;
-        const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+        const cudaError_t ec = eb == cudaSuccess ? cudaStreamEndCapture(st, &graph) : eb;
         cudaGraphExec_t exec = nullptr;
         cudaError_t ei = cudaSuccess;
         if (rc_cap == STWO_OK && ec == cudaSuccess) ei = cudaGraphInstantiate(&exec, graph, 0);
@@ -1280,5 +1284,41 @@ int stwo_wide_fib_prove(const stwo_wide_fib_job *job, const uint32_t *a0, const 
 }
 
 void stwo_free_proof(uint8_t *proof) { free(proof); }
+
+struct stwo_prove_cache {
+    ProveCache c;
+};
+
+stwo_prove_cache *stwo_prove_cache_create(void) { return new (std::nothrow) stwo_prove_cache(); }
+
+int stwo_wide_fib_prove_cached(stwo_prove_cache *cache, const stwo_wide_fib_job *job, const uint32_t *a0,
+                               const uint32_t *a1, const uint32_t *twiddles, const uint32_t *itwiddles,
+                               uint64_t tree_size, uint8_t **proof_out, uint64_t *proof_len, stwo_prove_stats *stats,
+                               void *stream) {
+    STWO_REQUIRE(cache, STWO_ERR_INVALID_ARGUMENT, "null proof cache");
+    STWO_REQUIRE(twiddles && itwiddles, STWO_ERR_INVALID_ARGUMENT, "a cached proof needs the caller's twiddle tree");
+    STWO_REQUIRE(proof_out && proof_len, STWO_ERR_INVALID_ARGUMENT, "null proof output");
+    *proof_out = nullptr;
+    *proof_len = 0;
+    std::vector<uint8_t> proof;
+    int rc = wide_fib_prove(job, a0, a1, twiddles, itwiddles, tree_size, proof, stats, as_stream(stream), &cache->c);
+    if (rc) return rc;
+    *proof_out = static_cast<uint8_t *>(malloc(proof.size()));
+    STWO_REQUIRE(*proof_out, STWO_ERR_OUT_OF_MEMORY, "proof buffer allocation failed");
+    memcpy(*proof_out, proof.data(), proof.size());
+    *proof_len = proof.size();
+    return STWO_OK;
+}
+
+void stwo_prove_cache_stats(const stwo_prove_cache *cache, uint64_t *device_bytes, uint64_t *graph_replays) {
+    if (device_bytes) *device_bytes = cache && cache->c.valid ? cache->c.cap : 0;
+    if (graph_replays) *graph_replays = cache ? cache->c.replays : 0;
+}
+
+void stwo_prove_cache_destroy(stwo_prove_cache *cache, void *stream) {
+    if (!cache) return;
+    prove_cache_release(&cache->c, as_stream(stream));
+    delete cache;
+}
 
 }  // extern "C"

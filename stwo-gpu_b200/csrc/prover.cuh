@@ -23,10 +23,11 @@ struct ProveCache {
     cudaGraphExec_t exec = nullptr;
     bool no_graph = false;  // the launch sequence did not capture: run it directly
     uint64_t launches = 0;  // kernel launches inside the graph
-    uint64_t replays = 0;
+    uint64_t replays = 0;   // graph replays over the cache's life
 };
 
-// Frees the slab (stream-ordered on st) and the graph, and empties the cache.
+// Frees the slab (stream-ordered on st) and the graph, and empties the cache (the
+// replay count runs on).
 void prove_cache_release(ProveCache *c, cudaStream_t st);
 
 // One proof. cache: optional (server workers pass theirs).

@@ -57,10 +57,44 @@ def wide_fib_inputs(log_n_rows, seed):
         draw *= 2
 
 
-def prove_wide_fib(job, a0, a1, twiddles=None, stream=None):
+class ProveCache:
+    """Device memory (and the CUDA graph of the launch sequence) kept between proofs of
+    one job shape: pass it to prove_wide_fib with a twiddle tree; the second proof of
+    a shape captures the graph, later ones replay it (include/stwo_b200.h)."""
+
+    def __init__(self):
+        self._c = L.lib().stwo_prove_cache_create()
+        if not self._c:
+            raise MemoryError("proof cache allocation failed")
+
+    def stats(self):
+        b, r = C.c_uint64(), C.c_uint64()
+        L.lib().stwo_prove_cache_stats(self._c, C.byref(b), C.byref(r))
+        return {"device_bytes": b.value, "graph_replays": r.value}
+
+    def close(self, stream=None):
+        if self._c:
+            L.lib().stwo_prove_cache_destroy(self._c, stream)
+            self._c = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def prove_wide_fib(job, a0, a1, twiddles=None, stream=None, cache=None):
     """Proves one job; returns (proof bytes, per-phase stats dict). a0, a1: host
     uint32 arrays of 2^log_n_rows M31 values. twiddles: optional TwiddleTree covering
-    CanonicCoset(log_n_rows + 1 + log_blowup)."""
+    CanonicCoset(log_n_rows + 1 + log_blowup). cache: optional ProveCache (needs
+    twiddles) for repeated proofs of one shape."""
     a0 = np.ascontiguousarray(a0, dtype=np.uint32)
     a1 = np.ascontiguousarray(a1, dtype=np.uint32)
     n = 1 << job.log_n_rows
@@ -74,8 +108,12 @@ def prove_wide_fib(job, a0, a1, twiddles=None, stream=None):
     if twiddles is not None:
         tw, itw, tsz = twiddles.twiddles.device_ptr, twiddles.itwiddles.device_ptr, len(twiddles.twiddles)
     L.clear_error()
-    L.check(L.lib().stwo_wide_fib_prove(C.byref(job.c()), a0.ctypes.data, a1.ctypes.data, tw, itw, tsz,
-                                        C.byref(out), C.byref(ln), C.byref(st), stream))
+    if cache is not None:
+        L.check(L.lib().stwo_wide_fib_prove_cached(cache._c, C.byref(job.c()), a0.ctypes.data, a1.ctypes.data, tw,
+                                                   itw, tsz, C.byref(out), C.byref(ln), C.byref(st), stream))
+    else:
+        L.check(L.lib().stwo_wide_fib_prove(C.byref(job.c()), a0.ctypes.data, a1.ctypes.data, tw, itw, tsz,
+                                            C.byref(out), C.byref(ln), C.byref(st), stream))
     try:
         proof = C.string_at(out, ln.value)
     finally:

@@ -176,6 +176,40 @@ def test_server_same_shape_runs_replay_equal_proofs(graphs, workers, monkeypatch
         assert gs["slab_reuses"] > 0 and gs["graph_replays"] > 0
 
 
+@pytest.mark.parametrize("stream_kind", ["own", "default"])
+def test_cached_proofs_replay_and_equal_plain_proofs(stream_kind):
+    """stwo_wide_fib_prove_cached: the first proof of a shape keeps its memory, the
+    second captures the launch sequence as a CUDA graph, later ones replay it; a new
+    shape replaces the cached one. On the legacy default stream the memory is reused
+    but nothing is captured. Every proof equals the plain call's."""
+    import torch
+    stwo = load_package()
+    s = torch.cuda.Stream() if stream_kind == "own" else None
+    sptr = s.cuda_stream if s is not None else None
+    tree = stwo.CudaBackend.precompute_twiddles(stwo.CanonicCoset(16).half_coset())
+    seq = [(10, 24, 1, 3, 5)] * 4 + [(12, 16, 2, 4, 2)] * 3 + [(2, 3, 1, 1, 0)] * 2 + [(10, 24, 1, 3, 5)] * 2
+    with stwo.ProveCache() as cache:
+        replays = []
+        for k, t in enumerate(seq):
+            a0, a1 = stwo.wide_fib_inputs(t[0], 3000 + k)
+            want, _ = stwo.prove_wide_fib(job_of(t), a0, a1)
+            got, st = stwo.prove_wide_fib(job_of(t), a0, a1, twiddles=tree, stream=sptr, cache=cache)
+            assert got == want, (k, t)
+            assert st["trace_ms"] > 0 and st["kernel_launches"] > 0
+            replays.append(cache.stats()["graph_replays"])
+        # replays from the third proof of a run on; log_n_rows 2 is not cached
+        if stream_kind == "own":
+            assert replays == [0, 0, 1, 2, 2, 2, 3, 3, 3, 3, 3]
+        else:
+            assert replays == [0] * len(seq)
+        assert cache.stats()["device_bytes"] == job_of(seq[-1]).device_bytes(own_twiddles=False)
+        cache.close(sptr)
+    with pytest.raises(stwo._lib.StwoError):  # the cache needs the caller's tree
+        with stwo.ProveCache() as c2:
+            a0, a1 = stwo.wide_fib_inputs(10, 1)
+            stwo.prove_wide_fib(job_of(seq[0]), a0, a1, cache=c2)
+
+
 def test_server_respects_the_memory_budget():
     stwo = load_package()
     t = (10, 32, 1, 3, 5)
