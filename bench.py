@@ -763,6 +763,21 @@ def run_ours(args, rank, world, local_rank):
                 want, _ = O.wide_fib_prove(t[0], t[1], a0, a1, *t[2:])
                 ent["oracle_ms"] = (time.perf_counter() - t0) * 1e3
                 ent["equal_to_oracle"] = want == proof
+            # The same proof repeated through a ProveCache (shared tree, own stream):
+            # memory reused, launch sequence replayed as a CUDA graph.
+            cs = torch.cuda.Stream(dev)
+            tree = stwo.CudaBackend.precompute_twiddles(stwo.CanonicCoset(t[0] + 1 + t[2]).half_coset())
+            ctimes = []
+            with stwo.ProveCache() as cache:
+                for k in range(8):
+                    t0 = time.perf_counter()
+                    cproof, _ = stwo.prove_wide_fib(job, a0, a1, twiddles=tree, stream=cs.cuda_stream, cache=cache)
+                    ctimes.append((time.perf_counter() - t0) * 1e3)
+                ent["cached_ms_median"] = float(np.median(ctimes[3:]))
+                ent["cached_graph_replays"] = cache.stats()["graph_replays"]
+                ent["cached_equal"] = cproof == proof
+                cache.close(cs.cuda_stream)
+            del tree
             singles[name] = ent
         verified = all(stwo.verify(batched_results[0][i]["proof"], *dataclasses.astuple(job_of(stwo, steps[0][i])))
                        for i in range(min(2, args.jobs)))
