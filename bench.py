@@ -652,6 +652,12 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    # Server workers poll the device for up to 2 ms before blocking; with more workers on
+    # this node than half its host threads (several replicas), polling would take cores
+    # from the workers that launch, so they block at once.
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    if "STWO_SERVER_SPIN_US" not in os.environ and world * args.workers > cores // 2:
+        os.environ["STWO_SERVER_SPIN_US"] = "0"
     stwo = load_package()
     import ctypes as C
     tune_buf = C.create_string_buffer(4096)
@@ -796,6 +802,7 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "m31 (u32)", "data": "synthetic (seeded SplitMix64 M31 trace inputs)",
             "config": {"workload": job_desc(args.jobs), "jobs_per_step": args.jobs, "workers": args.workers,
+                       "worker_poll_us_before_blocking": int(os.environ.get("STWO_SERVER_SPIN_US", "2000")),
                        "device_budget_gb": BUDGET >> 30, "inputs": "resident in HBM before the timed region",
                        "l2": "each job's columns and trees are freshly written; the stream's working set "
                              "(GBs) exceeds the 126 MB L2",
