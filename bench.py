@@ -410,11 +410,17 @@ def run_reference(args, rank, world):
     threads = os.cpu_count() or 1
     for w in range(args.warmup):  # warm-up: one 64-column x 2^12 job each
         cpu_stream_sample(O, stwo, [(12, 64, 7000 + w)], 0.0, threads)
-    n_total, t_total = 0, 0.0
+    # Each step: the stream's first jobs within --cpu-budget seconds (at least one job);
+    # steps stop early once --cpu-total-budget seconds have gone by, so the whole run
+    # stays within a few minutes (one large job alone takes tens of seconds).
+    n_total, t_total, steps_done = 0, 0.0, 0
     for s in range(args.steps):
+        if steps_done and t_total >= args.cpu_total_budget:
+            break
         n, dt, _ = cpu_stream_sample(O, stwo, job_stream(args.jobs, 1000 + s), args.cpu_budget, threads)
         n_total += n
         t_total += dt
+        steps_done += 1
     value = n_total / t_total
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
@@ -424,7 +430,8 @@ def run_reference(args, rank, world):
         "config": {"workload": job_desc(args.jobs) + f" (CPU: a bounded sample of each step, ~{args.cpu_budget:.0f} s)",
                    "jobs_per_step": args.jobs},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{n_total} jobs over {args.steps} steps, each step the stream's first jobs "
+                         "sample": f"{n_total} jobs over {steps_done} of {args.steps} steps (at most "
+                                   f"{args.cpu_total_budget:.0f} s in all), each step the stream's first jobs "
                                    f"within {args.cpu_budget:.0f} s (oracle prover, {threads} threads)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -925,6 +932,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--jobs", type=int, default=48, help="jobs per step")
     ap.add_argument("--workers", type=int, default=8, help="proof server jobs in flight")
+    ap.add_argument("--cpu-total-budget", type=float, default=120.0,
+                    help="--impl reference: stop starting steps after this many seconds of CPU proving")
     ap.add_argument("--latency-jobs", type=int, default=2000, help="jobs per Poisson load level")
     ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds of oracle work per CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
