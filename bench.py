@@ -837,8 +837,9 @@ def run_profile(args):
     """One workload between cudaProfilerStart/Stop for ncu (--profile-from-start off),
     after warm-up: `fft[:LOG]` (8 columns at LOG, interpolate + blowup-4 evaluate, two
     steps), `proof:L,N` (one wide-Fibonacci proof, log_blowup 1, 3 queries, pow_bits 5)
-    `merkle` (the 64 x 2^22 tree of the kernel sweep) or `quotients` (the sweep's 32
-    columns x 2^22 with 4 sample points)."""
+    `merkle` (the 64 x 2^22 tree of the kernel sweep), `quotients` (the sweep's 32
+    columns x 2^22 with 4 sample points), `fri` (the sweep's fold chain, 2^24 down to
+    2^4) or `inverse` (the sweep's batch inverse of 2^24 QM31)."""
     import numpy as np
     import torch
     stwo = load_package()
@@ -909,6 +910,35 @@ def run_profile(args):
             L.check(lib.stwo_accumulate_quotients(dom.half_coset.initial_index, dom.half_coset.step_size, lg, cp, nc,
                                                   rcoef, sp, sizes, idx, vals, nb, op, sptr))
         reps = 1
+    elif what == "fri":
+        lg = 24
+        sptr = torch.cuda.current_stream(dev).cuda_stream
+        hc = stwo.CanonicCoset(lg).half_coset()
+        tsz = 1 << hc.log_size
+        tree = torch.empty(tsz, dtype=torch.int32, device=dev)
+        itree = torch.empty_like(tree)
+        L.check(lib.stwo_precompute_twiddles(hc.initial_index, hc.step_size, hc.log_size, tree.data_ptr(),
+                                             itree.data_ptr(), sptr))
+        src = [torch.randint(0, P, (1 << lg,), dtype=torch.int64, device=dev).to(torch.int32) for _ in range(4)]
+        bufs = [[torch.empty(1 << l, dtype=torch.int32, device=dev) for _ in range(4)] for l in range(lg)]
+        bp = [L.ptr_array([b.data_ptr() for b in bl]) for bl in bufs]
+        sp = L.ptr_array([c.data_ptr() for c in src])
+        alpha = L.QM31(12345, 678, 91011, 1213)
+
+        def work():
+            L.check(lib.stwo_fold_circle_into_line(sp, 1 << lg, alpha, itree.data_ptr(), 0, bp[lg - 1], sptr))
+            for l in range(lg - 1, 4, -1):
+                L.check(lib.stwo_fold_line(bp[l], 1 << l, alpha, itree.data_ptr(), tsz - (1 << l), bp[l - 1], sptr))
+        reps = 1
+    elif what == "inverse":
+        n = 1 << 24
+        sptr = torch.cuda.current_stream(dev).cuda_stream
+        src = torch.randint(1, P, (4 * n,), dtype=torch.int64, device=dev).to(torch.int32)
+        dst = torch.empty_like(src)
+
+        def work():
+            L.check(lib.stwo_batch_inverse_qm31(src.data_ptr(), dst.data_ptr(), n, sptr))
+        reps = 1
     else:
         raise SystemExit(f"unknown --profile {what}")
     for _ in range(3):
@@ -939,7 +969,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-suite", action="store_true", help="skip the config-1 per-kernel sweep")
     ap.add_argument("--profile", default=None,
-                    help="run one workload for ncu instead: fft[:LOG] | proof:L,N | merkle | quotients")
+                    help="run one workload for ncu instead: fft[:LOG] | proof:L,N | merkle | quotients | fri | "
+                         "inverse")
     args = ap.parse_args()
     if args.profile:
         run_profile(args)
