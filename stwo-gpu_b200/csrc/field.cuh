@@ -131,14 +131,29 @@ __host__ __device__ __forceinline__ qm31 qm31_scale(qm31 x, uint32_t s) {
     return {{m31_mul2(x.a.a, s2), m31_mul2(x.a.b, s2)}, {m31_mul2(x.b.a, s2), m31_mul2(x.b.b, s2)}};
 }
 __host__ __device__ __forceinline__ qm31 qm31_mul_cm31(qm31 x, cm31 s) { return {cm31_mul(x.a, s), cm31_mul(x.b, s)}; }
-// (a + bu)(c + du) = (ac + (2+i) bd) + ((a+b)(c+d) - ac - bd) u
+// x y with x = (x0 + x1 i) + (x2 + x3 i) u, y likewise, u^2 = 2 + i, i^2 = -1:
+//   (x0 + x1 i)(y0 + y1 i) + (2 + i)(x2 + x3 i)(y2 + y3 i)
+//     + ((x0 + x1 i)(y2 + y3 i) + (x2 + x3 i)(y0 + y1 i)) u,
+// i.e. per output coordinate a dot product of x with four coefficients derived from y:
+//   r0 = x0 y0 - x1 y1 + x2 (2 y2 - y3) - x3 (y2 + 2 y3)
+//   r1 = x0 y1 + x1 y0 + x2 (y2 + 2 y3) + x3 (2 y2 - y3)
+//   r2 = x0 y2 - x1 y3 + x2 y0 - x3 y1
+//   r3 = x0 y3 + x1 y2 + x2 y1 + x3 y0
+// Negated coefficients are taken as P - c (in (0, P]), so every term is a product of
+// values below 2^31; each coordinate accumulates its four 64-bit products (below 2^64)
+// and is reduced once.
 __host__ __device__ __forceinline__ qm31 qm31_mul(qm31 x, qm31 y) {
-    cm31 ac = cm31_mul(x.a, y.a);
-    cm31 bd = cm31_mul(x.b, y.b);
-    cm31 m = cm31_mul(cm31_add(x.a, x.b), cm31_add(y.a, y.b));
-    // (2 + i) * bd = (2 bd.a - bd.b) + (2 bd.b + bd.a) i
-    cm31 rbd = {m31_sub(m31_add(bd.a, bd.a), bd.b), m31_add(m31_add(bd.b, bd.b), bd.a)};
-    return {cm31_add(ac, rbd), cm31_sub(m, cm31_add(ac, bd))};
+    const uint32_t y0 = y.a.a, y1 = y.a.b, y2 = y.b.a, y3 = y.b.b;
+    const uint32_t ny1 = P - y1, ny3 = P - y3;
+    const uint32_t e = m31_sub(m31_add(y2, y2), y3);  // 2 y2 - y3
+    const uint32_t f = m31_add(y2, m31_add(y3, y3));  // y2 + 2 y3
+    const uint32_t nf = P - f;
+    const uint32_t x0 = x.a.a, x1 = x.a.b, x2 = x.b.a, x3 = x.b.b;
+    const uint64_t r0 = mac64(mac64(mac64((uint64_t)x0 * y0, x1, ny1), x2, e), x3, nf);
+    const uint64_t r1 = mac64(mac64(mac64((uint64_t)x0 * y1, x1, y0), x2, f), x3, e);
+    const uint64_t r2 = mac64(mac64(mac64((uint64_t)x0 * y2, x1, ny3), x2, y0), x3, ny1);
+    const uint64_t r3 = mac64(mac64(mac64((uint64_t)x0 * y3, x1, y2), x2, y1), x3, y0);
+    return {{reduce64_p(r0), reduce64_p(r1)}, {reduce64_p(r2), reduce64_p(r3)}};
 }
 __host__ __device__ inline qm31 qm31_inv(qm31 x) {
     cm31 b2 = cm31_mul(x.b, x.b);
