@@ -194,6 +194,7 @@ int stwo_bit_reverse_qm31(uint32_t *column, uint64_t n, void *stream);
 int stwo_new_canonical_ordered(const uint32_t *src, uint32_t *dst, uint32_t log_size, void *stream);
 int stwo_batch_inverse_m31(const uint32_t *src, uint32_t *dst, uint64_t n, void *stream);
 int stwo_batch_inverse_qm31(const uint32_t *src, uint32_t *dst, uint64_t n, void *stream);
+/* (the batch inverses accept src == dst) */
 
 /* PolyOps::eval_at_point for n_polys polynomials, each at its own point; results
  * (device, AoS QM31) in results[i]. `scratch` is caller-owned device memory of at

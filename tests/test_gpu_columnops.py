@@ -47,7 +47,7 @@ def test_batch_inverse_base_field(stwo, oracle, n):
     assert (dst.to_numpy() == oracle.batch_inverse_m31(v)).all()
 
 
-@pytest.mark.parametrize("n", [1, 5, 1024, 3000, 1 << 18])
+@pytest.mark.parametrize("n", [1, 5, 1024, 3000, 8191, 8192, 8193, 1 << 18])
 def test_batch_inverse_secure_field(stwo, oracle, n):
     """field.rs:59 (QM31 values from 1..4n in the reference)."""
     v = m31(rng(9 + n), 4 * n).reshape(n, 4)
@@ -56,6 +56,23 @@ def test_batch_inverse_secure_field(stwo, oracle, n):
     dst = stwo.SecureFieldVec.new_uninitialized(n)
     stwo.CudaBackend.batch_inverse(src, dst)
     assert (dst.to_numpy() == oracle.batch_inverse_qm31(v)).all()
+
+
+@pytest.mark.parametrize("n", [7, 4096 + 33, 1 << 17])
+def test_batch_inverse_in_place(stwo, oracle, n):
+    """src == dst: each element is read before its inverse is written over it."""
+    L = stwo._lib
+    v = m31_nonzero(rng(700 + n), n)
+    b = stwo.BaseFieldVec.from_numpy(v)
+    L.check(L.lib().stwo_batch_inverse_m31(b.device_ptr, b.device_ptr, n, None))
+    L.check(L.lib().stwo_stream_synchronize(None))
+    assert (b.to_numpy() == oracle.batch_inverse_m31(v)).all()
+    q = m31(rng(800 + n), 4 * n).reshape(n, 4)
+    q[:, 0] |= 1
+    qb = stwo.SecureFieldVec.from_numpy(q)
+    L.check(L.lib().stwo_batch_inverse_qm31(qb.device_ptr, qb.device_ptr, n, None))
+    L.check(L.lib().stwo_stream_synchronize(None))
+    assert (qb.to_numpy() == oracle.batch_inverse_qm31(q)).all()
 
 
 def test_batch_inverse_reference_pattern_full_size(stwo):
