@@ -209,7 +209,7 @@ int stwo_eval_at_points(const uint32_t *const *coeffs, const uint32_t *log_sizes
  * reference (whose eval_at_point mallocs and frees scratch on every call); it is
  * for callers that cannot call cudaMalloc, for example a server whose device memory
  * all belongs to its own pool, or a loop that cannot afford cudaMalloc/cudaFree's
- * implicit synchronisation. The scratch is a fixed 512.5 KiB array inside the library,
+ * implicit synchronisation. The scratch is a fixed 32.5 KiB array inside the library,
  * held on every GPU that loads it until the process exits, so polynomials are
  * limited to 2^26 coefficients (larger sizes return STWO_ERR_UNSUPPORTED_SIZE).
  * result is a device pointer to one QM31; the call is asynchronous on `stream`.

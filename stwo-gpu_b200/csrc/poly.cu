@@ -87,19 +87,23 @@ __global__ void canonic_to_bitrev_kernel(const uint32_t *__restrict__ src, uint3
 
 // ------------------------------------------------------------------ eval_at_point
 // p(P) = sum_i c_i prod_{bit b of i} f_b with f_0 = y, f_1 = x, f_b = pi^(b-1)(x),
-// pi(x) = 2x^2 - 1 (eval_at_point.cu:99-109). A CTA folds a chunk of 2^15
-// coefficients as 4 groups of 8192: a thread takes 32 consecutive coefficients (bits
-// 0..4) and forms sum_i c_i F_i against the CTA's table F_i = prod_{b in i} f_b, an
-// M31-by-QM31 dot product of 64-bit multiply-accumulates; the lanes fold bits 5..9
-// and the warps bits 10..12. Group partials are weighted by their group index's
-// factors (bits 13..14) before the lane fold, which is linear, so one fold serves the
-// whole chunk. The chunk partial takes the factors of its chunk index; the last CTA
-// of each polynomial (atomic ticket) adds the partials.
+// pi(x) = 2x^2 - 1 (eval_at_point.cu:99-109). A CTA folds a chunk of
+// 2^(13 + iter_log) coefficients as groups of 8192: a warp reads 1024 consecutive
+// coefficients with coalesced loads, a thread's 32 of them cover index bits 0, 1 and
+// 7..9, and the thread forms sum_i c_i F_i against the CTA's table of the products of
+// those bits' factors, an M31-by-QM31 dot product of 64-bit multiply-accumulates; the
+// lanes fold bits 2..6 and the warps bits 10..12. Group partials are weighted by
+// their group index's factors (bits 13..) before the lane fold, which is linear, so
+// one fold serves the whole chunk. The chunk partial takes the factors of its chunk
+// index; the last CTA of each polynomial (atomic ticket) adds the partials.
 constexpr int EAP_THREADS = 256;
 constexpr int EAP_PER_THREAD_LOG = 5;                    // 32 coefficients per thread
 constexpr int EAP_GROUP_LOG = EAP_PER_THREAD_LOG + 8;    // x 256 threads
-constexpr int EAP_ITER_LOG = 2;                          // groups per CTA: 4
-constexpr int EAP_CHUNK_LOG = EAP_GROUP_LOG + EAP_ITER_LOG;
+// Groups per CTA, 2^iter_log, chosen per launch (eap_iter_log): larger chunks spread
+// each CTA's set-up over more coefficients; smaller ones keep small launches wide.
+constexpr int EAP_ITER_LOG_MIN = 2;
+constexpr int EAP_ITER_LOG_MAX = 4;
+constexpr int EAP_CHUNK_LOG_MIN = EAP_GROUP_LOG + EAP_ITER_LOG_MIN;
 constexpr int EAP_MAX_POLYS = 32;
 
 struct EapParams {
@@ -108,6 +112,7 @@ struct EapParams {
     uint32_t log_size[EAP_MAX_POLYS];
     uint32_t block_start[EAP_MAX_POLYS + 1];  // prefix sum of CTAs per polynomial
     uint32_t n_polys;
+    uint32_t iter_log;                         // groups per CTA: 2^iter_log
     qm31 *partials;                            // one per CTA
     uint32_t *tickets;                         // one per polynomial, zero on entry, reset on exit
     qm31 *results;
@@ -121,95 +126,137 @@ __device__ __forceinline__ qm31 shfl_xor_q(qm31 v, int m) {
     return v;
 }
 
-// One CTA's share of polynomial `poly`: chunk `chunk` of its 2^L coefficients c with
-// factors f; its CTAs are blk_first .. blk_first + nblk - 1 (partials indexed by CTA).
+// A warp reads 1024 consecutive coefficients of a group as 8 coalesced loads of 512
+// bytes: load u gives lane l coefficients 128u + 4l + k, k = 0..3. So a thread's 32
+// coefficients span index bits 0, 1 (k) and 7, 8, 9 (u), and the lanes bits 2..6.
+// First coefficient of this warp's share of group `it` of chunk `chunk` (chunks of
+// 2^chunk_log coefficients).
+__device__ __forceinline__ uint64_t eap_base(uint32_t chunk, uint32_t chunk_log, uint32_t it) {
+    return ((uint64_t)chunk << chunk_log) + ((uint64_t)it << EAP_GROUP_LOG) + ((uint64_t)(threadIdx.x >> 5) << 10);
+}
+
+// Factor index of bit b of a thread's term index 4u + k.
+__device__ __forceinline__ constexpr int eap_term_bit(int b) { return b < 2 ? b : b + 5; }
+
+// This thread's 32 coefficients of group `it` when the warp's 1024 all exist (a
+// ragged group is read coefficient by coefficient instead).
+__device__ __forceinline__ void eap_load(const uint32_t *c, uint64_t n, uint32_t chunk, uint32_t chunk_log, uint32_t it,
+                                         uint4 (&v)[8]) {
+    const uint64_t base = eap_base(chunk, chunk_log, it);
+    if (base + 1024 <= n) {
+        const uint4 *q = reinterpret_cast<const uint4 *>(c + base) + (threadIdx.x & 31u);
+#pragma unroll
+        for (int u = 0; u < 8; u++) v[u] = __ldg(q + 32 * u);
+    }
+}
+
+// Folds values held by 2^LEVELS consecutive lanes, lane bit j <-> factor fj[j]: the
+// lane with bit j clear forms lo + hi * fj[j], and its partner forms the same value.
+template <int LEVELS>
+__device__ __forceinline__ qm31 eap_lane_fold(qm31 acc, const qm31 *fj) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int j = 0; j < LEVELS; j++) {
+        qm31 other = shfl_xor_q(acc, 1 << j);
+        qm31 lo = (lane >> j) & 1u ? other : acc;
+        qm31 hi = (lane >> j) & 1u ? acc : other;
+        acc = qm31_add(lo, qm31_mul(hi, fj[j]));
+    }
+    return acc;
+}
+
+// One CTA's share of polynomial `poly`: chunk `chunk` (2^iter_log groups) of its 2^L
+// coefficients c with factors f; its CTAs are blk_first .. blk_first + nblk - 1
+// (partials indexed by CTA).
+// cur holds this thread's first group, loaded by the caller before the factors were
+// ready, so that those loads overlap the set-up of the tables.
 __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t L, const qm31 *f, const uint32_t *c,
-                                         uint32_t blk_first, uint32_t nblk, qm31 *partials, uint32_t *tickets,
-                                         qm31 *results) {
+                                         uint32_t iter_log, uint32_t blk_first, uint32_t nblk, qm31 *partials,
+                                         uint32_t *tickets, qm31 *results, uint4 (&cur)[8]) {
     __shared__ qm31 warp_vals[EAP_THREADS / 32];
-    __shared__ qm31 g[1 << EAP_ITER_LOG];
+    __shared__ qm31 g[1 << EAP_ITER_LOG_MAX];
     __shared__ qm31 F2[1 << EAP_PER_THREAD_LOG];  // F_i
+    __shared__ qm31 chunk_w;
     __shared__ bool is_last;
     const uint32_t tid = threadIdx.x;
     const uint64_t n = 1ull << L;
+    const uint32_t chunk_log = EAP_GROUP_LOG + iter_log;
     if (tid < (1u << EAP_PER_THREAD_LOG)) {
         qm31 w = qm31_one();
         for (int b = 0; b < EAP_PER_THREAD_LOG; b++)
-            if ((tid >> b) & 1u) w = qm31_mul(w, f[b]);
+            if ((tid >> b) & 1u) w = qm31_mul(w, f[eap_term_bit(b)]);
         F2[tid] = w;
-    } else if (tid < (1u << EAP_PER_THREAD_LOG) + (1u << EAP_ITER_LOG)) {
+    } else if (tid >= 32 && tid < 32 + (1u << iter_log)) {
         // group weights: products of f_{13+b} over the set bits b of the group index
-        const uint32_t it = tid - (1u << EAP_PER_THREAD_LOG);
+        const uint32_t it = tid - 32;
         qm31 w = qm31_one();
-        for (int b = 0; b < EAP_ITER_LOG; b++)
+        for (uint32_t b = 0; b < iter_log; b++)
             if ((it >> b) & 1u) w = qm31_mul(w, f[EAP_GROUP_LOG + b]);
         g[it] = w;
     }
     __syncthreads();
+    if (tid == 64) {
+        // The chunk weight (the factors of the chunk index's bits) is used only after
+        // the last group; one thread forms it while its own loads are in flight.
+        qm31 w = qm31_one();
+        for (uint32_t b = 0; chunk_log + b < L; b++)
+            if ((chunk >> b) & 1u) w = qm31_mul(w, f[chunk_log + b]);
+        chunk_w = w;
+    }
 
     qm31 acc = qm31_zero();
-    for (uint32_t it = 0; it < (1u << EAP_ITER_LOG); it++) {
-        const uint64_t base = ((uint64_t)chunk << EAP_CHUNK_LOG) + ((uint64_t)it << EAP_GROUP_LOG) +
-                              ((uint64_t)tid << EAP_PER_THREAD_LOG);
+    for (uint32_t it = 0; it < (1u << iter_log); it++) {
+        const uint64_t base = eap_base(chunk, chunk_log, it);
         if (base >= n) break;
+        if (it > 0) eap_load(c, n, chunk, chunk_log, it, cur);
         uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-        // 64-bit multiply-accumulates of canonical values, folded after every third term
+        // 64-bit multiply-accumulates of canonical values, folded after every fourth
+        // term: a fold leaves less than 2^34, and four products of values below 2^31 - 1
+        // add less than 2^64 - 2^34.
         auto term = [&](uint32_t v, uint32_t i) {
             const qm31 w = F2[i];
             s0 = mac64(s0, v, w.a.a);
             s1 = mac64(s1, v, w.a.b);
             s2 = mac64(s2, v, w.b.a);
             s3 = mac64(s3, v, w.b.b);
-            if (i % 3 == 2) {
+            if (i % 4 == 3) {
                 s0 = fold64(s0);
                 s1 = fold64(s1);
                 s2 = fold64(s2);
                 s3 = fold64(s3);
             }
         };
-        if (base + 32 <= n) {
-            const uint4 *q = reinterpret_cast<const uint4 *>(c + base);
+        if (base + 1024 <= n) {
 #pragma unroll
             for (int u = 0; u < 8; u++) {
-                const uint4 x = __ldg(q + u);
-                term(x.x, 4 * u);
-                term(x.y, 4 * u + 1);
-                term(x.z, 4 * u + 2);
-                term(x.w, 4 * u + 3);
+                term(cur[u].x, 4 * u);
+                term(cur[u].y, 4 * u + 1);
+                term(cur[u].z, 4 * u + 2);
+                term(cur[u].w, 4 * u + 3);
             }
         } else {
-            for (uint32_t i = 0; base + i < n && i < 32; i++) term(__ldg(c + base + i), i);
+            for (uint32_t i = 0; i < 32; i++) {
+                const uint64_t at = base + 128 * (i >> 2) + 4 * (tid & 31u) + (i & 3u);
+                if (at >= n) break;  // positions grow with i
+                term(__ldg(c + at), i);
+            }
         }
         const qm31 part = {{reduce64_p(s0), reduce64_p(s1)}, {reduce64_p(s2), reduce64_p(s3)}};
         acc = qm31_add(acc, it == 0 ? part : qm31_mul(part, g[it]));
     }
-    // Across lanes: bits 5..9 (lane bit j <-> factor 5 + j).
-    const uint32_t lane = tid & 31u;
-#pragma unroll
-    for (int j = 0; j < 5; j++) {
-        qm31 other = shfl_xor_q(acc, 1 << j);
-        // lane with bit j clear keeps lo + hi * f; the other result is discarded.
-        qm31 lo = (lane >> j) & 1u ? other : acc;
-        qm31 hi = (lane >> j) & 1u ? acc : other;
-        acc = qm31_add(lo, qm31_mul(hi, f[EAP_PER_THREAD_LOG + j]));
-    }
-    if (lane == 0) warp_vals[tid >> 5] = acc;
+    // Across lanes: bits 2..6; across the 8 warps (in warp 0): bits 10..12.
+    acc = eap_lane_fold<5>(acc, f + 2);
+    if ((tid & 31u) == 0) warp_vals[tid >> 5] = acc;
     __syncthreads();
-    if (tid == 0) {
-        // Warps: bits 10..12.
-        qm31 w[8];
-        for (int i = 0; i < 8; i++) w[i] = warp_vals[i];
-        for (int lvl = 0; lvl < 3; lvl++)
-            for (int i = 0; i < (8 >> (lvl + 1)); i++)
-                w[i] = qm31_add(w[2 * i], qm31_mul(w[2 * i + 1], f[EAP_PER_THREAD_LOG + 5 + lvl]));
-        qm31 s = w[0];
-        // Chunk index bits -> factors 15.. .
-        for (uint32_t b = 0; EAP_CHUNK_LOG + b < L; b++)
-            if ((chunk >> b) & 1u) s = qm31_mul(s, f[EAP_CHUNK_LOG + b]);
-        partials[blockIdx.x] = s;
-        __threadfence();
-        uint32_t t = atomicAdd(&tickets[poly], 1u);
-        is_last = (t == nblk - 1);
+    if (tid < 32) {
+        qm31 w = tid < EAP_THREADS / 32 ? warp_vals[tid] : qm31_zero();
+        w = eap_lane_fold<3>(w, f + 10);
+        if (tid == 0) {
+            partials[blockIdx.x] = qm31_mul(w, chunk_w);
+            __threadfence();
+            uint32_t t = atomicAdd(&tickets[poly], 1u);
+            is_last = (t == nblk - 1);
+        }
     }
     __syncthreads();
     if (is_last) {
@@ -225,7 +272,7 @@ __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t
         }
 #pragma unroll
         for (int m = 16; m >= 1; m >>= 1) s = qm31_add(s, shfl_xor_q(s, m));
-        if (lane == 0) warp_vals[tid >> 5] = s;
+        if ((tid & 31u) == 0) warp_vals[tid >> 5] = s;
         __syncthreads();
         if (tid == 0) {
             qm31 t = qm31_zero();
@@ -236,11 +283,16 @@ __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t
     }
 }
 
-__global__ void __launch_bounds__(EAP_THREADS) eval_at_point_kernel(const __grid_constant__ EapParams p) {
+// Three CTAs per SM: at four the per-polynomial factor tables read from the kernel
+// parameters spill (measured 3% slower over 32 x 2^22 coefficients).
+__global__ void __launch_bounds__(EAP_THREADS, 3) eval_at_point_kernel(const __grid_constant__ EapParams p) {
     uint32_t poly = 0;
     while (poly + 1 < p.n_polys && blockIdx.x >= p.block_start[poly + 1]) poly++;
-    eap_body(poly, blockIdx.x - p.block_start[poly], p.log_size[poly], p.factors[poly], p.coeffs[poly],
-             p.block_start[poly], p.block_start[poly + 1] - p.block_start[poly], p.partials, p.tickets, p.results);
+    const uint32_t chunk = blockIdx.x - p.block_start[poly];
+    uint4 cur[8];
+    eap_load(p.coeffs[poly], 1ull << p.log_size[poly], chunk, EAP_GROUP_LOG + p.iter_log, 0, cur);
+    eap_body(poly, chunk, p.log_size[poly], p.factors[poly], p.coeffs[poly], p.iter_log, p.block_start[poly],
+             p.block_start[poly + 1] - p.block_start[poly], p.partials, p.tickets, p.results, cur);
 }
 
 // Polynomials described in device memory, all evaluated at one point also in device
@@ -251,20 +303,27 @@ struct EapDevPoly {
     uint32_t block_start;  // first CTA of the polynomial
 };
 
-__global__ void __launch_bounds__(EAP_THREADS) eval_at_point_dev_kernel(const EapDevPoly *__restrict__ polys,
-                                                                        uint32_t n_polys, const qm31 *point,
-                                                                        qm31 *partials, uint32_t *tickets,
-                                                                        qm31 *results) {
+__global__ void __launch_bounds__(EAP_THREADS, 4) eval_at_point_dev_kernel(const EapDevPoly *__restrict__ polys,
+                                                                           uint32_t n_polys, uint32_t iter_log,
+                                                                           const qm31 *point, qm31 *partials,
+                                                                           uint32_t *tickets, qm31 *results) {
     __shared__ qm31 f[32];
-    // the last polynomial whose first CTA is <= blockIdx.x
-    uint32_t lo = 0, hi = n_polys - 1;
-    while (lo < hi) {
-        uint32_t mid = (lo + hi + 1) / 2;
-        if (polys[mid].block_start <= blockIdx.x) lo = mid;
-        else hi = mid - 1;
+    // The last polynomial whose first CTA is <= blockIdx.x, by a 32-way search: each
+    // round lane k tests candidate lo + k * step, and polys[lo] always qualifies.
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t lo = 0, count = n_polys;
+    while (count > 1) {
+        const uint32_t step = (count + 31) / 32;
+        const bool ok = lane * step < count && polys[lo + lane * step].block_start <= blockIdx.x;
+        const uint32_t t = 31 - __clz(__ballot_sync(0xffffffffu, ok));
+        lo += t * step;
+        count = min(step, count - t * step);
     }
     const EapDevPoly d = polys[lo];
     const uint32_t next = lo + 1 < n_polys ? polys[lo + 1].block_start : gridDim.x;
+    const uint32_t chunk = blockIdx.x - d.block_start;
+    uint4 cur[8];
+    eap_load(d.coeffs, 1ull << d.log_size, chunk, EAP_GROUP_LOG + iter_log, 0, cur);
     if (threadIdx.x == 0) {
         // f_0 = y, f_1 = x, f_b = pi^(b-1)(x)
         f[0] = point[1];
@@ -276,10 +335,9 @@ __global__ void __launch_bounds__(EAP_THREADS) eval_at_point_dev_kernel(const Ea
         }
     }
     __syncthreads();
-    eap_body(lo, blockIdx.x - d.block_start, d.log_size, f, d.coeffs, d.block_start, next - d.block_start, partials,
-             tickets, results);
+    eap_body(lo, chunk, d.log_size, f, d.coeffs, iter_log, d.block_start, next - d.block_start, partials, tickets,
+             results, cur);
 }
-
 
 inline qm31 to_q(stwo_qm31 v) { return {{v.a, v.b}, {v.c, v.d}}; }
 inline stwo_qm31 from_q(qm31 v) { return {v.a.a, v.a.b, v.b.a, v.b.b}; }
@@ -296,17 +354,34 @@ void eap_factors(qm31 *f, stwo_spoint pt, uint32_t L) {
     }
 }
 
-uint32_t eap_blocks(uint32_t L) { return L <= (uint32_t)EAP_CHUNK_LOG ? 1u : 1u << (L - EAP_CHUNK_LOG); }
+uint32_t eap_blocks(uint32_t L, uint32_t iter_log) {
+    const uint32_t chunk_log = EAP_GROUP_LOG + iter_log;
+    return L <= chunk_log ? 1u : 1u << (L - chunk_log);
+}
+
+// Groups per CTA for a launch over these polynomials: the largest chunks that still
+// give at least two CTAs per SM.
+uint32_t eap_iter_log(const uint32_t *log_sizes, uint32_t n) {
+    const uint64_t want = 2ull * device_sm_count();
+    for (uint32_t k = EAP_ITER_LOG_MAX; k > EAP_ITER_LOG_MIN; k--) {
+        uint64_t blocks = 0;
+        for (uint32_t i = 0; i < n; i++) blocks += eap_blocks(log_sizes[i], k);
+        if (blocks >= want) return k;
+    }
+    return EAP_ITER_LOG_MIN;
+}
 
 }  // namespace
 
 size_t eval_at_points_scratch_bytes(const uint32_t *log_sizes, uint32_t n_polys) {
     size_t blocks = 0;
-    for (uint32_t i = 0; i < n_polys; i++) blocks += eap_blocks(log_sizes[i]);
+    for (uint32_t i = 0; i < n_polys; i++) blocks += eap_blocks(log_sizes[i], EAP_ITER_LOG_MIN);
     return blocks * sizeof(qm31) + ((size_t)n_polys * 4 + 15) / 16 * 16 + 256;
 }
 
-// scratch: partials followed by zeroed tickets (the kernel leaves them zero).
+// scratch: partials followed by zeroed tickets (the kernel leaves them zero); the
+// tickets sit after room for the partials of the smallest chunks, whatever a launch
+// chooses.
 int eval_at_points_async(const uint32_t *const *coeffs, const uint32_t *log_sizes, uint32_t n_polys,
                          const stwo_spoint *points, stwo_qm31 *results, void *scratch, size_t scratch_bytes,
                          bool tickets_zeroed, cudaStream_t st) {
@@ -315,7 +390,7 @@ int eval_at_points_async(const uint32_t *const *coeffs, const uint32_t *log_size
     size_t blocks_total = 0;
     for (uint32_t i = 0; i < n_polys; i++) {
         STWO_REQUIRE(log_sizes[i] <= 30, STWO_ERR_UNSUPPORTED_SIZE, "polynomial of log size %u unsupported", log_sizes[i]);
-        blocks_total += eap_blocks(log_sizes[i]);
+        blocks_total += eap_blocks(log_sizes[i], EAP_ITER_LOG_MIN);
     }
     uint32_t *tickets = reinterpret_cast<uint32_t *>(static_cast<char *>(scratch) + blocks_total * sizeof(qm31));
     if (!tickets_zeroed) STWO_CUDA_TRY(cudaMemsetAsync(tickets, 0, (size_t)n_polys * 4, st));
@@ -325,6 +400,7 @@ int eval_at_points_async(const uint32_t *const *coeffs, const uint32_t *log_size
     while (done < n_polys) {
         EapParams p{};
         uint32_t cnt = std::min<uint32_t>(EAP_MAX_POLYS, n_polys - done);
+        p.iter_log = eap_iter_log(log_sizes + done, cnt);
         uint32_t b = 0;
         for (uint32_t i = 0; i < cnt; i++) {
             uint32_t L = log_sizes[done + i];
@@ -332,7 +408,7 @@ int eval_at_points_async(const uint32_t *const *coeffs, const uint32_t *log_size
             p.log_size[i] = L;
             eap_factors(p.factors[i], points[done + i], L);
             p.block_start[i] = b;
-            b += eap_blocks(L);
+            b += eap_blocks(L, p.iter_log);
         }
         p.block_start[cnt] = b;
         p.n_polys = cnt;
@@ -348,19 +424,28 @@ int eval_at_points_async(const uint32_t *const *coeffs, const uint32_t *log_size
 }
 
 // eval_at_point for polynomials described in device memory (polys_dev: n_polys
-// EapDevPoly), at the device point point_dev (QM31 x then y). partials: total_blocks
-// QM31; tickets: n_polys zeroed words (left zeroed).
-int eval_at_points_dev_async(const void *polys_dev, uint32_t n_polys, uint32_t total_blocks, const void *point_dev,
-                             void *results, void *partials, uint32_t *tickets, cudaStream_t st) {
+// EapDevPoly, CTAs counted with eval_at_point_blocks(log size, iter_log)), at the
+// device point point_dev (QM31 x then y). partials: total_blocks QM31; tickets:
+// n_polys zeroed words (left zeroed).
+int eval_at_points_dev_async(const void *polys_dev, uint32_t n_polys, uint32_t iter_log, uint32_t total_blocks,
+                             const void *point_dev, void *results, void *partials, uint32_t *tickets, cudaStream_t st) {
     STWO_REQUIRE(n_polys >= 1 && total_blocks >= n_polys, STWO_ERR_INVALID_ARGUMENT, "eval_at_point descriptors");
+    STWO_REQUIRE(iter_log >= (uint32_t)EAP_ITER_LOG_MIN && iter_log <= (uint32_t)EAP_ITER_LOG_MAX,
+                 STWO_ERR_INVALID_ARGUMENT, "eval_at_point groups per CTA 2^%u", iter_log);
     eval_at_point_dev_kernel<<<total_blocks, EAP_THREADS, 0, st>>>(
-        static_cast<const EapDevPoly *>(polys_dev), n_polys, static_cast<const qm31 *>(point_dev),
+        static_cast<const EapDevPoly *>(polys_dev), n_polys, iter_log, static_cast<const qm31 *>(point_dev),
         static_cast<qm31 *>(partials), tickets, static_cast<qm31 *>(results));
     STWO_LAUNCH_CHECK("eval_at_point_dev_kernel");
     return STWO_OK;
 }
 
-uint32_t eval_at_point_blocks(uint32_t log_size) { return eap_blocks(log_size); }
+// CTAs of one polynomial of 2^log_size coefficients at 2^iter_log groups per CTA;
+// iter_log 0 asks for the most CTAs any launch uses (an upper bound for sizing).
+uint32_t eval_at_point_blocks(uint32_t log_size, uint32_t iter_log) {
+    return eap_blocks(log_size, iter_log ? iter_log : (uint32_t)EAP_ITER_LOG_MIN);
+}
+
+uint32_t eval_at_point_iter_log(const uint32_t *log_sizes, uint32_t n) { return eap_iter_log(log_sizes, n); }
 
 int extend_evaluate_async(const uint32_t *const *coeffs, const uint32_t *coeff_logs, uint32_t *const *outs,
                           uint32_t log_blowup, uint32_t n, const uint32_t *tw, uint64_t tree_size, cudaStream_t st) {
@@ -575,7 +660,7 @@ stwo_qm31 eval_at_point(const uint32_t *coeffs, uint32_t coeffs_size, stwo_qm31 
 // a fixed device array of this library instead of freshly allocated memory.
 //
 // The array is a file-scope __device__ variable: every GPU that loads the library
-// holds its 512.5 KiB until the process exits. Host code only knows a stand-in symbol
+// holds its 32.5 KiB until the process exits. Host code only knows a stand-in symbol
 // for it, so its device address is looked up with cudaGetSymbolAddress once per
 // device, on that device's first call (which therefore should come before any
 // stream capture), and the address is what the kernel receives.
@@ -584,9 +669,10 @@ stwo_qm31 eval_at_point(const uint32_t *coeffs, uint32_t coeffs_size, stwo_qm31 
 // completion tickets are cleared at the start of every call, and the partial sums
 // are fully rewritten before they are read.
 // ---------------------------------------------------------------------------
-constexpr uint32_t EAP_NOALLOC_MAX_LOG = 26;  // 2^26 coefficients, 2^15 partial sums
+constexpr uint32_t EAP_NOALLOC_MAX_LOG = 26;  // 2^26 coefficients, at most 2^11 partial sums
 constexpr size_t EAP_NOALLOC_BYTES =
-    (((size_t)1 << (EAP_NOALLOC_MAX_LOG - EAP_CHUNK_LOG)) * sizeof(qm31) + 16 + 256 + 255) / 256 * 256;
+    (((size_t)1 << (EAP_NOALLOC_MAX_LOG - EAP_CHUNK_LOG_MIN)) * sizeof(qm31) + 16 + 256 + 255) / 256 * 256;
+static_assert(EAP_NOALLOC_BYTES == 33280, "the documented size of the no-allocation scratch is 32.5 KiB");
 
 static __device__ __align__(256) unsigned char g_eap_noalloc_scratch[EAP_NOALLOC_BYTES];
 

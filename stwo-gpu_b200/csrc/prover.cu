@@ -61,9 +61,10 @@ int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const
                uint32_t *const *dst4, bool circle, cudaStream_t st, const void *alpha_dev);
 int wide_fib_dev_async(const uint32_t *const *trace_dev, uint32_t n_cols, uint32_t log_size, const uint32_t *powers_dev,
                        const uint32_t den_half[2], uint32_t *const *out4, cudaStream_t st);
-int eval_at_points_dev_async(const void *polys_dev, uint32_t n_polys, uint32_t total_blocks, const void *point_dev,
-                             void *results, void *partials, uint32_t *tickets, cudaStream_t st);
-uint32_t eval_at_point_blocks(uint32_t log_size);
+int eval_at_points_dev_async(const void *polys_dev, uint32_t n_polys, uint32_t iter_log, uint32_t total_blocks,
+                             const void *point_dev, void *results, void *partials, uint32_t *tickets, cudaStream_t st);
+uint32_t eval_at_point_blocks(uint32_t log_size, uint32_t iter_log);
+uint32_t eval_at_point_iter_log(const uint32_t *log_sizes, uint32_t n);
 
 namespace {
 
@@ -724,7 +725,7 @@ uint64_t job_device_bytes(const Job &j, bool own_twiddles) {
     b += tree(j.L + j.B) + tree(j.L + 1 + j.B);           // trace and composition trees
     b += 4 * r(4 * ne) + 4 * r(4 * neb);                  // composition, its evaluations
     b += r(16 * j.N);                                     // coefficient powers
-    const uint64_t eap_blocks = (uint64_t)j.N * eval_at_point_blocks(j.L) + 4 * eval_at_point_blocks(j.L + 1);
+    const uint64_t eap_blocks = (uint64_t)j.N * eval_at_point_blocks(j.L, 0) + 4 * eval_at_point_blocks(j.L + 1, 0);
     b += r(16 * eap_blocks);                              // eval_at_point partials
     b += 4 * r(4 * neb) + 4 * r(4 * nb);                  // quotients
     b += tree(j.L + 1 + j.B);                             // FRI first layer tree
@@ -858,10 +859,12 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     const uint32_t eap_n = N + 4;
     uint32_t eap_total = 0;
     std::vector<EapDevPoly> eap(eap_n);
+    std::vector<uint32_t> eap_logs(eap_n);
+    for (uint32_t i = 0; i < eap_n; i++) eap_logs[i] = i < N ? L : E;
+    const uint32_t eap_iter = eval_at_point_iter_log(eap_logs.data(), eap_n);
     for (uint32_t i = 0; i < eap_n; i++) {
-        const uint32_t lg = i < N ? L : E;
-        eap[i] = {i < N ? tpoly[i] : comp[i - N], lg, eap_total};
-        eap_total += eval_at_point_blocks(lg);
+        eap[i] = {i < N ? tpoly[i] : comp[i - N], eap_logs[i], eap_total};
+        eap_total += eval_at_point_blocks(eap_logs[i], eap_iter);
     }
     PV_ALLOC(eap_partials, qm31, eap_total);
 
@@ -1017,8 +1020,8 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         PV_TRY(record(2, capturing));
 
         // ---- 3. out-of-domain sampling
-        PV_TRY(eval_at_points_dev_async(dev_at(off_eap), eap_n, eap_total, dstate->oods, dsampled, eap_partials,
-                                        dtickets, st));
+        PV_TRY(eval_at_points_dev_async(dev_at(off_eap), eap_n, eap_iter, eap_total, dstate->oods, dsampled,
+                                        eap_partials, dtickets, st));
         fs_oods_kernel<<<1, 256, 0, st>>>(dstate, dsampled, powers, N, L, dqc, dqt);
         STWO_LAUNCH_CHECK("fs_oods_kernel");
         PV_TRY(record(3, capturing));
