@@ -66,6 +66,19 @@ __host__ __device__ __forceinline__ uint64_t mac64(uint64_t acc, uint32_t a, uin
 }
 // A value congruent to acc mod P, below 2^34.
 __host__ __device__ __forceinline__ uint64_t fold64(uint64_t acc) { return (acc & P) + (acc >> 31); }
+#ifdef __CUDACC__
+// fold64 as one wide multiply-add on the FMA pipe: acc = hi * 2^32 + lo = 2 hi + lo
+// (mod P), below 3 * 2^32 (so below 2^34 like fold64). After it, four products of
+// values below 2^31 still fit: 3 * 2^32 + 4 (2^31 - 1)^2 < 2^64. `two` must be 2,
+// passed at run time so that the compiler keeps the multiply-add instead of turning
+// it into shifts and adds on the ALU pipe, which the surrounding field arithmetic
+// already keeps busy.
+__device__ __forceinline__ uint64_t fold64_fma(uint64_t acc, uint32_t two) {
+    uint64_t r;
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(r) : "r"((uint32_t)(acc >> 32)), "r"(two), "l"(acc & 0xffffffffull));
+    return r;
+}
+#endif
 // acc mod P, canonical.
 __host__ __device__ __forceinline__ uint32_t reduce64_p(uint64_t acc) {
     uint64_t s = (acc & P) + (acc >> 31);

@@ -37,7 +37,8 @@ __global__ void accumulate_kernel(const __grid_constant__ Acc4 p, uint64_t n4, u
 }
 
 constexpr int WF_MAX_COLS = 2048;
-constexpr int WF_PREFETCH = 6;  // column loads in flight per thread (a multiple of the fold period 3)
+constexpr int WF_PREFETCH = 8;  // column loads in flight per thread (a multiple of the fold period 4)
+static_assert(WF_PREFETCH % 4 == 0, "the fold cadence needs groups of a multiple of 4 columns");
 
 // Trace column pointers in the parameter block (CAP of them) or, for CAP == 1, in a
 // device table.
@@ -51,13 +52,14 @@ struct WideFibParams {
     const qm31 *powers_dev;   // device powers
     uint32_t n_cols;
     uint32_t log_size;
+    uint32_t two;             // 2 (fold64_fma)
 };
 
 // Powers on the device (plain QM31). Two rows per thread (8-byte loads); the column
 // loop issues WF_PREFETCH loads before it consumes them, and the small per-thread
 // state keeps four CTAs of 256 threads per SM, so enough loads are in flight to cover
 // DRAM latency. Each coordinate of the sum is a 64-bit multiply-accumulate of
-// canonical values, folded after every third column.
+// canonical values, folded (fold64_fma) after every fourth column.
 template <int CAP>
 __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant__ WideFibParams<CAP> p) {
     const uint64_t n = 1ull << p.log_size;
@@ -99,8 +101,8 @@ __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant_
                     acc[r][1] = mac64(acc[r][1], cons, w.a.b);
                     acc[r][2] = mac64(acc[r][2], cons, w.b.a);
                     acc[r][3] = mac64(acc[r][3], cons, w.b.b);
-                    if (u % 3 == 2)
-                        for (int c = 0; c < 4; c++) acc[r][c] = fold64(acc[r][c]);
+                    if (u % 4 == 3)
+                        for (int c = 0; c < 4; c++) acc[r][c] = fold64_fma(acc[r][c], p.two);
                     s0[r] = s1[r];
                     s1[r] = m31_sqr(buf[u][r]);
                 }
@@ -149,6 +151,7 @@ int wide_fib_launch(const uint32_t *const *trace, const uint32_t *const *trace_d
     }
     p->n_cols = n_cols;
     p->log_size = log_size;
+    p->two = 2;
     p->powers_dev = reinterpret_cast<const qm31 *>(powers_dev);
     const uint64_t n = 1ull << log_size, pairs = (n + 1) / 2;
     if (powers_dev) {

@@ -212,7 +212,8 @@ __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t
         uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
         // 64-bit multiply-accumulates of canonical values, folded after every fourth
         // term: a fold leaves less than 2^34, and four products of values below 2^31 - 1
-        // add less than 2^64 - 2^34.
+        // add less than 2^64 - 2^34. (The folds stay on the ALU pipe here: as FMA-pipe
+        // multiply-adds, fold64_fma, this loop measured 5% slower.)
         auto term = [&](uint32_t v, uint32_t i) {
             const qm31 w = F2[i];
             s0 = mac64(s0, v, w.a.a);

@@ -30,10 +30,10 @@ namespace {
 
 using QuotParams = QuotParamsT<QUOT_MAX_COLS, QUOT_MAX_SAMPLES>;
 #ifndef QUOT_PREFETCH_N
-#define QUOT_PREFETCH_N 6
+#define QUOT_PREFETCH_N 8
 #endif
 constexpr int QUOT_PREFETCH = QUOT_PREFETCH_N;  // column loads per group (two groups in flight)
-static_assert(QUOT_PREFETCH % 3 == 0, "the fold cadence needs groups of a multiple of 3 columns");
+static_assert(QUOT_PREFETCH % 4 == 0, "the fold cadence needs groups of a multiple of 4 columns");
 
 // The kernel reads its parameters through get(): by value from the parameter block,
 // or from a device-resident block (the prover's, filled by the device channel).
@@ -82,7 +82,7 @@ __device__ __forceinline__ cm31 quot_den(const QP &p, uint32_t b, uint32_t px, u
 template <bool COLS_ON_DEVICE, bool STAGE, int NB, class PR>
 __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ PR pr,
                                                         const uint32_t *const *__restrict__ dev_cols,
-                                                        uint32_t n_stage) {
+                                                        uint32_t n_stage, uint32_t two) {
     const auto &p = pr.get();
     extern __shared__ uint4 q_smem[];
     qm31 *s_c2 = reinterpret_cast<qm31 *>(q_smem);
@@ -152,8 +152,8 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                 }
             };
             // 64-bit multiply-accumulates of canonical values (products below 2^62),
-            // folded after every third column: a folded sum (below 2^34) plus three
-            // products stays below 2^64. The group size is a multiple of 3.
+            // folded (fold64_fma) after every fourth column: a folded sum plus four
+            // products stays below 2^64. The group size is a multiple of 4.
             auto consume = [&](uint32_t jb, const uint2 (&v)[QUOT_PREFETCH]) {
 #pragma unroll
                 for (int u = 0; u < QUOT_PREFETCH; u++) {
@@ -163,9 +163,9 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                     s0[0][2] = mac64(s0[0][2], v[u].x, c.b.a); s0[0][3] = mac64(s0[0][3], v[u].x, c.b.b);
                     s0[1][0] = mac64(s0[1][0], v[u].y, c.a.a); s0[1][1] = mac64(s0[1][1], v[u].y, c.a.b);
                     s0[1][2] = mac64(s0[1][2], v[u].y, c.b.a); s0[1][3] = mac64(s0[1][3], v[u].y, c.b.b);
-                    if (u % 3 == 2)
+                    if (u % 4 == 3)
                         for (int s = 0; s < 2; s++)
-                            for (int t = 0; t < 4; t++) s0[s][t] = fold64(s0[s][t]);
+                            for (int t = 0; t < 4; t++) s0[s][t] = fold64_fma(s0[s][t], two);
                 }
             };
             uint2 va[QUOT_PREFETCH], vb[QUOT_PREFETCH];
@@ -280,9 +280,9 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
     auto launch = [&](auto nb) {
         constexpr int NBV = decltype(nb)::value;
         if (cols_on_device)
-            quotients_kernel<true, true, NBV><<<(unsigned)blocks, 256, smem, st>>>(*holder, cols, n_samples);
+            quotients_kernel<true, true, NBV><<<(unsigned)blocks, 256, smem, st>>>(*holder, cols, n_samples, 2u);
         else
-            quotients_kernel<false, true, NBV><<<(unsigned)blocks, 256, smem, st>>>(*holder, nullptr, n_samples);
+            quotients_kernel<false, true, NBV><<<(unsigned)blocks, 256, smem, st>>>(*holder, nullptr, n_samples, 2u);
     };
     switch (n_batches) {
     case 1: launch(std::integral_constant<int, 1>{}); break;
@@ -303,7 +303,7 @@ int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t 
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    quotients_kernel<false, true, 1><<<(unsigned)blocks, 256, smem, st>>>(QuotByRef{p_dev}, nullptr, n_samples);
+    quotients_kernel<false, true, 1><<<(unsigned)blocks, 256, smem, st>>>(QuotByRef{p_dev}, nullptr, n_samples, 2u);
     STWO_LAUNCH_CHECK("quotients_kernel");
     return STWO_OK;
 }
