@@ -160,7 +160,9 @@ int stwo_reserve_device_memory(uint64_t bytes);
 int stwo_autotune(char *report, size_t report_cap);
 /* Sets one tunable by name: fft_ept_contig_small / fft_ept_contig_large /
  * fft_ept_strided (5 or 6), merkle_sub_threads (128, 256 or 512), merkle_sub_spread
- * (0..5: log2 of the bottom-level nodes each thread hashes). */
+ * (0..5: log2 of the bottom-level nodes each thread hashes), eval_at_point_groups_log
+ * (2..4: log2 of the 8192-coefficient groups each eval_at_point CTA folds; 0, the
+ * default, chooses per launch). */
 int stwo_set_tunable(const char *name, int value);
 /* Number of kernel launches the library has made in this process (all threads). */
 uint64_t stwo_kernel_launches(void);

@@ -103,6 +103,12 @@ int stwo_set_tunable(const char *name, int value) {
         set_tunable(TUNE_MERKLE_SUB_SPREAD, value);
         return STWO_OK;
     }
+    if (n == "eval_at_point_groups_log") {
+        STWO_REQUIRE(value == 0 || (value >= 2 && value <= 4), STWO_ERR_INVALID_ARGUMENT,
+                     "eval_at_point_groups_log must be 0 (chosen per launch) or 2..4");
+        set_tunable(TUNE_EAP_GROUPS_LOG, value);
+        return STWO_OK;
+    }
     return set_error(STWO_ERR_INVALID_ARGUMENT, "unknown tunable %s", name);
 }
 

@@ -107,6 +107,7 @@ enum Tunable {
     TUNE_FFT_EPT_STRIDED,       // same, strided passes
     TUNE_MERKLE_SUB_THREADS,    // CTA size of the multi-layer Merkle kernel (log2 + 1 layers per launch)
     TUNE_MERKLE_SUB_SPREAD,     // log2 bottom-level nodes per thread of that kernel (0..5)
+    TUNE_EAP_GROUPS_LOG,        // eval_at_point: log2 groups of 8192 coefficients per CTA (2..4), 0 = per launch
     TUNE_COUNT
 };
 int tunable(Tunable t);

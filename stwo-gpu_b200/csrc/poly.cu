@@ -361,8 +361,10 @@ uint32_t eap_blocks(uint32_t L, uint32_t iter_log) {
 }
 
 // Groups per CTA for a launch over these polynomials: the largest chunks that still
-// give at least two CTAs per SM.
+// give at least two CTAs per SM (unless the eval_at_point_groups_log tunable fixes it).
 uint32_t eap_iter_log(const uint32_t *log_sizes, uint32_t n) {
+    const int forced = tunable(TUNE_EAP_GROUPS_LOG);
+    if (forced >= EAP_ITER_LOG_MIN && forced <= EAP_ITER_LOG_MAX) return (uint32_t)forced;
     const uint64_t want = 2ull * device_sm_count();
     for (uint32_t k = EAP_ITER_LOG_MAX; k > EAP_ITER_LOG_MIN; k--) {
         uint64_t blocks = 0;

@@ -190,3 +190,35 @@ def test_eval_at_points_batched(stwo, oracle):
         got = res.to_numpy()
         for i, (c, (x, y)) in enumerate(zip(cs, pts)):
             assert tuple(int(v) for v in got[i]) == oracle.eval_at_point(c, x, y)
+
+
+@pytest.mark.parametrize("groups_log", [0, 2, 3, 4])
+def test_eval_at_points_every_chunk_size(stwo, oracle, groups_log):
+    """Each forced CTA chunk (2^(13 + groups_log) coefficients) and the per-launch
+    choice (0) give the oracle's values: sizes below a warp's 1024 coefficients
+    (ragged), single groups, chunks with empty trailing groups and several chunks a
+    polynomial."""
+    L = stwo._lib
+    lib = L.lib()
+    r = rng(91 + groups_log)
+    logs = [0, 3, 9, 10, 13, 14, 16, 17, 18, 19]
+    cs = [m31(r, 1 << lg) for lg in logs]
+    bufs = [stwo.BaseFieldVec.from_numpy(c) for c in cs]
+    pts = [random_circle_point(r) for _ in logs]
+    sp = (L.SPoint * len(logs))(*[L.SPoint(L.QM31(*x), L.QM31(*y)) for x, y in pts])
+    scratch_n = lib.stwo_eval_at_points_scratch_bytes(L.u32_array(logs), len(logs))
+    scratch = stwo.BaseFieldVec.new_uninitialized(scratch_n // 4 + 1)
+    res = stwo.SecureFieldVec.new_uninitialized(len(logs))
+    L.check(lib.stwo_set_tunable(b"eval_at_point_groups_log", groups_log))
+    try:
+        for _ in range(2):  # tickets left zeroed by the first call serve the second
+            L.check(lib.stwo_eval_at_points(L.ptr_array([b.device_ptr for b in bufs]), L.u32_array(logs), len(logs),
+                                            sp, res.device_ptr, scratch.device_ptr, scratch_n, None))
+            L.check(lib.stwo_stream_synchronize(None))
+            got = res.to_numpy()
+            for i, (c, (x, y)) in enumerate(zip(cs, pts)):
+                assert tuple(int(v) for v in got[i]) == oracle.eval_at_point(c, x, y), logs[i]
+    finally:
+        lib.stwo_set_tunable(b"eval_at_point_groups_log", 0)
+    with pytest.raises(L.StwoError):
+        L.check(lib.stwo_set_tunable(b"eval_at_point_groups_log", 5))

@@ -276,9 +276,9 @@ def test_server_shutdown_with_queued_jobs_is_clean():
 
 
 def test_tunables_change_speed_not_results():
-    """Every FFT elements-per-thread, Merkle layers-per-launch and Merkle
-    nodes-per-thread setting gives the same proof bytes; stwo_autotune reports its
-    choices as JSON."""
+    """Every FFT elements-per-thread, Merkle layers-per-launch, Merkle nodes-per-thread
+    and eval_at_point chunk setting gives the same proof bytes; stwo_autotune reports
+    its choices as JSON."""
     import ctypes as C
     import json
     stwo = load_package()
@@ -292,7 +292,8 @@ def test_tunables_change_speed_not_results():
     base_b, _ = stwo.prove_wide_fib(job_of(tb), b0, b1)
     settings = [("fft_ept_contig_small", 5), ("fft_ept_contig_large", 5), ("fft_ept_strided", 5),
                 ("merkle_sub_threads", 128), ("merkle_sub_threads", 512), ("merkle_sub_spread", 0),
-                ("merkle_sub_spread", 5)]
+                ("merkle_sub_spread", 5), ("eval_at_point_groups_log", 2), ("eval_at_point_groups_log", 3),
+                ("eval_at_point_groups_log", 4)]
     try:
         for name, value in settings:
             stwo._lib.check(lib.stwo_set_tunable(name.encode(), value))
@@ -311,5 +312,5 @@ def test_tunables_change_speed_not_results():
         assert stwo.prove_wide_fib(job_of(tb), b0, b1)[0] == base_b
     finally:
         for name, value in [("fft_ept_contig_small", 6), ("fft_ept_contig_large", 6), ("fft_ept_strided", 6),
-                            ("merkle_sub_threads", 256), ("merkle_sub_spread", 3)]:
+                            ("merkle_sub_threads", 256), ("merkle_sub_spread", 3), ("eval_at_point_groups_log", 0)]:
             lib.stwo_set_tunable(name.encode(), value)
