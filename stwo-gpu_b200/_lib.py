@@ -163,8 +163,12 @@ def last_error():
 
 
 def check(status):
+    """Raise on a non-zero status; the raise consumes the recorded message, so a later
+    check_last() does not see it again."""
     if status != 0:
-        raise StwoError(f"stwo_b200 status {status}: {last_error()}")
+        msg = last_error()
+        clear_error()
+        raise StwoError(f"stwo_b200 status {status}: {msg}")
 
 
 def clear_error():
