@@ -335,6 +335,8 @@ typedef struct {
     uint8_t *proof;      /* malloc'd proof bytes (free with stwo_free_proof), NULL on error */
     uint64_t proof_len;
     double submit_ms, start_ms, done_ms; /* stwo_server_now_ms() clock */
+    double device_done_ms; /* device time at which the job's last GPU operation ended, in ms
+                              after the server's last stwo_server_mark_epoch(); -1 before any */
     stwo_prove_stats stats;
 } stwo_server_result;
 
@@ -359,6 +361,10 @@ void stwo_server_stats(stwo_prover_server *server, uint32_t *pending, uint32_t *
  * the first reuse of a slab). Off with STWO_SERVER_GRAPHS=0 at creation. */
 void stwo_server_graph_stats(stwo_prover_server *server, uint64_t *slab_reuses, uint64_t *graph_replays);
 double stwo_server_now_ms(void);
+/* Records the server's device epoch now (on an idle stream of its own) and waits for
+ * it: later results carry device_done_ms relative to it, so the device-side span of a
+ * batch submitted after the mark is the largest device_done_ms of its results. */
+int stwo_server_mark_epoch(stwo_prover_server *server);
 /* Drops queued jobs, waits for running ones, frees everything (including unpolled proofs). */
 void stwo_server_destroy(stwo_prover_server *server);
 

@@ -53,7 +53,7 @@ class ServerResult(C.Structure):
     """stwo_server_result: one finished job of the proof server."""
     _fields_ = [("job_id", u64), ("status", C.c_int), ("error", C.c_char * 256), ("proof", C.POINTER(C.c_uint8)),
                 ("proof_len", u64), ("submit_ms", C.c_double), ("start_ms", C.c_double), ("done_ms", C.c_double),
-                ("stats", ProveStats)]
+                ("device_done_ms", C.c_double), ("stats", ProveStats)]
 
 
 class StwoError(RuntimeError):
@@ -137,6 +137,7 @@ SIGNATURES = [
     ("stwo_server_stats", None, [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u64)]),
     ("stwo_server_graph_stats", None, [vp, C.POINTER(u64), C.POINTER(u64)]),
     ("stwo_server_now_ms", C.c_double, []),
+    ("stwo_server_mark_epoch", C.c_int, [vp]),
     ("stwo_server_destroy", None, [vp]),
 ]
 

@@ -89,9 +89,13 @@ int pool_alloc(void **p, size_t bytes, cudaStream_t st);
 // microseconds, more than a small proof's remaining device work), then yields its CPU
 // core on a blocking-sync event; the proof server's workers do, so many in-flight large
 // jobs do not compete for host cores. Other threads spin (cudaStreamSynchronize).
+// Every wait records a timing-capable event, so the device time at which the stream's
+// work ended can be read afterwards (last_wait_event).
 extern thread_local bool t_blocking_wait;
 extern thread_local uint32_t t_spin_us;
 int wait_stream(cudaStream_t st);
+// The event of this thread's last wait_stream on the current device, or null.
+cudaEvent_t last_wait_event();
 
 // Pinned host memory of at least `bytes`, owned by the calling thread and reused by its
 // next call: the staging area of the small device<->host copies (roots, sampled values,

@@ -142,19 +142,19 @@ int reserve_pool(uint64_t bytes) {
 }
 
 int wait_stream(cudaStream_t st) {
-    if (!t_blocking_wait) {
-        STWO_CUDA_TRY(cudaStreamSynchronize(st));
-        return STWO_OK;
-    }
     int dev = 0;
     STWO_CUDA_TRY(cudaGetDevice(&dev));
     if (!t_event.ev || t_event.device != dev) {
         if (t_event.ev) cudaEventDestroy(t_event.ev);
         t_event.ev = nullptr;
-        STWO_CUDA_TRY(cudaEventCreateWithFlags(&t_event.ev, cudaEventBlockingSync | cudaEventDisableTiming));
+        STWO_CUDA_TRY(cudaEventCreateWithFlags(&t_event.ev, cudaEventBlockingSync));
         t_event.device = dev;
     }
     STWO_CUDA_TRY(cudaEventRecord(t_event.ev, st));
+    if (!t_blocking_wait) {
+        STWO_CUDA_TRY(cudaStreamSynchronize(st));
+        return STWO_OK;
+    }
     if (t_spin_us) {
         const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(t_spin_us);
         for (;;) {
@@ -166,6 +166,12 @@ int wait_stream(cudaStream_t st) {
     }
     STWO_CUDA_TRY(cudaEventSynchronize(t_event.ev));
     return STWO_OK;
+}
+
+cudaEvent_t last_wait_event() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || t_event.device != dev) return nullptr;
+    return t_event.ev;
 }
 
 int sync_default_stream(int status) {

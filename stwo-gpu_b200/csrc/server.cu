@@ -58,6 +58,9 @@ struct stwo_prover_server {
     bool use_priorities = true; // per-job stream priority by job size
     bool use_graphs = true;     // same-shape jobs reuse a worker's slab and proof graph
     std::atomic<uint64_t> slab_reuses{0}, graph_replays{0};
+    cudaStream_t epoch_stream = nullptr;  // idle stream for the device epoch
+    cudaEvent_t epoch = nullptr;          // timing event: device time zero of device_done_ms
+    std::atomic<bool> epoch_set{false};
     uint32_t running = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -159,6 +162,14 @@ struct stwo_prover_server {
                 strncpy(r.error, stwo_last_error(), sizeof(r.error) - 1);
             }
             r.done_ms = steady_ms();
+            r.device_done_ms = -1.0;
+            if (r.status == STWO_OK && epoch_set.load()) {
+                // The prover's last wait recorded an event after its final device work.
+                float ms = 0.f;
+                cudaEvent_t ev = last_wait_event();
+                if (ev && cudaEventElapsedTime(&ms, epoch, ev) == cudaSuccess) r.device_done_ms = ms;
+                else cudaGetLastError();
+            }
             // A queued job of the same shape takes this one's place (and budget) at once.
             PendingJob next;
             {
@@ -240,6 +251,15 @@ stwo_prover_server *stwo_server_create(uint32_t n_workers, uint64_t device_budge
         const uint64_t want = std::min<uint64_t>(device_budget_bytes, free_b > margin ? free_b - margin : 0);
         if (reserve_pool(want) != STWO_OK) clear_error();  // a smaller pool only costs speed
     }
+    if (cudaStreamCreateWithFlags(&s->epoch_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&s->epoch) != cudaSuccess) {
+        set_error(STWO_ERR_CUDA, "server epoch event creation failed");
+        if (s->epoch_stream) cudaStreamDestroy(s->epoch_stream);
+        cudaFree(s->tw);
+        cudaFree(s->itw);
+        delete s;
+        return nullptr;
+    }
     for (uint32_t i = 0; i < n_workers; i++) s->workers.emplace_back([s] { s->worker(); });
     return s;
 }
@@ -311,6 +331,19 @@ void stwo_server_stats(stwo_prover_server *s, uint32_t *pending, uint32_t *runni
     if (device_bytes_in_use) *device_bytes_in_use = s->in_use;
 }
 
+int stwo_server_mark_epoch(stwo_prover_server *s) {
+    STWO_REQUIRE(s, STWO_ERR_INVALID_ARGUMENT, "null server");
+    int prev = 0;
+    STWO_CUDA_TRY(cudaGetDevice(&prev));
+    STWO_CUDA_TRY(cudaSetDevice(s->device));
+    cudaError_t e = cudaEventRecord(s->epoch, s->epoch_stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(s->epoch);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return set_error(STWO_ERR_CUDA, "server epoch: %s", cudaGetErrorString(e));
+    s->epoch_set.store(true);
+    return STWO_OK;
+}
+
 void stwo_server_graph_stats(stwo_prover_server *s, uint64_t *slab_reuses, uint64_t *graph_replays) {
     if (!s) return;
     if (slab_reuses) *slab_reuses = s->slab_reuses.load();
@@ -329,6 +362,8 @@ void stwo_server_destroy(stwo_prover_server *s) {
     for (auto &r : s->done) free(r.proof);
     cudaFree(s->tw);
     cudaFree(s->itw);
+    cudaEventDestroy(s->epoch);
+    cudaStreamDestroy(s->epoch_stream);
     delete s;
 }
 

@@ -152,8 +152,15 @@ class ProofServer:
         L.clear_error()
         L.check(L.lib().stwo_server_submit_device(self._s, job_id, C.byref(job.c()), a0_dev, a1_dev))
 
+    def mark_epoch(self):
+        """Sets the device epoch of device_done_ms (records and waits for an event on an
+        idle stream of the server's): call it with nothing running, before a batch."""
+        L.check(L.lib().stwo_server_mark_epoch(self._s))
+
     def poll(self, max_results=64, timeout_ms=-1):
-        """Finished jobs as dicts: job_id, status, error, proof, submit/start/done ms, stats."""
+        """Finished jobs as dicts: job_id, status, error, proof, submit/start/done ms (host
+        clock), device_done_ms (device time of the job's last GPU operation after the
+        last mark_epoch, or -1), stats."""
         buf = (L.ServerResult * max_results)()
         n = L.lib().stwo_server_poll(self._s, buf, max_results, timeout_ms)
         out = []
@@ -163,7 +170,7 @@ class ProofServer:
                 L.lib().stwo_free_proof(r.proof)
             out.append({"job_id": r.job_id, "status": r.status, "error": r.error.decode(errors="replace"),
                         "proof": proof, "submit_ms": r.submit_ms, "start_ms": r.start_ms, "done_ms": r.done_ms,
-                        "stats": r.stats.as_dict()})
+                        "device_done_ms": r.device_done_ms, "stats": r.stats.as_dict()})
         return out
 
     def stats(self):

@@ -134,6 +134,31 @@ def test_server_proofs_equal_single_job_proofs(priorities, monkeypatch):
         assert r["submit_ms"] <= r["start_ms"] <= r["done_ms"]
 
 
+def test_server_device_completion_times():
+    """Before any epoch mark a result carries device_done_ms = -1; after mark_epoch each
+    finished job carries the device time of its last GPU operation, after the mark and
+    no later than the host saw the job finish."""
+    stwo = load_package()
+    jobs = [(0, (9, 24, 1, 3, 5), 11), (1, (11, 16, 1, 3, 5), 12), (2, (10, 40, 1, 3, 5), 13)]
+    with stwo.ProofServer(n_workers=2, device_budget_bytes=8 << 30, max_domain_log=16) as srv:
+        a0, a1 = stwo.wide_fib_inputs(9, 10)
+        srv.submit(99, job_of((9, 24, 1, 3, 5)), a0, a1)
+        (r,) = srv.poll(timeout_ms=-1)
+        assert r["status"] == 0 and r["device_done_ms"] == -1.0
+        t0 = srv.now_ms()
+        srv.mark_epoch()
+        for jid, t, seed in jobs:
+            a0, a1 = stwo.wide_fib_inputs(t[0], seed)
+            srv.submit(jid, job_of(t), a0, a1)
+        got = {}
+        while len(got) < len(jobs):
+            for r in srv.poll(timeout_ms=-1):
+                assert r["status"] == 0, r["error"]
+                got[r["job_id"]] = r
+    for r in got.values():
+        assert 0.0 < r["device_done_ms"] <= r["done_ms"] - t0 + 1.0, r
+
+
 @pytest.mark.parametrize("graphs", ["1", "0"])
 @pytest.mark.parametrize("workers", [1, 3])
 def test_server_same_shape_runs_replay_equal_proofs(graphs, workers, monkeypatch):
