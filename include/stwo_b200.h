@@ -308,7 +308,8 @@ void stwo_free_proof(uint8_t *proof);
  * the same shape, twiddle tree and device reuses it, every buffer at the same address,
  * so the proof's launch sequence (trace to query words) is captured as a CUDA graph on
  * that second call and replayed with one launch from the third on. A call with a
- * different shape frees the memory first. Needs the caller's twiddle tree; jobs with
+ * different shape, or after any stwo_set_tunable / stwo_autotune, frees the memory
+ * first and starts over. Needs the caller's twiddle tree; jobs with
  * log_n_rows < 3 are proved without reuse, and on the legacy default stream (NULL) the
  * memory is reused but no graph is captured. A cache serves one thread and one stream
  * at a time; it holds up to stwo_wide_fib_prove_device_bytes(job, 0) bytes between

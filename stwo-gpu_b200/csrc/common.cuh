@@ -116,6 +116,9 @@ enum Tunable {
 };
 int tunable(Tunable t);
 void set_tunable(Tunable t, int v);
+// Counts set_tunable calls: a captured launch sequence is valid only for the settings
+// it was captured under.
+uint64_t tunables_generation();
 
 // Stream handle conversion for the C ABI.
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }

@@ -792,8 +792,12 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     STWO_CUDA_TRY(cudaGetDevice(&dev));
     const bool cacheable = cache && tw_in && itw_in && L >= 3;
     const uint32_t key[5] = {j.L, j.N, j.B, j.n_queries, j.pow_bits};
+    // Launch shapes (and the eval_at_point descriptors) follow the tunables, so a change
+    // of any tunable retires the cache.
+    const uint64_t tgen = tunables_generation();
     const bool hit = cacheable && cache->valid && cache->device == dev && cache->tw == tw_in &&
-                     cache->itw == itw_in && cache->tsz == tsz_in && memcmp(cache->key, key, sizeof(key)) == 0;
+                     cache->itw == itw_in && cache->tsz == tsz_in && memcmp(cache->key, key, sizeof(key)) == 0 &&
+                     cache->tunables_gen == tgen;
     if (cache && cache->valid && !hit) prove_cache_release(cache, st);
     // Phase events are recorded whenever the launch sequence may be captured, so that a
     // graph always carries them.
@@ -1213,6 +1217,7 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         if (cache_ok && !hit) {
             cache->valid = true;
             memcpy(cache->key, key, sizeof(key));
+            cache->tunables_gen = tgen;
             cache->tw = tw_in;
             cache->itw = itw_in;
             cache->tsz = tsz_in;

@@ -15,6 +15,7 @@ namespace stwo {
 struct ProveCache {
     bool valid = false;
     uint32_t key[5] = {};  // log_n_rows, n_columns, log_blowup, n_queries, pow_bits
+    uint64_t tunables_gen = 0;  // tunables_generation() when the slab and graph were made
     const uint32_t *tw = nullptr, *itw = nullptr;
     uint64_t tsz = 0;
     int device = -1;

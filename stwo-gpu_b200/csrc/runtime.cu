@@ -30,7 +30,12 @@ namespace {
 std::atomic<int> g_tunables[TUNE_COUNT] = {{6}, {6}, {6}, {256}, {3}, {0}};
 }
 int tunable(Tunable t) { return g_tunables[t].load(std::memory_order_relaxed); }
-void set_tunable(Tunable t, int v) { g_tunables[t].store(v, std::memory_order_relaxed); }
+std::atomic<uint64_t> g_tunables_gen{0};
+void set_tunable(Tunable t, int v) {
+    g_tunables[t].store(v, std::memory_order_relaxed);
+    g_tunables_gen.fetch_add(1, std::memory_order_relaxed);
+}
+uint64_t tunables_generation() { return g_tunables_gen.load(std::memory_order_relaxed); }
 thread_local uint64_t t_kernel_launches = 0;
 
 int device_sm_count() {

@@ -235,6 +235,35 @@ def test_cached_proofs_replay_and_equal_plain_proofs(stream_kind):
             stwo.prove_wide_fib(job_of(seq[0]), a0, a1, cache=c2)
 
 
+def test_cached_proofs_recapture_after_a_tunable_changes():
+    """Changing a tunable between cached proofs of one shape retires the captured
+    sequence (the eval_at_point chunking changes its descriptors and grid): the next
+    proof runs afresh, the one after captures again, and every proof equals the plain
+    call's."""
+    import torch
+    stwo = load_package()
+    lib = stwo._lib.lib()
+    s = torch.cuda.Stream()
+    tree = stwo.CudaBackend.precompute_twiddles(stwo.CanonicCoset(16).half_coset())
+    t = (13, 300, 1, 3, 5)  # 300 polynomials: the per-launch choice is 4 groups a CTA
+    plan = [None, None, None, 2, None, None, 0, None]  # a tunable set at proofs 3 and 6
+    try:
+        with stwo.ProveCache() as cache:
+            replays = []
+            for k, g in enumerate(plan):
+                if g is not None:
+                    stwo._lib.check(lib.stwo_set_tunable(b"eval_at_point_groups_log", g))
+                a0, a1 = stwo.wide_fib_inputs(t[0], 4000 + k)
+                want, _ = stwo.prove_wide_fib(job_of(t), a0, a1)
+                got, _ = stwo.prove_wide_fib(job_of(t), a0, a1, twiddles=tree, stream=s.cuda_stream, cache=cache)
+                assert got == want, (k, g)
+                replays.append(cache.stats()["graph_replays"])
+            assert replays == [0, 0, 1, 1, 1, 2, 2, 2]
+            cache.close(s.cuda_stream)
+    finally:
+        lib.stwo_set_tunable(b"eval_at_point_groups_log", 0)
+
+
 def test_server_respects_the_memory_budget():
     stwo = load_package()
     t = (10, 32, 1, 3, 5)
