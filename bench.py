@@ -375,6 +375,25 @@ def kernel_suite(stwo, reps=5):
         rec["equal"] = all(torch.equal(a, c) for a, c in zip(rout, outq))
         R.cuda_free_memory(dcols)
     out["quotients"] = rec
+    del cols, outq
+
+    # (f) eval_at_point: 32 polynomials of 2^22 coefficients, each at its own point, in
+    # one batched call (the OODS step's shape). The reference library's kernel is not
+    # run: its shared-memory arrays alias (eval_at_point.cu:17-18).
+    lg, npoly = 22, 32
+    polys = [rand(1 << lg) for _ in range(npoly)]
+    logs = (C.c_uint32 * npoly)(*([lg] * npoly))
+    spts = (L.SPoint * npoly)(*[L.SPoint(rq(), rq()) for _ in range(npoly)])
+    eap_scratch_n = lib.stwo_eval_at_points_scratch_bytes(logs, npoly)
+    eap_scratch = torch.zeros(eap_scratch_n // 4 + 1, dtype=torch.int32, device=dev)
+    eap_res = torch.empty(4 * npoly, dtype=torch.int32, device=dev)
+    pp = ptrs(polys)
+    t = timed(lambda: L.check(lib.stwo_eval_at_points(pp, logs, npoly, spts, eap_res.data_ptr(),
+                                                      eap_scratch.data_ptr(), eap_scratch_n, sptr)))
+    b = npoly * 4 * (1 << lg)
+    out["eval_at_point"] = {"ms": t, "gbs": b / t / 1e6, "frac_hbm": b / t / 1e6 / peak,
+                            "workload": "32 polynomials x 2^22 coefficients, one point each"}
+    del polys
     for k, v in out.items():
         if "reference_ms" in v:
             v["speedup_vs_reference"] = v["reference_ms"] / v["ms"]
