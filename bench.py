@@ -471,6 +471,7 @@ def run_reference(args, rank, world):
 def fft_roofline(stwo, dev, rank, args):
     """The M31 circle FFT step (8 columns at log 24: interpolate, extend-evaluate
     blowup 4), its HBM roofline and the reference CUDA library on the same step."""
+    import ctypes as C
     import torch
     L = stwo._lib
     lib = L.lib()
@@ -529,10 +530,36 @@ def fft_roofline(stwo, dev, rank, args):
     if rank == 0 and not args.no_suite:
         ns = argparse.Namespace(**vars(args))
         ref_gpu = reference_gpu_timing(ns, evals, lg, lb, ncols, tw, itw, tree_size)
+    # The integer ceiling, measured live: the passes' own butterfly on register operands
+    # (stwo_probe_m31_butterflies), against the step's butterflies (interpolate: lg
+    # layers of 2^(lg-1); evaluate: lg layers of 2^(N-1), the lb top layers of the
+    # zero-padded input being copies).
+    bf_step = ncols * lg * ((1 << (lg - 1)) + (1 << (N - 1)))
+    sink = torch.empty(2048 * torch.cuda.get_device_properties(dev).multi_processor_count, dtype=torch.int32,
+                       device=dev)
+    nbf = C.c_uint64()
+
+    def probe():
+        L.check(lib.stwo_probe_m31_butterflies(4096, sink.data_ptr(), sink.numel(), C.byref(nbf), sptr))
+
+    probe()
+    torch.cuda.synchronize()
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pe0.record(stream)
+    for _ in range(3):
+        probe()
+    pe1.record(stream)
+    torch.cuda.synchronize()
+    ceiling = 3 * nbf.value / (pe0.elapsed_time(pe1) / 1e3)
+    fft_rate = bf_step / ((t_interp + t_eval) / 1e3)
     roof = {"bound": "hbm", "kernel": "fftT_kernel / fft_pass_kernel (circle FFT, 8 columns x 2^24, blowup 4)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
             "traffic": traffic, "interpolate_ms": t_interp, "evaluate_ms": t_eval,
-            "algorithmic_bytes_per_step": b_interp + b_eval}
+            "algorithmic_bytes_per_step": b_interp + b_eval,
+            "integer_ceiling": {"butterflies_per_s": ceiling, "fft_butterflies_per_s": fft_rate,
+                                "frac": fft_rate / ceiling, "butterflies_per_step": bf_step,
+                                "what": "the passes' forward butterfly on register operands (probe kernel), "
+                                        "the bound the passes meet before HBM"}}
     fft = {"columns_per_s": ncols / ((t_interp + t_eval) / 1e3), "unit": FFT_UNIT, "reference_gpu": ref_gpu}
     del evals, outs, tw, itw
     torch.cuda.empty_cache()

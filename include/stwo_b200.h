@@ -164,6 +164,13 @@ int stwo_autotune(char *report, size_t report_cap);
  * (2..4: log2 of the 8192-coefficient groups each eval_at_point CTA folds; 0, the
  * default, chooses per launch). */
 int stwo_set_tunable(const char *name, int value);
+/* Diagnostics (no counterpart in the reference): the integer ceiling of the FFT. One
+ * launch runs the FFT passes' own forward butterfly on register-resident operands
+ * (16 independent chains a thread, 2048 threads an SM) for `iters` rounds and reports
+ * in *butterflies how many it executes; time it on `stream` to get the device's
+ * butterfly rate. `sink` is device memory of at least 2048 x SM-count words. */
+int stwo_probe_m31_butterflies(uint32_t iters, uint32_t *sink, uint64_t sink_words, uint64_t *butterflies,
+                               void *stream);
 /* Number of kernel launches the library has made in this process (all threads). */
 uint64_t stwo_kernel_launches(void);
 /* Waits for all work on `stream`; returns STWO_ERR_CUDA if any of it failed. */

@@ -138,6 +138,7 @@ SIGNATURES = [
     ("stwo_server_graph_stats", None, [vp, C.POINTER(u64), C.POINTER(u64)]),
     ("stwo_server_now_ms", C.c_double, []),
     ("stwo_server_mark_epoch", C.c_int, [vp]),
+    ("stwo_probe_m31_butterflies", C.c_int, [u32, vp, u64, C.POINTER(u64), vp]),
     ("stwo_server_destroy", None, [vp]),
 ]
 

@@ -25,6 +25,8 @@ int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_c
                 const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st);
 int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_cols, const uint32_t *level_ncols,
                           uint32_t *const *layers, cudaStream_t st);
+int butterfly_probe_async(uint32_t iters, uint32_t *sink, uint64_t sink_words, uint64_t *butterflies,
+                          cudaStream_t st);
 
 namespace {
 
@@ -110,6 +112,11 @@ int stwo_set_tunable(const char *name, int value) {
         return STWO_OK;
     }
     return set_error(STWO_ERR_INVALID_ARGUMENT, "unknown tunable %s", name);
+}
+
+int stwo_probe_m31_butterflies(uint32_t iters, uint32_t *sink, uint64_t sink_words, uint64_t *butterflies,
+                                void *stream) {
+    return butterfly_probe_async(iters, sink, sink_words, butterflies, as_stream(stream));
 }
 
 int stwo_autotune(char *report, size_t report_cap) {

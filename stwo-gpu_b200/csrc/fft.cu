@@ -637,7 +637,47 @@ std::vector<PassSpec> plan_passes(uint32_t L) {
     return v;
 }
 
+// The integer ceiling of every FFT pass: the rate of the passes' own forward butterfly
+// (butterfly<false>: an m31_mul2 product, a sum and a difference) with operands in
+// registers only. Each thread keeps 16 independent pairs and feeds every butterfly's
+// outputs into its next one; the XOR of the final values goes to sink so that nothing
+// is optimised away.
+constexpr int PROBE_PAIRS = 16;
+constexpr int PROBE_THREADS = 256;
+
+__global__ void __launch_bounds__(PROBE_THREADS) butterfly_probe_kernel(uint32_t iters, uint32_t *sink) {
+    const uint32_t tid = blockIdx.x * PROBE_THREADS + threadIdx.x;
+    uint32_t a[PROBE_PAIRS], b[PROBE_PAIRS], t2[PROBE_PAIRS];
+#pragma unroll
+    for (int k = 0; k < PROBE_PAIRS; k++) {
+        a[k] = (tid * 2654435761u + (uint32_t)k) & 0x3fffffffu;
+        b[k] = (tid * 40503u + 7919u * (uint32_t)k) & 0x3fffffffu;
+        t2[k] = ((tid ^ (0x9e3779b9u * (uint32_t)(k + 1))) & 0x3fffffffu) << 1;
+    }
+    for (uint32_t it = 0; it < iters; it++) {
+#pragma unroll
+        for (int k = 0; k < PROBE_PAIRS; k++) butterfly<false>(a[k], b[k], t2[k]);
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int k = 0; k < PROBE_PAIRS; k++) x ^= a[k] ^ b[k];
+    sink[tid] = x;
+}
+
 }  // namespace
+
+int butterfly_probe_async(uint32_t iters, uint32_t *sink, uint64_t sink_words, uint64_t *butterflies,
+                          cudaStream_t st) {
+    STWO_REQUIRE(butterflies && sink, STWO_ERR_INVALID_ARGUMENT, "null argument");
+    const uint64_t blocks = (uint64_t)device_sm_count() * (2048 / PROBE_THREADS);
+    const uint64_t threads = blocks * PROBE_THREADS;
+    STWO_REQUIRE(sink_words >= threads, STWO_ERR_INVALID_ARGUMENT, "the probe needs a sink of %llu words",
+                 (unsigned long long)threads);
+    butterfly_probe_kernel<<<(unsigned)blocks, PROBE_THREADS, 0, st>>>(iters, sink);
+    STWO_LAUNCH_CHECK("butterfly_probe_kernel");
+    *butterflies = threads * PROBE_PAIRS * (uint64_t)iters;
+    return STWO_OK;
+}
 
 // (x, y) of the first point of the half coset of a 2^N-point circle domain, N <= 2,
 // as twiddles (inv = false) or inverse twiddles (inv = true). The tree does not

@@ -222,3 +222,21 @@ def test_eval_at_points_every_chunk_size(stwo, oracle, groups_log):
         lib.stwo_set_tunable(b"eval_at_point_groups_log", 0)
     with pytest.raises(L.StwoError):
         L.check(lib.stwo_set_tunable(b"eval_at_point_groups_log", 5))
+
+
+def test_butterfly_probe_counts_and_checks_its_sink(stwo):
+    """stwo_probe_m31_butterflies runs 16 chains a thread, 2048 threads an SM, and
+    refuses a sink smaller than one word a thread."""
+    import ctypes as C
+    import torch
+    L = stwo._lib
+    lib = L.lib()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    sink = torch.zeros(2048 * sms, dtype=torch.int32, device="cuda")
+    n = C.c_uint64()
+    L.check(lib.stwo_probe_m31_butterflies(8, sink.data_ptr(), sink.numel(), C.byref(n), None))
+    L.check(lib.stwo_stream_synchronize(None))
+    assert n.value == 2048 * sms * 16 * 8
+    assert int(torch.count_nonzero(sink)) > 0
+    with pytest.raises(L.StwoError):
+        L.check(lib.stwo_probe_m31_butterflies(8, sink.data_ptr(), sink.numel() - 1, C.byref(n), None))
