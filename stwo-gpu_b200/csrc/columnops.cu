@@ -13,7 +13,8 @@
 // registers, a multiplicative scan of the lane products in both directions with
 // shuffles, one field inversion of the warp product (computed by every lane, so no
 // barrier is needed) and back-substitution: 3 multiplications per element and one
-// inversion per 256 elements.
+// inversion per 256 elements. QM31 elements are inverted through their M31 norms, so
+// the scan and its products stay in M31.
 #include <map>
 #include <mutex>
 #include <vector>
@@ -83,20 +84,6 @@ struct FieldT<uint32_t> {
     __device__ static uint32_t shfl_up(uint32_t v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
     __device__ static uint32_t shfl_down(uint32_t v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 };
-template <>
-struct FieldT<qm31> {
-    __device__ static qm31 one() { return qm31_one(); }
-    __device__ static qm31 mul(qm31 a, qm31 b) { return qm31_mul(a, b); }
-    __device__ static qm31 inv(qm31 a) { return qm31_inv(a); }
-    __device__ static qm31 shfl_up(qm31 v, int d) {
-        return {{__shfl_up_sync(0xffffffffu, v.a.a, d), __shfl_up_sync(0xffffffffu, v.a.b, d)},
-                {__shfl_up_sync(0xffffffffu, v.b.a, d), __shfl_up_sync(0xffffffffu, v.b.b, d)}};
-    }
-    __device__ static qm31 shfl_down(qm31 v, int d) {
-        return {{__shfl_down_sync(0xffffffffu, v.a.a, d), __shfl_down_sync(0xffffffffu, v.a.b, d)},
-                {__shfl_down_sync(0xffffffffu, v.b.a, d), __shfl_down_sync(0xffffffffu, v.b.b, d)}};
-    }
-};
 
 // Warp-level Montgomery batch inverse: each warp owns 32 x BI_PER_THREAD elements,
 // lane l holding elements base + i*32 + l (coalesced loads and stores). Prefix
@@ -140,6 +127,56 @@ __global__ void __launch_bounds__(BI_THREADS) batch_inverse_kernel(const F *__re
         const uint64_t idx = base + (uint64_t)i * 32;
         if (idx < n) dst[idx] = inv_i;
         r = T::mul(r, v[i]);
+    }
+}
+
+// QM31 batch inverse through norms. For z = a + b u (a, b in CM31, u^2 = R = 2 + i):
+// z (a - b u) = a^2 - R b^2 = N in CM31, and N conj(N) = |N|^2 in M31, so
+// z^-1 = (a - b u) conj(N) / |N|^2. The warp's Montgomery inverse then runs on the
+// M31 norms (three M31 products an element, one-word shuffles, one M31 inversion a
+// warp) instead of on QM31 values (three QM31 products an element); the inverse is
+// unique, so the values are the same.
+__global__ void __launch_bounds__(BI_THREADS) batch_inverse_qm31_norm_kernel(const qm31 *__restrict__ src,
+                                                                             qm31 *__restrict__ dst, uint64_t n) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp_global = ((uint64_t)blockIdx.x * BI_THREADS + threadIdx.x) >> 5;
+    const uint64_t base = warp_global * (32 * BI_PER_THREAD) + lane;
+    qm31 v[BI_PER_THREAD];
+    cm31 nrm[BI_PER_THREAD];
+    uint32_t pre[BI_PER_THREAD];
+    uint32_t run = 1;
+#pragma unroll
+    for (int i = 0; i < BI_PER_THREAD; i++) {
+        const uint64_t idx = base + (uint64_t)i * 32;
+        v[i] = (idx < n) ? src[idx] : qm31_one();
+        const cm31 a2 = cm31_mul(v[i].a, v[i].a), b2 = cm31_mul(v[i].b, v[i].b);
+        const cm31 rb2 = {m31_sub(m31_add(b2.a, b2.a), b2.b), m31_add(m31_add(b2.b, b2.b), b2.a)};  // R b^2
+        nrm[i] = cm31_sub(a2, rb2);
+        const uint32_t m = reduce64_p((uint64_t)nrm[i].a * nrm[i].a + (uint64_t)nrm[i].b * nrm[i].b);
+        run = m31_mul(run, m);
+        pre[i] = run;
+    }
+    // Inclusive scans of the lanes' norm products, forward (prefix) and backward (suffix).
+    uint32_t inc = run, suf = run;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, inc, d);
+        const uint32_t w = __shfl_down_sync(0xffffffffu, suf, d);
+        if (lane >= (uint32_t)d) inc = m31_mul(inc, u);
+        if (lane + d < 32u) suf = m31_mul(suf, w);
+    }
+    const uint32_t total = __shfl_down_sync(0xffffffffu, inc, 31 - lane);
+    uint32_t ex_pre = __shfl_up_sync(0xffffffffu, inc, 1), ex_suf = __shfl_down_sync(0xffffffffu, suf, 1);
+    if (lane == 0) ex_pre = 1;
+    if (lane == 31) ex_suf = 1;
+    uint32_t r = m31_mul(m31_inv(total), m31_mul(ex_pre, ex_suf));
+#pragma unroll
+    for (int i = BI_PER_THREAD - 1; i >= 0; i--) {
+        const uint32_t minv = i > 0 ? m31_mul(r, pre[i - 1]) : r;  // 1 / |N_i|^2
+        const uint64_t idx = base + (uint64_t)i * 32;
+        r = m31_mul(r, reduce64_p((uint64_t)nrm[i].a * nrm[i].a + (uint64_t)nrm[i].b * nrm[i].b));
+        const cm31 ninv = {m31_mul(nrm[i].a, minv), m31_neg(m31_mul(nrm[i].b, minv))};  // 1 / N_i
+        if (idx < n) dst[idx] = {cm31_mul(v[i].a, ninv), cm31_neg(cm31_mul(v[i].b, ninv))};
     }
 }
 
@@ -199,9 +236,9 @@ int batch_inverse_m31_async(const uint32_t *src, uint32_t *dst, uint64_t n, cuda
 int batch_inverse_qm31_async(const uint32_t *src, uint32_t *dst, uint64_t n, cudaStream_t st) {
     if (n == 0) return STWO_OK;
     uint64_t blocks = (n + BI_THREADS * BI_PER_THREAD - 1) / (BI_THREADS * BI_PER_THREAD);
-    batch_inverse_kernel<qm31><<<(unsigned)blocks, BI_THREADS, 0, st>>>(reinterpret_cast<const qm31 *>(src),
-                                                                         reinterpret_cast<qm31 *>(dst), n);
-    STWO_LAUNCH_CHECK("batch_inverse_kernel<qm31>");
+    batch_inverse_qm31_norm_kernel<<<(unsigned)blocks, BI_THREADS, 0, st>>>(reinterpret_cast<const qm31 *>(src),
+                                                                            reinterpret_cast<qm31 *>(dst), n);
+    STWO_LAUNCH_CHECK("batch_inverse_qm31_norm_kernel");
     return STWO_OK;
 }
 
