@@ -103,6 +103,19 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
         const uint32_t hidx = bit_reverse_bits((uint32_t)k, p.log_size - 1);
         const cpoint pt = point_from_tables(p.tab, (p.half_init + p.half_step * hidx) & 0x7fffffffu);
         const uint32_t ys[2] = {pt.y, m31_neg(pt.y)};
+        // The first column group's loads go out before the denominators' inversion, a
+        // chain of dependent products, so that their latency overlaps it.
+        uint2 va[QUOT_PREFETCH], vb[QUOT_PREFETCH];
+        {
+            const uint32_t j1 = p.batch_end[0];
+#pragma unroll
+            for (int u = 0; u < QUOT_PREFETCH; u++)
+                if ((uint32_t)u < j1) {
+                    const uint32_t *col = STAGE ? s_cols[u]
+                                                : (COLS_ON_DEVICE ? dev_cols[p.col_idx[u]] : p.cols[p.col_idx[u]]);
+                    va[u] = __ldg(reinterpret_cast<const uint2 *>(col) + k);
+                }
+        }
         // Denominator inverses of both rows, all batches: one inversion (Montgomery's trick).
         cm31 den[2][MAXB];
         {
@@ -168,8 +181,7 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                             for (int t = 0; t < 4; t++) s0[s][t] = fold64_fma(s0[s][t], two);
                 }
             };
-            uint2 va[QUOT_PREFETCH], vb[QUOT_PREFETCH];
-            if (j0 < j1) load_group(j0, va);
+            if (b > 0 && j0 < j1) load_group(j0, va);  // batch 0's first group is in flight
             for (uint32_t jb = j0; jb < j1; jb += 2 * QUOT_PREFETCH) {
                 if (jb + QUOT_PREFETCH < j1) load_group(jb + QUOT_PREFETCH, vb);
                 consume(jb, va);
