@@ -150,7 +150,7 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            raise ImportError(f"{LIB_PATH} is missing: build it with `python stwo-gpu_b200/build.py`")
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m stwo_gpu_b200.build`")
         L = C.CDLL(LIB_PATH)
         for name, res, args in SIGNATURES:
             f = getattr(L, name)

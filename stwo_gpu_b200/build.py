@@ -1,9 +1,9 @@
 """Builds libstwo_b200.so (the C-ABI CUDA library) in-tree for sm_100a.
 
-    python stwo-gpu_b200/build.py [--force] [--verbose]
+    python -m stwo_gpu_b200.build [--force] [--verbose]
 
-Each csrc/*.cu is compiled to an object under stwo-gpu_b200/_build/ (rebuilt
-when it or any header is newer), then linked into stwo-gpu_b200/lib/libstwo_b200.so.
+Each csrc/*.cu is compiled to an object under stwo_gpu_b200/_build/ (rebuilt
+when it or any header is newer), then linked into stwo_gpu_b200/lib/libstwo_b200.so.
 """
 import concurrent.futures
 import os

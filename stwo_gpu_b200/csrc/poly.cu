@@ -5,6 +5,8 @@
 #include <mutex>
 #include <vector>
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace stwo {
@@ -666,7 +668,9 @@ stwo_qm31 eval_at_point(const uint32_t *coeffs, uint32_t coeffs_size, stwo_qm31 
 // holds its 32.5 KiB until the process exits. Host code only knows a stand-in symbol
 // for it, so its device address is looked up with cudaGetSymbolAddress once per
 // device, on that device's first call (which therefore should come before any
-// stream capture), and the address is what the kernel receives.
+// stream capture), and the address is what the kernel receives. A device reset
+// gives the device a new context in which the array has a new address; the next
+// call sees the changed context and looks the address up again.
 // All calls share the one array, so calls whose work overlaps on the GPU (two
 // streams, or two host threads) race and must be serialised by the caller; the
 // completion tickets are cleared at the start of every call, and the partial sums
@@ -683,23 +687,66 @@ namespace {
 
 constexpr int EAP_NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mu;
-void *g_noalloc_addr[EAP_NOALLOC_MAX_DEVICES] = {};
+struct NoallocSlot {
+    void *addr;
+    unsigned long long ctx_id;  // unique id of the context the address belongs to
+};
+NoallocSlot g_noalloc[EAP_NOALLOC_MAX_DEVICES] = {};
 
-// Device address of the scratch array on the current device (looked up once).
+// Unique id of the calling thread's current context (0 when there is none). The
+// address of a __device__ array belongs to one context: after cudaDeviceReset, or a
+// released and re-created primary context, the array lives at a new address, and
+// the id (never reused within a process) tells the two apart. The driver functions
+// come through the runtime's entry-point query, so the library still links only
+// against cudart.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_current = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+                       q == cudaDriverEntryPointSuccess
+                   ? reinterpret_cast<CtxGetCurrentFn>(f)
+                   : nullptr;
+    }();
+    static CtxGetIdFn get_id = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+                       q == cudaDriverEntryPointSuccess
+                   ? reinterpret_cast<CtxGetIdFn>(f)
+                   : nullptr;
+    }();
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr ||
+        get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// Device address of the scratch array on the current device: looked up with the
+// device current on its first call, and again whenever the device's context has
+// changed since (a reset).
 int noalloc_scratch(void **out) {
     int dev = 0;
     STWO_CUDA_TRY(cudaGetDevice(&dev));
     STWO_REQUIRE(dev >= 0 && dev < EAP_NOALLOC_MAX_DEVICES, STWO_ERR_UNSUPPORTED_SIZE, "device ordinal %d", dev);
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    NoallocSlot &slot = g_noalloc[dev];
+    const unsigned long long id = current_context_id();
+    if (!slot.addr || id == 0 || id != slot.ctx_id) {
         void *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_eap_noalloc_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_eap_noalloc_scratch);  // makes the context current
         if (e != cudaSuccess || ptr == nullptr)
             return set_error(STWO_ERR_CUDA, "cudaGetSymbolAddress of the eval_at_point scratch failed: %s",
                              cudaGetErrorString(e));
-        g_noalloc_addr[dev] = ptr;
+        slot.addr = ptr;
+        slot.ctx_id = current_context_id();
     }
-    *out = g_noalloc_addr[dev];
+    *out = slot.addr;
     return STWO_OK;
 }
 

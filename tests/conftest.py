@@ -1,23 +1,15 @@
-import importlib.util
 import os
 import sys
 
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-PKG_DIR = os.path.join(ROOT, "stwo-gpu_b200")
+sys.path.insert(0, ROOT)
 
 
 def load_package():
-    """Import the package directory stwo-gpu_b200/ as module `stwo_gpu_b200`."""
-    if "stwo_gpu_b200" in sys.modules:
-        return sys.modules["stwo_gpu_b200"]
-    spec = importlib.util.spec_from_file_location(
-        "stwo_gpu_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
-    mod = importlib.util.module_from_spec(spec)
-    sys.modules["stwo_gpu_b200"] = mod
-    spec.loader.exec_module(mod)
-    return mod
+    import stwo_gpu_b200
+    return stwo_gpu_b200
 
 
 sys.path.insert(0, os.path.join(ROOT, "oracle"))

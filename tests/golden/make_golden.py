@@ -1,7 +1,7 @@
 """Extract the reference's literal test vectors into tests/golden/reference_literals.json.
 
 Run once in a container that has the reference tree (its path is the first
-argument, default /root/reference). The GPU box never runs this: the JSON it
+argument; there is no default). The GPU box never runs this: the JSON it
 writes is committed and is what the tests read.
 
 Sources (stwo_gpu_backend/src, NethermindEth/stwo-gpu):
@@ -19,7 +19,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit("usage: make_golden.py REFERENCE_TREE  (the NethermindEth/stwo-gpu checkout to read)")
+REF = sys.argv[1]
 SRC = os.path.join(REF, "stwo_gpu_backend", "src")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_literals.json")
 

@@ -50,13 +50,12 @@ def test_python_binding_covers_header(stwo):
     assert set(declared_functions()) <= bound, set(declared_functions()) - bound
 
 
-def test_library_is_sm100a(stwo):
-    # the fatbin must carry sm_100a code (cuobjdump lists the ELF targets; nothing is disassembled)
-    r = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", stwo._lib.LIB_PATH],
-                       capture_output=True, text=True)
-    if r.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    assert "sm_100a" in r.stdout
+def test_library_is_built_for_sm100a_only():
+    """Every object and the link step are compiled for sm_100a and nothing else."""
+    from stwo_gpu_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert build.FLAGS[:2] == build.ARCH
+    assert not any("compute_" in f or "sm_" in f for f in build.FLAGS[2:])
 
 
 def test_last_error_roundtrip_without_gpu(stwo):

@@ -1,5 +1,5 @@
 """The oracle prover (oracle/stwo_oracle_prover.c) against the plain-Python verifier
-(stwo-gpu_b200/verifier.py): honest proofs verify, every tampered byte is rejected,
+(stwo_gpu_b200/verifier.py): honest proofs verify, every tampered byte is rejected,
 proofs are deterministic. CPU only."""
 import numpy as np
 import pytest
