@@ -22,7 +22,6 @@ cores, a bounded sample per step. Prints one JSON line (rank 0).
 """
 import argparse
 import dataclasses
-import importlib.util
 import json
 import os
 import subprocess
@@ -31,7 +30,6 @@ import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-PKG_DIR = os.path.join(ROOT, "stwo-gpu_b200")
 P = (1 << 31) - 1
 METRIC = "bit-exact proofs/s & p99 latency: batched server vs per-job; FFT % HBM peak"
 UNIT = "proofs/s"
@@ -40,14 +38,10 @@ BUDGET = 150 << 30  # device-memory budget of the serving config
 
 
 def load_package():
-    if "stwo_gpu_b200" in sys.modules:
-        return sys.modules["stwo_gpu_b200"]
-    spec = importlib.util.spec_from_file_location(
-        "stwo_gpu_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
-    mod = importlib.util.module_from_spec(spec)
-    sys.modules["stwo_gpu_b200"] = mod
-    spec.loader.exec_module(mod)
-    return mod
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    import stwo_gpu_b200
+    return stwo_gpu_b200
 
 
 def load_oracle():
@@ -169,6 +163,35 @@ def reference_gpu_timing(args, evals, lg, lb, ncols, tw, itw, tree_size):
         for d in ext:
             R.cuda_free_memory(d)
 
+    # Equality first, on fresh copies of the step's inputs: our interpolate_columns +
+    # extend_evaluate_columns against the reference library's path above.
+    stwo = load_package()
+    L, lib = stwo._lib, stwo._lib.lib()
+    ours = [t.clone() for t in evals]
+    theirs = [t.clone() for t in evals]
+    ours_ext = [torch.empty(1 << N, dtype=torch.int32, device=t.device) for t in evals]
+    theirs_ext = [torch.zeros(1 << N, dtype=torch.int32, device=t.device) for t in evals]
+    logs = L.u32_array([lg] * ncols)
+    torch.cuda.synchronize()
+    L.check(lib.stwo_interpolate_columns(L.ptr_array([t.data_ptr() for t in ours]), logs, ncols, itw.data_ptr(),
+                                         tree_size, None))
+    L.check(lib.stwo_extend_evaluate_columns(L.ptr_array([t.data_ptr() for t in ours]), logs,
+                                             L.ptr_array([t.data_ptr() for t in ours_ext]), lb, ncols, tw.data_ptr(),
+                                             tree_size, None))
+    L.check(lib.stwo_stream_synchronize(None))
+    R.interpolate_columns(1 << (lg - 1), (C.c_void_p * ncols)(*[t.data_ptr() for t in theirs]), itw.data_ptr(),
+                          tree_size, ncols, 1 << lg)
+    for t, x in zip(theirs, theirs_ext):
+        R.copy_uint32_t_vec_from_device_to_device(t.data_ptr(), x.data_ptr(), 1 << lg)
+    R.evaluate_columns((C.c_int * ncols)(*([1 << (N - 1)] * ncols)),
+                       (C.c_void_p * ncols)(*[x.data_ptr() for x in theirs_ext]), tw.data_ptr(), tree_size, ncols,
+                       (C.c_int * ncols)(*([1 << N] * ncols)))
+    torch.cuda.synchronize()
+    equal_interp = all(torch.equal(a, b) for a, b in zip(ours, theirs))
+    equal_eval = all(torch.equal(a, b) for a, b in zip(ours_ext, theirs_ext))
+    del ours, theirs, ours_ext, theirs_ext
+    torch.cuda.empty_cache()
+
     torch.cuda.synchronize()
     step()
     torch.cuda.synchronize()
@@ -181,8 +204,9 @@ def reference_gpu_timing(args, evals, lg, lb, ncols, tw, itw, tree_size):
     torch.cuda.synchronize()
     ms = s.elapsed_time(e) / reps
     return {"ms_per_step": ms, "value": ncols / (ms / 1e3), "unit": FFT_UNIT,
+            "equal": equal_interp and equal_eval, "equal_interpolate": equal_interp, "equal_evaluate": equal_eval,
             "what": "reference CUDA library (oracle/_ref) on this GPU: interpolate_columns + extend + "
-                    "evaluate_columns, same 8 x 2^24 step"}
+                    "evaluate_columns, same 8 x 2^24 step; outputs compared element for element with ours"}
 
 
 def replica_throughput(local_ms, units_per_rank, world, device=None):
@@ -719,6 +743,73 @@ def same_shape(stwo, dev):
     return out
 
 
+def _sig(x, n=5):
+    """x with every float rounded to n significant digits (nested)."""
+    if isinstance(x, float):
+        return float(f"{x:.{n}g}")
+    if isinstance(x, dict):
+        return {k: _sig(v, n) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [_sig(v, n) for v in x]
+    return x
+
+
+def compact_line(full, detail_path):
+    """The printed JSON line: the contract's keys first, then short summaries of each
+    record, ending with the serving comparison (batched vs one at a time, latency
+    percentiles), so that the end of the line carries the metric. The full record is
+    written to detail_path."""
+    if detail_path:
+        os.makedirs(os.path.dirname(os.path.abspath(detail_path)), exist_ok=True)
+        with open(detail_path, "w") as f:
+            json.dump(full, f, indent=1)
+    keep = ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+            "vs_baseline", "dtype", "data", "config", "gpu_launches", "clocks", "cpu_baseline", "e2e")
+    line = {k: full[k] for k in keep}
+    line["detail"] = detail_path
+    k = full.get("kernels")
+    if k:
+        line["kernels"] = {
+            name: {kk: v[kk] for kk in ("ms", "frac_hbm", "frac_alu_bound", "speedup_vs_reference", "equal",
+                                        "root_equal", "equal_after_one_chain") if kk in v}
+            for name, v in k.items()}
+    sp = full.get("single_proofs")
+    if sp:
+        line["single_proofs"] = {
+            name: dict({kk: v.get(kk) for kk in ("ms_median", "cached_ms_median", "oracle_ms", "equal_to_oracle",
+                                                  "verified")},
+                       phases_ms=v.get("phases_ms"))
+            for name, v in sp.items()}
+    ss = full.get("same_shape")
+    if ss:
+        line["same_shape"] = {"batched_proofs_per_s": ss["batched"]["proofs_per_s"],
+                              "one_at_a_time_proofs_per_s": ss["one_at_a_time"]["proofs_per_s"]}
+    b = full.get("batch48")
+    if b:
+        line["batch48"] = {kk: b[kk] for kk in ("proofs_per_s", "per_job_proofs_per_s", "batched_vs_per_job",
+                                                "bit_identical")}
+        line["batch48"]["mixed_tree_root_equal_to_oracle"] = b["mixed_tree"]["root_equal_to_oracle"]
+    fft = full.get("fft")
+    if fft:
+        rg = fft.get("reference_gpu") or {}
+        line["fft"] = {"columns_per_s": fft["columns_per_s"], "reference_gpu_columns_per_s": rg.get("value"),
+                       "reference_gpu_equal": rg.get("equal")}
+    r = full["roofline"]
+    line["roofline"] = {kk: r[kk] for kk in ("bound", "kernel", "achieved", "peak", "unit", "frac", "peak_kind",
+                                             "traffic", "interpolate_ms", "evaluate_ms")}
+    line["roofline"]["integer_ceiling_frac"] = r["integer_ceiling"]["frac"]
+    s = full["serving"]
+    line["serving"] = {"batched_proofs_per_s": full["value"], "per_job_proofs_per_s": s["per_job_proofs_per_s"],
+                       "bit_identical": s["bit_identical"], "proofs_compared": s["proofs_compared"],
+                       "verified_sample": s["verified_sample"],
+                       "latency_ms_p50_p99_p999": {
+                           load: {mode: [e[mode]["p50_ms"], e[mode]["p99_ms"], e[mode]["p999_ms"]]
+                                  for mode in ("batched", "per_job")}
+                           for load, e in s["latency"].items()},
+                       "batched_vs_per_job": s["batched_vs_per_job"]}
+    return _sig(line)
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -827,7 +918,12 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0:
         O = load_oracle() if not args.no_cpu_baseline else None
         singles = {}
-        for name, t in (("cols64_log12", (12, 64, 1, 3, 5)), ("cols256_log20", (20, 256, 1, 3, 10))):
+        # The reference CpuBackend's case (64 x 2^12), the large single proof (256 x 2^20,
+        # pow_bits 10) and the reference's own end-to-end shape (1024 x 2^16,
+        # examples/wide_fibonacci.rs:19-20), each compared byte for byte with the oracle
+        # prover (on every host thread), whose time is reported beside the GPU's.
+        for name, t in (("cols64_log12", (12, 64, 1, 3, 5)), ("cols256_log20", (20, 256, 1, 3, 10)),
+                        ("cols1024_log16", (16, 1024, 1, 3, 5))):
             job = stwo.WideFibJob(*t)
             a0, a1 = stwo.wide_fib_inputs(t[0], 1)
             stwo.prove_wide_fib(job, a0, a1)
@@ -841,11 +937,14 @@ def run_ours(args, rank, world, local_rank):
                    ("trace_ms", "composition_ms", "oods_ms", "fri_ms", "decommit_ms")},
                    "kernel_launches": stats["kernel_launches"], "proof_bytes": len(proof),
                    "verified": bool(stwo.verify(proof, *t))}
-            if O is not None and t[0] <= 12:
+            if O is not None:
+                O.set_threads(os.cpu_count() or 1)
                 t0 = time.perf_counter()
                 want, _ = O.wide_fib_prove(t[0], t[1], a0, a1, *t[2:])
                 ent["oracle_ms"] = (time.perf_counter() - t0) * 1e3
+                ent["oracle_threads"] = os.cpu_count() or 1
                 ent["equal_to_oracle"] = want == proof
+                O.set_threads(1)
             # The same proof repeated through a ProveCache (shared tree, own stream):
             # memory reused, launch sequence replayed as a CUDA graph.
             cs = torch.cuda.Stream(dev)
@@ -874,7 +973,7 @@ def run_ours(args, rank, world, local_rank):
             cpu = {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
 
     if rank == 0:
-        line = {
+        full = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "m31 (u32)", "data": "synthetic (seeded SplitMix64 M31 trace inputs)",
@@ -905,7 +1004,7 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
-        print(json.dumps(line), flush=True)
+        print(json.dumps(compact_line(full, args.detail_out)), flush=True)
 
 
 def run_profile(args):
@@ -1042,6 +1141,8 @@ def main():
     ap.add_argument("--latency-jobs", type=int, default=2000, help="jobs per Poisson load level")
     ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds of oracle work per CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--detail-out", default=os.path.join("gpurun_out", "bench_detail.json"),
+                    help="where the full record goes (the printed line carries summaries)")
     ap.add_argument("--no-suite", action="store_true", help="skip the config-1 per-kernel sweep")
     ap.add_argument("--profile", default=None,
                     help="run one workload for ncu instead: fft[:LOG] | proof:L,N | merkle | quotients | fri | "

@@ -223,7 +223,8 @@ int stwo_eval_at_points(const uint32_t *const *coeffs, const uint32_t *log_sizes
  * limited to 2^26 coefficients (larger sizes return STWO_ERR_UNSUPPORTED_SIZE).
  * result is a device pointer to one QM31; the call is asynchronous on `stream`.
  * The first call on each device looks the array's device address up (make it
- * before any stream capture). All calls share the array: calls that overlap on the
+ * before any stream capture); after a device reset the first call in the new
+ * context looks it up again. All calls share the array: calls that overlap on the
  * GPU race and must be serialised by the caller. */
 int stwo_eval_at_point_no_alloc(const uint32_t *coeffs, uint32_t log_size, stwo_qm31 point_x, stwo_qm31 point_y,
                                 stwo_qm31 *result, void *stream);

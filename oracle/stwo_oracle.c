@@ -238,21 +238,33 @@ void or_batch_inverse_qm31(const qm31_t *src, qm31_t *dst, size_t n) {
  * for each doubling of the root coset, the x coordinates of its first half in
  * bit-reversed order, concatenated; then a single 1. itwiddles = inverses.
  * ====================================================================== */
+typedef struct { m31_t *tw; const m31_t *src; coset_t c; size_t off; } tw_ctx;
+static void tw_layer_range(void *cv, size_t lo, size_t hi) {
+    tw_ctx *x = (tw_ctx *)cv;
+    uint32_t hl = x->c.log_size - 1;
+    for (size_t h = lo; h < hi; h++)
+        x->tw[x->off + or_bit_reverse_index((uint32_t)h, hl)] = or_coset_at(x->c, h).x;
+}
+static void tw_inv_range(void *cv, size_t lo, size_t hi) {
+    tw_ctx *x = (tw_ctx *)cv;
+    for (size_t i = lo; i < hi; i++) x->tw[i] = m_inv(x->src[i]);
+}
 void or_precompute_twiddles(coset_t root, m31_t *tw, m31_t *itw) {
     size_t size = (size_t)1 << root.log_size;
     size_t off = 0;
     coset_t c = root;
     for (uint32_t layer = 0; layer < root.log_size; layer++) {
         size_t half = ((size_t)1 << c.log_size) / 2;
-        uint32_t hl = c.log_size - 1;
-        for (size_t h = 0; h < half; h++)
-            tw[off + or_bit_reverse_index((uint32_t)h, hl)] = or_coset_at(c, h).x;
+        tw_ctx x = {tw, NULL, c, off};
+        par_range(half, tw_layer_range, &x);
         off += half;
         c = coset_double(c);
     }
     tw[size - 1] = 1;
-    if (itw)
-        for (size_t i = 0; i < size; i++) itw[i] = m_inv(tw[i]);
+    if (itw) {
+        tw_ctx x = {itw, tw, c, 0};
+        par_range(size, tw_inv_range, &x);
+    }
 }
 
 /* PolyOps::new_canonical_ordered (twiddles.cu:4-27): even positions, then odd

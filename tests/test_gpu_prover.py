@@ -85,6 +85,35 @@ def test_gpu_prover_rejects_unsupported_jobs(bad):
     assert stwo.verify(proof, 4, 8, 1, 3, 5)
 
 
+LARGE_JOBS = [
+    # serving-stream shapes above 2^14 rows (log_n_rows 12..20, 16..256 columns)
+    (15, 64, 1, 3, 5),
+    (16, 128, 1, 3, 5),
+    (17, 32, 1, 3, 5),
+    (19, 16, 1, 3, 5),
+    # the reference's own end-to-end shape: 1024 columns, 2^16 rows
+    # (examples/wide_fibonacci.rs:19-20, 211-249)
+    (16, 1024, 1, 3, 5),
+]
+
+
+@pytest.mark.parametrize("t", LARGE_JOBS, ids=lambda j: "L%d_N%d_B%d_q%d_pow%d" % j)
+def test_large_gpu_proof_equals_oracle_proof(oracle, t):
+    """Proof bytes above 2^14 rows: the oracle prover runs on every host thread."""
+    import os
+    stwo = load_package()
+    a0, a1 = stwo.wide_fib_inputs(t[0], 3000 + t[0] * 7 + t[1])
+    proof, _ = stwo.prove_wide_fib(job_of(t), a0, a1)
+    oracle.set_threads(os.cpu_count() or 1)
+    try:
+        want, rc = oracle.wide_fib_prove(t[0], t[1], a0, a1, t[2], t[3], t[4])
+    finally:
+        oracle.set_threads(1)
+    assert rc == 0
+    assert proof == want
+    assert stwo.verify(proof, *t)
+
+
 def test_large_proof_verifies():
     """256 columns, 2^18 rows: checked by the verifier (the oracle is too slow here)."""
     stwo = load_package()

@@ -48,6 +48,18 @@ def test_no_alloc_matches_eval_at_point_twice(stwo, log_size):
         assert _no_alloc(stwo, buf, log_size, px, py, out) == _existing(stwo, buf, log_size, px, py), call
 
 
+@pytest.mark.parametrize("log_size", [20, 22])
+def test_no_alloc_matches_oracle(stwo, oracle, log_size):
+    """The same value as the oracle's eval_at_point (CpuBackend restated), not only as
+    the other entry point, which shares the kernel."""
+    r = rng(940 + log_size)
+    out = stwo.SecureFieldVec.new_uninitialized(1)
+    coeffs = m31(r, 1 << log_size)
+    buf = stwo.BaseFieldVec.from_numpy(coeffs)
+    px, py = random_circle_point(r)
+    assert _no_alloc(stwo, buf, log_size, px, py, out) == oracle.eval_at_point(coeffs, px, py)
+
+
 def test_no_alloc_largest_size_then_small(stwo):
     """The maximum size (2^26 coefficients fills the scratch), then a small call."""
     r = rng(926)
