@@ -418,10 +418,91 @@ def kernel_suite(stwo, reps=5):
     out["eval_at_point"] = {"ms": t, "gbs": b / t / 1e6, "frac_hbm": b / t / 1e6 / peak,
                             "workload": "32 polynomials x 2^22 coefficients, one point each"}
     del polys
+    out["fft_many_columns"] = many_columns_fft(stwo, R, timed, ptrs, rand, dev, peak)
     for k, v in out.items():
         if "reference_ms" in v:
             v["speedup_vs_reference"] = v["reference_ms"] / v["ms"]
     return out
+
+
+def many_columns_fft(stwo, R, timed, ptrs, rand, dev, peak):
+    """The reference's own FFT harness shape (benches/evaluate_columns.rs:11-13,
+    interpolate_columns.rs:10-11): 2^16 columns of 2^10 values, interpolated, and 2^16
+    polynomials of 2^10 coefficients evaluated at blowup 4. Ours through the native
+    column entry points (one launch per pass over a device table of the columns);
+    the reference library's interpolate_columns and evaluate_columns on the same
+    inputs, its evaluation on buffers already zero-extended (the extension copies of
+    its evaluate_polynomials are not timed). Outputs compared on sampled columns."""
+    import ctypes as C
+    import torch
+    L = stwo._lib
+    lib = L.lib()
+    lg, lb, ncols = 10, 2, 1 << 16
+    N = lg + lb
+    sptr = torch.cuda.current_stream(dev).cuda_stream
+    hc = stwo.CanonicCoset(N).half_coset()
+    tsz = 1 << hc.log_size
+    tw = torch.empty(tsz, dtype=torch.int32, device=dev)
+    itw = torch.empty_like(tw)
+    L.check(lib.stwo_precompute_twiddles(hc.initial_index, hc.step_size, hc.log_size, tw.data_ptr(), itw.data_ptr(),
+                                         sptr))
+    src = rand(ncols << lg)
+    work = src.clone()
+    ext = torch.empty(ncols << N, dtype=torch.int32, device=dev)
+    col_p = L.ptr_array([work.data_ptr() + 4 * (i << lg) for i in range(ncols)])
+    ext_p = L.ptr_array([ext.data_ptr() + 4 * (i << N) for i in range(ncols)])
+    logs = L.u32_array([lg] * ncols)
+
+    def interp():
+        L.check(lib.stwo_interpolate_columns(col_p, logs, ncols, itw.data_ptr(), tsz, sptr))
+
+    def evaluate():
+        L.check(lib.stwo_extend_evaluate_columns(col_p, logs, ext_p, lb, ncols, tw.data_ptr(), tsz, sptr))
+
+    n0 = lib.stwo_kernel_launches()
+    interp()
+    evaluate()
+    torch.cuda.synchronize()
+    launches = lib.stwo_kernel_launches() - n0
+    work.copy_(src)
+    t_i = timed(interp)
+    t_e = timed(evaluate)
+    rec = {"workload": "2^16 columns x 2^10: interpolate_columns; evaluate_polynomials at blowup 4",
+           "interpolate_ms": t_i, "evaluate_ms": t_e, "launches_per_step": launches,
+           "interpolate_gbs": ncols * (8 << lg) / t_i / 1e6,
+           "evaluate_gbs": ncols * ((4 << lg) + (4 << N)) / t_e / 1e6}
+    rec["evaluate_frac_hbm"] = rec["evaluate_gbs"] / peak
+    if R is not None:
+        # equality on the same inputs: ours and the reference's interpolation, then the
+        # reference's evaluation of its own zero-extended coefficients
+        ours = src.clone()
+        theirs = src.clone()
+        o_p = L.ptr_array([ours.data_ptr() + 4 * (i << lg) for i in range(ncols)])
+        t_p = (C.c_void_p * ncols)(*[theirs.data_ptr() + 4 * (i << lg) for i in range(ncols)])
+        L.check(lib.stwo_interpolate_columns(o_p, logs, ncols, itw.data_ptr(), tsz, sptr))
+        L.check(lib.stwo_extend_evaluate_columns(o_p, logs, ext_p, lb, ncols, tw.data_ptr(), tsz, sptr))
+        torch.cuda.synchronize()
+        R.interpolate_columns(1 << (lg - 1), t_p, itw.data_ptr(), tsz, ncols, 1 << lg)
+        rext = torch.zeros(ncols << N, dtype=torch.int32, device=dev)
+        rext.view(ncols, 1 << N)[:, : 1 << lg].copy_(theirs.view(ncols, 1 << lg))
+        re_p = (C.c_void_p * ncols)(*[rext.data_ptr() + 4 * (i << N) for i in range(ncols)])
+        dom = (C.c_int * ncols)(*([1 << (N - 1)] * ncols))
+        szs = (C.c_int * ncols)(*([1 << N] * ncols))
+        R.evaluate_columns(dom, re_p, tw.data_ptr(), tsz, ncols, szs)
+        torch.cuda.synchronize()
+        sample = [0, 1, 63, 64, 1000, ncols // 2, ncols - 1]
+        ov, tv = ours.view(ncols, -1), theirs.view(ncols, -1)
+        oe, te = ext.view(ncols, -1), rext.view(ncols, -1)
+        rec["equal_sampled_columns"] = all(torch.equal(ov[k], tv[k]) and torch.equal(oe[k], te[k]) for k in sample)
+        rec["reference_interpolate_ms"] = timed(
+            lambda: R.interpolate_columns(1 << (lg - 1), t_p, itw.data_ptr(), tsz, ncols, 1 << lg))
+        rec["reference_evaluate_ms"] = timed(lambda: R.evaluate_columns(dom, re_p, tw.data_ptr(), tsz, ncols, szs))
+        rec["reference_ms"] = rec["reference_interpolate_ms"] + rec["reference_evaluate_ms"]
+        del ours, theirs, rext
+    rec["ms"] = t_i + t_e
+    del src, work, ext
+    torch.cuda.empty_cache()
+    return rec
 
 
 def job_stream(n, seed):
@@ -770,8 +851,9 @@ def compact_line(full, detail_path):
     k = full.get("kernels")
     if k:
         line["kernels"] = {
-            name: {kk: v[kk] for kk in ("ms", "frac_hbm", "frac_alu_bound", "speedup_vs_reference", "equal",
-                                        "root_equal", "equal_after_one_chain") if kk in v}
+            name: {kk: v[kk] for kk in ("ms", "frac_hbm", "frac_alu_bound", "evaluate_frac_hbm", "launches_per_step",
+                                        "speedup_vs_reference", "equal", "root_equal", "equal_after_one_chain",
+                                        "equal_sampled_columns") if kk in v}
             for name, v in k.items()}
     sp = full.get("single_proofs")
     if sp:

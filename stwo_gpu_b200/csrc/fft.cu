@@ -24,8 +24,11 @@
 //    for the shift-free M31 product (field.cuh).
 //  * Zero extension for evaluate is fused into the first pass (the upper layers
 //    of a zero-padded input only copy it), the 2^-N rescale into the last pass.
-//  * One launch serves many columns of the same size; columns of different sizes
-//    use separate launches on the same stream.
+//  * One launch serves every column of one size: up to 64 columns travel by value
+//    in the parameter block; above that a device table of (src, dst) pointers
+//    (staged by the call, or resident in the caller's device memory) serves them
+//    all, so 2^16 columns take one launch per pass instead of 1024. Columns of
+//    different sizes use separate launches on the same stream.
 #include <algorithm>
 #include <cstdlib>
 #include <utility>
@@ -47,6 +50,8 @@ struct FftColumn {
 
 struct FftLaunch {
     FftColumn cols[MAX_COLS_PER_LAUNCH];
+    const FftColumn *table;  // device (src, dst) of every column, or null: cols[] above
+    uint32_t src_from_dst;   // with a table: this pass reads table[col].dst (passes after the first)
     const uint32_t *tw;   // suffix of the tree for a size-2^N domain (2^(N-1) entries)
     uint32_t N;           // log size of the (virtual) transform
     uint32_t lo, hi;      // layers [lo, hi) applied by this pass
@@ -57,6 +62,16 @@ struct FftLaunch {
 };
 
 __device__ __forceinline__ uint32_t swz(uint32_t j) { return j ^ (((j >> 5) ^ (j >> 10)) & 31u); }
+
+// Source and destination of column `col` of a launch.
+__device__ __forceinline__ FftColumn fft_col(const FftLaunch &p, uint32_t col) {
+    if (p.table) {
+        const ulonglong2 t = __ldg(reinterpret_cast<const ulonglong2 *>(p.table) + col);
+        FftColumn c{reinterpret_cast<const uint32_t *>(p.src_from_dst ? t.y : t.x), reinterpret_cast<uint32_t *>(t.y)};
+        return c;
+    }
+    return p.cols[col];
+}
 
 // Doubled twiddle for layer k, group h.
 __device__ __forceinline__ uint32_t twiddle2(const uint32_t *__restrict__ tw, uint32_t N, uint32_t k, uint32_t h) {
@@ -154,8 +169,9 @@ __global__ void __launch_bounds__(1 << MAX_THREADS_LOG) fft_pass_kernel(const __
     g.cmask = (1u << p.c) - 1u;
     g.gfix = ((T & ((1u << low_fixed) - 1u)) << p.c) | ((T >> low_fixed) << p.hi);
 
-    const uint32_t *__restrict__ src = p.cols[col].src;
-    uint32_t *__restrict__ dst = p.cols[col].dst;
+    const FftColumn fc = fft_col(p, col);
+    const uint32_t *__restrict__ src = fc.src;
+    uint32_t *__restrict__ dst = fc.dst;
 
     // Global -> shared: 4 consecutive tile elements are 4 consecutive words.
     for (uint32_t j = threadIdx.x * 4; j < tile; j += blockDim.x * 4) {
@@ -393,7 +409,7 @@ __device__ __forceinline__ void roundT(uint32_t *sm, const GeoT &geo) {
         for (int grp = 0; grp < GROUPS; grp++) {
             const uint32_t jb = jt | deposit<XBITS>((uint32_t)grp << W, M);
             tile_locate<G, C>(geo, jb, cols[grp], gbs[grp]);
-            const uint32_t *__restrict__ src = p.cols[cols[grp]].src;
+            const uint32_t *__restrict__ src = fft_col(p, cols[grp]).src;
             const uint32_t base = gbs[grp] & p.src_mask;
             if constexpr (C == 0 && A == 0 && RR >= 4) {
 #pragma unroll
@@ -410,7 +426,7 @@ __device__ __forceinline__ void roundT(uint32_t *sm, const GeoT &geo) {
         for (int grp = 0; grp < GROUPS; grp++) {
             round_butterflies<C, A, RB, INV>(v[grp], p, gbs[grp], sh);
             if constexpr (LAST) {
-                store_global<C, A, RB, INV>(v[grp], p, p.cols[cols[grp]].dst, gbs[grp], sh);
+                store_global<C, A, RB, INV>(v[grp], p, fft_col(p, cols[grp]).dst, gbs[grp], sh);
             } else {
                 const uint32_t sj = swz_c(jt | deposit<XBITS>((uint32_t)grp << W, M));
 #pragma unroll
@@ -429,7 +445,7 @@ __device__ __forceinline__ void roundT(uint32_t *sm, const GeoT &geo) {
             for (int m = 0; m < RR; m++) v[m] = sm[sj ^ swz_c((uint32_t)m << OA)];
             round_butterflies<C, A, RB, INV>(v, p, gb, sh);
             if constexpr (LAST) {
-                store_global<C, A, RB, INV>(v, p, p.cols[col].dst, gb, sh);
+                store_global<C, A, RB, INV>(v, p, fft_col(p, col).dst, gb, sh);
             } else {
 #pragma unroll
                 for (int m = 0; m < RR; m++) sm[sj ^ swz_c((uint32_t)m << OA)] = v[m];
@@ -479,6 +495,7 @@ int launchT_e(const FftLaunch &p, uint32_t n_cols, cudaStream_t st) {
     const uint64_t tiles = (uint64_t)n_cols << (p.N - C - G);
     const uint64_t per_cta = 1ull << (TT - C - G);
     STWO_REQUIRE(tiles % per_cta == 0, STWO_ERR_UNSUPPORTED_SIZE, "fft tile packing");
+    STWO_REQUIRE(tiles < (1ull << 32), STWO_ERR_UNSUPPORTED_SIZE, "fft launch of %llu tiles", (unsigned long long)tiles);
     const uint64_t blocks = tiles / per_cta;
     kern<<<(unsigned)blocks, 1 << (TT - E), smem, st>>>(p, n_cols);
     STWO_LAUNCH_CHECK("fftT_kernel");
@@ -714,8 +731,12 @@ int small_circle_point(const uint32_t *suffix_end, uint64_t avail, uint32_t N, b
 
 // Runs a transform over n_cols columns of one size. src[i] may equal dst[i]
 // (in place); for an extension read (L < N) src holds 2^L coefficients.
-int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
-                const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st) {
+// dev_table, when given, holds the same (srcs[i], dsts[i]) pairs in device memory; it
+// serves launches of more than 64 columns (the prover's tables travel in its uploaded
+// image, so its launch sequence stays capturable). Without it such launches stage a
+// table through the library's pool.
+int fft_columns_tab(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
+                    const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st, const void *dev_table) {
     if (n_cols == 0) return STWO_OK;
     STWO_REQUIRE(N >= 1 && N <= 30 && L <= N, STWO_ERR_UNSUPPORTED_SIZE, "fft log size %u unsupported", N);
     STWO_REQUIRE(tree != nullptr, STWO_ERR_INVALID_ARGUMENT, "null twiddle tree");
@@ -748,6 +769,29 @@ int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_c
     FftLaunch p{};
     p.tw = tree + (tree_size - (1ull << (N - 1)));
     p.N = N;
+    // More than 64 columns: every pass is one launch over a device table.
+    const FftColumn *table = nullptr;
+    void *staged = nullptr;
+    if (n_cols > (uint32_t)MAX_COLS_PER_LAUNCH) {
+        if (dev_table) {
+            table = static_cast<const FftColumn *>(dev_table);
+        } else {
+            std::vector<FftColumn> h(n_cols);
+            for (uint32_t i = 0; i < n_cols; i++) h[i] = FftColumn{srcs[i], dsts[i]};
+            int arc = pool_alloc(&staged, sizeof(FftColumn) * n_cols, st);
+            if (arc) return arc;
+            // from pageable memory: the copy has read h when it returns
+            STWO_CUDA_TRY(cudaMemcpyAsync(staged, h.data(), sizeof(FftColumn) * n_cols, cudaMemcpyHostToDevice, st));
+            table = static_cast<const FftColumn *>(staged);
+        }
+    }
+    struct FreeStaged {
+        void *p;
+        cudaStream_t st;
+        ~FreeStaged() {
+            if (p) cudaFreeAsync(p, st);
+        }
+    } free_staged{staged, st};
     std::vector<PassSpec> passes = plan_passes(L);
     if (!inv) std::reverse(passes.begin(), passes.end());
     for (size_t pi = 0; pi < passes.size(); pi++) {
@@ -759,10 +803,14 @@ int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_c
         bool first = pi == 0, last = pi + 1 == passes.size();
         p.src_mask = (first && L < N) ? ((1u << L) - 1u) : 0xffffffffu;
         p.scale2 = (inv && last) ? (m31_inv_pow2(N) << 1) : 0u;
-        for (uint32_t base = 0; base < n_cols; base += MAX_COLS_PER_LAUNCH) {
-            uint32_t cnt = std::min<uint32_t>(MAX_COLS_PER_LAUNCH, n_cols - base);
-            for (uint32_t i = 0; i < cnt; i++)
-                p.cols[i] = FftColumn{first ? srcs[base + i] : dsts[base + i], dsts[base + i]};
+        const uint32_t per_launch = table ? n_cols : (uint32_t)MAX_COLS_PER_LAUNCH;
+        p.table = table;
+        p.src_from_dst = first ? 0u : 1u;
+        for (uint32_t base = 0; base < n_cols; base += per_launch) {
+            uint32_t cnt = std::min<uint32_t>(per_launch, n_cols - base);
+            if (!table)
+                for (uint32_t i = 0; i < cnt; i++)
+                    p.cols[i] = FftColumn{first ? srcs[base + i] : dsts[base + i], dsts[base + i]};
             const uint32_t G = ps.hi - ps.lo;
             // Specialised 2^15 tiles: strided passes, or contiguous passes of >= 11 layers whose
             // tiles pack evenly into CTAs.
@@ -777,6 +825,11 @@ int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_c
         }
     }
     return STWO_OK;
+}
+
+int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
+                const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st) {
+    return fft_columns_tab(srcs, dsts, n_cols, N, L, tree, tree_size, inv, st, nullptr);
 }
 
 }  // namespace stwo

@@ -55,6 +55,8 @@ namespace stwo {
 
 int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
                 const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st);
+int fft_columns_tab(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
+                    const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st, const void *dev_table);
 int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_cols, const uint32_t *level_ncols,
                           uint32_t *const *layers, cudaStream_t st);
 int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const uint32_t *itw, uint64_t off,
@@ -734,6 +736,7 @@ uint64_t job_device_bytes(const Job &j, bool own_twiddles) {
     b += r(sizeof(ProofState) + 16 * (j.N + 4)) + r(4 * (j.N + 4)) + 2 * r(sizeof(QuotParamsDev));
     b += 2 * r(8 * j.N) + r(sizeof(EapDevPoly) * (j.N + 4)) + (2 * (j.L + j.B) + 8) * r(64) + r(8 * j.N);
     b += r(sizeof(TailParams));
+    b += 3 * r(16 * j.N);                                 // FFT column tables (src, dst) of the trace
     const uint64_t words = (uint64_t)j.n_queries * ((j.L + 2 + j.B) * 8 * 3 * 8 + 2 * (j.N + 16));
     b += r(words * sizeof(GatherReq)) + r(words * 4);     // decommitment gather
     return b;
@@ -901,6 +904,19 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     const size_t off_tpoly = up.add(tpoly.data(), sizeof(void *) * N);
     const size_t off_text = up.add(text.data(), sizeof(void *) * N);
     const size_t off_eap = up.add(eap.data(), sizeof(EapDevPoly) * eap_n);
+    // (src, dst) tables of the trace transforms: with more than 64 columns each pass is
+    // one launch over its table.
+    auto fft_table = [&](const std::vector<uint32_t *> &src, const std::vector<uint32_t *> &dst) {
+        std::vector<const void *> t(2 * N);
+        for (uint32_t c = 0; c < N; c++) {
+            t[2 * c] = src[c];
+            t[2 * c + 1] = dst[c];
+        }
+        return up.add(t.data(), sizeof(void *) * 2 * N);
+    };
+    const size_t off_fft_interp = fft_table(tpoly, tpoly);
+    const size_t off_fft_eval = fft_table(tpoly, tev);
+    const size_t off_fft_ext = B > 1 ? fft_table(tpoly, text) : 0;
     MerkleTree t_trace, t_comp, t_fri0;
     std::vector<MerkleTree> t_lay(n_layers);
     {
@@ -991,10 +1007,10 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
             STWO_LAUNCH_CHECK("wide_fib_trace_kernel");
         }
         // The trace columns are interpolated in place: they become the coefficient columns.
-        PV_TRY(fft_columns(tpoly.data(), tpoly.data(), N, L, L, itw, tsz, true, st));
+        PV_TRY(fft_columns_tab(tpoly.data(), tpoly.data(), N, L, L, itw, tsz, true, st, dev_at(off_fft_interp)));
         {
             std::vector<const uint32_t *> src(tpoly.begin(), tpoly.end());
-            PV_TRY(fft_columns(src.data(), tev.data(), N, L + B, L, tw, tsz, false, st));
+            PV_TRY(fft_columns_tab(src.data(), tev.data(), N, L + B, L, tw, tsz, false, st, dev_at(off_fft_eval)));
         }
         auto commit = [&](MerkleTree &t) {
             return merkle_tree_dev_async(t.max_log, t.level_tables.data(), t.level_n.data(), t.layers.data(), st);
@@ -1007,7 +1023,7 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         // ---- 2. composition on CanonicCoset(L + 1), committed on CanonicCoset(L + 1 + B)
         if (B > 1) {
             std::vector<const uint32_t *> src(tpoly.begin(), tpoly.end());
-            PV_TRY(fft_columns(src.data(), text.data(), N, E, L, tw, tsz, false, st));
+            PV_TRY(fft_columns_tab(src.data(), text.data(), N, E, L, tw, tsz, false, st, dev_at(off_fft_ext)));
         }
         uint32_t den_half[2];
         vanishing_inverses(L, den_half);

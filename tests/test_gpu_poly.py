@@ -142,6 +142,39 @@ def test_reference_abi_columns_entry_points(stwo, oracle):
         assert (b.to_numpy() == oracle.evaluate(hc, c, tw)).all()
 
 
+@pytest.mark.parametrize("log_size", [9, 12, 16])
+def test_fft_columns_beyond_one_parameter_block(stwo, oracle, log_size):
+    """More than 64 columns of one size run each pass as one launch over a device table
+    of column pointers: 300 columns, interpolated in place and extended to blowup 4,
+    compared with the oracle on columns around the 64-column boundaries."""
+    L = stwo._lib
+    lib = L.lib()
+    B = stwo.CudaBackend
+    r = rng(640 + log_size)
+    ncols, lb = 300, 2
+    tree = B.precompute_twiddles(stwo.CanonicCoset(log_size + lb).half_coset())
+    tw, itw = tree.twiddles.to_numpy(), tree.itwiddles.to_numpy()
+    vals = [m31(r, 1 << log_size) for _ in range(ncols)]
+    bufs = [stwo.BaseFieldVec.from_numpy(v) for v in vals]
+    outs = [stwo.BaseFieldVec.new_uninitialized(1 << (log_size + lb)) for _ in range(ncols)]
+    logs = L.u32_array([log_size] * ncols)
+    launches0 = lib.stwo_kernel_launches()
+    L.check(lib.stwo_interpolate_columns(L.ptr_array([b.device_ptr for b in bufs]), logs, ncols,
+                                         tree.itwiddles.device_ptr, len(tree.itwiddles), None))
+    L.check(lib.stwo_extend_evaluate_columns(L.ptr_array([b.device_ptr for b in bufs]), logs,
+                                             L.ptr_array([o.device_ptr for o in outs]), lb, ncols,
+                                             tree.twiddles.device_ptr, len(tree.twiddles), None))
+    L.check(lib.stwo_stream_synchronize(None))
+    passes = 1 if log_size <= 14 else 2
+    assert lib.stwo_kernel_launches() - launches0 == 2 * passes  # one launch per pass, not one per 64 columns
+    hc = _oc(oracle, stwo.CanonicCoset(log_size).half_coset())
+    ehc = _oc(oracle, stwo.CanonicCoset(log_size + lb).half_coset())
+    for k in (0, 63, 64, 127, 128, 255, 299):
+        coeffs = oracle.interpolate(hc, vals[k], itw)
+        assert (bufs[k].to_numpy() == coeffs).all(), k
+        assert (outs[k].to_numpy() == oracle.evaluate(ehc, coeffs, tw)).all(), k
+
+
 def test_fft_log24_roundtrip_and_linearity(stwo):
     """Full size (config: 8 columns at log 24, blowup 4): interpolate then evaluate
     is the identity; evaluation is linear (checked on a sampled subset)."""
