@@ -51,6 +51,15 @@ def load_oracle():
     return O
 
 
+def load_simd():
+    """The SIMD CPU baseline (oracle/simd.py: the oracle prover on vectorised, threaded
+    functions; a stand-in for stwo's SimdBackend with the same proof bytes)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import simd as S
+    S.lib()
+    return S
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -521,38 +530,39 @@ def job_desc(n_jobs):
             f"3 queries, pow_bits 5; {n_jobs} jobs per step admitted at once")
 
 
-def cpu_stream_sample(O, stwo, jobs, budget_s, threads):
-    """The oracle prover on jobs of the stream, in order, until budget_s of CPU work
-    (at least one job). Returns (jobs done, seconds, description)."""
-    O.set_threads(threads)
+def cpu_stream_sample(S, stwo, jobs, budget_s, threads, min_jobs=32):
+    """The SIMD CPU prover (S: oracle/simd.py) on jobs of the stream, in order, until
+    min_jobs are done or budget_s of CPU work has gone by (at least one job). Returns
+    (jobs done, seconds, description)."""
+    S.set_threads(threads)
     done, t0 = 0, time.perf_counter()
     for t in jobs:
         a0, a1 = stwo.wide_fib_inputs(t[0], t[2])
-        O.wide_fib_prove(t[0], t[1], a0, a1, 1, 3, 5)
+        S.wide_fib_prove(t[0], t[1], a0, a1, 1, 3, 5)
         done += 1
-        if time.perf_counter() - t0 >= budget_s:
+        if done >= min_jobs or time.perf_counter() - t0 >= budget_s:
             break
     dt = time.perf_counter() - t0
-    O.set_threads(1)
-    return done, dt, f"first {done} jobs of the stream, oracle prover on {threads} host threads"
+    return done, dt, (f"first {done} jobs of the stream, SIMD CPU prover ({S.variant()}, {S.lanes()} lanes) on "
+                      f"{threads} host threads")
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    O = load_oracle()
+    S = load_simd()
     stwo = load_package()
     threads = os.cpu_count() or 1
     for w in range(args.warmup):  # warm-up: one 64-column x 2^12 job each
-        cpu_stream_sample(O, stwo, [(12, 64, 7000 + w)], 0.0, threads)
-    # Each step: the stream's first jobs within --cpu-budget seconds (at least one job);
-    # steps stop early once --cpu-total-budget seconds have gone by, so the whole run
-    # stays within a few minutes (one large job alone takes tens of seconds).
+        cpu_stream_sample(S, stwo, [(12, 64, 7000 + w)], 0.0, threads, 1)
+    # Each step: the stream's first jobs until 32 are done or --cpu-budget seconds have
+    # gone by (at least one job); steps stop once --cpu-total-budget seconds have gone
+    # by, so the whole run stays within a few minutes.
     n_total, t_total, steps_done = 0, 0.0, 0
     for s in range(args.steps):
         if steps_done and t_total >= args.cpu_total_budget:
             break
-        n, dt, _ = cpu_stream_sample(O, stwo, job_stream(args.jobs, 1000 + s), args.cpu_budget, threads)
+        n, dt, _ = cpu_stream_sample(S, stwo, job_stream(args.jobs, 1000 + s), args.cpu_budget, threads)
         n_total += n
         t_total += dt
         steps_done += 1
@@ -566,8 +576,10 @@ def run_reference(args, rank, world):
                    "jobs_per_step": args.jobs},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{n_total} jobs over {steps_done} of {args.steps} steps (at most "
-                                   f"{args.cpu_total_budget:.0f} s in all), each step the stream's first jobs "
-                                   f"within {args.cpu_budget:.0f} s (oracle prover, {threads} threads)"},
+                                   f"{args.cpu_total_budget:.0f} s in all), each step the stream's first 32 jobs "
+                                   f"or {args.cpu_budget:.0f} s of them; SIMD CPU prover (SimdBackend stand-in, "
+                                   f"{S.variant()}, {S.lanes()} lanes, proof bytes equal to the oracle's), "
+                                   f"{threads} threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -859,7 +871,7 @@ def compact_line(full, detail_path):
     if sp:
         line["single_proofs"] = {
             name: dict({kk: v.get(kk) for kk in ("ms_median", "cached_ms_median", "oracle_ms", "equal_to_oracle",
-                                                  "verified")},
+                                                  "simd_cpu_ms", "simd_cpu_equal", "verified")},
                        phases_ms=v.get("phases_ms"))
             for name, v in sp.items()}
     ss = full.get("same_shape")
@@ -999,6 +1011,7 @@ def run_ours(args, rank, world, local_rank):
     singles, kernels, cpu, verified, batch, repeated = None, None, None, None, None, None
     if rank == 0:
         O = load_oracle() if not args.no_cpu_baseline else None
+        S = load_simd() if not args.no_cpu_baseline else None
         singles = {}
         # The reference CpuBackend's case (64 x 2^12), the large single proof (256 x 2^20,
         # pow_bits 10) and the reference's own end-to-end shape (1024 x 2^16,
@@ -1027,6 +1040,11 @@ def run_ours(args, rank, world, local_rank):
                 ent["oracle_threads"] = os.cpu_count() or 1
                 ent["equal_to_oracle"] = want == proof
                 O.set_threads(1)
+                S.set_threads(os.cpu_count() or 1)
+                t0 = time.perf_counter()
+                sproof, _ = S.wide_fib_prove(t[0], t[1], a0, a1, *t[2:])
+                ent["simd_cpu_ms"] = (time.perf_counter() - t0) * 1e3
+                ent["simd_cpu_equal"] = sproof == proof
             # The same proof repeated through a ProveCache (shared tree, own stream):
             # memory reused, launch sequence replayed as a CUDA graph.
             cs = torch.cuda.Stream(dev)
@@ -1049,9 +1067,9 @@ def run_ours(args, rank, world, local_rank):
             kernels = kernel_suite(stwo)
             batch = batch48(stwo, dev, args, O)
             repeated = same_shape(stwo, dev)
-        if O is not None and world == 1:
+        if S is not None and world == 1:
             threads = os.cpu_count() or 1
-            n, dt, desc = cpu_stream_sample(O, stwo, steps[0], args.cpu_budget, threads)
+            n, dt, desc = cpu_stream_sample(S, stwo, steps[0], args.cpu_stream_budget, threads)
             cpu = {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
 
     if rank == 0:
@@ -1221,7 +1239,10 @@ def main():
     ap.add_argument("--cpu-total-budget", type=float, default=120.0,
                     help="--impl reference: stop starting steps after this many seconds of CPU proving")
     ap.add_argument("--latency-jobs", type=int, default=2000, help="jobs per Poisson load level")
-    ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds of oracle work per CPU sample")
+    ap.add_argument("--cpu-budget", type=float, default=20.0,
+                    help="--impl reference: seconds of CPU proving per step at most (32 jobs otherwise)")
+    ap.add_argument("--cpu-stream-budget", type=float, default=45.0,
+                    help="seconds of CPU proving for the cpu_baseline leg at most (32 jobs otherwise)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--detail-out", default=os.path.join("gpurun_out", "bench_detail.json"),
                     help="where the full record goes (the printed line carries summaries)")

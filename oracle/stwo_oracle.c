@@ -405,6 +405,22 @@ int or_evaluate(coset_t hc, m31_t *v, const m31_t *tw, size_t tree_size) {
     return 0;
 }
 
+/* Column batches, as the prover drives them: every column interpolated in place;
+ * every column's coeff_len coefficients evaluated on the domain of half coset hc
+ * into out (zero-extended). */
+void or_interpolate_many(coset_t hc, m31_t *const *cols, size_t n_cols, const m31_t *itw, size_t tree_size) {
+    for (size_t c = 0; c < n_cols; c++) or_interpolate(hc, cols[c], itw, tree_size);
+}
+void or_evaluate_many(coset_t hc, const m31_t *const *coeffs, size_t coeff_len, m31_t *const *out, size_t n_cols,
+                      const m31_t *tw, size_t tree_size) {
+    const size_t n = (size_t)2 << hc.log_size;
+    for (size_t c = 0; c < n_cols; c++) {
+        memcpy(out[c], coeffs[c], coeff_len * 4);
+        memset(out[c] + coeff_len, 0, (n - coeff_len) * 4);
+        or_evaluate(hc, out[c], tw, tree_size);
+    }
+}
+
 /* Generic fold (CpuBackend poly/utils.rs `fold`): values split in halves, the
  * first factor multiplies the upper half. */
 static qm31_t fold_m31(const m31_t *vals, size_t n, const qm31_t *factors) {
@@ -438,6 +454,10 @@ qm31_t or_eval_at_point(const m31_t *coeffs, uint32_t L, spoint_t p) {
         x = double_x_q(x);
     }
     return fold_m31(coeffs, (size_t)1 << L, f);
+}
+
+void or_eval_at_point_many(const m31_t *const *coeffs, const uint32_t *log_sizes, size_t n, spoint_t p, qm31_t *out) {
+    for (size_t i = 0; i < n; i++) out[i] = or_eval_at_point(coeffs[i], log_sizes[i], p);
 }
 
 /* LinePoly::eval_at_point (bit-reversed coefficient storage): factors
@@ -709,6 +729,30 @@ void or_wide_fib_trace_row(m31_t a, m31_t b, size_t n, m31_t *row) {
     row[0] = a;
     if (n > 1) row[1] = b;
     for (size_t i = 2; i < n; i++) row[i] = m_add(m_mul(row[i - 1], row[i - 1]), m_mul(row[i - 2], row[i - 2]));
+}
+
+/* The trace's columns: row r of write_trace_row (wide_fibonacci.rs:177-191) in
+ * cols[c][r]. */
+void or_wide_fib_trace(const m31_t *a0, const m31_t *a1, size_t n_rows, size_t n_columns, m31_t *const *cols) {
+    m31_t *row = (m31_t *)malloc(sizeof(m31_t) * (n_columns ? n_columns : 1));
+    for (size_t r = 0; r < n_rows; r++) {
+        or_wide_fib_trace_row(a0[r], a1[r], n_columns, row);
+        for (size_t c = 0; c < n_columns; c++) cols[c][r] = row[c];
+    }
+    free(row);
+}
+
+/* Inverses of the vanishing polynomial of CanonicCoset(L) over CanonicCoset(L + 1)
+ * in bit-reversed order (wide_fibonacci.rs:101-104): 2^(L+1) values. */
+void or_vanishing_inverses(uint32_t L, m31_t *den_inv) {
+    const uint32_t E = L + 1;
+    const size_t ne = (size_t)1 << E;
+    coset_t hc = or_canonic_half_coset(E), vc = or_canonic_coset(L);
+    m31_t *den = (m31_t *)malloc(sizeof(m31_t) * ne);
+    for (size_t pos = 0; pos < ne; pos++)
+        den[pos] = or_coset_vanishing_m31(vc, or_circle_domain_at(hc, or_bit_reverse_index((uint32_t)pos, E)));
+    or_batch_inverse_m31(den, den_inv, ne);
+    free(den);
 }
 
 typedef struct { const m31_t *const *tr; size_t nc; const qm31_t *pw; const m31_t *den_inv; m31_t *const *out; } wf_ctx;

@@ -59,6 +59,12 @@ int  or_evaluate(coset_t half_coset, m31_t *values, const m31_t *twiddles, size_
 void or_evaluate_direct(coset_t half_coset, const m31_t *coeffs, uint32_t coeffs_log, m31_t *out);
 qm31_t or_eval_at_point(const m31_t *coeffs, uint32_t log_size, spoint_t p);
 qm31_t or_line_eval_at_point(const qm31_t *coeffs, uint32_t log_size, qm31_t x);
+void or_interpolate_many(coset_t half_coset, m31_t *const *cols, size_t n_cols, const m31_t *itwiddles,
+                         size_t tree_size);
+void or_evaluate_many(coset_t half_coset, const m31_t *const *coeffs, size_t coeff_len, m31_t *const *out,
+                      size_t n_cols, const m31_t *twiddles, size_t tree_size);
+void or_eval_at_point_many(const m31_t *const *coeffs, const uint32_t *log_sizes, size_t n, spoint_t p,
+                           qm31_t *out);
 
 /* ---- FriOps ---- */
 void or_fold_line(const m31_t *const src[4], size_t n, coset_t line_domain, qm31_t alpha,
@@ -86,6 +92,8 @@ void or_accumulate(m31_t *const left[4], const m31_t *const right[4], size_t n);
 /* ---- wide-Fibonacci AIR ---- */
 m31_t or_coset_vanishing_m31(coset_t coset, cpoint_t p);
 void or_wide_fib_trace_row(m31_t a, m31_t b, size_t n_columns, m31_t *row);
+void or_wide_fib_trace(const m31_t *a0, const m31_t *a1, size_t n_rows, size_t n_columns, m31_t *const *cols);
+void or_vanishing_inverses(uint32_t log_n_rows, m31_t *den_inv);
 void or_wide_fib_composition(const m31_t *const *trace_evals, size_t n_columns, size_t ext_size,
                              const qm31_t *coeff_powers, const m31_t *den_inv,
                              m31_t *const out[4]);

@@ -283,18 +283,10 @@ int or_wide_fib_prove(const or_wide_fib_job *job, const uint32_t *a0, const uint
 
     /* 1. trace: rows, interpolation, evaluation, commitment */
     m31_t **poly = (m31_t **)malloc(sizeof(m31_t *) * N), **tev = (m31_t **)malloc(sizeof(m31_t *) * N);
-    m31_t *row = col_alloc(N);
     for (uint32_t c = 0; c < N; c++) { poly[c] = col_alloc(n); tev[c] = col_alloc(nb); }
-    for (size_t r = 0; r < n; r++) {
-        or_wide_fib_trace_row(a0[r], a1[r], N, row);
-        for (uint32_t c = 0; c < N; c++) poly[c][r] = row[c];
-    }
-    free(row);
-    for (uint32_t c = 0; c < N; c++) {
-        or_interpolate(or_canonic_half_coset(L), poly[c], itw, tsz);
-        memcpy(tev[c], poly[c], n * 4);
-        or_evaluate(or_canonic_half_coset(L + B), tev[c], tw, tsz);
-    }
+    or_wide_fib_trace(a0, a1, n, N, poly);
+    or_interpolate_many(or_canonic_half_coset(L), poly, N, itw, tsz);
+    or_evaluate_many(or_canonic_half_coset(L + B), (const m31_t *const *)poly, n, tev, N, tw, tsz);
     tree_t t_trace;
     {
         uint32_t *logs = (uint32_t *)malloc(4 * N);
@@ -309,29 +301,18 @@ int or_wide_fib_prove(const or_wide_fib_job *job, const uint32_t *a0, const uint
     /* 2. composition on CanonicCoset(L + 1) */
     const qm31_t rc = ch_draw_felt(&ch);
     m31_t **text = (m31_t **)malloc(sizeof(m31_t *) * N);
-    for (uint32_t c = 0; c < N; c++) {
-        text[c] = col_alloc(ne);
-        memcpy(text[c], poly[c], n * 4);
-        or_evaluate(or_canonic_half_coset(E), text[c], tw, tsz);
-    }
-    m31_t *den = col_alloc(ne), *den_inv = col_alloc(ne);
-    {
-        coset_t hc = or_canonic_half_coset(E), vc = or_canonic_coset(L);
-        for (size_t pos = 0; pos < ne; pos++)
-            den[pos] = or_coset_vanishing_m31(vc, or_circle_domain_at(hc, or_bit_reverse_index((uint32_t)pos, E)));
-        or_batch_inverse_m31(den, den_inv, ne);
-    }
+    for (uint32_t c = 0; c < N; c++) text[c] = col_alloc(ne);
+    or_evaluate_many(or_canonic_half_coset(E), (const m31_t *const *)poly, n, text, N, tw, tsz);
+    m31_t *den_inv = col_alloc(ne);
+    or_vanishing_inverses(L, den_inv);
     qm31_t *powers = (qm31_t *)malloc(sizeof(qm31_t) * N);
     powers[0] = qone();
     for (uint32_t k = 1; k + 2 < N; k++) powers[k] = or_qm31_mul(powers[k - 1], rc);
     m31_t *comp[4], *cev[4];
     for (int k = 0; k < 4; k++) { comp[k] = col_alloc(ne); cev[k] = col_alloc(neb); }
     or_wide_fib_composition((const m31_t *const *)text, N, ne, powers, den_inv, comp);
-    for (int k = 0; k < 4; k++) {
-        or_interpolate(or_canonic_half_coset(E), comp[k], itw, tsz);
-        memcpy(cev[k], comp[k], ne * 4);
-        or_evaluate(or_canonic_half_coset(E + B), cev[k], tw, tsz);
-    }
+    or_interpolate_many(or_canonic_half_coset(E), comp, 4, itw, tsz);
+    or_evaluate_many(or_canonic_half_coset(E + B), (const m31_t *const *)comp, ne, cev, 4, tw, tsz);
     tree_t t_comp;
     {
         uint32_t logs[4] = {E + B, E + B, E + B, E + B};
@@ -350,8 +331,15 @@ int or_wide_fib_prove(const or_wide_fib_job *job, const uint32_t *a0, const uint
         oods.y = or_qm31_mul(qa(t, t), inv);
     }
     qm31_t *sampled = (qm31_t *)malloc(sizeof(qm31_t) * (N + 4));
-    for (uint32_t c = 0; c < N; c++) sampled[c] = or_eval_at_point(poly[c], L, oods);
-    for (int k = 0; k < 4; k++) sampled[N + k] = or_eval_at_point(comp[k], E, oods);
+    {
+        const m31_t **polys = (const m31_t **)malloc(sizeof(m31_t *) * (N + 4));
+        uint32_t *logs = (uint32_t *)malloc(sizeof(uint32_t) * (N + 4));
+        for (uint32_t c = 0; c < N; c++) { polys[c] = poly[c]; logs[c] = L; }
+        for (int k = 0; k < 4; k++) { polys[N + k] = comp[k]; logs[N + k] = E; }
+        or_eval_at_point_many(polys, logs, N + 4, oods, sampled);
+        free(polys);
+        free(logs);
+    }
     ch_mix_felts(&ch, sampled, N + 4);
     int rc_status = 0;
     {
@@ -568,7 +556,7 @@ int or_wide_fib_prove(const or_wide_fib_job *job, const uint32_t *a0, const uint
     tree_free(&t_fri0);
     for (uint32_t c = 0; c < N; c++) { free(poly[c]); free(tev[c]); free(text[c]); }
     free(poly); free(tev); free(text);
-    free(den); free(den_inv); free(powers); free(sampled);
+    free(den_inv); free(powers); free(sampled);
     free(tq[L + B].v);
     free(tq);
     free(queries.v);
