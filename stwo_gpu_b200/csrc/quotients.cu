@@ -30,10 +30,14 @@ namespace {
 
 using QuotParams = QuotParamsT<QUOT_MAX_COLS, QUOT_MAX_SAMPLES>;
 #ifndef QUOT_PREFETCH_N
-#define QUOT_PREFETCH_N 8
+#define QUOT_PREFETCH_N 4
 #endif
 constexpr int QUOT_PREFETCH = QUOT_PREFETCH_N;  // column loads per group (two groups in flight)
 static_assert(QUOT_PREFETCH % 4 == 0, "the fold cadence needs groups of a multiple of 4 columns");
+#ifndef QUOT_MIN_BLOCKS_N
+#define QUOT_MIN_BLOCKS_N 3
+#endif
+constexpr int QUOT_MIN_BLOCKS = QUOT_MIN_BLOCKS_N;  // CTAs of 256 threads resident per SM (register cap)
 
 // The kernel reads its parameters through get(): by value from the parameter block,
 // or from a device-resident block (the prover's, filled by the device channel).
@@ -64,118 +68,129 @@ __device__ __forceinline__ uint32_t reduce64(uint64_t x) {
     return reduce_once((uint32_t)s);
 }
 
-// den_b(p) of batch b at a domain point with x coordinate px and y coordinate py.
-template <class QP>
-__device__ __forceinline__ cm31 quot_den(const QP &p, uint32_t b, uint32_t px, uint32_t py) {
-    const cm31 t1 = {m31_sub(p.prx[b].a, px), p.prx[b].b};
-    const cm31 t2 = {m31_sub(p.pry[b].a, py), p.pry[b].b};
-    return cm31_sub(cm31_mul(t1, p.piy[b]), cm31_mul(t2, p.pix[b]));
+// 64-bit multiply-accumulate acc += a * b (one wide multiply-add on the FMA pipe).
+// (Written as plain C++: the same wide multiply-add as inline PTX measured 13% slower
+// over the whole kernel on B200, the compiler scheduling around the asm blocks.)
+__device__ __forceinline__ void mac_wide(uint64_t &acc, uint32_t a, uint32_t b) { acc = mac64(acc, a, b); }
+
+// Samples staged per batch: the batch's count rounded up to whole column groups.
+__host__ __device__ __forceinline__ uint32_t quot_padded(uint32_t count) {
+    return (count + QUOT_PREFETCH - 1) / QUOT_PREFETCH * QUOT_PREFETCH;
 }
 
-// STAGE: the CTA first copies every sample's column pointer and doubled coefficient
-// into shared memory (n_stage samples), so the column loop reads them there instead
-// of chasing col_idx -> cols through global memory (device-resident parameters).
+// The CTA first copies every sample's column pointer and coefficient into shared
+// memory, each batch padded to whole groups of QUOT_PREFETCH samples with zero
+// coefficients (and the batch's first column, so the padding loads stay in bounds):
+// the column loop then runs whole groups with no per-sample bound checks.
 // NB > 0: exactly NB sample batches, known at compile time, so the per-row
 // denominators stay in registers (the prover's two quotient groups have one batch
 // each: every column sampled at the OODS point); NB == 0: any count up to
-// QUOT_MAX_BATCHES.
-template <bool COLS_ON_DEVICE, bool STAGE, int NB, class PR>
-__global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ PR pr,
-                                                        const uint32_t *const *__restrict__ dev_cols,
-                                                        uint32_t n_stage, uint32_t two) {
+// QUOT_MAX_BATCHES. n_stage: the padded sample total.
+//
+// Per row pair (rows 2k and 2k + 1, at the domain point p and its conjugate):
+//  * den_b = K_b - p.x Pi.y +- p.y Pi.x: the two rows share both products;
+//  * the 2 NB denominators are inverted through their M31 norms
+//    (1 / (a + b i) = (a - b i) / (a^2 + b^2)) with one field inversion;
+//  * the batches' Horner coefficients are folded into their fields
+//    (quot_scale_batches), so each batch adds num_b / den_b to the sum.
+template <bool COLS_ON_DEVICE, int NB, class PR>
+__global__ void __launch_bounds__(256, QUOT_MIN_BLOCKS) quotients_kernel(const __grid_constant__ PR pr,
+                                                                         const uint32_t *const *__restrict__ dev_cols,
+                                                                         uint32_t n_stage, uint32_t two) {
     const auto &p = pr.get();
     extern __shared__ uint4 q_smem[];
     qm31 *s_c2 = reinterpret_cast<qm31 *>(q_smem);
-    const uint32_t **s_cols = reinterpret_cast<const uint32_t **>(s_c2 + (STAGE ? n_stage : 0));
-    if (STAGE) {
-        for (uint32_t j = threadIdx.x; j < n_stage; j += blockDim.x) {
-            s_c2[j] = p.c2[j];
-            s_cols[j] = COLS_ON_DEVICE ? dev_cols[p.col_idx[j]] : p.cols[p.col_idx[j]];
-        }
-        __syncthreads();
-    }
+    const uint32_t **s_cols = reinterpret_cast<const uint32_t **>(s_c2 + n_stage);
     constexpr int MAXB = NB > 0 ? NB : QUOT_MAX_BATCHES;
-    const uint64_t n_pairs = 1ull << (p.log_size - 1);
     const uint32_t n_batches = NB > 0 ? (uint32_t)NB : p.n_batches;
+    uint32_t ps[MAXB + 1];  // padded staged start of each batch
+    ps[0] = 0;
+#pragma unroll
+    for (int b = 0; b < MAXB; b++) {
+        if (NB == 0 && b >= (int)n_batches) break;
+        ps[b + 1] = ps[b] + quot_padded(p.batch_end[b] - (b > 0 ? p.batch_end[b - 1] : 0u));
+    }
+    for (uint32_t js = threadIdx.x; js < n_stage; js += blockDim.x) {
+        uint32_t b = 0, start = 0;  // the batch of staged index js and its padded start
+        for (;;) {
+            const uint32_t next = start + quot_padded(p.batch_end[b] - (b > 0 ? p.batch_end[b - 1] : 0u));
+            if (b + 1 >= n_batches || js < next) break;
+            start = next;
+            b++;
+        }
+        const uint32_t e0 = b > 0 ? p.batch_end[b - 1] : 0u, u = js - start;
+        const uint32_t j = e0 + u < p.batch_end[b] ? e0 + u : e0;
+        s_c2[js] = e0 + u < p.batch_end[b] ? p.c2[j] : qm31_zero();
+        s_cols[js] = COLS_ON_DEVICE ? dev_cols[p.col_idx[j]] : p.cols[p.col_idx[j]];
+    }
+    __syncthreads();
+    const uint64_t n_pairs = 1ull << (p.log_size - 1);
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_pairs;
          k += (uint64_t)gridDim.x * blockDim.x) {
-        // Rows 2k and 2k+1 are the domain point and its conjugate.
         const uint32_t hidx = bit_reverse_bits((uint32_t)k, p.log_size - 1);
         const cpoint pt = point_from_tables(p.tab, (p.half_init + p.half_step * hidx) & 0x7fffffffu);
-        const uint32_t ys[2] = {pt.y, m31_neg(pt.y)};
-        // The first column group's loads go out before the denominators' inversion, a
-        // chain of dependent products, so that their latency overlaps it.
+        // Column loads in groups of QUOT_PREFETCH, double-buffered: the next group's
+        // loads are in flight while this group is accumulated.
         uint2 va[QUOT_PREFETCH], vb[QUOT_PREFETCH];
-        {
-            const uint32_t j1 = p.batch_end[0];
+        auto load_group = [&](uint32_t jb, uint2 (&v)[QUOT_PREFETCH]) {
 #pragma unroll
             for (int u = 0; u < QUOT_PREFETCH; u++)
-                if ((uint32_t)u < j1) {
-                    const uint32_t *col = STAGE ? s_cols[u]
-                                                : (COLS_ON_DEVICE ? dev_cols[p.col_idx[u]] : p.cols[p.col_idx[u]]);
-                    va[u] = __ldg(reinterpret_cast<const uint2 *>(col) + k);
-                }
-        }
-        // Denominator inverses of both rows, all batches: one inversion (Montgomery's trick).
-        cm31 den[2][MAXB];
+                v[u] = __ldg(reinterpret_cast<const uint2 *>(s_cols[jb + u]) + k);
+        };
+        // The first column group's loads go out before the denominators' inversion, a
+        // chain of dependent products, so that their latency overlaps it.
+        if (ps[1] > 0) load_group(0, va);
+        // Inverse denominators of both rows, every batch.
+        cm31 dinv[2][MAXB];
         {
-            cm31 prefix = {1, 0};
-            cm31 pre[2][MAXB];
+            uint32_t nrm[2][MAXB], pre[2][MAXB];
+            uint32_t prefix = 1;
 #pragma unroll
             for (int b = 0; b < MAXB; b++) {
                 if (NB == 0 && b >= (int)n_batches) break;
+                const cm31 u = cm31_sub(p.den_k[b], cm31_scale(p.piy[b], pt.x));
+                const cm31 v = cm31_scale(p.pix[b], pt.y);
+                dinv[0][b] = cm31_add(u, v);
+                dinv[1][b] = cm31_sub(u, v);
 #pragma unroll
                 for (int s = 0; s < 2; s++) {
-                    den[s][b] = quot_den(p, b, pt.x, ys[s]);
-                    prefix = cm31_mul(prefix, den[s][b]);
+                    uint64_t n = (uint64_t)dinv[s][b].a * dinv[s][b].a;
+                    mac_wide(n, dinv[s][b].b, dinv[s][b].b);
+                    nrm[s][b] = reduce64_p(n);
+                    prefix = m31_mul(prefix, nrm[s][b]);
                     pre[s][b] = prefix;
                 }
             }
-            cm31 inv = cm31_inv(prefix);
+            uint32_t inv = m31_inv(prefix);
 #pragma unroll
             for (int b = MAXB - 1; b >= 0; b--) {
                 if (NB == 0 && b >= (int)n_batches) continue;
 #pragma unroll
                 for (int s = 1; s >= 0; s--) {
-                    const cm31 prev = (s == 1) ? pre[0][b] : (b > 0 ? pre[1][b - 1] : cm31{1, 0});
-                    const cm31 d = den[s][b];
-                    den[s][b] = cm31_mul(inv, prev);  // inverse of d
-                    inv = cm31_mul(inv, d);
+                    const uint32_t prev = (s == 1) ? pre[0][b] : (b > 0 ? pre[1][b - 1] : 1u);
+                    const uint32_t ni = m31_mul(inv, prev);  // 1 / norm
+                    inv = m31_mul(inv, nrm[s][b]);
+                    dinv[s][b] = {m31_mul(dinv[s][b].a, ni), m31_mul(m31_neg(dinv[s][b].b), ni)};
                 }
             }
         }
         qm31 acc[2] = {qm31_zero(), qm31_zero()};
-        uint32_t j0 = 0;
 #pragma unroll
         for (int b = 0; b < MAXB; b++) {
             if (NB == 0 && b >= (int)n_batches) break;
             uint64_t s0[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-            const uint32_t j1 = p.batch_end[b];
-            // Column loads in groups of QUOT_PREFETCH, double-buffered: the next group's
-            // loads are in flight while this group is accumulated.
-            auto load_group = [&](uint32_t jb, uint2 (&v)[QUOT_PREFETCH]) {
-#pragma unroll
-                for (int u = 0; u < QUOT_PREFETCH; u++) {
-                    const uint32_t j = jb + u;
-                    if (j < j1) {
-                        const uint32_t *col = STAGE ? s_cols[j]
-                                                    : (COLS_ON_DEVICE ? dev_cols[p.col_idx[j]] : p.cols[p.col_idx[j]]);
-                        v[u] = __ldg(reinterpret_cast<const uint2 *>(col) + k);
-                    }
-                }
-            };
+            const uint32_t j0 = ps[b], j1 = ps[b + 1];
             // 64-bit multiply-accumulates of canonical values (products below 2^62),
             // folded (fold64_fma) after every fourth column: a folded sum plus four
             // products stays below 2^64. The group size is a multiple of 4.
             auto consume = [&](uint32_t jb, const uint2 (&v)[QUOT_PREFETCH]) {
 #pragma unroll
                 for (int u = 0; u < QUOT_PREFETCH; u++) {
-                    if (jb + u >= j1) break;
-                    const qm31 c = STAGE ? s_c2[jb + u] : p.c2[jb + u];
-                    s0[0][0] = mac64(s0[0][0], v[u].x, c.a.a); s0[0][1] = mac64(s0[0][1], v[u].x, c.a.b);
-                    s0[0][2] = mac64(s0[0][2], v[u].x, c.b.a); s0[0][3] = mac64(s0[0][3], v[u].x, c.b.b);
-                    s0[1][0] = mac64(s0[1][0], v[u].y, c.a.a); s0[1][1] = mac64(s0[1][1], v[u].y, c.a.b);
-                    s0[1][2] = mac64(s0[1][2], v[u].y, c.b.a); s0[1][3] = mac64(s0[1][3], v[u].y, c.b.b);
+                    const qm31 c = s_c2[jb + u];
+                    mac_wide(s0[0][0], v[u].x, c.a.a); mac_wide(s0[0][1], v[u].x, c.a.b);
+                    mac_wide(s0[0][2], v[u].x, c.b.a); mac_wide(s0[0][3], v[u].x, c.b.b);
+                    mac_wide(s0[1][0], v[u].y, c.a.a); mac_wide(s0[1][1], v[u].y, c.a.b);
+                    mac_wide(s0[1][2], v[u].y, c.b.a); mac_wide(s0[1][3], v[u].y, c.b.b);
                     if (u % 4 == 3)
                         for (int s = 0; s < 2; s++)
                             for (int t = 0; t < 4; t++) s0[s][t] = fold64_fma(s0[s][t], two);
@@ -188,13 +203,14 @@ __global__ void __launch_bounds__(256) quotients_kernel(const __grid_constant__ 
                 if (jb + 2 * QUOT_PREFETCH < j1) load_group(jb + 2 * QUOT_PREFETCH, va);
                 if (jb + QUOT_PREFETCH < j1) consume(jb + QUOT_PREFETCH, vb);
             }
-            j0 = j1;
+            // num_s = sum_j c_j col_j - (a y_s + b) with y_1 = -y_0: the rows share a y_0.
+            const qm31 ay = qm31_scale(p.a_sum[b], pt.y);
+            const qm31 lin[2] = {qm31_add(p.b_sum[b], ay), qm31_sub(p.b_sum[b], ay)};
+#pragma unroll
             for (int s = 0; s < 2; s++) {
-                qm31 num = {{reduce64(s0[s][0]), reduce64(s0[s][1])}, {reduce64(s0[s][2]), reduce64(s0[s][3])}};
-                qm31 lin = qm31_add(qm31_scale(p.a_sum[b], ys[s]), p.b_sum[b]);
-                num = qm31_sub(num, lin);
-                acc[s] = b == 0 ? qm31_mul_cm31(num, den[s][b])
-                                : qm31_add(qm31_mul(acc[s], p.batch_coeff[b]), qm31_mul_cm31(num, den[s][b]));
+                qm31 num = {{reduce64_p(s0[s][0]), reduce64_p(s0[s][1])}, {reduce64_p(s0[s][2]), reduce64_p(s0[s][3])}};
+                num = qm31_sub(num, lin[s]);
+                acc[s] = qm31_add(acc[s], qm31_mul_cm31(num, dinv[s][b]));
             }
         }
         reinterpret_cast<uint2 *>(p.out[0])[k] = make_uint2(acc[0].a.a, acc[1].a.a);
@@ -280,21 +296,24 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
         off += bsz[b];
         p->batch_end[b] = off;
     }
+    quot_scale_batches(*p, n_batches);
     uint64_t pairs = 1ull << (log_size - 1);
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    // Every sample's coefficient and column pointer staged in shared memory (at most
-    // QUOT_MAX_SAMPLES x 24 bytes = 12 KiB): the column loop then reads them there
+    // Every sample's coefficient and column pointer staged in shared memory, each batch
+    // padded to whole column groups (at most (QUOT_MAX_SAMPLES + QUOT_MAX_BATCHES *
+    // QUOT_PREFETCH) x 24 bytes, 15 KiB): the column loop then reads them there
     // instead of indexing the parameter block at run time.
-    const uint32_t n_samples = off;
-    const size_t smem = (size_t)n_samples * (sizeof(qm31) + sizeof(void *));
+    uint32_t n_stage = 0;
+    for (uint32_t b = 0; b < n_batches; b++) n_stage += quot_padded(bsz[b]);
+    const size_t smem = (size_t)n_stage * (sizeof(qm31) + sizeof(void *));
     auto launch = [&](auto nb) {
         constexpr int NBV = decltype(nb)::value;
         if (cols_on_device)
-            quotients_kernel<true, true, NBV><<<(unsigned)blocks, 256, smem, st>>>(*holder, cols, n_samples, 2u);
+            quotients_kernel<true, NBV><<<(unsigned)blocks, 256, smem, st>>>(*holder, cols, n_stage, 2u);
         else
-            quotients_kernel<false, true, NBV><<<(unsigned)blocks, 256, smem, st>>>(*holder, nullptr, n_samples, 2u);
+            quotients_kernel<false, NBV><<<(unsigned)blocks, 256, smem, st>>>(*holder, nullptr, n_stage, 2u);
     };
     switch (n_batches) {
     case 1: launch(std::integral_constant<int, 1>{}); break;
@@ -310,12 +329,13 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
 int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t n_samples, cudaStream_t st) {
     STWO_REQUIRE(log_size >= 1 && log_size <= 31, STWO_ERR_UNSUPPORTED_SIZE, "domain log size %u", log_size);
     STWO_REQUIRE(n_samples >= 1 && n_samples <= 1024, STWO_ERR_UNSUPPORTED_SIZE, "%u samples", n_samples);
-    const size_t smem = (size_t)n_samples * (sizeof(qm31) + sizeof(void *));
+    const uint32_t n_stage = quot_padded(n_samples);  // one batch
+    const size_t smem = (size_t)n_stage * (sizeof(qm31) + sizeof(void *));
     uint64_t pairs = 1ull << (log_size - 1);
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    quotients_kernel<false, true, 1><<<(unsigned)blocks, 256, smem, st>>>(QuotByRef{p_dev}, nullptr, n_samples, 2u);
+    quotients_kernel<false, 1><<<(unsigned)blocks, 256, smem, st>>>(QuotByRef{p_dev}, nullptr, n_stage, 2u);
     STWO_LAUNCH_CHECK("quotients_kernel");
     return STWO_OK;
 }

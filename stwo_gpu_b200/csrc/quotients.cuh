@@ -26,6 +26,7 @@ struct QuotParamsT {
     uint16_t col_idx[MAXS];
     qm31 a_sum[QUOT_MAX_BATCHES], b_sum[QUOT_MAX_BATCHES], batch_coeff[QUOT_MAX_BATCHES];
     cm31 prx[QUOT_MAX_BATCHES], pry[QUOT_MAX_BATCHES], pix[QUOT_MAX_BATCHES], piy[QUOT_MAX_BATCHES];
+    cm31 den_k[QUOT_MAX_BATCHES];          // Pr.x Pi.y - Pr.y Pi.x: den_b(p) = K_b - p.x Pi.y + p.y Pi.x
     uint32_t batch_end[QUOT_MAX_BATCHES];  // cumulative sample counts
     uint32_t n_batches;
     uint32_t half_init, half_step;        // half coset indices
@@ -41,13 +42,21 @@ using QuotParamsDev = QuotParamsT<1024, 1024>;
 // the batch coefficient rc^count and, per sample j with alpha = rc^(j+1),
 // (a, b, c) = alpha * (conj(v) - v, v*c0 - a*py, c0), c0 = conj(py) - py
 // (complex_conjugate_line_coeffs); a and b summed per batch, c stored per sample.
+// With several batches, quot_scale_batches then folds the accumulation's Horner
+// coefficients into these fields.
 template <class QP>
-__host__ __device__ inline void quot_fill_batch(QP &p, uint32_t b, qm31 rc, qm31 px, qm31 py, const qm31 *vals,
-                                                uint32_t count, uint32_t off) {
+__host__ __device__ inline void quot_fill_point(QP &p, uint32_t b, qm31 px, qm31 py) {
     p.prx[b] = px.a;
     p.pix[b] = px.b;
     p.pry[b] = py.a;
     p.piy[b] = py.b;
+    p.den_k[b] = cm31_sub(cm31_mul(px.a, py.b), cm31_mul(py.a, px.b));
+}
+
+template <class QP>
+__host__ __device__ inline void quot_fill_batch(QP &p, uint32_t b, qm31 rc, qm31 px, qm31 py, const qm31 *vals,
+                                                uint32_t count, uint32_t off) {
+    quot_fill_point(p, b, px, py);
     p.batch_coeff[b] = qm31_pow(rc, count);
     const qm31 c0 = qm31_sub(qm31_conj(py), py);
     qm31 alpha = qm31_one(), as = qm31_zero(), bs = qm31_zero();
@@ -65,6 +74,25 @@ __host__ __device__ inline void quot_fill_batch(QP &p, uint32_t b, qm31 rc, qm31
     }
     p.a_sum[b] = as;
     p.b_sum[b] = bs;
+}
+
+// The accumulation over batches, acc = acc * rc^|b| + num_b / den_b in batch order
+// (quotients.cu:111-178), equals sum_b C_b num_b / den_b with C_b the product of the
+// later batches' coefficients rc^|b'|. num_b is linear in the batch's a, b and c
+// fields, so multiplying those by C_b (here, once per call) leaves the kernel a plain
+// sum over batches. The last batch has C = 1; with one batch nothing changes.
+template <class QP>
+__host__ __device__ inline void quot_scale_batches(QP &p, uint32_t n_batches) {
+    qm31 cb = qm31_one();
+    for (int b = (int)n_batches - 1; b >= 0; b--) {
+        if (b + 1 < (int)n_batches) {
+            cb = qm31_mul(cb, p.batch_coeff[b + 1]);
+            const uint32_t j0 = b == 0 ? 0u : p.batch_end[b - 1];
+            for (uint32_t j = j0; j < p.batch_end[b]; j++) p.c2[j] = qm31_mul(p.c2[j], cb);
+            p.a_sum[b] = qm31_mul(p.a_sum[b], cb);
+            p.b_sum[b] = qm31_mul(p.b_sum[b], cb);
+        }
+    }
 }
 
 // Sum of one QM31 per thread over a CTA of blockDim.x <= 1024 threads; every thread
@@ -85,7 +113,8 @@ __device__ inline qm31 block_sum_qm31(qm31 v, qm31 *sh) {
 }
 
 // quot_fill_batch by a whole CTA: thread t takes samples t, t + T, ... with
-// alpha = rc^(j+1), and the a / b sums are reduced across the CTA.
+// alpha = rc^(j+1), and the a / b sums are reduced across the CTA. For the prover's
+// single-batch groups (no quot_scale_batches step is needed with one batch).
 template <class QP>
 __device__ inline void quot_fill_batch_block(QP &p, uint32_t b, qm31 rc, qm31 px, qm31 py, const qm31 *vals,
                                              uint32_t count, uint32_t off, qm31 *sh) {
@@ -108,10 +137,7 @@ __device__ inline void quot_fill_batch_block(QP &p, uint32_t b, qm31 rc, qm31 px
     as = block_sum_qm31(as, sh);
     bs = block_sum_qm31(bs, sh);
     if (threadIdx.x == 0) {
-        p.prx[b] = px.a;
-        p.pix[b] = px.b;
-        p.pry[b] = py.a;
-        p.piy[b] = py.b;
+        quot_fill_point(p, b, px, py);
         p.batch_coeff[b] = qm31_pow(rc, count);
         p.a_sum[b] = as;
         p.b_sum[b] = bs;
