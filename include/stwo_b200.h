@@ -49,6 +49,8 @@ enum {
     STWO_ERR_UNSUPPORTED_SIZE = 2,
     STWO_ERR_OUT_OF_MEMORY = 3,
     STWO_ERR_CUDA = 4,
+    STWO_ERR_CANCELLED = 5,  /* a queued server job removed by stwo_server_cancel */
+    STWO_ERR_TIMEOUT = 6,    /* a server job that waited in the queue past its limit */
 };
 
 /* =====================================================================
@@ -376,6 +378,19 @@ double stwo_server_now_ms(void);
 int stwo_server_mark_epoch(stwo_prover_server *server);
 /* Drops queued jobs, waits for running ones, frees everything (including unpolled proofs). */
 void stwo_server_destroy(stwo_prover_server *server);
+/* Removes a job that is still queued: its result (status STWO_ERR_CANCELLED) is
+ * posted for stwo_server_poll. A job that is already running cannot be cancelled (its
+ * kernels are in flight on its stream); it finishes normally. Returns
+ * STWO_ERR_INVALID_ARGUMENT when no queued job has that id. */
+int stwo_server_cancel(stwo_prover_server *server, uint64_t job_id);
+/* Jobs that wait in the queue longer than queue_timeout_ms (0: no limit, the default)
+ * are not started: their result carries STWO_ERR_TIMEOUT. Checked whenever a worker
+ * looks for work and while stwo_server_poll waits. */
+int stwo_server_set_queue_timeout(stwo_prover_server *server, double queue_timeout_ms);
+/* Test hook: the next n device allocations from the library's pool fail with
+ * STWO_ERR_OUT_OF_MEMORY as if the device were full (the allocation call is not made),
+ * so tests can check that a server job fails alone and the server carries on. */
+void stwo_debug_fail_allocations(uint32_t n);
 
 #ifdef __cplusplus
 }

@@ -60,6 +60,10 @@ class StwoError(RuntimeError):
     pass
 
 
+# status codes (include/stwo_b200.h)
+OK, ERR_INVALID_ARGUMENT, ERR_UNSUPPORTED_SIZE, ERR_OUT_OF_MEMORY, ERR_CUDA, ERR_CANCELLED, ERR_TIMEOUT = range(7)
+
+
 # (name, restype, argtypes); every symbol declared in include/stwo_b200.h.
 SIGNATURES = [
     # reference-compatible tier (stwo_gpu_backend/src/cuda/bindings.rs:75-271)
@@ -140,6 +144,9 @@ SIGNATURES = [
     ("stwo_server_mark_epoch", C.c_int, [vp]),
     ("stwo_probe_m31_butterflies", C.c_int, [u32, vp, u64, C.POINTER(u64), vp]),
     ("stwo_server_destroy", None, [vp]),
+    ("stwo_server_cancel", C.c_int, [vp, u64]),
+    ("stwo_server_set_queue_timeout", C.c_int, [vp, C.c_double]),
+    ("stwo_debug_fail_allocations", None, [u32]),
 ]
 
 _lib = None

@@ -112,7 +112,22 @@ int library_pool(cudaMemPool_t *pool) {
     return STWO_OK;
 }
 
+namespace {
+std::atomic<uint32_t> g_fail_allocs{0};  // stwo_debug_fail_allocations
+
+bool take_injected_failure() {
+    uint32_t n = g_fail_allocs.load();
+    while (n > 0)
+        if (g_fail_allocs.compare_exchange_weak(n, n - 1)) return true;
+    return false;
+}
+}  // namespace
+
 int pool_alloc(void **p, size_t bytes, cudaStream_t st) {
+    if (take_injected_failure()) {
+        *p = nullptr;
+        return set_error(STWO_ERR_OUT_OF_MEMORY, "device allocation of %zu bytes failed: injected failure", bytes);
+    }
     cudaMemPool_t pool;
     int rc = library_pool(&pool);
     if (rc) return rc;
@@ -218,6 +233,8 @@ extern "C" {
 const char *stwo_last_error(void) { return g_last_error; }
 
 void stwo_clear_last_error(void) { clear_error(); }
+
+void stwo_debug_fail_allocations(uint32_t n) { g_fail_allocs.store(n); }
 
 uint64_t stwo_kernel_launches(void) { return g_kernel_launches.load(std::memory_order_relaxed); }
 

@@ -53,6 +53,7 @@ struct stwo_prover_server {
     uint32_t *tw = nullptr, *itw = nullptr;
     uint64_t tree_size = 0;
     bool stopping = false;
+    double queue_timeout_ms = 0;  // 0: queued jobs wait without limit
     bool blocking_wait = true;  // workers yield their core while waiting on the device...
     uint32_t spin_us = 2000;    // ...after polling this long
     bool use_priorities = true; // per-job stream priority by job size
@@ -68,8 +69,38 @@ struct stwo_prover_server {
     std::deque<stwo_server_result> done;
     std::vector<std::thread> workers;
 
+    // A finished result for a job that never ran (cancelled or timed out).
+    void post_unrun(const PendingJob &j, int status, const char *msg) {
+        stwo_server_result r{};
+        r.job_id = j.id;
+        r.status = status;
+        strncpy(r.error, msg, sizeof(r.error) - 1);
+        r.submit_ms = j.submit_ms;
+        r.start_ms = r.done_ms = steady_ms();
+        r.device_done_ms = -1.0;
+        done.push_back(r);
+    }
+
+    // Queued jobs past the queue timeout leave the queue with STWO_ERR_TIMEOUT (mu held).
+    bool expire() {
+        if (queue_timeout_ms <= 0) return false;
+        const double now = steady_ms();
+        bool any = false;
+        for (auto it = pending.begin(); it != pending.end();) {
+            if (now - it->submit_ms > queue_timeout_ms) {
+                post_unrun(*it, STWO_ERR_TIMEOUT, "job waited in the queue past the server's queue timeout");
+                it = pending.erase(it);
+                any = true;
+            } else {
+                ++it;
+            }
+        }
+        return any;
+    }
+
     // The first pending job (in arrival order) whose bound fits the budget's remainder.
     bool take(PendingJob &out) {
+        if (expire()) cv_done.notify_all();
         for (auto it = pending.begin(); it != pending.end(); ++it) {
             if (in_use + it->bytes <= budget) {
                 out = std::move(*it);
@@ -170,19 +201,25 @@ struct stwo_prover_server {
                 if (ev && cudaEventElapsedTime(&ms, epoch, ev) == cudaSuccess) r.device_done_ms = ms;
                 else cudaGetLastError();
             }
-            // A queued job of the same shape takes this one's place (and budget) at once.
+            // A queued job of the same shape takes this one's place (and budget) at once, if
+            // it is the job that admission in arrival order would take next with this job's
+            // budget released: a job queued ahead of it that would fit goes first, so a
+            // run of same-shape arrivals cannot hold back an earlier job of another shape.
             PendingJob next;
             {
                 std::lock_guard<std::mutex> lock(mu);
                 done.push_back(r);
+                expire();
                 if (cache.valid && !stopping)
-                    for (auto it = pending.begin(); it != pending.end(); ++it)
+                    for (auto it = pending.begin(); it != pending.end(); ++it) {
+                        if (in_use - j.bytes + it->bytes > budget) continue;  // admission would pass it
                         if (same_shape(it->job, j.job) && it->bytes == j.bytes) {
                             next = std::move(*it);
                             pending.erase(it);
                             have_next = true;
-                            break;
                         }
+                        break;
+                    }
             }
             cv_done.notify_all();
             if (have_next) {
@@ -265,15 +302,22 @@ stwo_prover_server *stwo_server_create(uint32_t n_workers, uint64_t device_budge
 }
 
 namespace {
-int submit_job(stwo_prover_server *s, PendingJob &&j) {
-    const uint64_t bytes = wide_fib_job_device_bytes(&j.job, false);
+// Checks a job against the server before anything is copied: its parameters, its
+// domain against the shared twiddle tree, its device bound against the budget.
+int validate_job(stwo_prover_server *s, const stwo_wide_fib_job &job, uint64_t *bytes_out) {
+    STWO_REQUIRE(job.log_n_rows <= 30 && job.log_blowup <= 30 &&
+                     job.log_n_rows + 1 + job.log_blowup <= s->max_domain_log,
+                 STWO_ERR_UNSUPPORTED_SIZE, "job domain log size %u exceeds the server's %u",
+                 job.log_n_rows + 1 + job.log_blowup, s->max_domain_log);
+    const uint64_t bytes = wide_fib_job_device_bytes(&job, false);
     STWO_REQUIRE(bytes, STWO_ERR_UNSUPPORTED_SIZE, "job parameters unsupported");
-    STWO_REQUIRE(j.job.log_n_rows + 1 + j.job.log_blowup <= s->max_domain_log, STWO_ERR_UNSUPPORTED_SIZE,
-                 "job domain log size %u exceeds the server's %u", j.job.log_n_rows + 1 + j.job.log_blowup,
-                 s->max_domain_log);
     STWO_REQUIRE(bytes <= s->budget, STWO_ERR_OUT_OF_MEMORY, "job needs %llu device bytes, budget is %llu",
                  (unsigned long long)bytes, (unsigned long long)s->budget);
-    j.bytes = bytes;
+    *bytes_out = bytes;
+    return STWO_OK;
+}
+
+int submit_job(stwo_prover_server *s, PendingJob &&j) {
     j.submit_ms = steady_ms();
     {
         std::lock_guard<std::mutex> lock(s->mu);
@@ -288,8 +332,9 @@ int submit_job(stwo_prover_server *s, PendingJob &&j) {
 int stwo_server_submit(stwo_prover_server *s, uint64_t job_id, const stwo_wide_fib_job *job, const uint32_t *a0,
                        const uint32_t *a1) {
     STWO_REQUIRE(s && job && a0 && a1, STWO_ERR_INVALID_ARGUMENT, "null argument");
-    STWO_REQUIRE(job->log_n_rows <= 30, STWO_ERR_UNSUPPORTED_SIZE, "job parameters unsupported");
     PendingJob j;
+    int rc = validate_job(s, *job, &j.bytes);  // before copying 2^log_n_rows words of each input
+    if (rc) return rc;
     j.id = job_id;
     j.job = *job;
     const size_t rows = 1ull << job->log_n_rows;
@@ -302,6 +347,8 @@ int stwo_server_submit_device(stwo_prover_server *s, uint64_t job_id, const stwo
                               const uint32_t *a0_dev, const uint32_t *a1_dev) {
     STWO_REQUIRE(s && job && a0_dev && a1_dev, STWO_ERR_INVALID_ARGUMENT, "null argument");
     PendingJob j;
+    int rc = validate_job(s, *job, &j.bytes);
+    if (rc) return rc;
     j.id = job_id;
     j.job = *job;
     j.a0_dev = a0_dev;
@@ -313,8 +360,20 @@ uint32_t stwo_server_poll(stwo_prover_server *s, stwo_server_result *out, uint32
     if (!s || !out || max_results == 0) return 0;
     std::unique_lock<std::mutex> lock(s->mu);
     auto ready = [&] { return !s->done.empty() || (s->pending.empty() && s->running == 0); };
-    if (timeout_ms < 0) s->cv_done.wait(lock, ready);
-    else if (timeout_ms > 0) s->cv_done.wait_for(lock, std::chrono::milliseconds(timeout_ms), ready);
+    if (s->queue_timeout_ms > 0) {
+        // With a queue timeout, jobs may expire while every worker is busy: check every
+        // few milliseconds while waiting.
+        const double until = timeout_ms < 0 ? 1e300 : steady_ms() + timeout_ms;
+        for (;;) {
+            s->expire();
+            if (ready() || steady_ms() >= until) break;
+            s->cv_done.wait_for(lock, std::chrono::milliseconds(2));
+        }
+    } else if (timeout_ms < 0) {
+        s->cv_done.wait(lock, ready);
+    } else if (timeout_ms > 0) {
+        s->cv_done.wait_for(lock, std::chrono::milliseconds(timeout_ms), ready);
+    }
     uint32_t n = 0;
     while (n < max_results && !s->done.empty()) {
         out[n++] = s->done.front();
@@ -348,6 +407,30 @@ void stwo_server_graph_stats(stwo_prover_server *s, uint64_t *slab_reuses, uint6
     if (!s) return;
     if (slab_reuses) *slab_reuses = s->slab_reuses.load();
     if (graph_replays) *graph_replays = s->graph_replays.load();
+}
+
+int stwo_server_cancel(stwo_prover_server *s, uint64_t job_id) {
+    STWO_REQUIRE(s, STWO_ERR_INVALID_ARGUMENT, "null server");
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        auto it = std::find_if(s->pending.begin(), s->pending.end(), [&](const PendingJob &j) { return j.id == job_id; });
+        STWO_REQUIRE(it != s->pending.end(), STWO_ERR_INVALID_ARGUMENT,
+                     "job %llu is not queued (running, finished or unknown)", (unsigned long long)job_id);
+        s->post_unrun(*it, STWO_ERR_CANCELLED, "job cancelled before it started");
+        s->pending.erase(it);
+    }
+    s->cv_done.notify_all();
+    return STWO_OK;
+}
+
+int stwo_server_set_queue_timeout(stwo_prover_server *s, double queue_timeout_ms) {
+    STWO_REQUIRE(s && queue_timeout_ms >= 0, STWO_ERR_INVALID_ARGUMENT, "invalid queue timeout");
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->queue_timeout_ms = queue_timeout_ms;
+    }
+    s->cv_work.notify_all();
+    return STWO_OK;
 }
 
 void stwo_server_destroy(stwo_prover_server *s) {

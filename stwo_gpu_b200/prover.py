@@ -152,6 +152,16 @@ class ProofServer:
         L.clear_error()
         L.check(L.lib().stwo_server_submit_device(self._s, job_id, C.byref(job.c()), a0_dev, a1_dev))
 
+    def cancel(self, job_id):
+        """Removes a job that is still queued (its result reports STWO_ERR_CANCELLED);
+        raises if the job is running, finished or unknown."""
+        L.check(L.lib().stwo_server_cancel(self._s, job_id))
+
+    def set_queue_timeout(self, ms):
+        """Queued jobs that wait longer than ms (0: no limit) are not started; their
+        results report STWO_ERR_TIMEOUT."""
+        L.check(L.lib().stwo_server_set_queue_timeout(self._s, float(ms)))
+
     def mark_epoch(self):
         """Sets the device epoch of device_done_ms (records and waits for an event on an
         idle stream of the server's): call it with nothing running, before a batch."""

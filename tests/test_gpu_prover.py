@@ -397,3 +397,112 @@ def test_tunables_change_speed_not_results():
         for name, value in [("fft_ept_contig_small", 6), ("fft_ept_contig_large", 6), ("fft_ept_strided", 6),
                             ("merkle_sub_threads", 256), ("merkle_sub_spread", 3), ("eval_at_point_groups_log", 0)]:
             lib.stwo_set_tunable(name.encode(), value)
+
+
+def _collect(srv, n):
+    got = {}
+    while len(got) < n:
+        for r in srv.poll(timeout_ms=-1):
+            got[r["job_id"]] = r
+    return got
+
+
+def _wait_running(srv):
+    import time
+    t0 = time.time()
+    while srv.stats()["running"] == 0:
+        assert time.time() - t0 < 30, "the first job never started"
+        time.sleep(0.0005)
+
+
+BUSY_JOB = (19, 256, 1, 3, 5)  # keeps a single worker busy for several milliseconds
+
+
+def _small_jobs(n):
+    return [(8 + (i % 3), 16, 1, 3, 5) for i in range(n)]
+
+
+def test_server_cancels_queued_jobs_only():
+    """A queued job leaves the queue with STWO_ERR_CANCELLED and never runs; the running
+    job and unknown ids cannot be cancelled; every other job proves exactly as alone."""
+    stwo = load_package()
+    L = stwo._lib
+    small = _small_jobs(3)
+    alone = [stwo.prove_wide_fib(job_of(t), *stwo.wide_fib_inputs(t[0], 50 + i))[0] for i, t in enumerate(small)]
+    with stwo.ProofServer(n_workers=1, device_budget_bytes=16 << 30, max_domain_log=21) as srv:
+        srv.submit(0, job_of(BUSY_JOB), *stwo.wide_fib_inputs(BUSY_JOB[0], 5))
+        _wait_running(srv)
+        for i, t in enumerate(small):
+            srv.submit(1 + i, job_of(t), *stwo.wide_fib_inputs(t[0], 50 + i))
+        srv.cancel(2)
+        with pytest.raises(L.StwoError):
+            srv.cancel(2)  # no longer queued
+        with pytest.raises(L.StwoError):
+            srv.cancel(99)  # unknown
+        got = _collect(srv, 4)
+        assert srv.stats() == {"pending": 0, "running": 0, "device_bytes_in_use": 0}
+    assert got[0]["status"] == L.OK
+    assert got[2]["status"] == L.ERR_CANCELLED and got[2]["proof"] is None
+    assert got[1]["status"] == got[3]["status"] == L.OK
+    assert got[1]["proof"] == alone[0] and got[3]["proof"] == alone[2]
+
+
+def test_server_queue_timeout():
+    """Jobs that wait in the queue past the server's queue timeout end with
+    STWO_ERR_TIMEOUT without running (reported while the worker is still busy); with
+    the limit lifted, jobs run again."""
+    stwo = load_package()
+    L = stwo._lib
+    small = _small_jobs(3)
+    with stwo.ProofServer(n_workers=1, device_budget_bytes=16 << 30, max_domain_log=21) as srv:
+        srv.submit(0, job_of(BUSY_JOB), *stwo.wide_fib_inputs(BUSY_JOB[0], 6))
+        _wait_running(srv)
+        srv.set_queue_timeout(0.2)
+        for i, t in enumerate(small):
+            srv.submit(1 + i, job_of(t), *stwo.wide_fib_inputs(t[0], 60 + i))
+        got = _collect(srv, 4)
+        assert got[0]["status"] == L.OK and stwo.verify(got[0]["proof"], *BUSY_JOB)
+        for k in (1, 2, 3):
+            assert got[k]["status"] == L.ERR_TIMEOUT and got[k]["proof"] is None
+        srv.set_queue_timeout(0)
+        t = small[0]
+        srv.submit(7, job_of(t), *stwo.wide_fib_inputs(t[0], 70))
+        r = _collect(srv, 1)[7]
+        assert r["status"] == L.OK and stwo.verify(r["proof"], *t)
+        assert srv.stats()["device_bytes_in_use"] == 0
+
+
+def test_server_job_survives_injected_allocation_failure():
+    """An allocation failure of one job (injected on the host: the pool call fails as if
+    the device were full) fails that job alone with STWO_ERR_OUT_OF_MEMORY; its budget
+    returns and the following jobs prove exactly as alone."""
+    stwo = load_package()
+    L = stwo._lib
+    jobs = [(9, 16, 1, 3, 5), (10, 32, 1, 3, 5), (9, 20, 2, 4, 3)]
+    alone = [stwo.prove_wide_fib(job_of(t), *stwo.wide_fib_inputs(t[0], 80 + i))[0] for i, t in enumerate(jobs)]
+    with stwo.ProofServer(n_workers=1, device_budget_bytes=8 << 30, max_domain_log=16) as srv:
+        L.lib().stwo_debug_fail_allocations(1)
+        try:
+            for i, t in enumerate(jobs):
+                srv.submit(i, job_of(t), *stwo.wide_fib_inputs(t[0], 80 + i))
+            got = _collect(srv, len(jobs))
+        finally:
+            L.lib().stwo_debug_fail_allocations(0)
+        assert srv.stats() == {"pending": 0, "running": 0, "device_bytes_in_use": 0}
+    failed = [k for k, r in got.items() if r["status"] != L.OK]
+    assert failed == [0] and got[0]["status"] == L.ERR_OUT_OF_MEMORY and "injected" in got[0]["error"]
+    assert got[1]["proof"] == alone[1] and got[2]["proof"] == alone[2]
+
+
+def test_server_submit_checks_before_copying_inputs():
+    """A job whose domain exceeds the server's twiddle tree is refused at submission,
+    before its inputs are read: the input arrays may be shorter than 2^log_n_rows."""
+    import numpy as np
+    stwo = load_package()
+    L = stwo._lib
+    with stwo.ProofServer(n_workers=1, device_budget_bytes=1 << 30, max_domain_log=12) as srv:
+        tiny = np.zeros(4, np.uint32)
+        L.clear_error()
+        rc = L.lib().stwo_server_submit(srv._s, 1, stwo.WideFibJob(28, 16).c(), tiny.ctypes.data, tiny.ctypes.data)
+        assert rc == L.ERR_UNSUPPORTED_SIZE and "exceeds" in L.last_error()
+        L.clear_error()
