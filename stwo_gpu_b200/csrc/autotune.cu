@@ -7,7 +7,9 @@
 //   Merkle layers per launch (CTA of 128, 256 or 512 threads); measured on a tree of
 //   64 columns x 2^19 leaves;
 //   Merkle bottom-level nodes per thread (2^1 .. 2^5); measured on a tree of 4
-//   columns x 2^20 leaves.
+//   columns x 2^20 leaves;
+//   FFT radix split: the most layers a strided pass takes (10, 7 or 5: one strided
+//   pass above the bottom pass, or two); measured like the elements per thread, at 2^22.
 //
 // Each candidate runs once to warm up, then three times; the least time wins. Every
 // variant computes the same values, so tuning changes speed only. Device memory for
@@ -105,6 +107,11 @@ int stwo_set_tunable(const char *name, int value) {
         set_tunable(TUNE_MERKLE_SUB_SPREAD, value);
         return STWO_OK;
     }
+    if (n == "fft_max_strided_layers") {
+        STWO_REQUIRE(value >= 4 && value <= 10, STWO_ERR_INVALID_ARGUMENT, "fft_max_strided_layers must be 4..10");
+        set_tunable(TUNE_FFT_MAX_STRIDED, value);
+        return STWO_OK;
+    }
     if (n == "eval_at_point_groups_log") {
         STWO_REQUIRE(value == 0 || (value >= 2 && value <= 4), STWO_ERR_INVALID_ARGUMENT,
                      "eval_at_point_groups_log must be 0 (chosen per launch) or 2..4");
@@ -132,10 +139,12 @@ int stwo_autotune(char *report, size_t report_cap) {
             uint32_t L;
             Tunable t;
             const char *name;
+            int candidates[3];
         };
-        const Case cases[] = {{18, TUNE_FFT_EPT_CONTIG_SMALL, "fft_ept_contig_small"},
-                              {22, TUNE_FFT_EPT_CONTIG_LARGE, "fft_ept_contig_large"},
-                              {22, TUNE_FFT_EPT_STRIDED, "fft_ept_strided"}};
+        const Case cases[] = {{18, TUNE_FFT_EPT_CONTIG_SMALL, "fft_ept_contig_small", {6, 5, 0}},
+                              {22, TUNE_FFT_EPT_CONTIG_LARGE, "fft_ept_contig_large", {6, 5, 0}},
+                              {22, TUNE_FFT_EPT_STRIDED, "fft_ept_strided", {6, 5, 0}},
+                              {22, TUNE_FFT_MAX_STRIDED, "fft_max_strided_layers", {10, 7, 5}}};
         const uint32_t Dmax = 24;
         const uint64_t tsz = 1ull << (Dmax - 1);
         uint32_t *tw = buf.get(tsz), *itw = buf.get(tsz);
@@ -155,7 +164,8 @@ int stwo_autotune(char *report, size_t report_cap) {
             int best = tunable(cs.t);
             char part[128];
             std::string times;
-            for (int v : {6, 5}) {
+            for (int v : cs.candidates) {
+                if (v == 0) break;
                 set_tunable(cs.t, v);
                 float ms = 0;
                 rc = time_best(st, [&] {

@@ -633,8 +633,11 @@ int launch_pass(const FftLaunch &p, uint32_t n_cols, bool inv, cudaStream_t st) 
 struct PassSpec { uint32_t lo, hi, c, tile_log; };
 
 // Layer ranges for a transform whose non-trivial layers are [0, L): a bottom
-// contiguous pass of up to 14 layers and strided passes of up to 10 layers above,
-// each over 2^14-element tiles (rows of >= 16 contiguous words).
+// contiguous pass of up to 14 layers and strided passes above, each over 2^14-element
+// tiles (rows of >= 16 contiguous words). The radix split of the upper layers — how
+// many a strided pass takes at most, 4..10, spread evenly over the passes — is a
+// tunable (fft_max_strided_layers, measured by stwo_autotune): fewer layers a pass
+// means wider contiguous tile rows but one more round trip through HBM.
 std::vector<PassSpec> plan_passes(uint32_t L) {
     std::vector<PassSpec> v;
     if (L <= (uint32_t)TT) {
@@ -643,7 +646,7 @@ std::vector<PassSpec> plan_passes(uint32_t L) {
     }
     v.push_back({0, (uint32_t)TT, 0, (uint32_t)TT});
     uint32_t lo = TT;
-    const uint32_t max_g = TT - 4;
+    const uint32_t max_g = (uint32_t)std::min(TT - 4, std::max(4, tunable(TUNE_FFT_MAX_STRIDED)));
     while (lo < L) {
         uint32_t rem = L - lo;
         uint32_t chunks = (rem + max_g - 1) / max_g;

@@ -136,3 +136,29 @@ def test_fft_step_matches_reference_library(stwo, big_tree, log_size):
     for k in range(ncols):
         assert (ours[k].to_numpy() == refs[k].to_numpy()).all(), f"interpolate column {k}"
         assert (outs[k].to_numpy() == ext[k].to_numpy()).all(), f"blowup-4 evaluation column {k}"
+
+
+@pytest.mark.parametrize("max_layers", [4, 5, 7])
+def test_radix_split_setting_gives_the_same_transform(stwo, oracle, big_tree, threads, max_layers):
+    """The FFT radix split (fft_max_strided_layers: at most this many layers a strided
+    pass; fewer means more passes) changes the pass plan, not the values: 2^22 and
+    2^24 transforms against the oracle under each setting."""
+    L = stwo._lib
+    lib = L.lib()
+    B = stwo.CudaBackend
+    tree, tw, itw = big_tree
+    L.check(lib.stwo_set_tunable(b"fft_max_strided_layers", max_layers))
+    try:
+        for log_size in (22, 24):
+            r = rng(2700 + log_size + max_layers)
+            dom = stwo.CanonicCoset(log_size).circle_domain()
+            hc = _oc(oracle, stwo.CanonicCoset(log_size).half_coset())
+            v = m31(r, 1 << log_size)
+            poly = B.interpolate(stwo.CircleEvaluation(dom, stwo.BaseFieldVec.from_numpy(v)), tree)
+            coeffs = poly.coeffs.to_numpy()
+            assert (coeffs == oracle.interpolate(hc, v, itw)).all(), log_size
+            ev = B.evaluate_polynomials([poly], 2, tree)[0].values.to_numpy()
+            ehc = _oc(oracle, stwo.CanonicCoset(log_size + 2).half_coset())
+            assert (ev == oracle.evaluate(ehc, coeffs, tw)).all(), log_size
+    finally:
+        lib.stwo_set_tunable(b"fft_max_strided_layers", 10)

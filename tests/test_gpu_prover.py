@@ -376,7 +376,7 @@ def test_tunables_change_speed_not_results():
     settings = [("fft_ept_contig_small", 5), ("fft_ept_contig_large", 5), ("fft_ept_strided", 5),
                 ("merkle_sub_threads", 128), ("merkle_sub_threads", 512), ("merkle_sub_spread", 0),
                 ("merkle_sub_spread", 5), ("eval_at_point_groups_log", 2), ("eval_at_point_groups_log", 3),
-                ("eval_at_point_groups_log", 4)]
+                ("eval_at_point_groups_log", 4), ("fft_max_strided_layers", 4), ("fft_max_strided_layers", 7)]
     try:
         for name, value in settings:
             stwo._lib.check(lib.stwo_set_tunable(name.encode(), value))
@@ -386,16 +386,19 @@ def test_tunables_change_speed_not_results():
             stwo._lib.check(lib.stwo_set_tunable(b"merkle_sub_threads", 100))
         with pytest.raises(stwo._lib.StwoError):
             stwo._lib.check(lib.stwo_set_tunable(b"merkle_sub_spread", 6))
+        with pytest.raises(stwo._lib.StwoError):
+            stwo._lib.check(lib.stwo_set_tunable(b"fft_max_strided_layers", 11))
         buf = C.create_string_buffer(4096)
         stwo._lib.check(lib.stwo_autotune(buf, 4096))
         rep = json.loads(buf.value.decode())
-        assert set(rep) == {"fft_ept_contig_small", "fft_ept_contig_large", "fft_ept_strided", "merkle_sub_threads",
-                            "merkle_sub_spread"}
+        assert set(rep) == {"fft_ept_contig_small", "fft_ept_contig_large", "fft_ept_strided", "fft_max_strided_layers",
+                            "merkle_sub_threads", "merkle_sub_spread"}
         assert stwo.prove_wide_fib(job_of(t), a0, a1)[0] == base
         assert stwo.prove_wide_fib(job_of(tb), b0, b1)[0] == base_b
     finally:
         for name, value in [("fft_ept_contig_small", 6), ("fft_ept_contig_large", 6), ("fft_ept_strided", 6),
-                            ("merkle_sub_threads", 256), ("merkle_sub_spread", 3), ("eval_at_point_groups_log", 0)]:
+                            ("merkle_sub_threads", 256), ("merkle_sub_spread", 3), ("eval_at_point_groups_log", 0),
+                            ("fft_max_strided_layers", 10)]:
             lib.stwo_set_tunable(name.encode(), value)
 
 
