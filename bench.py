@@ -783,15 +783,34 @@ def batch48(stwo, dev, args, O=None):
             L.check(lib.stwo_merkle_commit_layer(l, layers[l + 1].data_ptr() if l < top else None,
                                                  L.ptr_array([c.data_ptr() for c in cs]), len(cs),
                                                  layers[l].data_ptr(), sptr))
-    tree()
+    # the same tree through stwo_merkle_commit_tree: a few launches for all 23 layers
+    all_cols = [c for l in range(top, 11, -1) for c in cols[l]]
+    all_logs = [l for l in range(top, 11, -1) for _ in cols[l]]
+    layers_t = [torch.empty(8 << l, dtype=torch.int32, device=dev) for l in range(top + 1)]
+    col_p, log_a = L.ptr_array([c.data_ptr() for c in all_cols]), L.u32_array(all_logs)
+    lay_p = L.ptr_array([x.data_ptr() for x in layers_t])
+
+    def tree_one_call():
+        L.check(lib.stwo_merkle_commit_tree(col_p, log_a, len(all_cols), top, lay_p, sptr))
+
+    def timed3(fn):
+        fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(torch.cuda.current_stream(dev))
+        for _ in range(3):
+            fn()
+        e.record(torch.cuda.current_stream(dev))
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / 3
+
+    tree_ms = timed3(tree)
+    n0 = lib.stwo_kernel_launches()
+    tree_one_call()
     torch.cuda.synchronize()
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record(torch.cuda.current_stream(dev))
-    for _ in range(3):
-        tree()
-    e.record(torch.cuda.current_stream(dev))
-    torch.cuda.synchronize()
-    tree_ms = s.elapsed_time(e) / 3
+    tree_call_launches = lib.stwo_kernel_launches() - n0
+    tree_call_ms = timed3(tree_one_call)
+    tree_call_equal = all(torch.equal(a, b) for a, b in zip(layers, layers_t))
     root_equal = None
     if O is not None:
         O.set_threads(os.cpu_count() or 1)
@@ -804,7 +823,9 @@ def batch48(stwo, dev, args, O=None):
                                     "pow_bits 5, all 48 admitted at once",
             "proofs_per_s": len(jobs) / (ms_b / 1e3), "per_job_proofs_per_s": len(jobs) / (ms_s / 1e3),
             "batched_vs_per_job": ms_s / ms_b, "bit_identical": identical,
-            "mixed_tree": {"columns": "4 per log size 12..22", "ms": tree_ms, "root_equal_to_oracle": root_equal}}
+            "mixed_tree": {"columns": "4 per log size 12..22", "ms": tree_ms, "root_equal_to_oracle": root_equal,
+                           "one_call_ms": tree_call_ms, "one_call_launches": tree_call_launches,
+                           "one_call_equal": tree_call_equal}}
 
 
 def same_shape(stwo, dev):
@@ -883,6 +904,8 @@ def compact_line(full, detail_path):
         line["batch48"] = {kk: b[kk] for kk in ("proofs_per_s", "per_job_proofs_per_s", "batched_vs_per_job",
                                                 "bit_identical")}
         line["batch48"]["mixed_tree_root_equal_to_oracle"] = b["mixed_tree"]["root_equal_to_oracle"]
+        line["batch48"]["mixed_tree_ms_layer_calls_vs_one_call"] = [b["mixed_tree"]["ms"], b["mixed_tree"]["one_call_ms"]]
+        line["batch48"]["mixed_tree_one_call_launches"] = b["mixed_tree"]["one_call_launches"]
     fft = full.get("fft")
     if fft:
         rg = fft.get("reference_gpu") or {}

@@ -245,6 +245,15 @@ int stwo_accumulate(uint32_t *const *left4, const uint32_t *const *right4, uint6
  * columns of 2^log_size elements. */
 int stwo_merkle_commit_layer(uint32_t log_size, const uint32_t *prev_layer, const uint32_t *const *columns,
                              uint32_t n_columns, uint32_t *out, void *stream);
+/* A whole Merkle tree (MerkleProver::commit, blake2s.rs:19-97 driven layer by layer)
+ * over columns of mixed power-of-two sizes in a few launches (each hashes up to
+ * log2(CTA) + 1 + spread layers) instead of one per layer. columns / log_sizes: host
+ * arrays of n_columns device column pointers and their log sizes (at most max_log);
+ * a layer's columns are hashed in their order in `columns`. layers: host array of
+ * max_log + 1 device buffers, layers[l] receiving the 2^l nodes of layer l (16-byte
+ * aligned); layers[0] is the root. */
+int stwo_merkle_commit_tree(const uint32_t *const *columns, const uint32_t *log_sizes, uint32_t n_columns,
+                            uint32_t max_log, uint32_t *const *layers, void *stream);
 
 /* DEEP quotient accumulation over the circle domain with half coset
  * {initial_index, step_size, 2^(domain_log_size-1)}. Batch b samples batch_sizes[b]

@@ -117,6 +117,7 @@ SIGNATURES = [
     ("stwo_fold_circle_into_line", C.c_int, [vp, u64, QM31, vp, u64, vp, vp]),
     ("stwo_accumulate", C.c_int, [vp, vp, u64, vp]),
     ("stwo_merkle_commit_layer", C.c_int, [u32, vp, vp, u32, vp, vp]),
+    ("stwo_merkle_commit_tree", C.c_int, [vp, vp, u32, u32, vp, vp]),
     ("stwo_accumulate_quotients", C.c_int, [u32, u32, u32, vp, u32, QM31, vp, vp, vp, vp, u32, vp, vp]),
     ("stwo_wide_fib_composition", C.c_int, [vp, u32, u32, vp, vp, vp, vp]),
     ("stwo_kernel_launches", u64, []),

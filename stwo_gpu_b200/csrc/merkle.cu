@@ -10,6 +10,7 @@
 // registers (the round permutation is resolved at compile time). Column reads are
 // coalesced across the threads of a warp (consecutive nodes, consecutive words).
 #include <algorithm>
+#include <vector>
 
 #include "blake2s.cuh"
 #include "common.cuh"
@@ -195,6 +196,44 @@ extern "C" {
 int stwo_merkle_commit_layer(uint32_t log_size, const uint32_t *prev_layer, const uint32_t *const *columns,
                              uint32_t n_columns, uint32_t *out, void *stream) {
     return merkle_layer_async(log_size, prev_layer, columns, n_columns, false, out, as_stream(stream));
+}
+
+int stwo_merkle_commit_tree(const uint32_t *const *columns, const uint32_t *log_sizes, uint32_t n_columns,
+                            uint32_t max_log, uint32_t *const *layers, void *stream) {
+    STWO_REQUIRE(max_log <= 30 && layers && (n_columns == 0 || (columns && log_sizes)), STWO_ERR_INVALID_ARGUMENT,
+                 "merkle tree arguments");
+    cudaStream_t st = as_stream(stream);
+    // Per-layer column tables, in one staged device buffer: layer l's columns in the
+    // caller's order.
+    std::vector<const uint32_t *> flat;
+    std::vector<uint32_t> start(max_log + 1, 0), count(max_log + 1, 0);
+    for (int l = (int)max_log; l >= 0; l--) {
+        start[l] = (uint32_t)flat.size();
+        for (uint32_t i = 0; i < n_columns; i++) {
+            STWO_REQUIRE(log_sizes[i] <= max_log, STWO_ERR_INVALID_ARGUMENT, "column %u of log size %u above the tree's %u",
+                         i, log_sizes[i], max_log);
+            STWO_REQUIRE(columns[i], STWO_ERR_INVALID_ARGUMENT, "null column pointer");
+            if (log_sizes[i] == (uint32_t)l) flat.push_back(columns[i]);
+        }
+        count[l] = (uint32_t)flat.size() - start[l];
+    }
+    void *table = nullptr;
+    if (!flat.empty()) {
+        int arc = pool_alloc(&table, sizeof(void *) * flat.size(), st);
+        if (arc) return arc;
+        // from pageable memory: the copy has read `flat` when it returns
+        cudaError_t e = cudaMemcpyAsync(table, flat.data(), sizeof(void *) * flat.size(), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(table, st);
+            return set_error(STWO_ERR_CUDA, "merkle column table: %s", cudaGetErrorString(e));
+        }
+    }
+    std::vector<const uint32_t *const *> level_cols(max_log + 1, nullptr);
+    for (uint32_t l = 0; l <= max_log; l++)
+        if (count[l]) level_cols[l] = static_cast<const uint32_t *const *>(table) + start[l];
+    int rc = merkle_tree_dev_async(max_log, level_cols.data(), count.data(), layers, st);
+    if (table) cudaFreeAsync(table, st);
+    return rc;
 }
 
 void commit_on_first_layer(size_t size, size_t amount_of_columns, uint32_t *const *columns, stwo_blake2s_hash *result) {

@@ -157,6 +157,27 @@ def test_merkle_tree_mixed_sizes(stwo, oracle):
         assert (g == e).all()
 
 
+@pytest.mark.parametrize("logs", [[12, 12, 11, 9, 9, 9, 6, 4], [20] * 3 + [18] * 20 + [15] * 33 + [3, 0],
+                                  [14, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1]])
+def test_merkle_commit_tree_matches_layer_by_layer_oracle(stwo, oracle, logs):
+    """stwo_merkle_commit_tree hashes a whole mixed-size tree in a few launches: every
+    layer equals the oracle's MerkleProver::commit layer (columns of one size hashed in
+    their order; sizes with no columns, more than 16 columns a layer, a 1-element
+    column)."""
+    L = stwo._lib
+    r = rng(sum(logs))
+    cols = [m31(r, 1 << lg) for lg in logs]
+    bufs = [stwo.BaseFieldVec.from_numpy(c) for c in cols]
+    top = max(logs)
+    layers = [stwo.BaseFieldVec.new_uninitialized(8 << l) for l in range(top + 1)]
+    L.check(L.lib().stwo_merkle_commit_tree(L.ptr_array([b.device_ptr for b in bufs]), L.u32_array(logs), len(logs),
+                                            top, L.ptr_array([x.device_ptr for x in layers]), None))
+    L.check(L.lib().stwo_stream_synchronize(None))
+    want = oracle.merkle_commit(cols)
+    for l in range(top + 1):
+        assert (layers[l].to_numpy().reshape(-1, 8) == want[l]).all(), l
+
+
 def test_merkle_64_columns_log22_root_property(stwo, oracle):
     """Config shape (64 columns at log 22): spot-check leaves against the oracle."""
     r = rng(22)
