@@ -294,7 +294,24 @@ def kernel_suite(stwo, reps=5):
     rec = {"ms": t, "gbs": b / t / 1e6, "frac_hbm": b / t / 1e6 / peak, "compressions_per_s": comp / (t / 1e3),
            "alu_bound_compressions_per_s": alu_bound, "frac_alu_bound": comp / (t / 1e3) / alu_bound,
            "alu_bound_basis": f"{sms} SMs x 64 ALU lanes x 1965 MHz / 640 ALU instructions per compression",
-           "workload": "64 cols x 2^22, full tree"}
+           "workload": "64 cols x 2^22, full tree",
+           "path": "stwo_merkle_commit_layer per layer (the reference's commit_on_layer calls)"}
+    # The same tree through stwo_merkle_commit_tree, the prover's path: one launch.
+    layers_t = [torch.empty((1 << l) * 8, dtype=torch.int32, device=dev) for l in range(lg + 1)]
+    tlogs, tlay = L.u32_array([lg] * nc), L.ptr_array([x.data_ptr() for x in layers_t])
+
+    def merkle_tree():
+        L.check(lib.stwo_merkle_commit_tree(cptr, tlogs, nc, lg, tlay, sptr))
+
+    n0 = lib.stwo_kernel_launches()
+    merkle_tree()
+    tree_launches = lib.stwo_kernel_launches() - n0
+    tt = timed(merkle_tree)
+    rec["tree_one_call"] = {"ms": tt, "compressions_per_s": comp / (tt / 1e3),
+                            "frac_alu_bound": comp / (tt / 1e3) / alu_bound, "kernel_launches": tree_launches,
+                            "equal": all(bool(torch.equal(x, y)) for x, y in zip(layers_t, layers))}
+    rec["tree_frac_alu_bound"] = rec["tree_one_call"]["frac_alu_bound"]
+    del layers_t
     if R is not None:
         dcols = R.copy_device_pointer_vec_from_host_to_device(cptr, nc)
         rl = [torch.empty((1 << l) * 8, dtype=torch.int32, device=dev) for l in range(lg + 1)]
@@ -783,7 +800,7 @@ def batch48(stwo, dev, args, O=None):
             L.check(lib.stwo_merkle_commit_layer(l, layers[l + 1].data_ptr() if l < top else None,
                                                  L.ptr_array([c.data_ptr() for c in cs]), len(cs),
                                                  layers[l].data_ptr(), sptr))
-    # the same tree through stwo_merkle_commit_tree: a few launches for all 23 layers
+    # the same tree through stwo_merkle_commit_tree: one launch for all 23 layers
     all_cols = [c for l in range(top, 11, -1) for c in cols[l]]
     all_logs = [l for l in range(top, 11, -1) for _ in cols[l]]
     layers_t = [torch.empty(8 << l, dtype=torch.int32, device=dev) for l in range(top + 1)]
@@ -884,9 +901,9 @@ def compact_line(full, detail_path):
     k = full.get("kernels")
     if k:
         line["kernels"] = {
-            name: {kk: v[kk] for kk in ("ms", "frac_hbm", "frac_alu_bound", "evaluate_frac_hbm", "launches_per_step",
-                                        "speedup_vs_reference", "equal", "root_equal", "equal_after_one_chain",
-                                        "equal_sampled_columns") if kk in v}
+            name: {kk: v[kk] for kk in ("ms", "frac_hbm", "frac_alu_bound", "tree_frac_alu_bound", "evaluate_frac_hbm",
+                                        "launches_per_step", "speedup_vs_reference", "equal", "root_equal",
+                                        "equal_after_one_chain", "equal_sampled_columns") if kk in v}
             for name, v in k.items()}
     sp = full.get("single_proofs")
     if sp:
@@ -1184,6 +1201,17 @@ def run_profile(args):
             for l in range(lg - 1, -1, -1):
                 L.check(lib.stwo_merkle_commit_layer(l, layers[l + 1].data_ptr(), None, 0, layers[l].data_ptr(), sptr))
         reps = 1
+    elif what.startswith("merkle_tree"):  # merkle_tree[:COLS,LOG]: one stwo_merkle_commit_tree call
+        nc, lg = (int(x) for x in what.split(":")[1].split(",")) if ":" in what else (64, 22)
+        sptr = torch.cuda.current_stream(dev).cuda_stream
+        cols = [torch.randint(0, P, (1 << lg,), dtype=torch.int64, device=dev).to(torch.int32) for _ in range(nc)]
+        layers = [torch.empty(8 << l, dtype=torch.int32, device=dev) for l in range(lg + 1)]
+        cptr, logs = L.ptr_array([c.data_ptr() for c in cols]), L.u32_array([lg] * nc)
+        lay = L.ptr_array([x.data_ptr() for x in layers])
+
+        def work():
+            L.check(lib.stwo_merkle_commit_tree(cptr, logs, nc, lg, lay, sptr))
+        reps = 1
     elif what == "quotients":
         import ctypes as C
         import random
@@ -1271,7 +1299,8 @@ def main():
                     help="where the full record goes (the printed line carries summaries)")
     ap.add_argument("--no-suite", action="store_true", help="skip the config-1 per-kernel sweep")
     ap.add_argument("--profile", default=None,
-                    help="run one workload for ncu instead: fft[:LOG] | proof:L,N | merkle | quotients | fri | "
+                    help="run one workload for ncu instead: fft[:LOG] | proof:L,N | merkle | merkle_tree[:COLS,LOG] | "
+                         "quotients | fri | "
                          "inverse")
     args = ap.parse_args()
     if args.profile:

@@ -187,7 +187,11 @@ int stwo_precompute_twiddles(uint32_t root_initial_index, uint32_t root_step_siz
 
 /* In-place circle FFTs over columns of mixed sizes; column i has 2^log_sizes[i]
  * elements and its domain's half coset is a doubling of the tree's root coset.
- * Inverse FFTs include the 2^-log rescale. */
+ * Inverse FFTs include the 2^-log rescale.
+ * Up to 64 columns travel in the launch parameters. Beyond that, these three
+ * calls copy the column table into a pool buffer with a stream-ordered copy from
+ * pageable host memory. Such a call may not be recorded into a CUDA graph; the
+ * prover's own calls pass a prebuilt device table and stay graph-capturable. */
 int stwo_interpolate_columns(uint32_t *const *columns, const uint32_t *log_sizes, uint32_t n_columns,
                              const uint32_t *itwiddles, uint64_t tree_size, void *stream);
 int stwo_evaluate_columns(uint32_t *const *columns, const uint32_t *log_sizes, uint32_t n_columns,
@@ -246,8 +250,7 @@ int stwo_accumulate(uint32_t *const *left4, const uint32_t *const *right4, uint6
 int stwo_merkle_commit_layer(uint32_t log_size, const uint32_t *prev_layer, const uint32_t *const *columns,
                              uint32_t n_columns, uint32_t *out, void *stream);
 /* A whole Merkle tree (MerkleProver::commit, blake2s.rs:19-97 driven layer by layer)
- * over columns of mixed power-of-two sizes in a few launches (each hashes up to
- * log2(CTA) + 1 + spread layers) instead of one per layer. columns / log_sizes: host
+ * over columns of mixed power-of-two sizes in one launch instead of one per layer. columns / log_sizes: host
  * arrays of n_columns device column pointers and their log sizes (at most max_log);
  * a layer's columns are hashed in their order in `columns`. layers: host array of
  * max_log + 1 device buffers, layers[l] receiving the 2^l nodes of layer l (16-byte

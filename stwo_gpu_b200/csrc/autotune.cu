@@ -26,11 +26,14 @@ namespace stwo {
 int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
                 const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st);
 int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_cols, const uint32_t *level_ncols,
-                          uint32_t *const *layers, cudaStream_t st);
+                          uint32_t *const *layers, uint32_t *tickets, uint32_t n_tickets, cudaStream_t st);
 int butterfly_probe_async(uint32_t iters, uint32_t *sink, uint64_t sink_words, uint64_t *butterflies,
                           cudaStream_t st);
 
 namespace {
+
+// Ticket words for the Merkle tree kernel: more than any tree timed here needs.
+constexpr uint32_t TICKETS = 1024;
 
 struct Buffers {
     cudaStream_t st;
@@ -194,7 +197,9 @@ int stwo_autotune(char *report, size_t report_cap) {
             uint32_t *table = buf.get(NC * 2);
             std::vector<uint32_t *> layers(LOG + 1);
             for (uint32_t l = 0; l <= LOG; l++) layers[l] = buf.get(8ull << l);
-            STWO_REQUIRE(table && layers[LOG], STWO_ERR_OUT_OF_MEMORY, "autotune allocation failed");
+            uint32_t *tickets = buf.get(TICKETS);  // the tree kernel's, zeroed once
+            STWO_REQUIRE(table && layers[LOG] && tickets, STWO_ERR_OUT_OF_MEMORY, "autotune allocation failed");
+            STWO_CUDA_TRY(cudaMemsetAsync(tickets, 0, TICKETS * sizeof(uint32_t), st));
             STWO_CUDA_TRY(cudaMemcpyAsync(table, cols.data(), NC * sizeof(void *), cudaMemcpyHostToDevice, st));
             std::vector<const uint32_t *const *> lt(LOG + 1, nullptr);
             std::vector<uint32_t> ln(LOG + 1, 0);
@@ -207,8 +212,12 @@ int stwo_autotune(char *report, size_t report_cap) {
             for (int v : {256, 128, 512}) {
                 set_tunable(TUNE_MERKLE_SUB_THREADS, v);
                 float ms = 0;
-                rc = time_best(st, [&] { return merkle_tree_dev_async(LOG, lt.data(), ln.data(), layers.data(), st); },
-                               &ms);
+                rc = time_best(
+                    st,
+                    [&] {
+                        return merkle_tree_dev_async(LOG, lt.data(), ln.data(), layers.data(), tickets, TICKETS, st);
+                    },
+                    &ms);
                 if (rc) break;
                 snprintf(part, sizeof(part), "%s\"%d\": %.4f", times.empty() ? "" : ", ", v, ms);
                 times += part;
@@ -229,7 +238,9 @@ int stwo_autotune(char *report, size_t report_cap) {
             uint32_t *table = buf.get(NC * 2);
             std::vector<uint32_t *> layers(LOG + 1);
             for (uint32_t l = 0; l <= LOG; l++) layers[l] = buf.get(8ull << l);
-            STWO_REQUIRE(table && layers[LOG], STWO_ERR_OUT_OF_MEMORY, "autotune allocation failed");
+            uint32_t *tickets = buf.get(TICKETS);  // the tree kernel's, zeroed once
+            STWO_REQUIRE(table && layers[LOG] && tickets, STWO_ERR_OUT_OF_MEMORY, "autotune allocation failed");
+            STWO_CUDA_TRY(cudaMemsetAsync(tickets, 0, TICKETS * sizeof(uint32_t), st));
             STWO_CUDA_TRY(cudaMemcpyAsync(table, cols.data(), NC * sizeof(void *), cudaMemcpyHostToDevice, st));
             std::vector<const uint32_t *const *> lt(LOG + 1, nullptr);
             std::vector<uint32_t> ln(LOG + 1, 0);
@@ -242,8 +253,12 @@ int stwo_autotune(char *report, size_t report_cap) {
             for (int v : {3, 1, 2, 4, 5}) {
                 set_tunable(TUNE_MERKLE_SUB_SPREAD, v);
                 float ms = 0;
-                rc = time_best(st, [&] { return merkle_tree_dev_async(LOG, lt.data(), ln.data(), layers.data(), st); },
-                               &ms);
+                rc = time_best(
+                    st,
+                    [&] {
+                        return merkle_tree_dev_async(LOG, lt.data(), ln.data(), layers.data(), tickets, TICKETS, st);
+                    },
+                    &ms);
                 if (rc) break;
                 snprintf(part, sizeof(part), "%s\"%d\": %.4f", times.empty() ? "" : ", ", v, ms);
                 times += part;

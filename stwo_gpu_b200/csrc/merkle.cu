@@ -79,34 +79,190 @@ __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, co
     }
 }
 
-// Up to log2(THREADS) + 1 + spread layers in one launch. CTA c owns the
-// (THREADS << spread) >> j nodes of level j (layer top_log - j) that start at
-// c * ((THREADS << spread) >> j): exactly the parents of the nodes it owned one level
-// down, which it wrote itself before the barrier. Level j hashes the children (absent
-// on the leaf layer) and the layer's columns (device pointer tables, one per level).
-// With spread s a thread hashes 2^s nodes of the bottom level, so the CTA stays dense
-// for s + 1 levels before its upper levels thin out.
-constexpr int MERKLE_SUB_MAX_LEVELS = 15;  // 512 threads, spread 5: 16384 nodes -> 1 node
+// A whole tree in one launch. The layers are cut into bands of at most
+// log2(THREADS) + 1 + spread layers; a band is a grid of units, and unit u of a band
+// hashes the (THREADS << spread) >> j nodes of its level j that start at
+// u * ((THREADS << spread) >> j): the parents of the nodes it hashed one level down,
+// so a barrier is the only synchronisation inside a unit. A unit of every band but the
+// last ends in a single node. The band above needs 2 * (THREADS << spread') such
+// nodes per unit: the CTA that finishes the last of them (a per-unit ticket, counted
+// with an atomic add after a device-scope fence) hashes that unit next, so no CTA ever
+// waits and the tree's upper layers need no launch of their own. Tickets are reset by
+// the CTA that takes them: the array is zero again when the tree is done.
+//
+// Levels of at most THREADS nodes keep each node's hash in shared memory as well, and
+// their parents read it from there instead of from L2: these levels are short of
+// warps and bound by the latency of one compression plus its loads.
+//
+// With spread s a thread hashes 2^s bottom-level nodes, so a unit stays dense for s + 1
+// levels before its upper levels thin out.
+constexpr int MERKLE_MAX_BANDS = 6;
 
-struct SubtreeParams {
-    uint4 *layer[32];                                   // layer[l]: 2^l nodes
-    const uint32_t *const *cols[MERKLE_SUB_MAX_LEVELS];  // device column tables per level
-    uint32_t n_cols[MERKLE_SUB_MAX_LEVELS];
-    uint32_t top_log, levels, has_prev, spread;
+struct TreeBand {
+    uint32_t top;          // the band's lowest level (largest layer)
+    uint32_t levels;       // layers top .. top - levels + 1
+    uint32_t spread;       // a unit's first level has THREADS << spread nodes (fewer for a single unit)
+    uint32_t has_prev;     // the first level hashes children
+    uint32_t units;
+    uint32_t fan;          // units of the band below per unit of this one (every band but the first)
+    uint32_t ticket_base;  // this band's tickets, one per unit (every band but the first)
 };
 
+struct TreeParams {
+    uint4 *layer[31];                     // layer[l]: 2^l nodes
+    const uint32_t *const *cols[31];      // device column table per layer
+    uint32_t n_cols[31];
+    TreeBand band[MERKLE_MAX_BANDS];
+    uint32_t n_bands;
+    uint32_t *tickets;
+};
+
+
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) merkle_subtree_kernel(const __grid_constant__ SubtreeParams p, uint32_t one) {
-    for (uint32_t j = 0; j < p.levels; j++) {
-        const uint32_t l = p.top_log - j;
-        const uint64_t per_cta = ((uint64_t)THREADS << p.spread) >> j;
-        const uint64_t first = blockIdx.x * per_cta, n_l = 1ull << l;
-        const uint4 *prev = (j > 0 || p.has_prev) ? p.layer[l + 1] : nullptr;
-        const uint32_t *const *ct = p.cols[j];
-        for (uint64_t k = threadIdx.x; k < per_cta && first + k < n_l; k += blockDim.x)
-            merkle_node(first + k, prev, [&](uint32_t c) { return ct[c]; }, p.n_cols[j], p.layer[l], one);
-        __syncthreads();  // this level's global writes are visible to the whole CTA
+__device__ __forceinline__ void merkle_unit(const TreeParams &p, const TreeBand &bd, uint64_t u,
+                                            uint4 (*thin)[THREADS][2], uint32_t one) {
+    const uint64_t per0 = (uint64_t)THREADS << bd.spread;
+    for (uint32_t j = 0; j < bd.levels; j++) {
+        const uint32_t l = bd.top - j;
+        const uint64_t per = per0 >> j, first = u * per, n_l = 1ull << l;
+        const uint32_t *const *ct = p.cols[l];
+        const uint32_t nc = p.n_cols[l];
+        // children: none (a leaf layer), this CTA's shared memory (when the level below
+        // had at most THREADS nodes), or global memory: other CTAs' nodes on a band's
+        // first level (read from L2, since this SM's L1 never held them), else this CTA's
+        // own nodes of a dense level below
+        const bool kids = j > 0 || bd.has_prev;
+        const bool kids_shared = j > 0 && (per0 >> (j - 1)) <= (uint64_t)THREADS;
+        const bool to_shared = per <= (uint64_t)THREADS && j + 1 < bd.levels;
+        const uint4 *below = kids ? p.layer[l + 1] : nullptr;
+        uint4 *out = p.layer[l];
+        for (uint64_t k = threadIdx.x; k < per && first + k < n_l; k += THREADS) {
+            const uint64_t i = first + k;
+            uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            uint32_t m[16];
+            if (kids) {
+                uint4 v[4];
+                if (kids_shared) {
+                    const uint4 *s = &thin[(j - 1) & 1][2 * k][0];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) v[q] = s[q];
+                } else if (j == 0) {  // other CTAs' nodes: from L2
+#pragma unroll
+                    for (int q = 0; q < 4; q++) v[q] = __ldcg(below + 4 * i + q);
+                } else {  // this CTA's nodes of the level below
+#pragma unroll
+                    for (int q = 0; q < 4; q++) v[q] = below[4 * i + q];
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    m[4 * q] = v[q].x; m[4 * q + 1] = v[q].y; m[4 * q + 2] = v[q].z; m[4 * q + 3] = v[q].w;
+                }
+                compress(h, m, one);
+            }
+            uint32_t c0 = 0;
+            for (; c0 + 16 <= nc; c0 += 16) {  // full chunks: no per-word bound checks
+#pragma unroll
+                for (int w = 0; w < 16; w++) m[w] = __ldg(ct[c0 + w] + i);
+                compress(h, m, one);
+            }
+            if (c0 < nc) {  // the zero-padded last chunk
+#pragma unroll
+                for (int w = 0; w < 16; w++) {
+                    const uint32_t cw = c0 + w;
+                    m[w] = cw < nc ? __ldg(ct[cw] + i) : 0u;
+                }
+                compress(h, m, one);
+            }
+            const uint4 lo = make_uint4(h[0], h[1], h[2], h[3]), hi = make_uint4(h[4], h[5], h[6], h[7]);
+            out[2 * i] = lo;
+            out[2 * i + 1] = hi;
+            if (to_shared) {
+                thin[j & 1][k][0] = lo;
+                thin[j & 1][k][1] = hi;
+            }
+        }
+        __syncthreads();  // this level's nodes are visible to the whole CTA
     }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) merkle_tree_kernel(const __grid_constant__ TreeParams p, uint32_t one) {
+    __shared__ uint4 thin[2][THREADS][2];
+    __shared__ uint32_t next;
+    uint32_t b = 0;
+    uint64_t u = blockIdx.x;
+    for (;;) {
+        merkle_unit<THREADS>(p, p.band[b], u, thin, one);
+        if (b + 1 >= p.n_bands) return;
+        const TreeBand &up = p.band[b + 1];
+        const uint64_t parent = u / up.fan;
+        // The unit's last level is its one node, written by thread 0 (the barrier that
+        // ends merkle_unit is behind it): only that store needs to be visible to other
+        // CTAs before the ticket.
+        if (threadIdx.x == 0) {
+            __threadfence();
+            uint32_t *t = p.tickets + up.ticket_base + parent;
+            const uint32_t want = up.fan < p.band[b].units ? up.fan : p.band[b].units;
+            const uint32_t arrived = atomicAdd(t, 1u) + 1;
+            next = arrived == want;
+            if (arrived == want) *t = 0;
+        }
+        __syncthreads();
+        if (!next) return;
+        __threadfence();  // the other units' nodes, after their tickets
+        u = parent;
+        b++;
+    }
+}
+
+// The band partition of a tree of 2^max_log leaves under the current launch tunables.
+struct TreePlan {
+    int threads = 256;
+    TreeBand band[MERKLE_MAX_BANDS];
+    uint32_t n_bands = 0;
+    uint32_t n_tickets = 0;
+};
+
+int plan_tree_bands(uint32_t max_log, TreePlan &tp) {
+    STWO_REQUIRE(max_log <= 30, STWO_ERR_UNSUPPORTED_SIZE, "merkle tree of log size %u", max_log);
+    // CTA size (tunable): 128, 256 or 512 threads, i.e. 8, 9 or 10 layers per band,
+    // plus `spread` more (tunable, 0..5) while a band still fills every SM with 2048
+    // threads.
+    const int threads = tunable(TUNE_MERKLE_SUB_THREADS);
+    tp.threads = threads;
+    const int tlog = threads == 512 ? 9 : threads == 128 ? 7 : 8;
+    const int max_spread = tunable(TUNE_MERKLE_SUB_SPREAD);
+    const uint64_t min_blocks = (uint64_t)device_sm_count() * 2048 / threads;
+    tp.n_bands = 0;
+    tp.n_tickets = 0;
+    int top = (int)max_log;
+    while (top >= 0) {
+        STWO_REQUIRE(tp.n_bands < (uint32_t)MERKLE_MAX_BANDS, STWO_ERR_UNSUPPORTED_SIZE, "merkle tree bands");
+        int spread = max_spread;
+        while (spread > 0 && (top < tlog + spread || ((1ull << top) >> (tlog + spread)) < min_blocks)) spread--;
+        const int max_levels = tlog + 1 + spread;
+        const uint32_t levels = (uint32_t)std::min(top + 1, max_levels);
+        const uint64_t nodes = 1ull << top, per = (uint64_t)threads << spread;
+        const uint64_t units = nodes > per ? nodes / per : 1;
+        STWO_REQUIRE(levels == (uint32_t)max_levels || units == 1, STWO_ERR_UNSUPPORTED_SIZE, "merkle subtree partition");
+        TreeBand &bd = tp.band[tp.n_bands];
+        bd.top = (uint32_t)top;
+        bd.levels = levels;
+        bd.spread = (uint32_t)spread;
+        bd.has_prev = top < (int)max_log;
+        bd.units = (uint32_t)units;
+        bd.fan = tp.n_bands > 0 ? (uint32_t)(2 * per) : 0;
+        bd.ticket_base = tp.n_bands > 0 ? tp.n_tickets : 0;
+        if (tp.n_bands > 0) tp.n_tickets += (uint32_t)units;
+        tp.n_bands++;
+        top -= (int)levels;
+    }
+    return STWO_OK;
+}
+
+template <int THREADS>
+void launch_tree(const TreeParams &p, uint32_t blocks, cudaStream_t st) {
+    merkle_tree_kernel<THREADS><<<blocks, THREADS, 0, st>>>(p, 1u);
 }
 
 template <int CAP>
@@ -125,46 +281,45 @@ void launch_layer(uint32_t log_size, const uint32_t *prev, const uint32_t *const
 
 }  // namespace
 
+uint32_t merkle_tree_tickets(uint32_t max_log) {
+    TreePlan tp;
+    return plan_tree_bands(max_log, tp) == STWO_OK ? tp.n_tickets : 0;
+}
+
 // A whole tree whose per-layer columns are device pointer tables: level_cols[l],
 // level_ncols[l] for layer l (table may be null when the count is 0); layers[l] the
-// 2^l-node outputs. ceil((max_log + 1) / (log2(CTA size) + 1)) launches.
+// 2^l-node outputs. With `tickets` (n_tickets zeroed words, at least
+// merkle_tree_tickets(max_log); left zeroed) one launch; otherwise one launch per band.
 int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_cols, const uint32_t *level_ncols,
-                          uint32_t *const *layers, cudaStream_t st) {
-    STWO_REQUIRE(max_log <= 30, STWO_ERR_UNSUPPORTED_SIZE, "merkle tree of log size %u", max_log);
-    SubtreeParams p{};
+                          uint32_t *const *layers, uint32_t *tickets, uint32_t n_tickets, cudaStream_t st) {
+    TreePlan tp;
+    int rc = plan_tree_bands(max_log, tp);
+    if (rc) return rc;
+    TreeParams p{};
     for (uint32_t l = 0; l <= max_log; l++) {
-        p.layer[l] = reinterpret_cast<uint4 *>(layers[l]);
         STWO_REQUIRE(((uintptr_t)layers[l] & 15) == 0, STWO_ERR_INVALID_ARGUMENT, "hash buffers must be 16-byte aligned");
+        p.layer[l] = reinterpret_cast<uint4 *>(layers[l]);
+        p.cols[l] = level_cols[l];
+        p.n_cols[l] = level_ncols[l];
     }
-    // CTA size (tunable): 128, 256 or 512 threads, i.e. 8, 9 or 10 layers per launch,
-    // plus `spread` more (tunable, 0..5) while the launch still fills every SM with
-    // 2048 threads.
-    const int threads = tunable(TUNE_MERKLE_SUB_THREADS);
-    const int tlog = threads == 512 ? 9 : threads == 128 ? 7 : 8;
-    const int max_spread = tunable(TUNE_MERKLE_SUB_SPREAD);
-    const uint64_t min_blocks = (uint64_t)device_sm_count() * 2048 / threads;
-    int top = (int)max_log;
-    while (top >= 0) {
-        int spread = max_spread;
-        while (spread > 0 && (top < tlog + spread || ((1ull << top) >> (tlog + spread)) < min_blocks)) spread--;
-        const int max_levels = tlog + 1 + spread;
-        const uint32_t levels = (uint32_t)std::min(top + 1, max_levels);
-        p.top_log = (uint32_t)top;
-        p.levels = levels;
-        p.has_prev = top < (int)max_log;
-        p.spread = (uint32_t)spread;
-        for (uint32_t j = 0; j < levels; j++) {
-            p.cols[j] = level_cols[top - j];
-            p.n_cols[j] = level_ncols[top - j];
-        }
-        const uint64_t nodes = 1ull << top, per_cta = (uint64_t)threads << spread;
-        const uint64_t blocks = nodes > per_cta ? nodes / per_cta : 1;
-        STWO_REQUIRE(levels == (uint32_t)max_levels || blocks == 1, STWO_ERR_UNSUPPORTED_SIZE, "merkle subtree partition");
-        if (threads == 512) merkle_subtree_kernel<512><<<(unsigned)blocks, 512, 0, st>>>(p, 1u);
-        else if (threads == 128) merkle_subtree_kernel<128><<<(unsigned)blocks, 128, 0, st>>>(p, 1u);
-        else merkle_subtree_kernel<256><<<(unsigned)blocks, 256, 0, st>>>(p, 1u);
-        STWO_LAUNCH_CHECK("merkle_subtree_kernel");
-        top -= (int)levels;
+    auto launch = [&](uint32_t blocks) {
+        if (tp.threads == 512) launch_tree<512>(p, blocks, st);
+        else if (tp.threads == 128) launch_tree<128>(p, blocks, st);
+        else launch_tree<256>(p, blocks, st);
+    };
+    if (tickets && n_tickets >= tp.n_tickets) {
+        for (uint32_t b = 0; b < tp.n_bands; b++) p.band[b] = tp.band[b];
+        p.n_bands = tp.n_bands;
+        p.tickets = tickets;
+        launch(tp.band[0].units);
+        STWO_LAUNCH_CHECK("merkle_tree_kernel");
+        return STWO_OK;
+    }
+    p.n_bands = 1;
+    for (uint32_t b = 0; b < tp.n_bands; b++) {
+        p.band[0] = tp.band[b];
+        launch(tp.band[b].units);
+        STWO_LAUNCH_CHECK("merkle_tree_kernel");
     }
     return STWO_OK;
 }
@@ -217,22 +372,26 @@ int stwo_merkle_commit_tree(const uint32_t *const *columns, const uint32_t *log_
         }
         count[l] = (uint32_t)flat.size() - start[l];
     }
+    // The tree kernel's tickets (zeroed words) follow the tables in the same buffer.
+    const uint32_t n_tickets = merkle_tree_tickets(max_log);
+    const size_t tick_words = ((size_t)n_tickets + 1) / 2;  // in pointer-sized words
+    const size_t table_words = flat.size();
+    flat.resize(table_words + tick_words + 1, nullptr);  // (never an empty allocation)
     void *table = nullptr;
-    if (!flat.empty()) {
-        int arc = pool_alloc(&table, sizeof(void *) * flat.size(), st);
-        if (arc) return arc;
-        // from pageable memory: the copy has read `flat` when it returns
-        cudaError_t e = cudaMemcpyAsync(table, flat.data(), sizeof(void *) * flat.size(), cudaMemcpyHostToDevice, st);
-        if (e != cudaSuccess) {
-            cudaFreeAsync(table, st);
-            return set_error(STWO_ERR_CUDA, "merkle column table: %s", cudaGetErrorString(e));
-        }
+    int arc = pool_alloc(&table, sizeof(void *) * flat.size(), st);
+    if (arc) return arc;
+    // from pageable memory: the copy has read `flat` when it returns
+    cudaError_t e = cudaMemcpyAsync(table, flat.data(), sizeof(void *) * flat.size(), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(table, st);
+        return set_error(STWO_ERR_CUDA, "merkle column table: %s", cudaGetErrorString(e));
     }
     std::vector<const uint32_t *const *> level_cols(max_log + 1, nullptr);
     for (uint32_t l = 0; l <= max_log; l++)
         if (count[l]) level_cols[l] = static_cast<const uint32_t *const *>(table) + start[l];
-    int rc = merkle_tree_dev_async(max_log, level_cols.data(), count.data(), layers, st);
-    if (table) cudaFreeAsync(table, st);
+    uint32_t *tickets = reinterpret_cast<uint32_t *>(static_cast<const uint32_t **>(table) + table_words);
+    int rc = merkle_tree_dev_async(max_log, level_cols.data(), count.data(), layers, tickets, n_tickets, st);
+    cudaFreeAsync(table, st);
     return rc;
 }
 

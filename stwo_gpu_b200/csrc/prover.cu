@@ -58,7 +58,8 @@ int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_c
 int fft_columns_tab(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
                     const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st, const void *dev_table);
 int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_cols, const uint32_t *level_ncols,
-                          uint32_t *const *layers, cudaStream_t st);
+                          uint32_t *const *layers, uint32_t *tickets, uint32_t n_tickets, cudaStream_t st);
+uint32_t merkle_tree_tickets(uint32_t max_log);
 int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const uint32_t *itw, uint64_t off,
                uint32_t *const *dst4, bool circle, cudaStream_t st, const void *alpha_dev);
 int wide_fib_dev_async(const uint32_t *const *trace_dev, uint32_t n_cols, uint32_t log_size, const uint32_t *powers_dev,
@@ -547,6 +548,9 @@ struct MerkleTree {
     std::vector<const uint32_t *const *> level_tables;        // device column table per layer
     std::vector<uint32_t> level_n;
     std::vector<std::pair<size_t, uint32_t>> table_offsets;   // (image offset, layer) of each table
+    size_t ticket_offset = 0;                                 // image offset of the tree kernel's tickets
+    uint32_t *tickets = nullptr;
+    uint32_t n_tickets = 0;
     uint32_t max_log = 0;
 };
 
@@ -568,6 +572,9 @@ int plan_tree(MerkleTree &t, std::vector<std::pair<uint32_t, const uint32_t *>> 
             t.level_n[l] = (uint32_t)lc.size();
         }
     }
+    // zeroed in the image; the kernel leaves them zeroed
+    t.n_tickets = merkle_tree_tickets(t.max_log);
+    t.ticket_offset = up.add(nullptr, 4 * std::max<size_t>(t.n_tickets, 1));
     return STWO_OK;
 }
 
@@ -737,6 +744,9 @@ uint64_t job_device_bytes(const Job &j, bool own_twiddles) {
     b += 2 * r(8 * j.N) + r(sizeof(EapDevPoly) * (j.N + 4)) + (2 * (j.L + j.B) + 8) * r(64) + r(8 * j.N);
     b += r(sizeof(TailParams));
     b += 3 * r(16 * j.N);                                 // FFT column tables (src, dst) of the trace
+    auto tickets = [&](uint32_t log) { return r(4 * std::max<uint64_t>(merkle_tree_tickets(log), 1)); };
+    b += tickets(j.L + j.B) + 2 * tickets(j.L + 1 + j.B);  // Merkle tree tickets
+    for (uint32_t l = j.B; l <= j.L + j.B; l++) b += tickets(l);
     const uint64_t words = (uint64_t)j.n_queries * ((j.L + 2 + j.B) * 8 * 3 * 8 + 2 * (j.N + 16));
     b += r(words * sizeof(GatherReq)) + r(words * 4);     // decommitment gather
     return b;
@@ -965,6 +975,7 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     auto fix_tables = [&](MerkleTree &t) {
         for (auto &f : t.table_offsets)
             t.level_tables[f.second] = reinterpret_cast<const uint32_t *const *>(dev_at(f.first));
+        t.tickets = reinterpret_cast<uint32_t *>(dev_at(t.ticket_offset));
     };
     fix_tables(t_trace);
     fix_tables(t_comp);
@@ -1013,7 +1024,8 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
             PV_TRY(fft_columns_tab(src.data(), tev.data(), N, L + B, L, tw, tsz, false, st, dev_at(off_fft_eval)));
         }
         auto commit = [&](MerkleTree &t) {
-            return merkle_tree_dev_async(t.max_log, t.level_tables.data(), t.level_n.data(), t.layers.data(), st);
+            return merkle_tree_dev_async(t.max_log, t.level_tables.data(), t.level_n.data(), t.layers.data(), t.tickets,
+                                         t.n_tickets, st);
         };
         PV_TRY(commit(t_trace));
         fs_trace_kernel<<<1, 32, 0, st>>>(dstate, t_trace.layers[0], powers, N - 2);

@@ -160,7 +160,7 @@ def test_merkle_tree_mixed_sizes(stwo, oracle):
 @pytest.mark.parametrize("logs", [[12, 12, 11, 9, 9, 9, 6, 4], [20] * 3 + [18] * 20 + [15] * 33 + [3, 0],
                                   [14, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1]])
 def test_merkle_commit_tree_matches_layer_by_layer_oracle(stwo, oracle, logs):
-    """stwo_merkle_commit_tree hashes a whole mixed-size tree in a few launches: every
+    """stwo_merkle_commit_tree hashes a whole mixed-size tree in one launch: every
     layer equals the oracle's MerkleProver::commit layer (columns of one size hashed in
     their order; sizes with no columns, more than 16 columns a layer, a 1-element
     column)."""
@@ -176,6 +176,46 @@ def test_merkle_commit_tree_matches_layer_by_layer_oracle(stwo, oracle, logs):
     want = oracle.merkle_commit(cols)
     for l in range(top + 1):
         assert (layers[l].to_numpy().reshape(-1, 8) == want[l]).all(), l
+
+
+@pytest.mark.parametrize("threads,spread", [(256, 3), (128, 0), (128, 5), (256, 0), (512, 1), (512, 5)])
+def test_merkle_tree_one_launch_every_band_split(stwo, threads, spread):
+    """The whole-tree kernel hashes every layer in one launch: the CTA that finishes the
+    last unit under a node of the next band goes on to hash that band's unit. Each
+    CTA size and spread cuts the layers into different bands (one to four); every
+    layer must equal the layer-by-layer kernel's (pinned to the oracle above), the call
+    must be a single launch, and a second call into zeroed buffers must give the same
+    layers (the order in which CTAs finish does not change the tree)."""
+    L = stwo._lib
+    lib = L.lib()
+    L.check(lib.stwo_set_tunable(b"merkle_sub_threads", threads))
+    L.check(lib.stwo_set_tunable(b"merkle_sub_spread", spread))
+    try:
+        for nc, lg in [(4, 0), (1, 1), (4, 8), (8, 9), (4, 13), (20, 16), (4, 21), (64, 19)]:
+            r = rng(lg * 1000 + nc + threads + spread)
+            bufs = [stwo.BaseFieldVec.from_numpy(m31(r, 1 << lg)) for _ in range(nc)]
+            want = [stwo.BaseFieldVec.new_uninitialized(8 << l) for l in range(lg + 1)]
+            L.check(lib.stwo_merkle_commit_layer(lg, None, L.ptr_array([b.device_ptr for b in bufs]), nc,
+                                                 want[lg].device_ptr, None))
+            for l in range(lg - 1, -1, -1):
+                L.check(lib.stwo_merkle_commit_layer(l, want[l + 1].device_ptr, None, 0, want[l].device_ptr, None))
+            layers = [stwo.BaseFieldVec.new_uninitialized(8 << l) for l in range(lg + 1)]
+            args = (L.ptr_array([b.device_ptr for b in bufs]), L.u32_array([lg] * nc), nc, lg,
+                    L.ptr_array([x.device_ptr for x in layers]), None)
+            n0 = lib.stwo_kernel_launches()
+            L.check(lib.stwo_merkle_commit_tree(*args))
+            assert lib.stwo_kernel_launches() - n0 == 1, (nc, lg)
+            L.check(lib.stwo_stream_synchronize(None))
+            first = [x.to_numpy() for x in layers]
+            for l in range(lg + 1):
+                assert (first[l] == want[l].to_numpy()).all(), (nc, lg, l)
+            again = [stwo.BaseFieldVec.new_zeroes(8 << l) for l in range(lg + 1)]
+            L.check(lib.stwo_merkle_commit_tree(*args[:4], L.ptr_array([x.device_ptr for x in again]), None))
+            L.check(lib.stwo_stream_synchronize(None))
+            assert all((x.to_numpy() == f).all() for x, f in zip(again, first)), (nc, lg)
+    finally:
+        lib.stwo_set_tunable(b"merkle_sub_threads", 256)
+        lib.stwo_set_tunable(b"merkle_sub_spread", 3)
 
 
 def test_merkle_64_columns_log22_root_property(stwo, oracle):
