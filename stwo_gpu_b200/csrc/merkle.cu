@@ -32,12 +32,12 @@ struct MerkleCols {
 // Hashes node i of a layer: children (if prev) then n_cols column words, 16 per
 // compression, the last chunk zero-padded.
 template <class ColAt>
-__device__ __forceinline__ void merkle_node(uint64_t i, const uint4 *prev, ColAt col_at, uint32_t n_cols, uint4 *out,
+__device__ __forceinline__ void merkle_node(uint32_t i, const uint4 *prev, ColAt col_at, uint32_t n_cols, uint4 *out,
                                             uint32_t one) {
     uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     uint32_t m[16];
     if (prev) {
-        const uint4 *p = prev + 4 * i;
+        const uint4 *p = prev + 4 * (size_t)i;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             uint4 v = p[q];
@@ -59,8 +59,8 @@ __device__ __forceinline__ void merkle_node(uint64_t i, const uint4 *prev, ColAt
         }
         compress(h, m, one);
     }
-    out[2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
-    out[2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+    out[2 * (size_t)i] = make_uint4(h[0], h[1], h[2], h[3]);
+    out[2 * (size_t)i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
 
 // One layer, one thread per node. COLS_ON_DEVICE: column pointers come from a device
@@ -70,8 +70,9 @@ __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, co
                                                            const __grid_constant__ MerkleCols<CAP> cols,
                                                            const uint32_t *const *__restrict__ dev_cols,
                                                            uint32_t n_cols, uint4 *__restrict__ out, uint32_t one) {
-    const uint64_t n = 1ull << log_size;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    // 32-bit node indices: at most 2^31 nodes, and i + the grid's stride stays below 2^32
+    const uint32_t n = 1u << log_size;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (COLS_ON_DEVICE)
             merkle_node(i, prev, [&](uint32_t c) { return dev_cols[c]; }, n_cols, out, one);
         else
@@ -119,12 +120,13 @@ struct TreeParams {
 
 
 template <int THREADS>
-__device__ __forceinline__ void merkle_unit(const TreeParams &p, const TreeBand &bd, uint64_t u,
+__device__ __forceinline__ void merkle_unit(const TreeParams &p, const TreeBand &bd, uint32_t u,
                                             uint4 (*thin)[THREADS][2], uint32_t one) {
-    const uint64_t per0 = (uint64_t)THREADS << bd.spread;
+    // node indices fit 32 bits: a layer has at most 2^30 nodes
+    const uint32_t per0 = (uint32_t)THREADS << bd.spread;
     for (uint32_t j = 0; j < bd.levels; j++) {
         const uint32_t l = bd.top - j;
-        const uint64_t per = per0 >> j, first = u * per, n_l = 1ull << l;
+        const uint32_t per = per0 >> j, first = u * per, n_l = 1u << l;
         const uint32_t *const *ct = p.cols[l];
         const uint32_t nc = p.n_cols[l];
         // children: none (a leaf layer), this CTA's shared memory (when the level below
@@ -132,12 +134,12 @@ __device__ __forceinline__ void merkle_unit(const TreeParams &p, const TreeBand 
         // first level (read from L2, since this SM's L1 never held them), else this CTA's
         // own nodes of a dense level below
         const bool kids = j > 0 || bd.has_prev;
-        const bool kids_shared = j > 0 && (per0 >> (j - 1)) <= (uint64_t)THREADS;
-        const bool to_shared = per <= (uint64_t)THREADS && j + 1 < bd.levels;
+        const bool kids_shared = j > 0 && (per0 >> (j - 1)) <= (uint32_t)THREADS;
+        const bool to_shared = per <= (uint32_t)THREADS && j + 1 < bd.levels;
         const uint4 *below = kids ? p.layer[l + 1] : nullptr;
         uint4 *out = p.layer[l];
-        for (uint64_t k = threadIdx.x; k < per && first + k < n_l; k += THREADS) {
-            const uint64_t i = first + k;
+        for (uint32_t k = threadIdx.x; k < per && first + k < n_l; k += THREADS) {
+            const uint32_t i = first + k;
             uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             uint32_t m[16];
             if (kids) {
@@ -189,13 +191,12 @@ template <int THREADS>
 __global__ void __launch_bounds__(THREADS) merkle_tree_kernel(const __grid_constant__ TreeParams p, uint32_t one) {
     __shared__ uint4 thin[2][THREADS][2];
     __shared__ uint32_t next;
-    uint32_t b = 0;
-    uint64_t u = blockIdx.x;
+    uint32_t b = 0, u = blockIdx.x;
     for (;;) {
         merkle_unit<THREADS>(p, p.band[b], u, thin, one);
         if (b + 1 >= p.n_bands) return;
         const TreeBand &up = p.band[b + 1];
-        const uint64_t parent = u / up.fan;
+        const uint32_t parent = u / up.fan;
         // The unit's last level is its one node, written by thread 0 (the barrier that
         // ends merkle_unit is behind it): only that store needs to be visible to other
         // CTAs before the ticket.
