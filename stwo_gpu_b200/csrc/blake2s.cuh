@@ -42,14 +42,29 @@ __device__ __forceinline__ uint32_t add_on_fma(uint32_t c, uint32_t d, uint32_t 
     return r;
 }
 
+// FMA: the additions as multiply-adds on the FMA pipe, for many threads hashing at
+// once (the xors and rotations keep the ALU pipe busy). Otherwise the three-input
+// a + b + m and c + d on the ALU pipe: two instructions fewer a G, for one thread
+// hashing alone (the device channel), whose time is its own instruction stream.
+template <bool FMA>
+__device__ __forceinline__ uint32_t add3(uint32_t a, uint32_t x, uint32_t b, uint32_t one) {
+    if (FMA) return add_on_fma(add_on_fma(a, x, one), b, one);
+    return a + x + b;
+}
+template <bool FMA>
+__device__ __forceinline__ uint32_t add2(uint32_t c, uint32_t d, uint32_t one) {
+    if (FMA) return add_on_fma(c, d, one);
+    return c + d;
+}
+
 #define STWO_G(a, b, c, d, x, y)    \
-    a = add_on_fma(add_on_fma(a, (x), one), b, one); \
+    a = add3<FMA>(a, (x), b, one);  \
     d = rotr16(d ^ a);              \
-    c = add_on_fma(c, d, one);      \
+    c = add2<FMA>(c, d, one);       \
     b = rotr(b ^ c, 12);            \
-    a = add_on_fma(add_on_fma(a, (y), one), b, one); \
+    a = add3<FMA>(a, (y), b, one);  \
     d = rotr8(d ^ a);               \
-    c = add_on_fma(c, d, one);      \
+    c = add2<FMA>(c, d, one);       \
     b = rotr(b ^ c, 7);
 
 // One BLAKE2s round with message permutation s0..s15 (RFC 7693 SIGMA rows).
@@ -65,6 +80,7 @@ __device__ __forceinline__ uint32_t add_on_fma(uint32_t c, uint32_t d, uint32_t 
 
 // Compression with byte counter t (low word) and finalisation flag f0; the Merkle
 // hasher and the nonce mixing use t = f0 = 0.
+template <bool FMA = true>
 __device__ __forceinline__ void compress_tf(uint32_t h[8], const uint32_t m[16], uint32_t t, uint32_t f0,
                                             uint32_t one) {
     uint32_t v0 = h[0], v1 = h[1], v2 = h[2], v3 = h[3], v4 = h[4], v5 = h[5], v6 = h[6], v7 = h[7];
@@ -90,8 +106,9 @@ __device__ __forceinline__ void compress_tf(uint32_t h[8], const uint32_t m[16],
     h[7] ^= v7 ^ v15;
 }
 
+template <bool FMA = true>
 __device__ __forceinline__ void compress(uint32_t h[8], const uint32_t m[16], uint32_t one) {
-    compress_tf(h, m, 0u, 0u, one);
+    compress_tf<FMA>(h, m, 0u, 0u, one);
 }
 
 }  // namespace blake

@@ -30,7 +30,8 @@ struct DevChannel {
 };
 
 // BLAKE2s-256 (RFC 7693, unkeyed, 32-byte digest) of the words word(0..n_words-1),
-// little endian.
+// little endian. One thread runs the channel, so its compressions take the
+// short-chain form (additions on the ALU pipe).
 template <class W>
 __device__ void blake2s_words(W word, uint32_t n_words, uint32_t out[8]) {
     const uint32_t one = 1;
@@ -42,10 +43,10 @@ __device__ void blake2s_words(W word, uint32_t n_words, uint32_t out[8]) {
     while (n_words - off > 16) {
         for (int k = 0; k < 16; k++) m[k] = word(off + k);
         off += 16;
-        blake::compress_tf(h, m, off * 4, 0u, one);
+        blake::compress_tf<false>(h, m, off * 4, 0u, one);
     }
     for (uint32_t k = 0; k < 16; k++) m[k] = off + k < n_words ? word(off + k) : 0u;
-    blake::compress_tf(h, m, n_words * 4, 0xffffffffu, one);
+    blake::compress_tf<false>(h, m, n_words * 4, 0xffffffffu, one);
 #pragma unroll
     for (int i = 0; i < 8; i++) out[i] = h[i];
 }
@@ -83,7 +84,7 @@ __device__ inline void ch_mix_nonce(DevChannel &c, uint64_t nonce) {
     for (int i = 0; i < 8; i++) h[i] = c.digest[i];
     m[0] = (uint32_t)nonce;
     m[1] = (uint32_t)(nonce >> 32);
-    blake::compress(h, m, 1u);
+    blake::compress<false>(h, m, 1u);
     ch_update(c, h);
 }
 

@@ -189,41 +189,53 @@ __global__ void fs_comp_kernel(ProofState *s, const uint32_t *root) {
 // vanishing polynomial at the OODS point; thread 0 mixes the sampled values (N trace
 // values, then the composition's 4 coordinates) and draws the quotient coefficient;
 // then the quotient kernels' sample-dependent parameters of both column groups.
+// The sampled values are first staged in shared memory (up to OODS_STAGED of them), so
+// that the serial hash reads each chunk without an L2 round trip; the constraint check
+// runs on another warp while thread 0 hashes. vsh: vanishing_shift(L), from the host.
+constexpr uint32_t OODS_STAGED = 1024;
 __global__ void __launch_bounds__(256) fs_oods_kernel(ProofState *s, const qm31 *sampled, const qm31 *powers,
-                                                      uint32_t N, uint32_t L, QuotParamsDev *q_comp,
+                                                      uint32_t N, uint32_t L, cpoint vsh, QuotParamsDev *q_comp,
                                                       QuotParamsDev *q_trace) {
     __shared__ qm31 sh[32];
     __shared__ qm31 qrc_sh;
+    __shared__ qm31 staged[OODS_STAGED];
+    __shared__ uint32_t bad_sh;
+    const uint32_t n_vals = N + 4;
+    const bool stage = n_vals <= OODS_STAGED;
+    if (stage)
+        for (uint32_t i = threadIdx.x; i < n_vals; i += blockDim.x) staged[i] = sampled[i];
+    __syncthreads();
+    const qm31 *vals = stage ? staged : sampled;
     qm31 part = qm31_zero();
     for (uint32_t i = threadIdx.x; i + 2 < N; i += blockDim.x) {
-        const qm31 cons = qm31_sub(
-            qm31_add(qm31_mul(sampled[i], sampled[i]), qm31_mul(sampled[i + 1], sampled[i + 1])), sampled[i + 2]);
+        const qm31 cons = qm31_sub(qm31_add(qm31_mul(vals[i], vals[i]), qm31_mul(vals[i + 1], vals[i + 1])), vals[i + 2]);
         part = qm31_add(part, qm31_mul(cons, powers[N - 3 - i]));
     }
     const qm31 acc = block_sum_qm31(part, sh);
     const qm31 ox = s->oods[0], oy = s->oods[1];
     if (threadIdx.x == 0) {
+        fs::ch_mix_felts(s->ch, vals, n_vals);
+        const qm31 qrc = fs::ch_draw_felt(s->ch, s->error);
+        s->qrc = qrc;
+        qrc_sh = qrc;
+    } else if (threadIdx.x == 32) {
         // composition value: from_partial_evals over the basis 1, i, u, iu
         const qm31 basis[4] = {{{1, 0}, {0, 0}}, {{0, 1}, {0, 0}}, {{0, 0}, {1, 0}}, {{0, 0}, {0, 1}}};
         qm31 comp = qm31_zero();
-        for (int k = 0; k < 4; k++) comp = qm31_add(comp, qm31_mul(sampled[N + k], basis[k]));
+        for (int k = 0; k < 4; k++) comp = qm31_add(comp, qm31_mul(vals[N + k], basis[k]));
         // coset_vanishing(CanonicCoset(L).coset, oods)
-        const cpoint sh_pt = vanishing_shift(L);
-        qm31 x = qm31_sub(qm31_scale(ox, sh_pt.x), qm31_scale(oy, sh_pt.y));
+        qm31 x = qm31_sub(qm31_scale(ox, vsh.x), qm31_scale(oy, vsh.y));
         for (uint32_t d = 0; d + 1 < L; d++) {
             qm31 q = qm31_mul(x, x);
             x = qm31_sub(qm31_add(q, q), qm31_one());
         }
-        if (!qm31_eq(qm31_mul(acc, qm31_inv(x)), comp)) s->error |= fs::ERR_CONSTRAINTS;
-        fs::ch_mix_felts(s->ch, sampled, N + 4);
-        const qm31 qrc = fs::ch_draw_felt(s->ch, s->error);
-        s->qrc = qrc;
-        qrc_sh = qrc;
+        bad_sh = qm31_eq(qm31_mul(acc, qm31_inv(x)), comp) ? 0u : fs::ERR_CONSTRAINTS;
     }
     __syncthreads();
+    if (threadIdx.x == 0) s->error |= bad_sh;
     const qm31 qrc = qrc_sh;
-    quot_fill_batch_block(*q_comp, 0, qrc, ox, oy, sampled + N, 4, 0, sh);
-    quot_fill_batch_block(*q_trace, 0, qrc, ox, oy, sampled, N, 0, sh);
+    quot_fill_batch_block(*q_comp, 0, qrc, ox, oy, vals + N, 4, 0, sh);
+    quot_fill_batch_block(*q_trace, 0, qrc, ox, oy, vals, N, 0, sh);
 }
 
 // Channel step after an FRI tree: mix its root, draw the folding alpha.
@@ -292,7 +304,9 @@ struct TailParams {
 __global__ void __launch_bounds__(TAIL_THREADS) fri_tail_kernel(ProofState *s, const TailParams *__restrict__ tp,
                                                                  uint32_t one) {
     extern __shared__ uint4 t_buf[];
-    uint4 *buf[2] = {t_buf, t_buf + (2u << TAIL_MAX_LOG)};
+    // the two node buffers, by computed address (an indexed pointer array would live
+    // in local memory)
+    auto buf = [&](uint32_t which) { return t_buf + (which ? (2u << TAIL_MAX_LOG) : 0u); };
     __shared__ qm31 alpha_sh;
     const uint32_t tid = threadIdx.x;
     for (uint32_t t = 0; t < tp->n_tail; t++) {
@@ -323,8 +337,8 @@ __global__ void __launch_bounds__(TAIL_THREADS) fri_tail_kernel(ProofState *s, c
             const uint4 lo = make_uint4(h[0], h[1], h[2], h[3]), hi = make_uint4(h[4], h[5], h[6], h[7]);
             tp->nodes[t][lg][2 * i] = lo;
             tp->nodes[t][lg][2 * i + 1] = hi;
-            buf[0][2 * i] = lo;
-            buf[0][2 * i + 1] = hi;
+            buf(0)[2 * i] = lo;
+            buf(0)[2 * i + 1] = hi;
         }
         __syncthreads();
         // Nodes, level by level: children from one shared buffer, parents into the other.
@@ -335,15 +349,15 @@ __global__ void __launch_bounds__(TAIL_THREADS) fri_tail_kernel(ProofState *s, c
             uint32_t m[16];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const uint4 v = buf[src][4 * k + q];
+                const uint4 v = buf(src)[4 * k + q];
                 m[4 * q] = v.x; m[4 * q + 1] = v.y; m[4 * q + 2] = v.z; m[4 * q + 3] = v.w;
             }
             blake::compress(h, m, one);
             const uint4 lo = make_uint4(h[0], h[1], h[2], h[3]), hi = make_uint4(h[4], h[5], h[6], h[7]);
             tp->nodes[t][l][2 * k] = lo;
             tp->nodes[t][l][2 * k + 1] = hi;
-            buf[src ^ 1][2 * k] = lo;
-            buf[src ^ 1][2 * k + 1] = hi;
+            buf(src ^ 1)[2 * k] = lo;
+            buf(src ^ 1)[2 * k + 1] = hi;
         };
         uint32_t src = 0;
         int l = (int)lg - 1;
@@ -360,7 +374,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) fri_tail_kernel(ProofState *s, c
             }
         }
         if (tid == 0) {
-            const uint4 lo = buf[src][0], hi = buf[src][1];
+            const uint4 lo = buf(src)[0], hi = buf(src)[1];
             const uint32_t root[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
             for (int i = 0; i < 8; i++) s->roots[3 + li][i] = root[i];
             fs::ch_mix_root(s->ch, root);
@@ -1054,7 +1068,7 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         // ---- 3. out-of-domain sampling
         PV_TRY(eval_at_points_dev_async(dev_at(off_eap), eap_n, eap_iter, eap_total, dstate->oods, dsampled,
                                         eap_partials, dtickets, st));
-        fs_oods_kernel<<<1, 256, 0, st>>>(dstate, dsampled, powers, N, L, dqc, dqt);
+        fs_oods_kernel<<<1, 256, 0, st>>>(dstate, dsampled, powers, N, L, vanishing_shift(L), dqc, dqt);
         STWO_LAUNCH_CHECK("fs_oods_kernel");
         PV_TRY(record(3, capturing));
 
