@@ -38,8 +38,7 @@ __global__ void accumulate_kernel(const __grid_constant__ Acc4 p, uint64_t n4, u
 
 constexpr int WF_MAX_COLS = 2048;
 static_assert(WF_MAX_COLS * (16 + 8) <= 48 * 1024, "staged powers and pointers fit the default shared memory");
-constexpr int WF_PREFETCH = 8;  // column loads in flight per thread (a multiple of the fold period 4)
-static_assert(WF_PREFETCH % 4 == 0, "the fold cadence needs groups of a multiple of 4 columns");
+constexpr int WF_GROUP = 4;  // columns a load group (the fold period: one fold after every group)
 
 // Trace column pointers in the parameter block (CAP of them) or, for CAP == 1, in a
 // device table.
@@ -56,11 +55,13 @@ struct WideFibParams {
     uint32_t two;             // 2 (fold64_fma)
 };
 
-// Powers on the device (plain QM31). Two rows per thread (8-byte loads); the column
-// loop issues WF_PREFETCH loads before it consumes them, and the small per-thread
-// state keeps four CTAs of 256 threads per SM, so enough loads are in flight to cover
-// DRAM latency. Each coordinate of the sum is a 64-bit multiply-accumulate of
-// canonical values, folded (fold64_fma) after every fourth column.
+// Powers on the device (plain QM31). Two rows per thread (8-byte loads). The column
+// loop runs over whole groups of WF_GROUP columns in two register buffers, the next
+// group's loads issued before the current group is consumed (a warp keeps loads in
+// flight while it computes), then over the remaining columns one at a time; the small
+// per-thread state keeps four CTAs of 256 threads per SM. Each coordinate of the sum
+// is a 64-bit multiply-accumulate of canonical values, folded (fold64_fma) after every
+// group of four columns: a folded sum plus at most four products stays below 2^64.
 template <int CAP>
 __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant__ WideFibParams<CAP> p) {
     const uint64_t n = 1ull << p.log_size;
@@ -79,47 +80,59 @@ __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant_
     auto colp = [&](uint32_t c) { return s_col[c]; };
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < pairs; k += (uint64_t)gridDim.x * blockDim.x) {
         const bool full = 2 * k + 1 < n;
-        auto load = [&](uint32_t col, uint32_t *v) {
+        auto load = [&](uint32_t col) -> uint2 {
             const uint32_t *c = colp(col);
-            if (full) {
-                uint2 t = __ldg(reinterpret_cast<const uint2 *>(c) + k);
-                v[0] = t.x;
-                v[1] = t.y;
-            } else {
-                v[0] = c[2 * k];
-                v[1] = 0u;
-            }
+            if (full) return __ldg(reinterpret_cast<const uint2 *>(c) + k);
+            return make_uint2(c[2 * k], 0u);
         };
         uint64_t acc[2][4] = {};
-        uint32_t c0[2], c1[2];
-        load(0, c0);
-        load(1, c1);
         uint32_t s0[2], s1[2];
-        for (int r = 0; r < 2; r++) { s0[r] = m31_sqr(c0[r]); s1[r] = m31_sqr(c1[r]); }
-        for (uint32_t base = 2; base < p.n_cols; base += WF_PREFETCH) {
-            uint32_t buf[WF_PREFETCH][2];
-#pragma unroll
-            for (int u = 0; u < WF_PREFETCH; u++)
-                if (base + u < p.n_cols) load(base + u, buf[u]);
-#pragma unroll
-            for (int u = 0; u < WF_PREFETCH; u++) {
-                const uint32_t col = base + u;
-                if (col >= p.n_cols) break;
-                const qm31 w = s_pow[col];  // constraint col - 2 takes powers[N-3-(col-2)]
-#pragma unroll
-                for (int r = 0; r < 2; r++) {
-                    const uint32_t cons = m31_sub(m31_add(s0[r], s1[r]), buf[u][r]);
-                    acc[r][0] = mac64(acc[r][0], cons, w.a.a);
-                    acc[r][1] = mac64(acc[r][1], cons, w.a.b);
-                    acc[r][2] = mac64(acc[r][2], cons, w.b.a);
-                    acc[r][3] = mac64(acc[r][3], cons, w.b.b);
-                    if (u % 4 == 3)
-                        for (int c = 0; c < 4; c++) acc[r][c] = fold64_fma(acc[r][c], p.two);
-                    s0[r] = s1[r];
-                    s1[r] = m31_sqr(buf[u][r]);
-                }
-            }
+        {
+            const uint2 c0 = load(0), c1 = load(1);
+            s0[0] = m31_sqr(c0.x); s0[1] = m31_sqr(c0.y);
+            s1[0] = m31_sqr(c1.x); s1[1] = m31_sqr(c1.y);
         }
+        // constraint col - 2 takes powers[N-3-(col-2)]
+        auto consume_one = [&](uint32_t col, uint2 v) {
+            const qm31 w = s_pow[col];
+            const uint32_t vv[2] = {v.x, v.y};
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                const uint32_t cons = m31_sub(m31_add(s0[r], s1[r]), vv[r]);
+                acc[r][0] = mac64(acc[r][0], cons, w.a.a);
+                acc[r][1] = mac64(acc[r][1], cons, w.a.b);
+                acc[r][2] = mac64(acc[r][2], cons, w.b.a);
+                acc[r][3] = mac64(acc[r][3], cons, w.b.b);
+                s0[r] = s1[r];
+                s1[r] = m31_sqr(vv[r]);
+            }
+        };
+        auto fold = [&] {
+#pragma unroll
+            for (int r = 0; r < 2; r++)
+                for (int c = 0; c < 4; c++) acc[r][c] = fold64_fma(acc[r][c], p.two);
+        };
+        auto load_group = [&](uint32_t base, uint2 (&v)[WF_GROUP]) {
+#pragma unroll
+            for (int u = 0; u < WF_GROUP; u++) v[u] = load(base + u);
+        };
+        auto consume_group = [&](uint32_t base, const uint2 (&v)[WF_GROUP]) {
+#pragma unroll
+            for (int u = 0; u < WF_GROUP; u++) consume_one(base + u, v[u]);
+            fold();
+        };
+        const uint32_t nc = p.n_cols;
+        const uint32_t groups_end = nc < 2 ? nc : 2 + (nc - 2) / WF_GROUP * WF_GROUP;
+        uint2 ga[WF_GROUP], gb[WF_GROUP];
+        if (2 < groups_end) load_group(2, ga);
+        for (uint32_t base = 2; base < groups_end; base += 2 * WF_GROUP) {
+            if (base + WF_GROUP < groups_end) load_group(base + WF_GROUP, gb);
+            consume_group(base, ga);
+            if (base + WF_GROUP >= groups_end) break;
+            if (base + 2 * WF_GROUP < groups_end) load_group(base + 2 * WF_GROUP, ga);
+            consume_group(base + WF_GROUP, gb);
+        }
+        for (uint32_t col = groups_end; col < nc; col++) consume_one(col, load(col));  // at most three
         uint32_t o[4][2];
         for (int r = 0; r < 2; r++) {
             const uint64_t row = 2 * k + r;
