@@ -227,13 +227,16 @@ struct TreePlan {
 int plan_tree_bands(uint32_t max_log, TreePlan &tp) {
     STWO_REQUIRE(max_log <= 30, STWO_ERR_UNSUPPORTED_SIZE, "merkle tree of log size %u", max_log);
     // CTA size (tunable): 128, 256 or 512 threads, i.e. 8, 9 or 10 layers per band,
-    // plus `spread` more (tunable, 0..5) while a band still fills every SM with 2048
-    // threads.
+    // plus `spread` more (tunable, 0..5) while a band still fills every SM with 1024
+    // threads (the CTAs that are resident at once: four of 256 threads at 64 registers).
+    // Requiring 2048 capped the spread of mid-size trees and so their units' size: at 4
+    // columns x 2^19..2^21 leaves 0.0995 / 0.150 / 0.242 ms against 0.0884 / 0.137 /
+    // 0.227 ms now.
     const int threads = tunable(TUNE_MERKLE_SUB_THREADS);
     tp.threads = threads;
     const int tlog = threads == 512 ? 9 : threads == 128 ? 7 : 8;
     const int max_spread = tunable(TUNE_MERKLE_SUB_SPREAD);
-    const uint64_t min_blocks = (uint64_t)device_sm_count() * 2048 / threads;
+    const uint64_t min_blocks = (uint64_t)device_sm_count() * 1024 / threads;
     tp.n_bands = 0;
     tp.n_tickets = 0;
     int top = (int)max_log;
