@@ -250,11 +250,13 @@ int stwo_accumulate(uint32_t *const *left4, const uint32_t *const *right4, uint6
 int stwo_merkle_commit_layer(uint32_t log_size, const uint32_t *prev_layer, const uint32_t *const *columns,
                              uint32_t n_columns, uint32_t *out, void *stream);
 /* A whole Merkle tree (MerkleProver::commit, blake2s.rs:19-97 driven layer by layer)
- * over columns of mixed power-of-two sizes in one launch instead of one per layer. columns / log_sizes: host
- * arrays of n_columns device column pointers and their log sizes (at most max_log);
- * a layer's columns are hashed in their order in `columns`. layers: host array of
- * max_log + 1 device buffers, layers[l] receiving the 2^l nodes of layer l (16-byte
- * aligned); layers[0] is the root. */
+ * over columns of mixed power-of-two sizes in one launch instead of one per layer.
+ * columns / log_sizes: host arrays of n_columns device column pointers and their log
+ * sizes (at most max_log); a layer's columns are hashed in their order in `columns`.
+ * layers: host array of max_log + 1 device buffers, layers[l] receiving the 2^l nodes
+ * of layer l (16-byte aligned); layers[0] is the root. The column tables and the
+ * kernel's tickets are staged through the library's pool with a copy from pageable
+ * memory, so the call may not be recorded into a CUDA graph. */
 int stwo_merkle_commit_tree(const uint32_t *const *columns, const uint32_t *log_sizes, uint32_t n_columns,
                             uint32_t max_log, uint32_t *const *layers, void *stream);
 
