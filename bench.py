@@ -1,4 +1,4 @@
-"""Benchmark: wide-Fibonacci proof serving on one B200 (the BASELINE metric:
+"""Benchmark: wide-Fibonacci proof serving on one B200 (the headline metric:
 "bit-exact proofs/s & p99 latency: batched server vs per-job; FFT % HBM peak").
 
 Workload: a seeded stream of wide-Fibonacci proof jobs shaped like the serving
