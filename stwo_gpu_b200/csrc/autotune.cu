@@ -26,7 +26,8 @@ namespace stwo {
 int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
                 const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st);
 int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_cols, const uint32_t *level_ncols,
-                          uint32_t *const *layers, uint32_t *tickets, uint32_t n_tickets, cudaStream_t st);
+                          uint32_t *const *layers, uint32_t *tickets, uint32_t n_tickets, uint32_t jobs, size_t js,
+                          cudaStream_t st);
 int butterfly_probe_async(uint32_t iters, uint32_t *sink, uint64_t sink_words, uint64_t *butterflies,
                           cudaStream_t st);
 
@@ -215,7 +216,7 @@ int stwo_autotune(char *report, size_t report_cap) {
                 rc = time_best(
                     st,
                     [&] {
-                        return merkle_tree_dev_async(LOG, lt.data(), ln.data(), layers.data(), tickets, TICKETS, st);
+                        return merkle_tree_dev_async(LOG, lt.data(), ln.data(), layers.data(), tickets, TICKETS, 1, 0, st);
                     },
                     &ms);
                 if (rc) break;
@@ -256,7 +257,7 @@ int stwo_autotune(char *report, size_t report_cap) {
                 rc = time_best(
                     st,
                     [&] {
-                        return merkle_tree_dev_async(LOG, lt.data(), ln.data(), layers.data(), tickets, TICKETS, st);
+                        return merkle_tree_dev_async(LOG, lt.data(), ln.data(), layers.data(), tickets, TICKETS, 1, 0, st);
                     },
                     &ms);
                 if (rc) break;

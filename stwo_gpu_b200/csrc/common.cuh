@@ -128,4 +128,13 @@ inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s
 // legacy default stream and wait, as the reference's host functions do.
 int sync_default_stream(int status);
 
+// Several proofs of one shape in one launch sequence: job k's device memory is job 0's
+// moved by k * stride bytes (identical allocation sequences in equal slabs), so a
+// kernel launched once over K jobs moves every pointer into job memory by
+// job * stride. Pointers outside the jobs' slabs (a shared twiddle tree) do not move.
+template <class T>
+__host__ __device__ __forceinline__ T *job_ptr(T *p, size_t stride, uint32_t job) {
+    return p ? reinterpret_cast<T *>(reinterpret_cast<uintptr_t>(p) + (size_t)job * stride) : p;
+}
+
 }  // namespace stwo

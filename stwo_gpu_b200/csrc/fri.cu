@@ -21,10 +21,31 @@ struct Cols4 { const uint32_t *c[4]; };
 struct MutCols4 { uint32_t *c[4]; };
 
 // alpha_dev: when set, alpha is read from device memory (a challenge the device
-// channel drew) instead of the by-value argument.
-template <bool CIRCLE>
-__global__ void fold_kernel(const __grid_constant__ Cols4 src, const __grid_constant__ MutCols4 dst, uint64_t n_out,
-                            const uint32_t *__restrict__ tw, qm31 alpha, qm31 alpha_sq, const qm31 *alpha_dev) {
+// channel drew) instead of the by-value argument. JOBS: blockIdx.y is the job, whose
+// columns and alpha are job 0's moved by blockIdx.y * js bytes (the twiddles are
+// shared); the single-job instance carries no offset arithmetic.
+template <bool CIRCLE, bool JOBS>
+__global__ void fold_kernel(const __grid_constant__ Cols4 src_p, const __grid_constant__ MutCols4 dst_p, uint64_t n_out,
+                            const uint32_t *__restrict__ tw, qm31 alpha, qm31 alpha_sq, const qm31 *alpha_dev,
+                            size_t js) {
+    // the column pointers stay in the parameter block; a job's offset is added at each
+    // use (a multiply-add) rather than holding eight moved pointers in registers
+    const size_t jo = JOBS ? (size_t)blockIdx.y * js : 0;
+    struct {
+        const Cols4 &p;
+        size_t jo;
+        __device__ const uint32_t *operator[](int c) const {
+            return JOBS ? reinterpret_cast<const uint32_t *>(reinterpret_cast<uintptr_t>(p.c[c]) + jo) : p.c[c];
+        }
+    } src{src_p, jo};
+    struct {
+        const MutCols4 &p;
+        size_t jo;
+        __device__ uint32_t *operator[](int c) const {
+            return JOBS ? reinterpret_cast<uint32_t *>(reinterpret_cast<uintptr_t>(p.c[c]) + jo) : p.c[c];
+        }
+    } dst{dst_p, jo};
+    if (JOBS) alpha_dev = job_ptr(alpha_dev, js, blockIdx.y);
     if (alpha_dev) {
         alpha = *alpha_dev;
         alpha_sq = qm31_mul(alpha, alpha);
@@ -35,7 +56,7 @@ __global__ void fold_kernel(const __grid_constant__ Cols4 src, const __grid_cons
         uint32_t in[4][4];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-            uint4 v = __ldg(reinterpret_cast<const uint4 *>(src.c[c]) + k);
+            uint4 v = __ldg(reinterpret_cast<const uint4 *>(src[c]) + k);
             in[c][0] = v.x; in[c][1] = v.y; in[c][2] = v.z; in[c][3] = v.w;
         }
         qm31 f0 = {{in[0][0], in[1][0]}, {in[2][0], in[3][0]}};
@@ -56,16 +77,16 @@ __global__ void fold_kernel(const __grid_constant__ Cols4 src, const __grid_cons
         if (CIRCLE) {
             uint2 d[4];
 #pragma unroll
-            for (int c = 0; c < 4; c++) d[c] = *(reinterpret_cast<const uint2 *>(dst.c[c]) + k);
+            for (int c = 0; c < 4; c++) d[c] = *(reinterpret_cast<const uint2 *>(dst[c]) + k);
             qm31 p0 = {{d[0].x, d[1].x}, {d[2].x, d[3].x}};
             qm31 p1 = {{d[0].y, d[1].y}, {d[2].y, d[3].y}};
             r0 = qm31_add(qm31_mul(p0, alpha_sq), r0);
             r1 = qm31_add(qm31_mul(p1, alpha_sq), r1);
         }
-        *(reinterpret_cast<uint2 *>(dst.c[0]) + k) = make_uint2(r0.a.a, r1.a.a);
-        *(reinterpret_cast<uint2 *>(dst.c[1]) + k) = make_uint2(r0.a.b, r1.a.b);
-        *(reinterpret_cast<uint2 *>(dst.c[2]) + k) = make_uint2(r0.b.a, r1.b.a);
-        *(reinterpret_cast<uint2 *>(dst.c[3]) + k) = make_uint2(r0.b.b, r1.b.b);
+        *(reinterpret_cast<uint2 *>(dst[0]) + k) = make_uint2(r0.a.a, r1.a.a);
+        *(reinterpret_cast<uint2 *>(dst[1]) + k) = make_uint2(r0.a.b, r1.a.b);
+        *(reinterpret_cast<uint2 *>(dst[2]) + k) = make_uint2(r0.b.a, r1.b.a);
+        *(reinterpret_cast<uint2 *>(dst[3]) + k) = make_uint2(r0.b.b, r1.b.b);
     }
 }
 
@@ -73,9 +94,16 @@ __global__ void fold_kernel(const __grid_constant__ Cols4 src, const __grid_cons
 // circle fold of a 2- or 4-point domain they are +-1/y of the half coset's first
 // point, which the tree does not hold at those sizes (see small_circle_point).
 template <bool CIRCLE>
-__global__ void fold_small_kernel(const __grid_constant__ Cols4 src, const __grid_constant__ MutCols4 dst,
+__global__ void fold_small_kernel(const __grid_constant__ Cols4 src_p, const __grid_constant__ MutCols4 dst_p,
                                   uint32_t n_out, uint32_t t0, uint32_t t1, const uint32_t *tw, qm31 alpha,
-                                  qm31 alpha_sq, const qm31 *alpha_dev) {
+                                  qm31 alpha_sq, const qm31 *alpha_dev, size_t js) {
+    Cols4 src;
+    MutCols4 dst;
+    for (int c = 0; c < 4; c++) {
+        src.c[c] = job_ptr(src_p.c[c], js, blockIdx.x);  // one thread a job
+        dst.c[c] = job_ptr(dst_p.c[c], js, blockIdx.x);
+    }
+    alpha_dev = job_ptr(alpha_dev, js, blockIdx.x);
     if (alpha_dev) {
         alpha = *alpha_dev;
         alpha_sq = qm31_mul(alpha, alpha);
@@ -98,9 +126,12 @@ __global__ void fold_small_kernel(const __grid_constant__ Cols4 src, const __gri
 
 }  // namespace
 
+// jobs folds of one shape at once: fold k's columns and alpha are fold 0's moved by
+// k * js bytes; the twiddles are shared.
 int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const uint32_t *itw, uint64_t off,
-               uint32_t *const *dst4, bool circle, cudaStream_t st, const void *alpha_dev) {
+               uint32_t *const *dst4, bool circle, cudaStream_t st, const void *alpha_dev, uint32_t jobs, size_t js) {
     const qm31 *ad = static_cast<const qm31 *>(alpha_dev);
+    STWO_REQUIRE(jobs >= 1 && jobs <= 65535, STWO_ERR_INVALID_ARGUMENT, "folds per launch: %u", jobs);
     STWO_REQUIRE(n >= 2 && is_pow2(n), STWO_ERR_INVALID_ARGUMENT, "fold of %llu values", (unsigned long long)n);
     Cols4 s;
     MutCols4 d;
@@ -123,8 +154,9 @@ int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const
             t[0] = iy;
             t[1] = m31_neg(iy);
         }
-        if (circle) fold_small_kernel<true><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, t[0], t[1], nullptr, alpha, a2, ad);
-        else fold_small_kernel<false><<<1, 1, 0, st>>>(s, d, (uint32_t)n_out, 0u, 0u, tw, alpha, a2, ad);
+        if (circle)
+            fold_small_kernel<true><<<jobs, 1, 0, st>>>(s, d, (uint32_t)n_out, t[0], t[1], nullptr, alpha, a2, ad, js);
+        else fold_small_kernel<false><<<jobs, 1, 0, st>>>(s, d, (uint32_t)n_out, 0u, 0u, tw, alpha, a2, ad, js);
         STWO_LAUNCH_CHECK("fold_small_kernel");
         return STWO_OK;
     }
@@ -134,8 +166,14 @@ int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const
     uint32_t blocks = (uint32_t)((threads + 255) / 256);
     uint32_t cap = (uint32_t)device_sm_count() * 16;
     if (blocks > cap) blocks = cap;
-    if (circle) fold_kernel<true><<<blocks, 256, 0, st>>>(s, d, n_out, tw, alpha, a2, ad);
-    else fold_kernel<false><<<blocks, 256, 0, st>>>(s, d, n_out, tw, alpha, a2, ad);
+    const dim3 grid(blocks, jobs);
+    if (jobs > 1) {
+        if (circle) fold_kernel<true, true><<<grid, 256, 0, st>>>(s, d, n_out, tw, alpha, a2, ad, js);
+        else fold_kernel<false, true><<<grid, 256, 0, st>>>(s, d, n_out, tw, alpha, a2, ad, js);
+    } else {
+        if (circle) fold_kernel<true, false><<<grid, 256, 0, st>>>(s, d, n_out, tw, alpha, a2, ad, 0);
+        else fold_kernel<false, false><<<grid, 256, 0, st>>>(s, d, n_out, tw, alpha, a2, ad, 0);
+    }
     STWO_LAUNCH_CHECK("fold_kernel");
     return STWO_OK;
 }
@@ -148,22 +186,24 @@ extern "C" {
 
 int stwo_fold_line(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha, const uint32_t *itwiddles,
                    uint64_t twiddle_offset, uint32_t *const *dst4, void *stream) {
-    return fold_async(src4, n, alpha, itwiddles, twiddle_offset, dst4, false, as_stream(stream), nullptr);
+    return fold_async(src4, n, alpha, itwiddles, twiddle_offset, dst4, false, as_stream(stream), nullptr, 1, 0);
 }
 
 int stwo_fold_circle_into_line(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha, const uint32_t *itwiddles,
                                uint64_t twiddle_offset, uint32_t *const *dst4, void *stream) {
-    return fold_async(src4, n, alpha, itwiddles, twiddle_offset, dst4, true, as_stream(stream), nullptr);
+    return fold_async(src4, n, alpha, itwiddles, twiddle_offset, dst4, true, as_stream(stream), nullptr, 1, 0);
 }
 
 void fold_line(const uint32_t *gpu_domain, size_t twiddle_offset, size_t n, uint32_t *const *eval_values,
                stwo_qm31 alpha, uint32_t *const *folded_values) {
-    sync_default_stream(fold_async(eval_values, n, alpha, gpu_domain, twiddle_offset, folded_values, false, 0, nullptr));
+    sync_default_stream(
+        fold_async(eval_values, n, alpha, gpu_domain, twiddle_offset, folded_values, false, 0, nullptr, 1, 0));
 }
 
 void fold_circle_into_line(const uint32_t *gpu_domain, size_t twiddle_offset, size_t n, uint32_t *const *eval_values,
                            stwo_qm31 alpha, uint32_t *const *folded_values) {
-    sync_default_stream(fold_async(eval_values, n, alpha, gpu_domain, twiddle_offset, folded_values, true, 0, nullptr));
+    sync_default_stream(
+        fold_async(eval_values, n, alpha, gpu_domain, twiddle_offset, folded_values, true, 0, nullptr, 1, 0));
 }
 
 }  // extern "C"

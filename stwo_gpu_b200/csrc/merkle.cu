@@ -116,18 +116,20 @@ struct TreeParams {
     TreeBand band[MERKLE_MAX_BANDS];
     uint32_t n_bands;
     uint32_t *tickets;
+    size_t js;  // jobs' memory stride: blockIdx.y's tree is job 0's moved by blockIdx.y * js
 };
 
 
 template <int THREADS>
 __device__ __forceinline__ void merkle_unit(const TreeParams &p, const TreeBand &bd, uint32_t u,
                                             uint4 (*thin)[THREADS][2], uint32_t one) {
+    const uint32_t job = blockIdx.y;
     // node indices fit 32 bits: a layer has at most 2^30 nodes
     const uint32_t per0 = (uint32_t)THREADS << bd.spread;
     for (uint32_t j = 0; j < bd.levels; j++) {
         const uint32_t l = bd.top - j;
         const uint32_t per = per0 >> j, first = u * per, n_l = 1u << l;
-        const uint32_t *const *ct = p.cols[l];
+        const uint32_t *const *ct = job_ptr(p.cols[l], p.js, job);
         const uint32_t nc = p.n_cols[l];
         // children: none (a leaf layer), this CTA's shared memory (when the level below
         // had at most THREADS nodes), or global memory: other CTAs' nodes on a band's
@@ -136,8 +138,8 @@ __device__ __forceinline__ void merkle_unit(const TreeParams &p, const TreeBand 
         const bool kids = j > 0 || bd.has_prev;
         const bool kids_shared = j > 0 && (per0 >> (j - 1)) <= (uint32_t)THREADS;
         const bool to_shared = per <= (uint32_t)THREADS && j + 1 < bd.levels;
-        const uint4 *below = kids ? p.layer[l + 1] : nullptr;
-        uint4 *out = p.layer[l];
+        const uint4 *below = kids ? job_ptr(p.layer[l + 1], p.js, job) : nullptr;
+        uint4 *out = job_ptr(p.layer[l], p.js, job);
         for (uint32_t k = threadIdx.x; k < per && first + k < n_l; k += THREADS) {
             const uint32_t i = first + k;
             uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -202,7 +204,7 @@ __global__ void __launch_bounds__(THREADS) merkle_tree_kernel(const __grid_const
         // CTAs before the ticket.
         if (threadIdx.x == 0) {
             __threadfence();
-            uint32_t *t = p.tickets + up.ticket_base + parent;
+            uint32_t *t = job_ptr(p.tickets, p.js, blockIdx.y) + up.ticket_base + parent;
             const uint32_t want = up.fan < p.band[b].units ? up.fan : p.band[b].units;
             const uint32_t arrived = atomicAdd(t, 1u) + 1;
             next = arrived == want;
@@ -265,8 +267,8 @@ int plan_tree_bands(uint32_t max_log, TreePlan &tp) {
 }
 
 template <int THREADS>
-void launch_tree(const TreeParams &p, uint32_t blocks, cudaStream_t st) {
-    merkle_tree_kernel<THREADS><<<blocks, THREADS, 0, st>>>(p, 1u);
+void launch_tree(const TreeParams &p, uint32_t blocks, uint32_t jobs, cudaStream_t st) {
+    merkle_tree_kernel<THREADS><<<dim3(blocks, jobs), THREADS, 0, st>>>(p, 1u);
 }
 
 template <int CAP>
@@ -294,8 +296,11 @@ uint32_t merkle_tree_tickets(uint32_t max_log) {
 // level_ncols[l] for layer l (table may be null when the count is 0); layers[l] the
 // 2^l-node outputs. With `tickets` (n_tickets zeroed words, at least
 // merkle_tree_tickets(max_log); left zeroed) one launch; otherwise one launch per band.
+// jobs trees of one shape at once: tree k's layers, tables and tickets are tree 0's
+// moved by k * js bytes.
 int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_cols, const uint32_t *level_ncols,
-                          uint32_t *const *layers, uint32_t *tickets, uint32_t n_tickets, cudaStream_t st) {
+                          uint32_t *const *layers, uint32_t *tickets, uint32_t n_tickets, uint32_t jobs, size_t js,
+                          cudaStream_t st) {
     TreePlan tp;
     int rc = plan_tree_bands(max_log, tp);
     if (rc) return rc;
@@ -306,10 +311,12 @@ int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_
         p.cols[l] = level_cols[l];
         p.n_cols[l] = level_ncols[l];
     }
+    STWO_REQUIRE(jobs >= 1 && jobs <= 65535, STWO_ERR_INVALID_ARGUMENT, "merkle trees per launch: %u", jobs);
+    p.js = js;
     auto launch = [&](uint32_t blocks) {
-        if (tp.threads == 512) launch_tree<512>(p, blocks, st);
-        else if (tp.threads == 128) launch_tree<128>(p, blocks, st);
-        else launch_tree<256>(p, blocks, st);
+        if (tp.threads == 512) launch_tree<512>(p, blocks, jobs, st);
+        else if (tp.threads == 128) launch_tree<128>(p, blocks, jobs, st);
+        else launch_tree<256>(p, blocks, jobs, st);
     };
     if (tickets && n_tickets >= tp.n_tickets) {
         for (uint32_t b = 0; b < tp.n_bands; b++) p.band[b] = tp.band[b];
@@ -394,7 +401,7 @@ int stwo_merkle_commit_tree(const uint32_t *const *columns, const uint32_t *log_
     for (uint32_t l = 0; l <= max_log; l++)
         if (count[l]) level_cols[l] = static_cast<const uint32_t *const *>(table) + start[l];
     uint32_t *tickets = reinterpret_cast<uint32_t *>(static_cast<const uint32_t **>(table) + table_words);
-    int rc = merkle_tree_dev_async(max_log, level_cols.data(), count.data(), layers, tickets, n_tickets, st);
+    int rc = merkle_tree_dev_async(max_log, level_cols.data(), count.data(), layers, tickets, n_tickets, 1, 0, st);
     cudaFreeAsync(table, st);
     return rc;
 }

@@ -53,6 +53,7 @@ struct WideFibParams {
     uint32_t n_cols;
     uint32_t log_size;
     uint32_t two;             // 2 (fold64_fma)
+    size_t js;                // jobs' memory stride: blockIdx.y's job is job 0's moved by blockIdx.y * js
 };
 
 // Powers on the device (plain QM31). Two rows per thread (8-byte loads). The column
@@ -72,9 +73,13 @@ __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant_
     extern __shared__ uint4 wf_smem[];
     qm31 *s_pow = reinterpret_cast<qm31 *>(wf_smem);
     const uint32_t **s_col = reinterpret_cast<const uint32_t **>(s_pow + p.n_cols);
+    const uint32_t job = blockIdx.y;
+    const uint32_t *const *trace_dev = job_ptr(p.trace_dev, p.js, job);
+    const qm31 *powers_dev = job_ptr(p.powers_dev, p.js, job);
+    const uint32_t *den_inv = job_ptr(p.den_inv, p.js, job);
     for (uint32_t c = threadIdx.x; c < p.n_cols; c += blockDim.x) {
-        s_col[c] = CAP == 1 ? p.trace_dev[c] : p.trace[c];
-        if (c >= 2) s_pow[c] = p.powers_dev[p.n_cols - 1 - c];
+        s_col[c] = CAP == 1 ? trace_dev[c] : p.trace[c];
+        if (c >= 2) s_pow[c] = powers_dev[p.n_cols - 1 - c];
     }
     __syncthreads();
     auto colp = [&](uint32_t c) { return s_col[c]; };
@@ -136,31 +141,33 @@ __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant_
         uint32_t o[4][2];
         for (int r = 0; r < 2; r++) {
             const uint64_t row = 2 * k + r;
-            uint32_t d = row >= n ? 0u : p.den_inv ? __ldg(p.den_inv + row) : p.den_half[row >> (p.log_size - 1)];
+            uint32_t d = row >= n ? 0u : den_inv ? __ldg(den_inv + row) : p.den_half[row >> (p.log_size - 1)];
             uint32_t d2 = d << 1;
             for (int c = 0; c < 4; c++) o[c][r] = m31_mul2(reduce64_p(acc[r][c]), d2);
         }
         for (int c = 0; c < 4; c++) {
-            if (full) reinterpret_cast<uint2 *>(p.out[c])[k] = make_uint2(o[c][0], o[c][1]);
-            else p.out[c][2 * k] = o[c][0];
+            uint32_t *out = job_ptr(p.out[c], p.js, job);
+            if (full) reinterpret_cast<uint2 *>(out)[k] = make_uint2(o[c][0], o[c][1]);
+            else out[2 * k] = o[c][0];
         }
     }
 }
 
 template <int CAP>
-void launch_wf(const WideFibParams<CAP> &p, uint64_t pairs, cudaStream_t st) {
+void launch_wf(const WideFibParams<CAP> &p, uint64_t pairs, uint32_t jobs, cudaStream_t st) {
     // Small domains: 64-thread CTAs so that more SMs share the rows.
     const uint32_t threads = pairs < (uint64_t)device_sm_count() * 256 ? 64 : 256;
     uint64_t blocks = (pairs + threads - 1) / threads, cap = (uint64_t)device_sm_count() * 32;
     if (blocks > cap) blocks = cap;
     // n_cols <= WF_MAX_COLS: at most 2048 x 24 bytes, the default dynamic limit.
-    wide_fib_kernel<CAP><<<(unsigned)blocks, threads, (size_t)p.n_cols * (sizeof(qm31) + sizeof(void *)), st>>>(p);
+    wide_fib_kernel<CAP>
+        <<<dim3((unsigned)blocks, jobs), threads, (size_t)p.n_cols * (sizeof(qm31) + sizeof(void *)), st>>>(p);
 }
 
 template <int CAP>
 int wide_fib_launch(const uint32_t *const *trace, const uint32_t *const *trace_dev, uint32_t n_cols, uint32_t log_size,
                     const stwo_qm31 *powers_host, const uint32_t *powers_dev, const uint32_t *den_inv,
-                    const uint32_t *den_half, uint32_t *const *out4, cudaStream_t st) {
+                    const uint32_t *den_half, uint32_t *const *out4, uint32_t jobs, size_t js, cudaStream_t st) {
     auto p = std::make_unique<WideFibParams<CAP>>();
     if (CAP > 1)
         for (uint32_t i = 0; i < n_cols; i++) {
@@ -178,10 +185,11 @@ int wide_fib_launch(const uint32_t *const *trace, const uint32_t *const *trace_d
     p->n_cols = n_cols;
     p->log_size = log_size;
     p->two = 2;
+    p->js = js;
     p->powers_dev = reinterpret_cast<const qm31 *>(powers_dev);
     const uint64_t n = 1ull << log_size, pairs = (n + 1) / 2;
     if (powers_dev) {
-        launch_wf(*p, pairs, st);
+        launch_wf(*p, pairs, jobs, st);
         STWO_LAUNCH_CHECK("wide_fib_kernel");
         return STWO_OK;
     }
@@ -200,7 +208,7 @@ int wide_fib_launch(const uint32_t *const *trace, const uint32_t *const *trace_d
     cudaError_t e = cudaMemcpyAsync(buf, w2.get(), sizeof(qm31) * (n_cols - 2), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         p->powers_dev = static_cast<const qm31 *>(buf);
-        launch_wf(*p, pairs, st);
+        launch_wf(*p, pairs, 1, st);
         count_launch();
         e = cudaGetLastError();
     }
@@ -239,24 +247,28 @@ int wide_fib_async(const uint32_t *const *trace, uint32_t n_cols, uint32_t log_s
         return STWO_OK;
     }
     if (n_cols <= 64)
-        return wide_fib_launch<64>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, nullptr, out4,
-                                   st);
+        return wide_fib_launch<64>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, nullptr, out4, 1,
+                                   0, st);
     if (n_cols <= 256)
         return wide_fib_launch<256>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, nullptr, out4,
-                                    st);
+                                    1, 0, st);
     return wide_fib_launch<WF_MAX_COLS>(trace, nullptr, n_cols, log_size, powers_host, powers_dev, den_inv, nullptr,
-                                        out4, st);
+                                        out4, 1, 0, st);
 }
 
 // Same, with the trace column pointers in a device table and the powers on the device;
 // the denominator inverse of a row is den_half[0] on the first half of the rows and
 // den_half[1] on the second (the vanishing polynomial of a canonic coset takes one
 // value on each half of its blowup-2 domain in bit-reversed order).
+// jobs compositions of one shape at once: job k's tables, powers and outputs are job
+// 0's moved by k * js bytes.
 int wide_fib_dev_async(const uint32_t *const *trace_dev, uint32_t n_cols, uint32_t log_size, const uint32_t *powers_dev,
-                       const uint32_t den_half[2], uint32_t *const *out4, cudaStream_t st) {
+                       const uint32_t den_half[2], uint32_t *const *out4, uint32_t jobs, size_t js, cudaStream_t st) {
     STWO_REQUIRE(n_cols >= 3 && log_size >= 1 && log_size <= 31 && powers_dev, STWO_ERR_UNSUPPORTED_SIZE,
                  "wide-Fibonacci composition over %u columns", n_cols);
-    return wide_fib_launch<1>(nullptr, trace_dev, n_cols, log_size, nullptr, powers_dev, nullptr, den_half, out4, st);
+    STWO_REQUIRE(jobs >= 1 && jobs <= 65535, STWO_ERR_INVALID_ARGUMENT, "compositions per launch: %u", jobs);
+    return wide_fib_launch<1>(nullptr, trace_dev, n_cols, log_size, nullptr, powers_dev, nullptr, den_half, out4, jobs,
+                              js, st);
 }
 
 }  // namespace stwo

@@ -172,9 +172,11 @@ __device__ __forceinline__ qm31 eap_lane_fold(qm31 acc, const qm31 *fj) {
 // (partials indexed by CTA).
 // cur holds this thread's first group, loaded by the caller before the factors were
 // ready, so that those loads overlap the set-up of the tables.
+// partials, tickets and results belong to job 0; this CTA's job is blockIdx.y, whose
+// are moved by blockIdx.y * js bytes (applied where they are used, after the loop).
 __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t L, const qm31 *f, const uint32_t *c,
                                          uint32_t iter_log, uint32_t blk_first, uint32_t nblk, qm31 *partials,
-                                         uint32_t *tickets, qm31 *results, uint4 (&cur)[8]) {
+                                         uint32_t *tickets, qm31 *results, uint4 (&cur)[8], size_t js = 0) {
     __shared__ qm31 warp_vals[EAP_THREADS / 32];
     __shared__ qm31 g[1 << EAP_ITER_LOG_MAX];
     __shared__ qm31 F2[1 << EAP_PER_THREAD_LOG];  // F_i
@@ -255,14 +257,17 @@ __device__ __forceinline__ void eap_body(uint32_t poly, uint32_t chunk, uint32_t
         qm31 w = tid < EAP_THREADS / 32 ? warp_vals[tid] : qm31_zero();
         w = eap_lane_fold<3>(w, f + 10);
         if (tid == 0) {
-            partials[blockIdx.x] = qm31_mul(w, chunk_w);
+            job_ptr(partials, js, blockIdx.y)[blockIdx.x] = qm31_mul(w, chunk_w);
             __threadfence();
-            uint32_t t = atomicAdd(&tickets[poly], 1u);
+            uint32_t t = atomicAdd(&job_ptr(tickets, js, blockIdx.y)[poly], 1u);
             is_last = (t == nblk - 1);
         }
     }
     __syncthreads();
     if (is_last) {
+        partials = job_ptr(partials, js, blockIdx.y);
+        tickets = job_ptr(tickets, js, blockIdx.y);
+        results = job_ptr(results, js, blockIdx.y);
         // The whole last CTA sums the partials: strided per thread, then across lanes
         // and warps (field addition, so the order does not change the sum).
         __threadfence();
@@ -309,7 +314,10 @@ struct EapDevPoly {
 __global__ void __launch_bounds__(EAP_THREADS, 4) eval_at_point_dev_kernel(const EapDevPoly *__restrict__ polys,
                                                                            uint32_t n_polys, uint32_t iter_log,
                                                                            const qm31 *point, qm31 *partials,
-                                                                           uint32_t *tickets, qm31 *results) {
+                                                                           uint32_t *tickets, qm31 *results, size_t js) {
+    // blockIdx.y: the job, whose descriptors, point, partials, tickets and results are
+    // job 0's moved by blockIdx.y * js bytes
+    polys = job_ptr(polys, js, blockIdx.y);
     __shared__ qm31 f[32];
     // The last polynomial whose first CTA is <= blockIdx.x, by a 32-way search: each
     // round lane k tests candidate lo + k * step, and polys[lo] always qualifies.
@@ -329,6 +337,7 @@ __global__ void __launch_bounds__(EAP_THREADS, 4) eval_at_point_dev_kernel(const
     eap_load(d.coeffs, 1ull << d.log_size, chunk, EAP_GROUP_LOG + iter_log, 0, cur);
     if (threadIdx.x == 0) {
         // f_0 = y, f_1 = x, f_b = pi^(b-1)(x)
+        point = job_ptr(point, js, blockIdx.y);
         f[0] = point[1];
         qm31 x = point[0];
         for (uint32_t b = 1; b < 32; b++) {
@@ -339,7 +348,7 @@ __global__ void __launch_bounds__(EAP_THREADS, 4) eval_at_point_dev_kernel(const
     }
     __syncthreads();
     eap_body(lo, chunk, d.log_size, f, d.coeffs, iter_log, d.block_start, next - d.block_start, partials, tickets,
-             results, cur);
+             results, cur, js);
 }
 
 inline qm31 to_q(stwo_qm31 v) { return {{v.a, v.b}, {v.c, v.d}}; }
@@ -431,15 +440,18 @@ int eval_at_points_async(const uint32_t *const *coeffs, const uint32_t *log_size
 // eval_at_point for polynomials described in device memory (polys_dev: n_polys
 // EapDevPoly, CTAs counted with eval_at_point_blocks(log size, iter_log)), at the
 // device point point_dev (QM31 x then y). partials: total_blocks QM31; tickets:
-// n_polys zeroed words (left zeroed).
+// n_polys zeroed words (left zeroed). jobs sets of one shape at once: set k's
+// descriptors, point, results, partials and tickets are set 0's moved by k * js bytes.
 int eval_at_points_dev_async(const void *polys_dev, uint32_t n_polys, uint32_t iter_log, uint32_t total_blocks,
-                             const void *point_dev, void *results, void *partials, uint32_t *tickets, cudaStream_t st) {
+                             const void *point_dev, void *results, void *partials, uint32_t *tickets, uint32_t jobs,
+                             size_t js, cudaStream_t st) {
     STWO_REQUIRE(n_polys >= 1 && total_blocks >= n_polys, STWO_ERR_INVALID_ARGUMENT, "eval_at_point descriptors");
+    STWO_REQUIRE(jobs >= 1 && jobs <= 65535, STWO_ERR_INVALID_ARGUMENT, "eval_at_point sets per launch: %u", jobs);
     STWO_REQUIRE(iter_log >= (uint32_t)EAP_ITER_LOG_MIN && iter_log <= (uint32_t)EAP_ITER_LOG_MAX,
                  STWO_ERR_INVALID_ARGUMENT, "eval_at_point groups per CTA 2^%u", iter_log);
-    eval_at_point_dev_kernel<<<total_blocks, EAP_THREADS, 0, st>>>(
+    eval_at_point_dev_kernel<<<dim3(total_blocks, jobs), EAP_THREADS, 0, st>>>(
         static_cast<const EapDevPoly *>(polys_dev), n_polys, iter_log, static_cast<const qm31 *>(point_dev),
-        static_cast<qm31 *>(partials), tickets, static_cast<qm31 *>(results));
+        static_cast<qm31 *>(partials), tickets, static_cast<qm31 *>(results), js);
     STWO_LAUNCH_CHECK("eval_at_point_dev_kernel");
     return STWO_OK;
 }

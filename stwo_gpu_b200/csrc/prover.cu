@@ -58,14 +58,16 @@ int fft_columns(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_c
 int fft_columns_tab(const uint32_t *const *srcs, uint32_t *const *dsts, uint32_t n_cols, uint32_t N, uint32_t L,
                     const uint32_t *tree, uint64_t tree_size, bool inv, cudaStream_t st, const void *dev_table);
 int merkle_tree_dev_async(uint32_t max_log, const uint32_t *const *const *level_cols, const uint32_t *level_ncols,
-                          uint32_t *const *layers, uint32_t *tickets, uint32_t n_tickets, cudaStream_t st);
+                          uint32_t *const *layers, uint32_t *tickets, uint32_t n_tickets, uint32_t jobs, size_t js,
+                          cudaStream_t st);
 uint32_t merkle_tree_tickets(uint32_t max_log);
 int fold_async(const uint32_t *const *src4, uint64_t n, stwo_qm31 alpha_c, const uint32_t *itw, uint64_t off,
-               uint32_t *const *dst4, bool circle, cudaStream_t st, const void *alpha_dev);
+               uint32_t *const *dst4, bool circle, cudaStream_t st, const void *alpha_dev, uint32_t jobs, size_t js);
 int wide_fib_dev_async(const uint32_t *const *trace_dev, uint32_t n_cols, uint32_t log_size, const uint32_t *powers_dev,
-                       const uint32_t den_half[2], uint32_t *const *out4, cudaStream_t st);
+                       const uint32_t den_half[2], uint32_t *const *out4, uint32_t jobs, size_t js, cudaStream_t st);
 int eval_at_points_dev_async(const void *polys_dev, uint32_t n_polys, uint32_t iter_log, uint32_t total_blocks,
-                             const void *point_dev, void *results, void *partials, uint32_t *tickets, cudaStream_t st);
+                             const void *point_dev, void *results, void *partials, uint32_t *tickets, uint32_t jobs,
+                             size_t js, cudaStream_t st);
 uint32_t eval_at_point_blocks(uint32_t log_size, uint32_t iter_log);
 uint32_t eval_at_point_iter_log(const uint32_t *log_sizes, uint32_t n);
 
@@ -105,10 +107,14 @@ struct EapDevPoly {
 // Trace rows (write_trace_row, wide_fibonacci.rs:196-203): a_0 = a0[r], a_1 = a1[r],
 // a_{j+2} = a_j^2 + a_{j+1}^2. Row r is position r of every column, the bit-reversed
 // storage order of the trace evaluations. Column pointers come from a device table.
+// blockIdx.y: the job (js: the jobs' memory stride).
 __global__ void __launch_bounds__(256) wide_fib_trace_kernel(const uint32_t *__restrict__ a0,
                                                              const uint32_t *__restrict__ a1,
                                                              uint32_t *const *__restrict__ cols, uint32_t n_cols,
-                                                             uint64_t rows) {
+                                                             uint64_t rows, size_t js) {
+    a0 = job_ptr(a0, js, blockIdx.y);
+    a1 = job_ptr(a1, js, blockIdx.y);
+    cols = job_ptr(cols, js, blockIdx.y);
     for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t x = a0[r], y = a1[r];
         cols[0][r] = x;
@@ -153,7 +159,10 @@ inline void vanishing_inverses(uint32_t L, uint32_t out[2]) {
 
 // Channel step after the trace tree: mix its root, draw the composition coefficient r,
 // and write powers[k] = r^k (k < n_powers; lane l computes k = l, l + 32, ...).
-__global__ void fs_trace_kernel(ProofState *s, const uint32_t *root, qm31 *powers, uint32_t n_powers) {
+__global__ void fs_trace_kernel(ProofState *s, const uint32_t *root, qm31 *powers, uint32_t n_powers, size_t js) {
+    s = job_ptr(s, js, blockIdx.x);  // one CTA a job
+    root = job_ptr(root, js, blockIdx.x);
+    powers = job_ptr(powers, js, blockIdx.x);
     __shared__ qm31 rc;
     if (threadIdx.x == 0) {
         for (int i = 0; i < 8; i++) s->roots[0][i] = root[i];
@@ -173,7 +182,9 @@ __global__ void fs_trace_kernel(ProofState *s, const uint32_t *root, qm31 *power
 
 // Channel step after the composition tree: mix its root, draw t and take the OODS
 // point (CirclePoint::get_random_point): x = (1 - t^2) / (1 + t^2), y = 2t / (1 + t^2).
-__global__ void fs_comp_kernel(ProofState *s, const uint32_t *root) {
+__global__ void fs_comp_kernel(ProofState *s, const uint32_t *root, size_t js) {
+    s = job_ptr(s, js, blockIdx.x);  // one thread a job
+    root = job_ptr(root, js, blockIdx.x);
     for (int i = 0; i < 8; i++) s->roots[1][i] = root[i];
     fs::ch_mix_root(s->ch, root);
     const qm31 t = fs::ch_draw_felt(s->ch, s->error), t2 = qm31_mul(t, t);
@@ -195,7 +206,12 @@ __global__ void fs_comp_kernel(ProofState *s, const uint32_t *root) {
 constexpr uint32_t OODS_STAGED = 1024;
 __global__ void __launch_bounds__(256) fs_oods_kernel(ProofState *s, const qm31 *sampled, const qm31 *powers,
                                                       uint32_t N, uint32_t L, cpoint vsh, QuotParamsDev *q_comp,
-                                                      QuotParamsDev *q_trace) {
+                                                      QuotParamsDev *q_trace, size_t js) {
+    s = job_ptr(s, js, blockIdx.x);  // one CTA a job
+    sampled = job_ptr(sampled, js, blockIdx.x);
+    powers = job_ptr(powers, js, blockIdx.x);
+    q_comp = job_ptr(q_comp, js, blockIdx.x);
+    q_trace = job_ptr(q_trace, js, blockIdx.x);
     __shared__ qm31 sh[32];
     __shared__ qm31 qrc_sh;
     __shared__ qm31 staged[OODS_STAGED];
@@ -239,7 +255,10 @@ __global__ void __launch_bounds__(256) fs_oods_kernel(ProofState *s, const qm31 
 }
 
 // Channel step after an FRI tree: mix its root, draw the folding alpha.
-__global__ void fs_layer_kernel(ProofState *s, const uint32_t *root, uint32_t root_slot, uint32_t alpha_slot) {
+__global__ void fs_layer_kernel(ProofState *s, const uint32_t *root, uint32_t root_slot, uint32_t alpha_slot,
+                                size_t js) {
+    s = job_ptr(s, js, blockIdx.x);  // one thread a job
+    root = job_ptr(root, js, blockIdx.x);
     for (int i = 0; i < 8; i++) s->roots[root_slot][i] = root[i];
     fs::ch_mix_root(s->ch, root);
     s->alphas[alpha_slot] = fs::ch_draw_felt(s->ch, s->error);
@@ -302,7 +321,9 @@ struct TailParams {
 };
 
 __global__ void __launch_bounds__(TAIL_THREADS) fri_tail_kernel(ProofState *s, const TailParams *__restrict__ tp,
-                                                                 uint32_t one) {
+                                                                 uint32_t one, size_t js) {
+    s = job_ptr(s, js, blockIdx.x);  // one CTA a job; the job's parameters hold its own pointers
+    tp = job_ptr(tp, js, blockIdx.x);
     extern __shared__ uint4 t_buf[];
     // the two node buffers, by computed address (an indexed pointer array would live
     // in local memory)
@@ -400,14 +421,14 @@ __global__ void __launch_bounds__(TAIL_THREADS) fri_tail_kernel(ProofState *s, c
     if (tid == 0) fs_last(s, tp->lay[tp->n_tail], tp->last_log);
 }
 
-int launch_fri_tail(ProofState *s, const TailParams *tp, cudaStream_t st) {
+int launch_fri_tail(ProofState *s, const TailParams *tp, uint32_t jobs, size_t js, cudaStream_t st) {
     static std::atomic<uint64_t> attr_set{0};
     int rc = once_per_device(attr_set, [] {
         STWO_CUDA_TRY(cudaFuncSetAttribute(fri_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM));
         return (int)STWO_OK;
     });
     if (rc) return rc;
-    fri_tail_kernel<<<1, TAIL_THREADS, TAIL_SMEM, st>>>(s, tp, 1u);
+    fri_tail_kernel<<<jobs, TAIL_THREADS, TAIL_SMEM, st>>>(s, tp, 1u, js);
     STWO_LAUNCH_CHECK("fri_tail_kernel");
     return STWO_OK;
 }
@@ -425,7 +446,8 @@ __device__ __forceinline__ uint32_t ctz128(const uint32_t w[4]) {
     return 128;
 }
 
-__global__ void __launch_bounds__(256) grind_kernel(ProofState *s, uint32_t pow_bits, uint64_t max_k) {
+__global__ void __launch_bounds__(256) grind_kernel(ProofState *s, uint32_t pow_bits, uint64_t max_k, size_t js) {
+    s = job_ptr(s, js, blockIdx.y);
     const uint32_t one = 1;
     uint32_t d[8];
 #pragma unroll
@@ -451,7 +473,8 @@ __global__ void __launch_bounds__(256) grind_kernel(ProofState *s, uint32_t pow_
 
 // After the search: mix the nonce and draw the raw query words (Queries::generate takes
 // each u32 masked to the largest domain's log size).
-__global__ void fs_finish_kernel(ProofState *s, uint32_t n_queries) {
+__global__ void fs_finish_kernel(ProofState *s, uint32_t n_queries, size_t js) {
+    s = job_ptr(s, js, blockIdx.x);  // one thread a job
     if (s->nonce == ~0ull) {
         s->error |= fs::ERR_GRIND;
         return;
@@ -1019,6 +1042,8 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
                                 : cudaEventRecord(ev[k], st));
         return STWO_OK;
     };
+    const uint32_t K = 1;  // jobs of this launch sequence
+    const size_t js = 0;   // their memory stride
     auto launch_all = [&](bool capturing) -> int {
         // ---- 1. trace: twiddles, generation, interpolation, evaluation, tree
         if (own_tw)
@@ -1027,8 +1052,8 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
             const uint32_t threads = rows < (uint64_t)device_sm_count() * 256 ? 64 : 256;
             const uint64_t blocks =
                 std::min<uint64_t>((rows + threads - 1) / threads, (uint64_t)device_sm_count() * 16);
-            wide_fib_trace_kernel<<<(unsigned)blocks, threads, 0, st>>>(
-                a0, a1, reinterpret_cast<uint32_t *const *>(dev_at(off_tpoly)), N, rows);
+            wide_fib_trace_kernel<<<dim3((unsigned)blocks, K), threads, 0, st>>>(
+                a0, a1, reinterpret_cast<uint32_t *const *>(dev_at(off_tpoly)), N, rows, js);
             STWO_LAUNCH_CHECK("wide_fib_trace_kernel");
         }
         // The trace columns are interpolated in place: they become the coefficient columns.
@@ -1039,10 +1064,10 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         }
         auto commit = [&](MerkleTree &t) {
             return merkle_tree_dev_async(t.max_log, t.level_tables.data(), t.level_n.data(), t.layers.data(), t.tickets,
-                                         t.n_tickets, st);
+                                         t.n_tickets, K, js, st);
         };
         PV_TRY(commit(t_trace));
-        fs_trace_kernel<<<1, 32, 0, st>>>(dstate, t_trace.layers[0], powers, N - 2);
+        fs_trace_kernel<<<K, 32, 0, st>>>(dstate, t_trace.layers[0], powers, N - 2, js);
         STWO_LAUNCH_CHECK("fs_trace_kernel");
         PV_TRY(record(1, capturing));
 
@@ -1054,35 +1079,35 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         uint32_t den_half[2];
         vanishing_inverses(L, den_half);
         PV_TRY(wide_fib_dev_async(reinterpret_cast<const uint32_t *const *>(dev_at(off_text)), N, E,
-                                  reinterpret_cast<const uint32_t *>(powers), den_half, comp.data(), st));
+                                  reinterpret_cast<const uint32_t *>(powers), den_half, comp.data(), K, js, st));
         PV_TRY(fft_columns(comp.data(), comp.data(), 4, E, E, itw, tsz, true, st));  // in place -> coefficients
         {
             std::vector<const uint32_t *> src(comp.begin(), comp.end());
             PV_TRY(fft_columns(src.data(), cev.data(), 4, D, E, tw, tsz, false, st));
         }
         PV_TRY(commit(t_comp));
-        fs_comp_kernel<<<1, 1, 0, st>>>(dstate, t_comp.layers[0]);
+        fs_comp_kernel<<<K, 1, 0, st>>>(dstate, t_comp.layers[0], js);
         STWO_LAUNCH_CHECK("fs_comp_kernel");
         PV_TRY(record(2, capturing));
 
         // ---- 3. out-of-domain sampling
         PV_TRY(eval_at_points_dev_async(dev_at(off_eap), eap_n, eap_iter, eap_total, dstate->oods, dsampled,
-                                        eap_partials, dtickets, st));
-        fs_oods_kernel<<<1, 256, 0, st>>>(dstate, dsampled, powers, N, L, vanishing_shift(L), dqc, dqt);
+                                        eap_partials, dtickets, K, js, st));
+        fs_oods_kernel<<<K, 256, 0, st>>>(dstate, dsampled, powers, N, L, vanishing_shift(L), dqc, dqt, js);
         STWO_LAUNCH_CHECK("fs_oods_kernel");
         PV_TRY(record(3, capturing));
 
         // ---- 4. DEEP quotients (largest columns first) and the FRI commitment
-        PV_TRY(quotients_dev_async(dqc, D, 4, st));
-        PV_TRY(quotients_dev_async(dqt, L + B, N, st));
+        PV_TRY(quotients_dev_async(dqc, D, 4, K, js, st));
+        PV_TRY(quotients_dev_async(dqt, L + B, N, K, js, st));
         PV_TRY(commit(t_fri0));
-        fs_layer_kernel<<<1, 1, 0, st>>>(dstate, t_fri0.layers[0], 2, 0);
+        fs_layer_kernel<<<K, 1, 0, st>>>(dstate, t_fri0.layers[0], 2, 0, js);
         STWO_LAUNCH_CHECK("fs_layer_kernel");
         for (int k = 0; k < 4; k++) STWO_CUDA_TRY(cudaMemsetAsync(lay[0][k], 0, 4ull << (D - 1), st));
         {
             std::vector<const uint32_t *> s(qc.begin(), qc.end());
             PV_TRY(fold_async(s.data(), 1ull << D, stwo_qm31{}, itw, tsz - (1ull << (D - 1)), lay[0].data(), true, st,
-                              &dstate->alphas[0]));
+                              &dstate->alphas[0], K, js));
         }
         for (uint32_t li = 0; li < li0; li++) {
             const uint32_t lg = D - 1 - li;
@@ -1090,16 +1115,16 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
                 // The trace quotient folds into this layer with the previous layer's alpha.
                 std::vector<const uint32_t *> s(qt.begin(), qt.end());
                 PV_TRY(fold_async(s.data(), 1ull << (L + B), stwo_qm31{}, itw, tsz - (1ull << lg), lay[li].data(), true,
-                                  st, &dstate->alphas[li]));
+                                  st, &dstate->alphas[li], K, js));
             }
             PV_TRY(commit(t_lay[li]));
-            fs_layer_kernel<<<1, 1, 0, st>>>(dstate, t_lay[li].layers[0], 3 + li, li + 1);
+            fs_layer_kernel<<<K, 1, 0, st>>>(dstate, t_lay[li].layers[0], 3 + li, li + 1, js);
             STWO_LAUNCH_CHECK("fs_layer_kernel");
             std::vector<const uint32_t *> s(lay[li].begin(), lay[li].end());
             PV_TRY(fold_async(s.data(), 1ull << lg, stwo_qm31{}, itw, tsz - (1ull << lg), lay[li + 1].data(), false, st,
-                              &dstate->alphas[li + 1]));
+                              &dstate->alphas[li + 1], K, js));
         }
-        PV_TRY(launch_fri_tail(dstate, reinterpret_cast<const TailParams *>(dev_at(off_tail)), st));
+        PV_TRY(launch_fri_tail(dstate, reinterpret_cast<const TailParams *>(dev_at(off_tail)), K, js, st));
         PV_TRY(record(4, capturing));
 
         // ---- 5. proof of work and query words, then the channel's record to the host
@@ -1109,9 +1134,9 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
                 std::max<uint64_t>(256, std::min<uint64_t>(want, (uint64_t)device_sm_count() * 1024));
             const uint64_t blocks = (threads + 255) / 256, grid = blocks * 256;
             const uint64_t max_k = ((1ull << (j.pow_bits + 6)) + grid - 1) / grid + 1;  // gives up after 2^(pow_bits+6)
-            grind_kernel<<<(unsigned)blocks, 256, 0, st>>>(dstate, j.pow_bits, max_k);
+            grind_kernel<<<dim3((unsigned)blocks, K), 256, 0, st>>>(dstate, j.pow_bits, max_k, js);
             STWO_LAUNCH_CHECK("grind_kernel");
-            fs_finish_kernel<<<1, 1, 0, st>>>(dstate, j.n_queries);
+            fs_finish_kernel<<<K, 1, 0, st>>>(dstate, j.n_queries, js);
             STWO_LAUNCH_CHECK("fs_finish_kernel");
         }
         return STWO_OK;

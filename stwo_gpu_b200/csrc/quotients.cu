@@ -47,7 +47,8 @@ struct QuotByValue {
 };
 struct QuotByRef {
     const QuotParamsDev *p;
-    __device__ const QuotParamsDev &get() const { return *p; }
+    size_t js;  // jobs' memory stride: blockIdx.y's block is job 0's moved by blockIdx.y * js
+    __device__ const QuotParamsDev &get() const { return *job_ptr(p, js, blockIdx.y); }
 };
 
 // G^idx for a 31-bit circle-group index: the product of three table entries,
@@ -326,8 +327,10 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
     return STWO_OK;
 }
 
-int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t n_samples, cudaStream_t st) {
+int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t n_samples, uint32_t jobs, size_t js,
+                        cudaStream_t st) {
     STWO_REQUIRE(log_size >= 1 && log_size <= 31, STWO_ERR_UNSUPPORTED_SIZE, "domain log size %u", log_size);
+    STWO_REQUIRE(jobs >= 1 && jobs <= 65535, STWO_ERR_INVALID_ARGUMENT, "quotient groups per launch: %u", jobs);
     STWO_REQUIRE(n_samples >= 1 && n_samples <= 1024, STWO_ERR_UNSUPPORTED_SIZE, "%u samples", n_samples);
     const uint32_t n_stage = quot_padded(n_samples);  // one batch
     const size_t smem = (size_t)n_stage * (sizeof(qm31) + sizeof(void *));
@@ -335,7 +338,8 @@ int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t 
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    quotients_kernel<false, 1><<<(unsigned)blocks, 256, smem, st>>>(QuotByRef{p_dev}, nullptr, n_stage, 2u);
+    quotients_kernel<false, 1><<<dim3((unsigned)blocks, jobs), 256, smem, st>>>(QuotByRef{p_dev, js}, nullptr, n_stage,
+                                                                               2u);
     STWO_LAUNCH_CHECK("quotients_kernel");
     return STWO_OK;
 }

@@ -156,7 +156,9 @@ inline void quot_init_static(QP &p, uint32_t half_init, uint32_t half_step, uint
 }
 
 // Launches the quotient kernel on parameters resident in device memory (n_samples:
-// the total sample count, batch_end of the last batch).
-int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t n_samples, cudaStream_t st);
+// the total sample count, batch_end of the last batch); jobs parameter blocks of one
+// shape at once, block k at p_dev moved by k * js bytes.
+int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t n_samples, uint32_t jobs, size_t js,
+                        cudaStream_t st);
 
 }  // namespace stwo
