@@ -327,6 +327,20 @@ int stwo_wide_fib_prove(const stwo_wide_fib_job *job, const uint32_t *a0, const 
                         uint64_t *proof_len, stwo_prove_stats *stats, void *stream);
 void stwo_free_proof(uint8_t *proof);
 
+/* n_jobs proofs of one job shape in one launch sequence (no counterpart in the
+ * reference): every kernel of the proof is launched once for all of them, job k's
+ * device memory being job 0's moved by one job's bound. a0[k], a1[k]: job k's first
+ * two trace columns (host or device). Needs the caller's twiddle tree; n_jobs <= 256,
+ * and the device memory of n_jobs jobs (n_jobs x stwo_wide_fib_prove_device_bytes).
+ * proofs[k] / proof_lens[k] receive job k's malloc'd proof (free with
+ * stwo_free_proof; NULL for a job that failed) and job_status[k] its status; the
+ * call's own status reports the launch sequence. The proofs are byte for byte those
+ * of stwo_wide_fib_prove. stats (may be NULL) describes the whole sequence. */
+int stwo_wide_fib_prove_batch(const stwo_wide_fib_job *job, uint32_t n_jobs, const uint32_t *const *a0,
+                              const uint32_t *const *a1, const uint32_t *twiddles, const uint32_t *itwiddles,
+                              uint64_t tree_size, uint8_t **proofs, uint64_t *proof_lens, int *job_status,
+                              stwo_prove_stats *stats, void *stream);
+
 /* Repeated proofs of one job shape (no counterpart in the reference). A cache keeps
  * the device memory of its last proof; the next stwo_wide_fib_prove_cached call with
  * the same shape, twiddle tree and device reuses it, every buffer at the same address,

@@ -11,5 +11,6 @@ from .backend import (  # noqa: F401
     Coset, CudaBackend, LineDomain, LineEvaluation, SecureColumnByCoords, SecureEvaluation, SecureFieldVec,
     TwiddleTree, index_to_point,
 )
-from .prover import ProofServer, ProveCache, WideFibJob, kernel_launches, prove_wide_fib, wide_fib_inputs  # noqa: F401
+from .prover import (  # noqa: F401
+    ProofServer, ProveCache, WideFibJob, kernel_launches, prove_wide_fib, prove_wide_fib_batch, wide_fib_inputs)
 from .verifier import VerificationError, verify  # noqa: F401

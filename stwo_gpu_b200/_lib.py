@@ -128,6 +128,9 @@ SIGNATURES = [
     ("stwo_wide_fib_prove_device_bytes", u64, [C.POINTER(WideFibJob), C.c_int]),
     ("stwo_wide_fib_prove", C.c_int, [C.POINTER(WideFibJob), vp, vp, vp, vp, u64, C.POINTER(C.POINTER(C.c_uint8)),
                                       C.POINTER(u64), C.POINTER(ProveStats), vp]),
+    ("stwo_wide_fib_prove_batch", C.c_int, [C.POINTER(WideFibJob), u32, vp, vp, vp, vp, u64,
+                                            C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(u64), C.POINTER(C.c_int),
+                                            C.POINTER(ProveStats), vp]),
     ("stwo_free_proof", None, [vp]),
     ("stwo_prove_cache_create", vp, []),
     ("stwo_wide_fib_prove_cached", C.c_int, [vp, C.POINTER(WideFibJob), vp, vp, vp, vp, u64,

@@ -74,6 +74,7 @@ uint32_t eval_at_point_iter_log(const uint32_t *log_sizes, uint32_t n);
 namespace {
 
 constexpr uint32_t WF_MAX_TRACE_COLS = 1024;
+constexpr uint32_t MAX_JOBS_PER_LAUNCH = 256;  // proofs of one shape in one launch sequence
 constexpr uint32_t MAX_DOMAIN_LOG = 27;  // largest committed domain CanonicCoset(L+1+B)
 constexpr uint32_t MAX_LAYERS = 32;      // FRI inner layers
 constexpr uint32_t MAX_QUERIES = 1024;
@@ -825,10 +826,225 @@ void prove_cache_release(ProveCache *c, cudaStream_t st) {
 
 namespace {
 
-int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const uint32_t *tw_in,
-               const uint32_t *itw_in, uint64_t tsz_in, std::vector<uint8_t> &proof, cudaStream_t st,
-               stwo_prove_stats *stats, ProveCache *cache) {
+// One job's device layout and host tables: everything a proof plans before its first
+// launch. The plan depends only on the job's shape, so jobs of one shape planned into
+// equal slabs lie at the same offsets, and job k's memory is job 0's moved by the slabs'
+// distance: one launch sequence (jobs x stride) then serves all of them.
+struct JobLayout {
+    const uint32_t *tw = nullptr, *itw = nullptr;
+    uint64_t tsz = 0;
+    uint32_t *own_tw = nullptr, *own_itw = nullptr;
+    uint32_t *a0 = nullptr, *a1 = nullptr;
+    std::vector<uint32_t *> tpoly, tev, text, comp, cev, qc, qt;
+    qm31 *powers = nullptr;
+    uint32_t n_layers = 0;
+    std::vector<std::vector<uint32_t *>> lay;
+    uint32_t eap_n = 0, eap_total = 0, eap_iter = 0;
+    qm31 *eap_partials = nullptr;
+    Upload up;
+    size_t off_state = 0, off_tickets = 0, off_qc = 0, off_qt = 0, off_tpoly = 0, off_text = 0, off_eap = 0;
+    size_t off_fft_interp = 0, off_fft_eval = 0, off_fft_ext = 0, off_tail = 0;
+    MerkleTree t_trace, t_comp, t_fri0;
+    std::vector<MerkleTree> t_lay;
+    uint32_t li0 = 0, li_circle = 0;
+    uint8_t *dev_img = nullptr;
+    ProofState *dstate = nullptr;
+    qm31 *dsampled = nullptr;
+    uint32_t *dtickets = nullptr;
+    QuotParamsDev *dqc = nullptr, *dqt = nullptr;
+
+    uint8_t *dev_at(size_t off) const { return dev_img + off; }
+
+    int plan(const Job &j, Arena &ar, const uint32_t *tw_in, const uint32_t *itw_in, uint64_t tsz_in) {
+        const uint32_t L = j.L, N = j.N, B = j.B, E = L + 1, D = E + B;
+        const uint64_t rows = 1ull << L;
+        // ---- buffers (all of the job's device memory, before the first launch)
+        tw = tw_in;
+        itw = itw_in;
+        tsz = tsz_in;
+        if (tw_in || itw_in) {
+            STWO_REQUIRE(tw_in && itw_in && is_pow2(tsz_in) && tsz_in >= (1ull << (L + B)), STWO_ERR_INVALID_ARGUMENT,
+                         "twiddle tree of %llu entries does not cover domain log size %u", (unsigned long long)tsz_in, D);
+        } else {
+            tsz = 1ull << (L + B);
+            own_tw = ar.alloc<uint32_t>(tsz);
+            own_itw = ar.alloc<uint32_t>(tsz);
+            STWO_REQUIRE(own_tw && own_itw, STWO_ERR_OUT_OF_MEMORY, "twiddle allocation failed");
+            tw = own_tw;
+            itw = own_itw;
+        }
+        a0 = ar.alloc<uint32_t>(rows);
+        a1 = ar.alloc<uint32_t>(rows);
+        if (!a0 || !a1) return STWO_ERR_OUT_OF_MEMORY;  // pool_alloc recorded the message
+        tpoly.assign(N, nullptr);
+        tev.assign(N, nullptr);
+        text.assign(N, nullptr);
+        for (uint32_t c = 0; c < N; c++) {
+            PV_ALLOC(p, uint32_t, rows);
+            PV_ALLOC(e, uint32_t, rows << B);
+            tpoly[c] = p;
+            tev[c] = e;
+            if (B == 1) {
+                text[c] = e;  // the committed evaluations are already on CanonicCoset(L + 1)
+            } else {
+                PV_ALLOC(x, uint32_t, 1ull << E);
+                text[c] = x;
+            }
+        }
+        powers = ar.alloc<qm31>(N);
+        if (!powers) return STWO_ERR_OUT_OF_MEMORY;
+        comp.assign(4, nullptr);
+        cev.assign(4, nullptr);
+        qc.assign(4, nullptr);
+        qt.assign(4, nullptr);
+        for (int k = 0; k < 4; k++) {
+            PV_ALLOC(c, uint32_t, 1ull << E);
+            PV_ALLOC(e, uint32_t, 1ull << D);
+            PV_ALLOC(a, uint32_t, 1ull << D);
+            PV_ALLOC(b, uint32_t, 1ull << (L + B));
+            comp[k] = c;
+            cev[k] = e;
+            qc[k] = a;
+            qt[k] = b;
+        }
+        // FRI layers: inner logs D-1 .. B+1, then the last layer (log B)
+        n_layers = D - 1 - B;
+        STWO_REQUIRE(n_layers <= MAX_LAYERS && L + B - 1 > B, STWO_ERR_UNSUPPORTED_SIZE, "FRI layer count unsupported");
+        lay.assign(n_layers + 1, std::vector<uint32_t *>(4));
+        for (uint32_t li = 0; li <= n_layers; li++)
+            for (int k = 0; k < 4; k++) {
+                PV_ALLOC(c, uint32_t, 1ull << (D - 1 - li));
+                lay[li][k] = c;
+            }
+        eap_n = N + 4;
+        eap_total = 0;
+        std::vector<EapDevPoly> eap(eap_n);
+        std::vector<uint32_t> eap_logs(eap_n);
+        for (uint32_t i = 0; i < eap_n; i++) eap_logs[i] = i < N ? L : E;
+        eap_iter = eval_at_point_iter_log(eap_logs.data(), eap_n);
+        for (uint32_t i = 0; i < eap_n; i++) {
+            eap[i] = {i < N ? tpoly[i] : comp[i - N], eap_logs[i], eap_total};
+            eap_total += eval_at_point_blocks(eap_logs[i], eap_iter);
+        }
+        eap_partials = ar.alloc<qm31>(eap_total);
+        if (!eap_partials) return STWO_ERR_OUT_OF_MEMORY;
+
+        // ---- the uploaded image: state (+ sampled values), tickets, quotient parameters, tables
+        off_state = up.add(nullptr, sizeof(ProofState) + sizeof(qm31) * eap_n);
+        up.at<ProofState>(off_state)->nonce = ~0ull;
+        off_tickets = up.add(nullptr, 4 * eap_n);
+        auto qpc = std::make_unique<QuotParamsDev>();
+        auto qpt = std::make_unique<QuotParamsDev>();
+        memset(qpc.get(), 0, sizeof(QuotParamsDev));
+        memset(qpt.get(), 0, sizeof(QuotParamsDev));
+        const cpoint *circle_tab = nullptr;
+        PV_TRY(circle_point_table(&circle_tab));
+        quot_init_static(*qpc, half_coset_init(D), half_coset_step(D), D, qc.data(), circle_tab);
+        quot_init_static(*qpt, half_coset_init(L + B), half_coset_step(L + B), L + B, qt.data(), circle_tab);
+        qpc->n_batches = qpt->n_batches = 1;
+        qpc->batch_end[0] = 4;
+        qpt->batch_end[0] = N;
+        for (int k = 0; k < 4; k++) {
+            qpc->cols[k] = cev[k];
+            qpc->col_idx[k] = (uint16_t)k;
+        }
+        for (uint32_t c = 0; c < N; c++) {
+            qpt->cols[c] = tev[c];
+            qpt->col_idx[c] = (uint16_t)c;
+        }
+        off_qc = up.add(qpc.get(), sizeof(QuotParamsDev));
+        off_qt = up.add(qpt.get(), sizeof(QuotParamsDev));
+        off_tpoly = up.add(tpoly.data(), sizeof(void *) * N);
+        off_text = up.add(text.data(), sizeof(void *) * N);
+        off_eap = up.add(eap.data(), sizeof(EapDevPoly) * eap_n);
+        // (src, dst) tables of the trace transforms: with more than 64 columns each pass is
+        // one launch over its table.
+        auto fft_table = [&](const std::vector<uint32_t *> &src, const std::vector<uint32_t *> &dst) {
+            std::vector<const void *> t(2 * N);
+            for (uint32_t c = 0; c < N; c++) {
+                t[2 * c] = src[c];
+                t[2 * c + 1] = dst[c];
+            }
+            return up.add(t.data(), sizeof(void *) * 2 * N);
+        };
+        off_fft_interp = fft_table(tpoly, tpoly);
+        off_fft_eval = fft_table(tpoly, tev);
+        off_fft_ext = B > 1 ? fft_table(tpoly, text) : 0;
+        t_lay.assign(n_layers, MerkleTree{});
+        {
+            std::vector<std::pair<uint32_t, const uint32_t *>> cols;
+            for (uint32_t c = 0; c < N; c++) cols.push_back({L + B, tev[c]});
+            PV_TRY(plan_tree(t_trace, cols, ar, up));
+            cols.clear();
+            for (int k = 0; k < 4; k++) cols.push_back({D, cev[k]});
+            PV_TRY(plan_tree(t_comp, cols, ar, up));
+            cols.clear();
+            for (int k = 0; k < 4; k++) cols.push_back({D, qc[k]});
+            for (int k = 0; k < 4; k++) cols.push_back({L + B, qt[k]});
+            PV_TRY(plan_tree(t_fri0, cols, ar, up));
+            for (uint32_t li = 0; li < n_layers; li++) {
+                cols.clear();
+                for (int k = 0; k < 4; k++) cols.push_back({D - 1 - li, lay[li][k]});
+                PV_TRY(plan_tree(t_lay[li], cols, ar, up));
+            }
+        }
+        // The FRI tail: inner layers of log size <= TAIL_MAX_LOG (from li0 on) and the last
+        // layer run in one launch. The trace quotient folds into layer 1 (log L + B - 1).
+        li0 = D - 1 > TAIL_MAX_LOG ? D - 1 - TAIL_MAX_LOG : 0;
+        li_circle = D - (L + B);
+        off_tail = 0;
+        {
+            auto tp = std::make_unique<TailParams>();
+            memset(tp.get(), 0, sizeof(TailParams));
+            tp->li0 = li0;
+            tp->n_tail = n_layers - li0;
+            tp->lg0 = D - 1 - li0;
+            tp->last_log = B;
+            tp->circle_t = li_circle >= li0 ? li_circle - li0 : ~0u;
+            for (int k = 0; k < 4; k++) tp->qt[k] = qt[k];
+            tp->circle_tw = itw + (tsz - (1ull << (L + B - 1)));
+            for (uint32_t t = 0; t <= tp->n_tail; t++)
+                for (int k = 0; k < 4; k++) tp->lay[t][k] = lay[li0 + t][k];
+            for (uint32_t t = 0; t < tp->n_tail; t++) {
+                const uint32_t lg = tp->lg0 - t;
+                for (uint32_t l = 0; l <= lg; l++) tp->nodes[t][l] = reinterpret_cast<uint4 *>(t_lay[li0 + t].layers[l]);
+                tp->line_tw[t] = itw + (tsz - (1ull << lg));
+            }
+            off_tail = up.add(tp.get(), sizeof(TailParams));
+        }
+        dev_img = ar.alloc<uint8_t>(up.host.size());
+        if (!dev_img) return STWO_ERR_OUT_OF_MEMORY;
+        auto fix_tables = [&](MerkleTree &t) {
+            for (auto &f : t.table_offsets)
+                t.level_tables[f.second] = reinterpret_cast<const uint32_t *const *>(dev_at(f.first));
+            t.tickets = reinterpret_cast<uint32_t *>(dev_at(t.ticket_offset));
+        };
+        fix_tables(t_trace);
+        fix_tables(t_comp);
+        fix_tables(t_fri0);
+        for (auto &t : t_lay) fix_tables(t);
+        dstate = reinterpret_cast<ProofState *>(dev_at(off_state));
+        dsampled = reinterpret_cast<qm31 *>(dev_at(off_state) + sizeof(ProofState));
+        dtickets = reinterpret_cast<uint32_t *>(dev_at(off_tickets));
+        dqc = reinterpret_cast<QuotParamsDev *>(dev_at(off_qc));
+        dqt = reinterpret_cast<QuotParamsDev *>(dev_at(off_qt));
+        return STWO_OK;
+    }
+};
+
+// K proofs of one shape (job j; inputs a0_in[k], a1_in[k]) in one launch sequence.
+// K = 1 is the single proof, which may use a ProveCache; K > 1 takes the caller's
+// twiddle tree and plans the jobs into K equal slabs. proofs[k] receive the proof
+// bytes; job_rc[k] (K > 1) each job's status, and the call's own status is that of
+// the launch sequence. With K = 1 the job's status is the call's.
+int prove_jobs(const Job &j, uint32_t K, const uint32_t *const *a0_in, const uint32_t *const *a1_in,
+               const uint32_t *tw_in, const uint32_t *itw_in, uint64_t tsz_in, std::vector<uint8_t> *proofs,
+               int *job_rc, cudaStream_t st, stwo_prove_stats *stats, ProveCache *cache) {
     PV_TRY(validate(j));
+    STWO_REQUIRE(K >= 1 && K <= MAX_JOBS_PER_LAUNCH, STWO_ERR_INVALID_ARGUMENT, "%u proofs in one launch sequence",
+                 K);
+    STWO_REQUIRE(K == 1 || (tw_in && itw_in && !cache), STWO_ERR_INVALID_ARGUMENT,
+                 "several proofs in one launch sequence take the caller's twiddle tree and no proof cache");
     const uint32_t L = j.L, N = j.N, B = j.B, E = L + 1, D = E + B;
     const uint64_t rows = 1ull << L;
     const double t0 = now_ms();
@@ -840,7 +1056,7 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     // log_n_rows >= 3 (a 4-point transform reads a twiddle back to the host).
     int dev = 0;
     STWO_CUDA_TRY(cudaGetDevice(&dev));
-    const bool cacheable = cache && tw_in && itw_in && L >= 3;
+    const bool cacheable = K == 1 && cache && tw_in && itw_in && L >= 3;
     const uint32_t key[5] = {j.L, j.N, j.B, j.n_queries, j.pow_bits};
     // Launch shapes (and the eval_at_point descriptors) follow the tunables, so a change
     // of any tunable retires the cache.
@@ -855,184 +1071,66 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     if (timing) PV_TRY(t_phase.ensure());
     cudaEvent_t *ev = t_phase.ev;
     Arena ar(st);
+    // One job's slab; K jobs take K equal slabs, and job k's memory is job 0's moved by k * S.
+    const uint64_t S = (job_device_bytes(j, !(tw_in || itw_in)) + 255) & ~uint64_t(255);
     if (hit) ar.adopt(cache->slab, cache->cap);
-    else PV_TRY(ar.reserve(job_device_bytes(j, !(tw_in || itw_in))));
+    else PV_TRY(ar.reserve(K == 1 ? job_device_bytes(j, !(tw_in || itw_in)) : S * K));
     if (timing) STWO_CUDA_TRY(cudaEventRecord(ev[0], st));
-
-    // ---- buffers (all of the job's device memory, before the first launch)
-    const uint32_t *tw = tw_in, *itw = itw_in;
-    uint64_t tsz = tsz_in;
-    uint32_t *own_tw = nullptr, *own_itw = nullptr;
-    if (tw_in || itw_in) {
-        STWO_REQUIRE(tw_in && itw_in && is_pow2(tsz_in) && tsz_in >= (1ull << (L + B)), STWO_ERR_INVALID_ARGUMENT,
-                     "twiddle tree of %llu entries does not cover domain log size %u", (unsigned long long)tsz_in, D);
+    std::vector<JobLayout> jl(K);
+    if (K == 1) {
+        PV_TRY(jl[0].plan(j, ar, tw_in, itw_in, tsz_in));
     } else {
-        tsz = 1ull << (L + B);
-        own_tw = ar.alloc<uint32_t>(tsz);
-        own_itw = ar.alloc<uint32_t>(tsz);
-        STWO_REQUIRE(own_tw && own_itw, STWO_ERR_OUT_OF_MEMORY, "twiddle allocation failed");
-        tw = own_tw;
-        itw = own_itw;
-    }
-    PV_ALLOC(a0, uint32_t, rows);
-    PV_ALLOC(a1, uint32_t, rows);
-    std::vector<uint32_t *> tpoly(N), tev(N), text(N);
-    for (uint32_t c = 0; c < N; c++) {
-        PV_ALLOC(p, uint32_t, rows);
-        PV_ALLOC(e, uint32_t, rows << B);
-        tpoly[c] = p;
-        tev[c] = e;
-        if (B == 1) {
-            text[c] = e;  // the committed evaluations are already on CanonicCoset(L + 1)
-        } else {
-            PV_ALLOC(x, uint32_t, 1ull << E);
-            text[c] = x;
+        uint64_t used0 = 0;
+        for (uint32_t k = 0; k < K; k++) {
+            Arena sub(st);
+            sub.adopt(ar.slab + (size_t)k * S, S);
+            PV_TRY(jl[k].plan(j, sub, tw_in, itw_in, tsz_in));
+            if (k == 0) used0 = sub.used;
+            STWO_REQUIRE(sub.extra.empty() && sub.used == used0, STWO_ERR_UNSUPPORTED_SIZE,
+                         "a job of the batch does not fit its slab");
+            ar.bytes += sub.bytes;
         }
+        ar.used = ar.cap;  // the jobs' slabs are taken: later allocations (the gather) go past them
     }
-    PV_ALLOC(powers, qm31, N);
-    std::vector<uint32_t *> comp(4), cev(4), qc(4), qt(4);
-    for (int k = 0; k < 4; k++) {
-        PV_ALLOC(c, uint32_t, 1ull << E);
-        PV_ALLOC(e, uint32_t, 1ull << D);
-        PV_ALLOC(a, uint32_t, 1ull << D);
-        PV_ALLOC(b, uint32_t, 1ull << (L + B));
-        comp[k] = c;
-        cev[k] = e;
-        qc[k] = a;
-        qt[k] = b;
-    }
-    // FRI layers: inner logs D-1 .. B+1, then the last layer (log B)
-    const uint32_t n_layers = D - 1 - B;
-    STWO_REQUIRE(n_layers <= MAX_LAYERS && L + B - 1 > B, STWO_ERR_UNSUPPORTED_SIZE, "FRI layer count unsupported");
-    std::vector<std::vector<uint32_t *>> lay(n_layers + 1, std::vector<uint32_t *>(4));
-    for (uint32_t li = 0; li <= n_layers; li++)
-        for (int k = 0; k < 4; k++) {
-            PV_ALLOC(c, uint32_t, 1ull << (D - 1 - li));
-            lay[li][k] = c;
-        }
-    const uint32_t eap_n = N + 4;
-    uint32_t eap_total = 0;
-    std::vector<EapDevPoly> eap(eap_n);
-    std::vector<uint32_t> eap_logs(eap_n);
-    for (uint32_t i = 0; i < eap_n; i++) eap_logs[i] = i < N ? L : E;
-    const uint32_t eap_iter = eval_at_point_iter_log(eap_logs.data(), eap_n);
-    for (uint32_t i = 0; i < eap_n; i++) {
-        eap[i] = {i < N ? tpoly[i] : comp[i - N], eap_logs[i], eap_total};
-        eap_total += eval_at_point_blocks(eap_logs[i], eap_iter);
-    }
-    PV_ALLOC(eap_partials, qm31, eap_total);
+    JobLayout &J = jl[0];
+    const uint32_t *tw = J.tw, *itw = J.itw;
+    const uint64_t tsz = J.tsz;
+    uint32_t *own_tw = J.own_tw, *own_itw = J.own_itw;
+    uint32_t *a0 = J.a0, *a1 = J.a1;
+    std::vector<uint32_t *> &tpoly = J.tpoly, &tev = J.tev, &text = J.text, &comp = J.comp, &cev = J.cev,
+                            &qc = J.qc, &qt = J.qt;
+    std::vector<std::vector<uint32_t *>> &lay = J.lay;
+    qm31 *powers = J.powers;
+    const uint32_t n_layers = J.n_layers, eap_n = J.eap_n, eap_total = J.eap_total, eap_iter = J.eap_iter;
+    qm31 *eap_partials = J.eap_partials;
+    MerkleTree &t_trace = J.t_trace, &t_comp = J.t_comp, &t_fri0 = J.t_fri0;
+    std::vector<MerkleTree> &t_lay = J.t_lay;
+    const uint32_t li0 = J.li0, li_circle = J.li_circle;
+    ProofState *dstate = J.dstate;
+    qm31 *dsampled = J.dsampled;
+    uint32_t *dtickets = J.dtickets;
+    QuotParamsDev *dqc = J.dqc, *dqt = J.dqt;
+    const size_t off_tpoly = J.off_tpoly, off_text = J.off_text, off_eap = J.off_eap, off_tail = J.off_tail;
+    const size_t off_fft_interp = J.off_fft_interp, off_fft_eval = J.off_fft_eval, off_fft_ext = J.off_fft_ext;
+    auto dev_at = [&](size_t off) { return J.dev_at(off); };
+    (void)rows;
 
-    // ---- the uploaded image: state (+ sampled values), tickets, quotient parameters, tables
-    Upload up;
-    const size_t off_state = up.add(nullptr, sizeof(ProofState) + sizeof(qm31) * eap_n);
-    up.at<ProofState>(off_state)->nonce = ~0ull;
-    const size_t off_tickets = up.add(nullptr, 4 * eap_n);
-    auto qpc = std::make_unique<QuotParamsDev>();
-    auto qpt = std::make_unique<QuotParamsDev>();
-    memset(qpc.get(), 0, sizeof(QuotParamsDev));
-    memset(qpt.get(), 0, sizeof(QuotParamsDev));
-    const cpoint *circle_tab = nullptr;
-    PV_TRY(circle_point_table(&circle_tab));
-    quot_init_static(*qpc, half_coset_init(D), half_coset_step(D), D, qc.data(), circle_tab);
-    quot_init_static(*qpt, half_coset_init(L + B), half_coset_step(L + B), L + B, qt.data(), circle_tab);
-    qpc->n_batches = qpt->n_batches = 1;
-    qpc->batch_end[0] = 4;
-    qpt->batch_end[0] = N;
-    for (int k = 0; k < 4; k++) {
-        qpc->cols[k] = cev[k];
-        qpc->col_idx[k] = (uint16_t)k;
-    }
-    for (uint32_t c = 0; c < N; c++) {
-        qpt->cols[c] = tev[c];
-        qpt->col_idx[c] = (uint16_t)c;
-    }
-    const size_t off_qc = up.add(qpc.get(), sizeof(QuotParamsDev));
-    const size_t off_qt = up.add(qpt.get(), sizeof(QuotParamsDev));
-    const size_t off_tpoly = up.add(tpoly.data(), sizeof(void *) * N);
-    const size_t off_text = up.add(text.data(), sizeof(void *) * N);
-    const size_t off_eap = up.add(eap.data(), sizeof(EapDevPoly) * eap_n);
-    // (src, dst) tables of the trace transforms: with more than 64 columns each pass is
-    // one launch over its table.
-    auto fft_table = [&](const std::vector<uint32_t *> &src, const std::vector<uint32_t *> &dst) {
-        std::vector<const void *> t(2 * N);
-        for (uint32_t c = 0; c < N; c++) {
-            t[2 * c] = src[c];
-            t[2 * c + 1] = dst[c];
-        }
-        return up.add(t.data(), sizeof(void *) * 2 * N);
-    };
-    const size_t off_fft_interp = fft_table(tpoly, tpoly);
-    const size_t off_fft_eval = fft_table(tpoly, tev);
-    const size_t off_fft_ext = B > 1 ? fft_table(tpoly, text) : 0;
-    MerkleTree t_trace, t_comp, t_fri0;
-    std::vector<MerkleTree> t_lay(n_layers);
     {
-        std::vector<std::pair<uint32_t, const uint32_t *>> cols;
-        for (uint32_t c = 0; c < N; c++) cols.push_back({L + B, tev[c]});
-        PV_TRY(plan_tree(t_trace, cols, ar, up));
-        cols.clear();
-        for (int k = 0; k < 4; k++) cols.push_back({D, cev[k]});
-        PV_TRY(plan_tree(t_comp, cols, ar, up));
-        cols.clear();
-        for (int k = 0; k < 4; k++) cols.push_back({D, qc[k]});
-        for (int k = 0; k < 4; k++) cols.push_back({L + B, qt[k]});
-        PV_TRY(plan_tree(t_fri0, cols, ar, up));
-        for (uint32_t li = 0; li < n_layers; li++) {
-            cols.clear();
-            for (int k = 0; k < 4; k++) cols.push_back({D - 1 - li, lay[li][k]});
-            PV_TRY(plan_tree(t_lay[li], cols, ar, up));
-        }
-    }
-    // The FRI tail: inner layers of log size <= TAIL_MAX_LOG (from li0 on) and the last
-    // layer run in one launch. The trace quotient folds into layer 1 (log L + B - 1).
-    const uint32_t li0 = D - 1 > TAIL_MAX_LOG ? D - 1 - TAIL_MAX_LOG : 0;
-    const uint32_t li_circle = D - (L + B);
-    size_t off_tail = 0;
-    {
-        auto tp = std::make_unique<TailParams>();
-        memset(tp.get(), 0, sizeof(TailParams));
-        tp->li0 = li0;
-        tp->n_tail = n_layers - li0;
-        tp->lg0 = D - 1 - li0;
-        tp->last_log = B;
-        tp->circle_t = li_circle >= li0 ? li_circle - li0 : ~0u;
-        for (int k = 0; k < 4; k++) tp->qt[k] = qt[k];
-        tp->circle_tw = itw + (tsz - (1ull << (L + B - 1)));
-        for (uint32_t t = 0; t <= tp->n_tail; t++)
-            for (int k = 0; k < 4; k++) tp->lay[t][k] = lay[li0 + t][k];
-        for (uint32_t t = 0; t < tp->n_tail; t++) {
-            const uint32_t lg = tp->lg0 - t;
-            for (uint32_t l = 0; l <= lg; l++) tp->nodes[t][l] = reinterpret_cast<uint4 *>(t_lay[li0 + t].layers[l]);
-            tp->line_tw[t] = itw + (tsz - (1ull << lg));
-        }
-        off_tail = up.add(tp.get(), sizeof(TailParams));
-    }
-    PV_ALLOC(dev_img, uint8_t, up.host.size());
-    auto dev_at = [&](size_t off) { return dev_img + off; };
-    auto fix_tables = [&](MerkleTree &t) {
-        for (auto &f : t.table_offsets)
-            t.level_tables[f.second] = reinterpret_cast<const uint32_t *const *>(dev_at(f.first));
-        t.tickets = reinterpret_cast<uint32_t *>(dev_at(t.ticket_offset));
-    };
-    fix_tables(t_trace);
-    fix_tables(t_comp);
-    fix_tables(t_fri0);
-    for (auto &t : t_lay) fix_tables(t);
-    ProofState *dstate = reinterpret_cast<ProofState *>(dev_at(off_state));
-    qm31 *dsampled = reinterpret_cast<qm31 *>(dev_at(off_state) + sizeof(ProofState));
-    uint32_t *dtickets = reinterpret_cast<uint32_t *>(dev_at(off_tickets));
-    QuotParamsDev *dqc = reinterpret_cast<QuotParamsDev *>(dev_at(off_qc));
-    QuotParamsDev *dqt = reinterpret_cast<QuotParamsDev *>(dev_at(off_qt));
-    {
-        // staged through pinned memory; the stage's next use comes after a wait on st
+        // the jobs' images, staged through pinned memory (the stage's next use comes after
+        // a wait on st) and uploaded in one copy
+        const size_t img = J.up.host.size();
+        for (uint32_t k = 1; k < K; k++)
+            STWO_REQUIRE(jl[k].up.host.size() == img, STWO_ERR_UNSUPPORTED_SIZE, "the batch's images differ");
         void *stage = nullptr;
-        PV_TRY(host_stage(up.host.size(), &stage));
-        memcpy(stage, up.host.data(), up.host.size());
-        STWO_CUDA_TRY(cudaMemcpyAsync(dev_img, stage, up.host.size(), cudaMemcpyHostToDevice, st));
+        PV_TRY(host_stage(img * K, &stage));
+        for (uint32_t k = 0; k < K; k++) memcpy(static_cast<uint8_t *>(stage) + img * k, jl[k].up.host.data(), img);
+        if (K == 1) STWO_CUDA_TRY(cudaMemcpyAsync(J.dev_img, stage, img, cudaMemcpyHostToDevice, st));
+        else STWO_CUDA_TRY(cudaMemcpy2DAsync(J.dev_img, S, stage, img, img, K, cudaMemcpyHostToDevice, st));
     }
-
-    STWO_CUDA_TRY(cudaMemcpyAsync(a0, a0_in, rows * 4, cudaMemcpyDefault, st));
-    STWO_CUDA_TRY(cudaMemcpyAsync(a1, a1_in, rows * 4, cudaMemcpyDefault, st));
+    for (uint32_t k = 0; k < K; k++) {
+        STWO_CUDA_TRY(cudaMemcpyAsync(jl[k].a0, a0_in[k], rows * 4, cudaMemcpyDefault, st));
+        STWO_CUDA_TRY(cudaMemcpyAsync(jl[k].a1, a1_in[k], rows * 4, cudaMemcpyDefault, st));
+    }
 
     // The launch sequence from the trace to the query words: device work only, no host
     // wait, every address inside the slab or the caller's twiddle tree.
@@ -1042,8 +1140,22 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
                                 : cudaEventRecord(ev[k], st));
         return STWO_OK;
     };
-    const uint32_t K = 1;  // jobs of this launch sequence
-    const size_t js = 0;   // their memory stride
+    const size_t js = K > 1 ? S : 0;  // the jobs' memory stride
+    // A transform over every job's columns: with one job the prover's own tables (in its
+    // image, so the sequence stays capturable); with several, all jobs' columns in one
+    // launch a pass (the call stages their table).
+    auto fft_all = [&](const std::vector<uint32_t *> &src, const std::vector<uint32_t *> &dst, uint32_t n_log,
+                       uint32_t coeff_log, const uint32_t *tree, bool inv, const void *table) -> int {
+        std::vector<const uint32_t *> s;
+        std::vector<uint32_t *> d;
+        for (uint32_t k = 0; k < K; k++)
+            for (size_t i = 0; i < src.size(); i++) {
+                s.push_back(job_ptr<const uint32_t>(src[i], js, k));
+                d.push_back(job_ptr(dst[i], js, k));
+            }
+        return fft_columns_tab(s.data(), d.data(), (uint32_t)s.size(), n_log, coeff_log, tree, tsz, inv, st,
+                               K == 1 ? table : nullptr);
+    };
     auto launch_all = [&](bool capturing) -> int {
         // ---- 1. trace: twiddles, generation, interpolation, evaluation, tree
         if (own_tw)
@@ -1057,11 +1169,8 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
             STWO_LAUNCH_CHECK("wide_fib_trace_kernel");
         }
         // The trace columns are interpolated in place: they become the coefficient columns.
-        PV_TRY(fft_columns_tab(tpoly.data(), tpoly.data(), N, L, L, itw, tsz, true, st, dev_at(off_fft_interp)));
-        {
-            std::vector<const uint32_t *> src(tpoly.begin(), tpoly.end());
-            PV_TRY(fft_columns_tab(src.data(), tev.data(), N, L + B, L, tw, tsz, false, st, dev_at(off_fft_eval)));
-        }
+        PV_TRY(fft_all(tpoly, tpoly, L, L, itw, true, dev_at(off_fft_interp)));
+        PV_TRY(fft_all(tpoly, tev, L + B, L, tw, false, dev_at(off_fft_eval)));
         auto commit = [&](MerkleTree &t) {
             return merkle_tree_dev_async(t.max_log, t.level_tables.data(), t.level_n.data(), t.layers.data(), t.tickets,
                                          t.n_tickets, K, js, st);
@@ -1072,19 +1181,13 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         PV_TRY(record(1, capturing));
 
         // ---- 2. composition on CanonicCoset(L + 1), committed on CanonicCoset(L + 1 + B)
-        if (B > 1) {
-            std::vector<const uint32_t *> src(tpoly.begin(), tpoly.end());
-            PV_TRY(fft_columns_tab(src.data(), text.data(), N, E, L, tw, tsz, false, st, dev_at(off_fft_ext)));
-        }
+        if (B > 1) PV_TRY(fft_all(tpoly, text, E, L, tw, false, dev_at(off_fft_ext)));
         uint32_t den_half[2];
         vanishing_inverses(L, den_half);
         PV_TRY(wide_fib_dev_async(reinterpret_cast<const uint32_t *const *>(dev_at(off_text)), N, E,
                                   reinterpret_cast<const uint32_t *>(powers), den_half, comp.data(), K, js, st));
-        PV_TRY(fft_columns(comp.data(), comp.data(), 4, E, E, itw, tsz, true, st));  // in place -> coefficients
-        {
-            std::vector<const uint32_t *> src(comp.begin(), comp.end());
-            PV_TRY(fft_columns(src.data(), cev.data(), 4, D, E, tw, tsz, false, st));
-        }
+        PV_TRY(fft_all(comp, comp, E, E, itw, true, nullptr));  // in place -> coefficients
+        PV_TRY(fft_all(comp, cev, D, E, tw, false, nullptr));
         PV_TRY(commit(t_comp));
         fs_comp_kernel<<<K, 1, 0, st>>>(dstate, t_comp.layers[0], js);
         STWO_LAUNCH_CHECK("fs_comp_kernel");
@@ -1103,7 +1206,10 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         PV_TRY(commit(t_fri0));
         fs_layer_kernel<<<K, 1, 0, st>>>(dstate, t_fri0.layers[0], 2, 0, js);
         STWO_LAUNCH_CHECK("fs_layer_kernel");
-        for (int k = 0; k < 4; k++) STWO_CUDA_TRY(cudaMemsetAsync(lay[0][k], 0, 4ull << (D - 1), st));
+        for (int k = 0; k < 4; k++) {
+            if (K == 1) STWO_CUDA_TRY(cudaMemsetAsync(lay[0][k], 0, 4ull << (D - 1), st));
+            else STWO_CUDA_TRY(cudaMemset2DAsync(lay[0][k], js, 0, 4ull << (D - 1), K, st));
+        }
         {
             std::vector<const uint32_t *> s(qc.begin(), qc.end());
             PV_TRY(fold_async(s.data(), 1ull << D, stwo_qm31{}, itw, tsz - (1ull << (D - 1)), lay[0].data(), true, st,
@@ -1174,110 +1280,147 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
     } else {
         PV_TRY(launch_all(false));
     }
+    // ---- the jobs' records (channel state and sampled values), in one copy
     const size_t rec_bytes = sizeof(ProofState) + sizeof(qm31) * eap_n;
-    std::vector<uint8_t> rec(rec_bytes);
+    std::vector<uint8_t> rec(rec_bytes * K);
     {
         void *rec_stage = nullptr;
-        PV_TRY(host_stage(rec_bytes, &rec_stage));
-        STWO_CUDA_TRY(cudaMemcpyAsync(rec_stage, dstate, rec_bytes, cudaMemcpyDeviceToHost, st));
+        PV_TRY(host_stage(rec_bytes * K, &rec_stage));
+        if (K == 1) STWO_CUDA_TRY(cudaMemcpyAsync(rec_stage, dstate, rec_bytes, cudaMemcpyDeviceToHost, st));
+        else
+            STWO_CUDA_TRY(
+                cudaMemcpy2DAsync(rec_stage, rec_bytes, dstate, js, rec_bytes, K, cudaMemcpyDeviceToHost, st));
         PV_TRY(wait_stream(st));
-        memcpy(rec.data(), rec_stage, rec_bytes);
+        memcpy(rec.data(), rec_stage, rec_bytes * K);
     }
-    const ProofState &ps = *reinterpret_cast<const ProofState *>(rec.data());
-    const qm31 *sampled = reinterpret_cast<const qm31 *>(rec.data() + sizeof(ProofState));
-    STWO_REQUIRE(!(ps.error & fs::ERR_DRAW), STWO_ERR_CUDA, "channel draw exceeded its retry bound");
-    STWO_REQUIRE(!(ps.error & fs::ERR_CONSTRAINTS), STWO_ERR_INVALID_ARGUMENT,
-                 "constraints not satisfied at the out-of-domain point");
-    STWO_REQUIRE(!(ps.error & fs::ERR_LAST_LAYER), STWO_ERR_INVALID_ARGUMENT, "FRI last layer exceeds its degree bound");
-    STWO_REQUIRE(!(ps.error & fs::ERR_GRIND), STWO_ERR_INVALID_ARGUMENT, "no proof-of-work nonce within 2^%u tries",
-                 j.pow_bits + 6);
+    // A job's status from the error bits its channel recorded.
+    auto job_status = [&](const ProofState &ps) -> int {
+        STWO_REQUIRE(!(ps.error & fs::ERR_DRAW), STWO_ERR_CUDA, "channel draw exceeded its retry bound");
+        STWO_REQUIRE(!(ps.error & fs::ERR_CONSTRAINTS), STWO_ERR_INVALID_ARGUMENT,
+                     "constraints not satisfied at the out-of-domain point");
+        STWO_REQUIRE(!(ps.error & fs::ERR_LAST_LAYER), STWO_ERR_INVALID_ARGUMENT,
+                     "FRI last layer exceeds its degree bound");
+        STWO_REQUIRE(!(ps.error & fs::ERR_GRIND), STWO_ERR_INVALID_ARGUMENT,
+                     "no proof-of-work nonce within 2^%u tries", j.pow_bits + 6);
+        return STWO_OK;
+    };
 
-    // Queries::generate over the largest quotient domain (log D).
-    std::vector<uint64_t> queries;
-    {
-        std::set<uint64_t> qs;
-        const uint32_t mask = (uint32_t)((1ull << D) - 1);
-        for (uint32_t i = 0; i < j.n_queries; i++) qs.insert(ps.query_words[i] & mask);
-        queries.assign(qs.begin(), qs.end());
-    }
-    const std::map<uint32_t, std::vector<uint64_t>> tree_queries = {{D, queries}, {L + B, fold_queries(queries, 1)}};
-
+    // Per job: its queries and decommitments, planned as device reads that one gather
+    // serves for all jobs.
+    struct JobDecommit {
+        int rc = STWO_OK;
+        TreeDecommit d_trace, d_comp, d_fri0;
+        std::vector<size_t> w_first;
+        std::vector<std::vector<size_t>> w_inner;
+        std::vector<TreeDecommit> d_inner;
+    };
+    std::vector<JobDecommit> jd(K);
     Gatherer g;
-    TreeDecommit d_trace = plan_decommit(t_trace, tree_queries, g);
-    TreeDecommit d_comp = plan_decommit(t_comp, tree_queries, g);
-    // FRI first layer: per quotient column, its folding pairs; partners are witnesses.
-    std::vector<size_t> w_first;
-    TreeDecommit d_fri0;
-    {
-        std::map<uint32_t, std::vector<uint64_t>> pos;
-        for (int grp = 0; grp < 2; grp++) {
-            const uint32_t lg = grp == 0 ? D : L + B;
-            const std::vector<uint32_t *> &col = grp == 0 ? qc : qt;
-            std::vector<uint64_t> p, wv;
-            fri_positions(fold_queries(queries, D - lg), p, wv);
-            pos[lg] = p;
-            for (uint64_t x : wv)
-                for (int k = 0; k < 4; k++) w_first.push_back(g.add(col[k], x));
+    for (uint32_t k = 0; k < K; k++) {
+        JobLayout &Jk = jl[k];
+        JobDecommit &o = jd[k];
+        const ProofState &ps = *reinterpret_cast<const ProofState *>(rec.data() + rec_bytes * k);
+        o.rc = job_status(ps);
+        if (o.rc) {
+            if (K == 1) return o.rc;
+            continue;
         }
-        d_fri0 = plan_decommit(t_fri0, pos, g);
-    }
-    std::vector<std::vector<size_t>> w_inner(n_layers);
-    std::vector<TreeDecommit> d_inner(n_layers);
-    {
-        std::vector<uint64_t> lq = fold_queries(queries, 1);
-        for (uint32_t li = 0; li < n_layers; li++) {
-            std::vector<uint64_t> p, wv;
-            fri_positions(lq, p, wv);
-            for (uint64_t x : wv)
-                for (int k = 0; k < 4; k++) w_inner[li].push_back(g.add(lay[li][k], x));
-            d_inner[li] = plan_decommit(t_lay[li], {{D - 1 - li, p}}, g);
-            lq = fold_queries(lq, 1);
+        // Queries::generate over the largest quotient domain (log D).
+        std::vector<uint64_t> queries;
+        {
+            std::set<uint64_t> qs;
+            const uint32_t mask = (uint32_t)((1ull << D) - 1);
+            for (uint32_t i = 0; i < j.n_queries; i++) qs.insert(ps.query_words[i] & mask);
+            queries.assign(qs.begin(), qs.end());
+        }
+        const std::map<uint32_t, std::vector<uint64_t>> tree_queries = {{D, queries},
+                                                                        {L + B, fold_queries(queries, 1)}};
+        o.d_trace = plan_decommit(Jk.t_trace, tree_queries, g);
+        o.d_comp = plan_decommit(Jk.t_comp, tree_queries, g);
+        // FRI first layer: per quotient column, its folding pairs; partners are witnesses.
+        {
+            std::map<uint32_t, std::vector<uint64_t>> pos;
+            for (int grp = 0; grp < 2; grp++) {
+                const uint32_t lg = grp == 0 ? D : L + B;
+                const std::vector<uint32_t *> &col = grp == 0 ? Jk.qc : Jk.qt;
+                std::vector<uint64_t> p, wv;
+                fri_positions(fold_queries(queries, D - lg), p, wv);
+                pos[lg] = p;
+                for (uint64_t x : wv)
+                    for (int c = 0; c < 4; c++) o.w_first.push_back(g.add(col[c], x));
+            }
+            o.d_fri0 = plan_decommit(Jk.t_fri0, pos, g);
+        }
+        o.w_inner.assign(n_layers, {});
+        o.d_inner.assign(n_layers, {});
+        {
+            std::vector<uint64_t> lq = fold_queries(queries, 1);
+            for (uint32_t li = 0; li < n_layers; li++) {
+                std::vector<uint64_t> p, wv;
+                fri_positions(lq, p, wv);
+                for (uint64_t x : wv)
+                    for (int c = 0; c < 4; c++) o.w_inner[li].push_back(g.add(Jk.lay[li][c], x));
+                o.d_inner[li] = plan_decommit(Jk.t_lay[li], {{D - 1 - li, p}}, g);
+                lq = fold_queries(lq, 1);
+            }
         }
     }
     PV_TRY(g.run(ar, st));
     const std::vector<uint32_t> &vals = g.vals;
 
     // ---- serialisation
-    Writer w;
-    w.u64(2);  // commitments
-    w.bytes(ps.roots[0], 32);
-    w.bytes(ps.roots[1], 32);
-    w.u64(2);  // sampled_values
-    w.u64(N);
-    for (uint32_t c = 0; c < N; c++) {
-        w.u64(1);
-        w.q(sampled[c]);
-    }
-    w.u64(4);
-    for (int k = 0; k < 4; k++) {
-        w.u64(1);
-        w.q(sampled[N + k]);
-    }
-    w.u64(2);  // decommitments
-    write_decommitment(w, d_trace, vals);
-    write_decommitment(w, d_comp, vals);
-    w.u64(2);  // queried_values
-    for (const TreeDecommit *d : {&d_trace, &d_comp}) {
-        w.u64(d->queried.size());
-        for (auto &col : d->queried) {
-            w.u64(col.size());
-            for (size_t gi : col) w.u32(vals[gi]);
+    uint64_t proof_bytes = 0;
+    for (uint32_t k = 0; k < K; k++) {
+        const JobDecommit &o = jd[k];
+        if (job_rc) job_rc[k] = o.rc;
+        if (o.rc) {
+            proofs[k].clear();
+            continue;
         }
+        const ProofState &ps = *reinterpret_cast<const ProofState *>(rec.data() + rec_bytes * k);
+        const qm31 *sampled = reinterpret_cast<const qm31 *>(rec.data() + rec_bytes * k + sizeof(ProofState));
+        Writer w;
+        w.u64(2);  // commitments
+        w.bytes(ps.roots[0], 32);
+        w.bytes(ps.roots[1], 32);
+        w.u64(2);  // sampled_values
+        w.u64(N);
+        for (uint32_t c = 0; c < N; c++) {
+            w.u64(1);
+            w.q(sampled[c]);
+        }
+        w.u64(4);
+        for (int c = 0; c < 4; c++) {
+            w.u64(1);
+            w.q(sampled[N + c]);
+        }
+        w.u64(2);  // decommitments
+        write_decommitment(w, o.d_trace, vals);
+        write_decommitment(w, o.d_comp, vals);
+        w.u64(2);  // queried_values
+        for (const TreeDecommit *d : {&o.d_trace, &o.d_comp}) {
+            w.u64(d->queried.size());
+            for (auto &col : d->queried) {
+                w.u64(col.size());
+                for (size_t gi : col) w.u32(vals[gi]);
+            }
+        }
+        w.u64(ps.nonce);  // proof_of_work
+        auto write_fri_layer = [&](const std::vector<size_t> &wit, const TreeDecommit &d, const uint32_t root[8]) {
+            w.u64(wit.size() / 4);
+            for (size_t gi : wit) w.u32(vals[gi]);
+            write_decommitment(w, d, vals);
+            w.bytes(root, 32);
+        };
+        write_fri_layer(o.w_first, o.d_fri0, ps.roots[2]);
+        w.u64(n_layers);
+        for (uint32_t li = 0; li < n_layers; li++) write_fri_layer(o.w_inner[li], o.d_inner[li], ps.roots[3 + li]);
+        w.u64(1);  // last_layer_poly.coeffs
+        w.q(ps.last_coeff);
+        w.u32(0);  // last_layer_poly.log_size
+        proofs[k] = std::move(w.b);
+        proof_bytes += proofs[k].size();
     }
-    w.u64(ps.nonce);  // proof_of_work
-    auto write_fri_layer = [&](const std::vector<size_t> &wit, const TreeDecommit &d, const uint32_t root[8]) {
-        w.u64(wit.size() / 4);
-        for (size_t gi : wit) w.u32(vals[gi]);
-        write_decommitment(w, d, vals);
-        w.bytes(root, 32);
-    };
-    write_fri_layer(w_first, d_fri0, ps.roots[2]);
-    w.u64(n_layers);
-    for (uint32_t li = 0; li < n_layers; li++) write_fri_layer(w_inner[li], d_inner[li], ps.roots[3 + li]);
-    w.u64(1);  // last_layer_poly.coeffs
-    w.q(ps.last_coeff);
-    w.u32(0);  // last_layer_poly.log_size
-    proof = std::move(w.b);
     const double t5 = now_ms();
 
     if (cacheable) {
@@ -1307,12 +1450,13 @@ int prove_impl(const Job &j, const uint32_t *a0_in, const uint32_t *a1_in, const
         stats->decommit_ms = std::max(0.0, stats->total_ms - (ms[0] + ms[1] + ms[2] + ms[3]));
         stats->device_bytes = ar.bytes;
         stats->kernel_launches = t_kernel_launches - launches0;
-        stats->proof_bytes = proof.size();
+        stats->proof_bytes = proof_bytes;
     }
     return STWO_OK;
 }
 
 }  // namespace
+
 
 // Shared with the batch server.
 int wide_fib_prove(const stwo_wide_fib_job *job, const uint32_t *a0, const uint32_t *a1, const uint32_t *tw,
@@ -1320,8 +1464,26 @@ int wide_fib_prove(const stwo_wide_fib_job *job, const uint32_t *a0, const uint3
                    cudaStream_t st, ProveCache *cache) {
     STWO_REQUIRE(job && a0 && a1, STWO_ERR_INVALID_ARGUMENT, "null argument");
     Job j{job->log_n_rows, job->n_columns, job->log_blowup, job->n_queries, job->pow_bits};
-    int rc = prove_impl(j, a0, a1, tw, itw, tree_size, proof, st, stats, cache);
+    int rc = prove_jobs(j, 1, &a0, &a1, tw, itw, tree_size, &proof, nullptr, st, stats, cache);
     if (rc) cudaStreamSynchronize(st);  // the arena's frees are queued; leave the stream idle
+    return rc;
+}
+
+// Several proofs of one shape in one launch sequence (the caller's twiddle tree);
+// proofs[k] and job_rc[k] receive job k's bytes and status.
+int wide_fib_prove_batch(const stwo_wide_fib_job *job, uint32_t n_jobs, const uint32_t *const *a0,
+                         const uint32_t *const *a1, const uint32_t *tw, const uint32_t *itw, uint64_t tree_size,
+                         std::vector<std::vector<uint8_t>> &proofs, int *job_rc, stwo_prove_stats *stats,
+                         cudaStream_t st) {
+    STWO_REQUIRE(job && a0 && a1 && job_rc && n_jobs >= 1, STWO_ERR_INVALID_ARGUMENT, "null argument");
+    for (uint32_t k = 0; k < n_jobs; k++) STWO_REQUIRE(a0[k] && a1[k], STWO_ERR_INVALID_ARGUMENT, "null input");
+    Job j{job->log_n_rows, job->n_columns, job->log_blowup, job->n_queries, job->pow_bits};
+    proofs.assign(n_jobs, {});
+    int rc = prove_jobs(j, n_jobs, a0, a1, tw, itw, tree_size, proofs.data(), job_rc, st, stats, nullptr);
+    if (rc) {
+        cudaStreamSynchronize(st);
+        for (uint32_t k = 0; k < n_jobs; k++) job_rc[k] = rc;
+    }
     return rc;
 }
 
@@ -1359,6 +1521,36 @@ int stwo_wide_fib_prove(const stwo_wide_fib_job *job, const uint32_t *a0, const 
 }
 
 void stwo_free_proof(uint8_t *proof) { free(proof); }
+
+int stwo_wide_fib_prove_batch(const stwo_wide_fib_job *job, uint32_t n_jobs, const uint32_t *const *a0,
+                              const uint32_t *const *a1, const uint32_t *twiddles, const uint32_t *itwiddles,
+                              uint64_t tree_size, uint8_t **proofs, uint64_t *proof_lens, int *job_status,
+                              stwo_prove_stats *stats, void *stream) {
+    STWO_REQUIRE(proofs && proof_lens && job_status && n_jobs >= 1 && n_jobs <= 256, STWO_ERR_INVALID_ARGUMENT,
+                 "batch outputs");
+    for (uint32_t k = 0; k < n_jobs; k++) {
+        proofs[k] = nullptr;
+        proof_lens[k] = 0;
+    }
+    std::vector<std::vector<uint8_t>> out;
+    int rc = wide_fib_prove_batch(job, n_jobs, a0, a1, twiddles, itwiddles, tree_size, out, job_status, stats,
+                                  as_stream(stream));
+    if (rc) return rc;
+    for (uint32_t k = 0; k < n_jobs; k++) {
+        if (job_status[k] != STWO_OK) continue;
+        proofs[k] = static_cast<uint8_t *>(malloc(out[k].size()));
+        if (!proofs[k]) {
+            for (uint32_t i = 0; i < k; i++) {
+                free(proofs[i]);
+                proofs[i] = nullptr;
+            }
+            return set_error(STWO_ERR_OUT_OF_MEMORY, "proof buffer allocation failed");
+        }
+        memcpy(proofs[k], out[k].data(), out[k].size());
+        proof_lens[k] = out[k].size();
+    }
+    return STWO_OK;
+}
 
 struct stwo_prove_cache {
     ProveCache c;

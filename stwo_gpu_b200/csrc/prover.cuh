@@ -36,5 +36,11 @@ int wide_fib_prove(const stwo_wide_fib_job *job, const uint32_t *a0, const uint3
                    const uint32_t *itw, uint64_t tree_size, std::vector<uint8_t> &proof, stwo_prove_stats *stats,
                    cudaStream_t st, ProveCache *cache = nullptr);
 uint64_t wide_fib_job_device_bytes(const stwo_wide_fib_job *job, bool own_twiddles);
+// n_jobs proofs of one shape in one launch sequence (the caller's twiddle tree):
+// proofs[k], job_rc[k] receive job k's bytes and status.
+int wide_fib_prove_batch(const stwo_wide_fib_job *job, uint32_t n_jobs, const uint32_t *const *a0,
+                         const uint32_t *const *a1, const uint32_t *tw, const uint32_t *itw, uint64_t tree_size,
+                         std::vector<std::vector<uint8_t>> &proofs, int *job_rc, stwo_prove_stats *stats,
+                         cudaStream_t st);
 
 }  // namespace stwo

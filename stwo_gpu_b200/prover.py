@@ -121,6 +121,44 @@ def prove_wide_fib(job, a0, a1, twiddles=None, stream=None, cache=None):
     return proof, st.as_dict()
 
 
+def prove_wide_fib_batch(job, inputs, twiddles, stream=None):
+    """Proves len(inputs) jobs of one shape in one launch sequence (every kernel of the
+    proof launched once for all of them); inputs: a list of (a0, a1) host uint32
+    arrays. Returns (list of proof bytes, or None for a job that failed, list of
+    statuses, stats dict of the whole sequence). The proofs are byte for byte those of
+    prove_wide_fib. twiddles: a TwiddleTree covering CanonicCoset(log_n_rows + 1 +
+    log_blowup)."""
+    n = 1 << job.log_n_rows
+    arrays = []
+    for a0, a1 in inputs:
+        a0 = np.ascontiguousarray(a0, dtype=np.uint32)
+        a1 = np.ascontiguousarray(a1, dtype=np.uint32)
+        if a0.size != n or a1.size != n:
+            raise ValueError(f"a0 and a1 need {n} values")
+        arrays.append((a0, a1))
+    k = len(arrays)
+    a0p = (C.c_void_p * k)(*[a[0].ctypes.data for a in arrays])
+    a1p = (C.c_void_p * k)(*[a[1].ctypes.data for a in arrays])
+    outs = (C.POINTER(C.c_uint8) * k)()
+    lens = (C.c_uint64 * k)()
+    status = (C.c_int * k)()
+    st = L.ProveStats()
+    L.clear_error()
+    L.check(L.lib().stwo_wide_fib_prove_batch(C.byref(job.c()), k, a0p, a1p, twiddles.twiddles.device_ptr,
+                                              twiddles.itwiddles.device_ptr, len(twiddles.twiddles), outs, lens,
+                                              status, C.byref(st), stream))
+    proofs = []
+    for i in range(k):
+        if outs[i]:
+            try:
+                proofs.append(C.string_at(outs[i], lens[i]))
+            finally:
+                L.lib().stwo_free_proof(outs[i])
+        else:
+            proofs.append(None)
+    return proofs, list(status), st.as_dict()
+
+
 def kernel_launches():
     """Kernel launches the library has made in this process."""
     return int(L.lib().stwo_kernel_launches())

@@ -509,3 +509,29 @@ def test_server_submit_checks_before_copying_inputs():
         rc = L.lib().stwo_server_submit(srv._s, 1, stwo.WideFibJob(28, 16).c(), tiny.ctypes.data, tiny.ctypes.data)
         assert rc == L.ERR_UNSUPPORTED_SIZE and "exceeds" in L.last_error()
         L.clear_error()
+
+
+@pytest.mark.parametrize("shape,k", [((4, 8, 1, 3, 5), 3), ((10, 100, 2, 3, 5), 2), ((12, 64, 1, 3, 5), 8),
+                                     ((13, 70, 1, 5, 5), 5), ((16, 16, 1, 3, 5), 2)],
+                         ids=lambda v: str(v))
+def test_batch_of_one_shape_in_one_launch_sequence(stwo, shape, k):
+    """stwo_wide_fib_prove_batch proves k jobs of one shape with every kernel of the proof
+    launched once for all of them (their device memory laid out alike, job k's at job
+    0's plus k slabs): each proof equals the one-job prover's byte for byte, and the
+    sequence launches about as many kernels as one proof (the transforms of more than
+    64 columns stage their table; nothing scales with k)."""
+    L, N, B, q, pw = shape
+    job = stwo.WideFibJob(L, N, B, q, pw)
+    tree = stwo.CudaBackend.precompute_twiddles(stwo.CanonicCoset(L + 1 + B).half_coset())
+    inputs = [stwo.wide_fib_inputs(L, 900 + 17 * i + L) for i in range(k)]
+    n0 = stwo.kernel_launches()
+    single = [stwo.prove_wide_fib(job, a0, a1, twiddles=tree)[0] for a0, a1 in inputs]
+    one = (stwo.kernel_launches() - n0) // k
+    n0 = stwo.kernel_launches()
+    proofs, status, stats = stwo.prove_wide_fib_batch(job, inputs, tree)
+    batched = stwo.kernel_launches() - n0
+    assert status == [0] * k
+    for i in range(k):
+        assert proofs[i] == single[i], f"job {i}"
+    assert batched <= one + 4, (batched, one)
+    stwo.verify(proofs[-1], L, N, log_blowup=B, n_queries=q, pow_bits=pw)
