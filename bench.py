@@ -706,7 +706,19 @@ class StreamRunner:
 
     def __init__(self, stwo, workers, max_domain_log=22):
         self.stwo = stwo
-        self.srv = stwo.ProofServer(n_workers=workers, device_budget_bytes=BUDGET, max_domain_log=max_domain_log)
+        # One worker is the one-job-at-a-time reference: it proves queued jobs of one
+        # shape one by one, not as a batch (STWO_SERVER_BATCH is read at creation).
+        saved = os.environ.get("STWO_SERVER_BATCH")
+        if workers == 1:
+            os.environ["STWO_SERVER_BATCH"] = "1"
+        try:
+            self.srv = stwo.ProofServer(n_workers=workers, device_budget_bytes=BUDGET,
+                                        max_domain_log=max_domain_log)
+        finally:
+            if saved is None:
+                os.environ.pop("STWO_SERVER_BATCH", None)
+            else:
+                os.environ["STWO_SERVER_BATCH"] = saved
 
     def run(self, jobs, inputs, resident, arrivals_ms=None, device_time=False):
         """jobs: list of (L, N, seed); inputs[i] = (host a0, host a1, dev a0, dev a1).
@@ -782,6 +794,7 @@ def batch48(stwo, dev, args, O=None):
     single.run(jobs[:2], ins[:2], resident=True)
     res_b, ms_b = batched.run(jobs, ins, resident=True, device_time=True)
     res_s, ms_s = single.run(jobs, ins, resident=True, device_time=True)
+    b48_batches = batched.srv.batch_stats()
     batched.close()
     single.close()
     identical = all(res_b[i]["proof"] == res_s[i]["proof"] for i in range(len(jobs)))
@@ -839,7 +852,7 @@ def batch48(stwo, dev, args, O=None):
     return {"jobs": 48, "workload": "log_n_rows U{10..20}, columns U{16,32,64,128}, log_blowup 1, 3 queries, "
                                     "pow_bits 5, all 48 admitted at once",
             "proofs_per_s": len(jobs) / (ms_b / 1e3), "per_job_proofs_per_s": len(jobs) / (ms_s / 1e3),
-            "batched_vs_per_job": ms_s / ms_b, "bit_identical": identical,
+            "batched_vs_per_job": ms_s / ms_b, "bit_identical": identical, "launch_sequence_batches": b48_batches,
             "mixed_tree": {"columns": "4 per log size 12..22", "ms": tree_ms, "root_equal_to_oracle": root_equal,
                            "one_call_ms": tree_call_ms, "one_call_launches": tree_call_launches,
                            "one_call_equal": tree_call_equal}}
@@ -847,7 +860,9 @@ def batch48(stwo, dev, args, O=None):
 
 def same_shape(stwo, dev):
     """Repeated-shape serving: 96 jobs of the 64-column x 2^12 proof (each with its own
-    inputs) through the server, batched (8 workers) and one at a time; a worker reuses
+    inputs) through the server, batched (8 workers) and one at a time. Batched, a worker
+    that takes a job also takes the queued jobs of its shape (up to 32) and proves them
+    in one launch sequence (stwo_wide_fib_prove_batch); one at a time, the worker reuses
     its slab for consecutive jobs of one shape and replays the proof's CUDA graph."""
     import numpy as np
     import torch
@@ -869,7 +884,7 @@ def same_shape(stwo, dev):
         res, ms = best
         per = sorted(v["done_ms"] - v["start_ms"] for v in res.values())
         out[name] = {"proofs_per_s": len(jobs) / (ms / 1e3), "median_job_ms": per[len(per) // 2],
-                     **r.srv.graph_stats()}
+                     **r.srv.graph_stats(), **r.srv.batch_stats()}
         r.close()
     return out
 
@@ -915,7 +930,9 @@ def compact_line(full, detail_path):
     ss = full.get("same_shape")
     if ss:
         line["same_shape"] = {"batched_proofs_per_s": ss["batched"]["proofs_per_s"],
-                              "one_at_a_time_proofs_per_s": ss["one_at_a_time"]["proofs_per_s"]}
+                              "one_at_a_time_proofs_per_s": ss["one_at_a_time"]["proofs_per_s"],
+                              "batched_launch_sequences": ss["batched"].get("batches"),
+                              "jobs_in_launch_sequences": ss["batched"].get("batched_jobs")}
     b = full.get("batch48")
     if b:
         line["batch48"] = {kk: b[kk] for kk in ("proofs_per_s", "per_job_proofs_per_s", "batched_vs_per_job",

@@ -399,6 +399,12 @@ void stwo_server_stats(stwo_prover_server *server, uint32_t *pending, uint32_t *
  * the proofs that replayed the captured launch sequence as one CUDA graph (all but
  * the first reuse of a slab). Off with STWO_SERVER_GRAPHS=0 at creation. */
 void stwo_server_graph_stats(stwo_prover_server *server, uint64_t *slab_reuses, uint64_t *graph_replays);
+/* Batches so far: launch sequences that proved several queued jobs of one shape at
+ * once (stwo_wide_fib_prove_batch), and the jobs they proved. A worker that takes a
+ * job of at most 2^16 trace rows also takes the queued jobs of its shape that
+ * arrival-order admission would take next, up to 32 a batch (STWO_SERVER_BATCH: the
+ * most, 1 for none; STWO_SERVER_BATCH_MAX_LOG: the largest log_n_rows, at creation). */
+void stwo_server_batch_stats(stwo_prover_server *server, uint64_t *batches, uint64_t *batched_jobs);
 double stwo_server_now_ms(void);
 /* Records the server's device epoch now (on an idle stream of its own) and waits for
  * it: later results carry device_done_ms relative to it, so the device-side span of a

@@ -144,6 +144,7 @@ SIGNATURES = [
     ("stwo_server_poll", u32, [vp, C.POINTER(ServerResult), u32, C.c_int32]),
     ("stwo_server_stats", None, [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u64)]),
     ("stwo_server_graph_stats", None, [vp, C.POINTER(u64), C.POINTER(u64)]),
+    ("stwo_server_batch_stats", None, [vp, C.POINTER(u64), C.POINTER(u64)]),
     ("stwo_server_now_ms", C.c_double, []),
     ("stwo_server_mark_epoch", C.c_int, [vp]),
     ("stwo_probe_m31_butterflies", C.c_int, [u32, vp, u64, C.POINTER(u64), vp]),

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <deque>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -58,6 +59,9 @@ struct stwo_prover_server {
     uint32_t spin_us = 2000;    // ...after polling this long
     bool use_priorities = true; // per-job stream priority by job size
     bool use_graphs = true;     // same-shape jobs reuse a worker's slab and proof graph
+    uint32_t batch_max = 32;       // queued jobs of one shape proved in one launch sequence
+    uint32_t batch_max_log = 16;   // ...for jobs of at most 2^batch_max_log trace rows
+    std::atomic<uint64_t> batches{0}, batched_jobs{0};
     std::atomic<uint64_t> slab_reuses{0}, graph_replays{0};
     cudaStream_t epoch_stream = nullptr;  // idle stream for the device epoch
     cudaEvent_t epoch = nullptr;          // timing event: device time zero of device_done_ms
@@ -129,6 +133,61 @@ struct stwo_prover_server {
         return std::min(c, n_classes - 1);
     }
 
+    // Proves j and the jobs of `more` (one shape) in one launch sequence and posts a
+    // result per job; every result carries the sequence's stats.
+    void prove_batch(const PendingJob &j, const std::vector<PendingJob> &more, cudaStream_t st) {
+        std::vector<const PendingJob *> jobs{&j};
+        for (auto &b : more) jobs.push_back(&b);
+        const uint32_t k = (uint32_t)jobs.size();
+        std::vector<const uint32_t *> a0(k), a1(k);
+        for (uint32_t i = 0; i < k; i++) {
+            a0[i] = jobs[i]->a0_dev ? jobs[i]->a0_dev : jobs[i]->a0.data();
+            a1[i] = jobs[i]->a1_dev ? jobs[i]->a1_dev : jobs[i]->a1.data();
+        }
+        const double start = steady_ms();
+        clear_error();
+        std::vector<std::vector<uint8_t>> proofs;
+        std::vector<int> rc(k, STWO_OK);
+        stwo_prove_stats stats{};
+        const int brc = wide_fib_prove_batch(&j.job, k, a0.data(), a1.data(), tw, itw, tree_size, proofs, rc.data(),
+                                             &stats, st);
+        const std::string err = brc ? stwo_last_error() : "";
+        batches++;
+        batched_jobs += k;
+        double device_done = -1.0;
+        if (brc == STWO_OK && epoch_set.load()) {
+            float ms = 0.f;
+            cudaEvent_t ev = last_wait_event();
+            if (ev && cudaEventElapsedTime(&ms, epoch, ev) == cudaSuccess) device_done = ms;
+            else cudaGetLastError();
+        }
+        const double end = steady_ms();
+        std::lock_guard<std::mutex> lock(mu);
+        for (uint32_t i = 0; i < k; i++) {
+            stwo_server_result r{};
+            r.job_id = jobs[i]->id;
+            r.submit_ms = jobs[i]->submit_ms;
+            r.start_ms = start;
+            r.done_ms = end;
+            r.stats = stats;
+            r.status = brc ? brc : rc[i];
+            r.device_done_ms = r.status == STWO_OK ? device_done : -1.0;
+            if (r.status == STWO_OK) {
+                r.proof = static_cast<uint8_t *>(malloc(proofs[i].size()));
+                if (r.proof) {
+                    memcpy(r.proof, proofs[i].data(), proofs[i].size());
+                    r.proof_len = proofs[i].size();
+                } else {
+                    r.status = STWO_ERR_OUT_OF_MEMORY;
+                }
+            }
+            if (r.status != STWO_OK)
+                strncpy(r.error, brc ? err.c_str() : "proof of the batch failed", sizeof(r.error) - 1);
+            done.push_back(r);
+        }
+        expire();
+    }
+
     void worker() {
         cudaSetDevice(device);
         t_blocking_wait = blocking_wait;
@@ -160,6 +219,35 @@ struct stwo_prover_server {
                 running++;
             }
             have_next = false;
+            // Queued jobs of this job's shape join it in one launch sequence while they
+            // are the jobs that arrival-order admission would take next.
+            std::vector<PendingJob> batch;
+            if (se == cudaSuccess && batch_max > 1 && j.job.log_n_rows <= batch_max_log) {
+                std::lock_guard<std::mutex> lock(mu);
+                for (auto it = pending.begin(); it != pending.end() && batch.size() + 1 < batch_max;) {
+                    if (in_use + it->bytes > budget) {  // admission would pass it as well
+                        ++it;
+                        continue;
+                    }
+                    if (!same_shape(it->job, j.job) || it->bytes != j.bytes) break;
+                    in_use += it->bytes;
+                    batch.push_back(std::move(*it));
+                    it = pending.erase(it);
+                }
+            }
+            if (!batch.empty()) {
+                if (cache.valid) prove_cache_release(&cache, cache_st);  // the batch plans its own slabs
+                prove_batch(j, batch, streams[priority_class(j.job, (uint32_t)streams.size())]);
+                {
+                    std::lock_guard<std::mutex> lock(mu);
+                    in_use -= j.bytes;
+                    for (auto &b : batch) in_use -= b.bytes;
+                    running--;
+                }
+                cv_done.notify_all();
+                cv_work.notify_all();
+                continue;
+            }
             stwo_server_result r{};
             r.job_id = j.id;
             r.submit_ms = j.submit_ms;
@@ -261,6 +349,9 @@ stwo_prover_server *stwo_server_create(uint32_t n_workers, uint64_t device_budge
     if (const char *w = getenv("STWO_SERVER_SPIN_US")) s->spin_us = (uint32_t)strtoul(w, nullptr, 10);
     if (const char *w = getenv("STWO_SERVER_PRIORITY")) s->use_priorities = strcmp(w, "0") != 0;
     if (const char *w = getenv("STWO_SERVER_GRAPHS")) s->use_graphs = strcmp(w, "0") != 0;
+    if (const char *w = getenv("STWO_SERVER_BATCH"))
+        s->batch_max = (uint32_t)std::min<unsigned long>(256, std::max<unsigned long>(1, strtoul(w, nullptr, 10)));
+    if (const char *w = getenv("STWO_SERVER_BATCH_MAX_LOG")) s->batch_max_log = (uint32_t)strtoul(w, nullptr, 10);
     s->max_domain_log = max_domain_log;
     // One twiddle tree for CanonicCoset(max_domain_log).half_coset serves every smaller
     // canonic domain: its doublings are the smaller domains' half cosets.
@@ -401,6 +492,11 @@ int stwo_server_mark_epoch(stwo_prover_server *s) {
     if (e != cudaSuccess) return set_error(STWO_ERR_CUDA, "server epoch: %s", cudaGetErrorString(e));
     s->epoch_set.store(true);
     return STWO_OK;
+}
+
+void stwo_server_batch_stats(stwo_prover_server *s, uint64_t *batches, uint64_t *batched_jobs) {
+    if (batches) *batches = s ? s->batches.load() : 0;
+    if (batched_jobs) *batched_jobs = s ? s->batched_jobs.load() : 0;
 }
 
 void stwo_server_graph_stats(stwo_prover_server *s, uint64_t *slab_reuses, uint64_t *graph_replays) {

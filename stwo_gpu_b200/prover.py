@@ -233,6 +233,13 @@ class ProofServer:
         L.lib().stwo_server_graph_stats(self._s, C.byref(a), C.byref(b))
         return {"slab_reuses": a.value, "graph_replays": b.value}
 
+    def batch_stats(self):
+        """Launch sequences that proved several queued jobs of one shape at once, and
+        the jobs they proved."""
+        a, b = C.c_uint64(), C.c_uint64()
+        L.lib().stwo_server_batch_stats(self._s, C.byref(a), C.byref(b))
+        return {"batches": a.value, "batched_jobs": b.value}
+
     @staticmethod
     def now_ms():
         return L.lib().stwo_server_now_ms()

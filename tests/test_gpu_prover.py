@@ -194,8 +194,10 @@ def test_server_same_shape_runs_replay_equal_proofs(graphs, workers, monkeypatch
     """Runs of same-shape jobs: a worker keeps its slab for the next job of the same
     shape, captures the proof's launch sequence as a CUDA graph on the second and
     replays it from the third. Every proof (each job with its own inputs) equals the
-    same job proved alone; STWO_SERVER_GRAPHS=0 turns the reuse off."""
+    same job proved alone; STWO_SERVER_GRAPHS=0 turns the reuse off. (Batching of
+    queued same-shape jobs is off here: it would take these runs as batches.)"""
     monkeypatch.setenv("STWO_SERVER_GRAPHS", graphs)
+    monkeypatch.setenv("STWO_SERVER_BATCH", "1")
     stwo = load_package()
     shapes = [(9, 24, 1, 3, 5), (11, 16, 2, 4, 3), (3, 5, 1, 2, 1), (2, 3, 1, 1, 0)]
     jobs = []
@@ -535,3 +537,32 @@ def test_batch_of_one_shape_in_one_launch_sequence(stwo, shape, k):
         assert proofs[i] == single[i], f"job {i}"
     assert batched <= one + 4, (batched, one)
     stwo.verify(proofs[-1], L, N, log_blowup=B, n_queries=q, pow_bits=pw)
+
+
+@pytest.mark.parametrize("batch", ["32", "5"])
+def test_server_batches_queued_jobs_of_one_shape(batch, monkeypatch):
+    """A worker that takes a small job also takes the queued jobs of its shape that
+    arrival-order admission would take next (up to STWO_SERVER_BATCH) and proves them in
+    one launch sequence. A larger job keeps the one worker busy while 40 jobs of one
+    shape and then 3 of another queue behind it: they come back in batches, every proof
+    equal to the job's proof alone, the other shape's jobs after them."""
+    monkeypatch.setenv("STWO_SERVER_BATCH", batch)
+    stwo = load_package()
+    L = stwo._lib
+    t, u = (12, 64, 1, 3, 5), (11, 16, 1, 3, 5)
+    jobs = [(1 + i, t, 900 + i) for i in range(40)] + [(41 + i, u, 990 + i) for i in range(3)]
+    alone = {jid: stwo.prove_wide_fib(job_of(sh), *stwo.wide_fib_inputs(sh[0], seed))[0] for jid, sh, seed in jobs}
+    with stwo.ProofServer(n_workers=1, device_budget_bytes=16 << 30, max_domain_log=21) as srv:
+        srv.submit(0, job_of(BUSY_JOB), *stwo.wide_fib_inputs(BUSY_JOB[0], 9))
+        _wait_running(srv)
+        for jid, sh, seed in jobs:
+            srv.submit(jid, job_of(sh), *stwo.wide_fib_inputs(sh[0], seed))
+        got = _collect(srv, len(jobs) + 1)
+        bs = srv.batch_stats()
+        assert srv.stats() == {"pending": 0, "running": 0, "device_bytes_in_use": 0}
+    for jid, sh, _ in jobs:
+        assert got[jid]["status"] == L.OK, got[jid]["error"]
+        assert got[jid]["proof"] == alone[jid], jid
+    k = int(batch)
+    assert bs["batches"] >= 40 // k and bs["batched_jobs"] >= 40 - 1
+    assert max(got[jid]["start_ms"] for jid in range(1, 41)) <= min(got[jid]["start_ms"] for jid in (41, 42, 43))
