@@ -408,7 +408,20 @@ def kernel_suite(stwo, reps=5):
 
     t = timed(quot_ours)
     b = (1 << lg) * (4 * nc + 16)
-    rec = {"ms": t, "gbs": b / t / 1e6, "frac_hbm": b / t / 1e6 / peak, "workload": "32 cols x 2^22, 4 points"}
+    rec = {"ms": t, "gbs": b / t / 1e6, "frac_hbm": b / t / 1e6 / peak, "workload": "32 cols x 2^22, 4 points",
+           "form": "tensor cores (tcgen05 kind::i8)"}
+    # the same call on the CUDA cores (the kernel the tensor-core form replaces)
+    tc_out = [o.clone() for o in outq]
+    L.check(lib.stwo_set_tunable(b"quotients_tensor_cores", 0))
+    try:
+        rec["cuda_cores_ms"] = timed(quot_ours)
+        rec["equal_cuda_cores"] = all(torch.equal(a, c) for a, c in zip(tc_out, outq))
+    finally:
+        L.check(lib.stwo_set_tunable(b"quotients_tensor_cores", 1))
+    del tc_out
+    nf = C.c_uint32()
+    L.check(lib.stwo_quotients_tc_faults(C.byref(nf), 1))
+    rec["tc_faults"] = nf.value
     if R is not None:
         dcols = R.copy_device_pointer_vec_from_host_to_device(cp, nc)
         rout = [torch.empty(1 << lg, dtype=torch.int32, device=dev) for _ in range(4)]

@@ -119,6 +119,7 @@ SIGNATURES = [
     ("stwo_merkle_commit_layer", C.c_int, [u32, vp, vp, u32, vp, vp]),
     ("stwo_merkle_commit_tree", C.c_int, [vp, vp, u32, u32, vp, vp]),
     ("stwo_accumulate_quotients", C.c_int, [u32, u32, u32, vp, u32, QM31, vp, vp, vp, vp, u32, vp, vp]),
+    ("stwo_quotients_tc_faults", C.c_int, [C.POINTER(u32), C.c_int]),
     ("stwo_wide_fib_composition", C.c_int, [vp, u32, u32, vp, vp, vp, vp]),
     ("stwo_kernel_launches", u64, []),
     ("stwo_reserve_device_memory", C.c_int, [u64]),

@@ -122,6 +122,11 @@ int stwo_set_tunable(const char *name, int value) {
         set_tunable(TUNE_EAP_GROUPS_LOG, value);
         return STWO_OK;
     }
+    if (n == "quotients_tensor_cores") {
+        STWO_REQUIRE(value >= 0 && value <= 2, STWO_ERR_INVALID_ARGUMENT, "quotients_tensor_cores must be 0, 1 or 2");
+        set_tunable(TUNE_QUOT_TENSOR, value);
+        return STWO_OK;
+    }
     return set_error(STWO_ERR_INVALID_ARGUMENT, "unknown tunable %s", name);
 }
 

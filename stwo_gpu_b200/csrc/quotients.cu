@@ -24,6 +24,7 @@
 
 #include "common.cuh"
 #include "quotients.cuh"
+#include "tc.cuh"
 
 namespace stwo {
 namespace {
@@ -221,6 +222,302 @@ __global__ void __launch_bounds__(256, QUOT_MIN_BLOCKS) quotients_kernel(const _
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Tensor-core form (tcgen05, 8-bit integer MMA). The column sums of every batch,
+// S_b,q(r) = sum_c W[c][b].q * col_c[r] with W[c][b] the sum of the batch's
+// coefficients on column c, are a product of the 2^n x C matrix of column values and
+// the C x 4 NB matrix W. Over bytes: with v = sum_i v_i 2^(8i) (column value) and
+// D_i = W.q * 2^(8i) mod p = sum_j d_ij 2^(8j),
+//   S_b,q(r) = sum_j 2^(8j) T_j(r) (mod p),  T_j(r) = sum_(c, i) v_i(r) d_ij,
+// a u8 x u8 product with K = 4 C (column c, byte i) and N = 16 NB (batch, component,
+// byte j), accumulated exactly in 32 bits (K * 255^2 < 2^31 for C < 8256). A CTA
+// of 13 warps streams tiles of 128 rows:
+//  * warps 8-11 copy 32 columns of the tile per stage into one of QTC_STAGES K-major
+//    stages in shared memory (4-byte asynchronous copies, up to QTC_STAGES stages in
+//    flight, each completing its stage's "full" barrier);
+//  * one thread of warp 12 issues the stage's MMAs (four of 128 x N x 32) into one of
+//    two TMEM accumulators and commits them to the stage's "empty" barrier;
+//  * warps 0-3 and 4-7 take the tiles in turn: each reads its tile's accumulator
+//    (a row a thread), frees it, and finishes the row as quotients_kernel does
+//    (denominators, one inversion for the NB of them, num_b / den_b summed).
+// B (the byte matrix of W) is built by each CTA in shared memory from the samples.
+// Every barrier wait gives up after QTC_WAIT_NS or once another role has given up;
+// a CTA that gave up counts itself in g_quot_tc_faults (stwo_quotients_tc_faults).
+constexpr int QTC_STAGES = 4;
+constexpr uint32_t QTC_STAGE_BYTES = 128 * 32 * 4;  // 128 rows x 32 columns x 4 bytes
+constexpr int QTC_THREADS = 13 * 32;
+constexpr uint64_t QTC_WAIT_NS = 1000000000ull;
+constexpr uint32_t QTC_MAX_B_BYTES = 64 * 1024;
+
+__device__ uint32_t g_quot_tc_faults;
+
+__host__ __device__ constexpr size_t qtc_b_bytes(uint32_t c8, int nb) { return (size_t)c8 * 16 * nb * 4; }
+__host__ __device__ constexpr size_t qtc_smem_bytes(uint32_t c8, int nb) {
+    return (size_t)QTC_STAGES * QTC_STAGE_BYTES + qtc_b_bytes(c8, nb) + (size_t)c8 * 8 + (2 * QTC_STAGES + 5) * 8 + 8;
+}
+
+template <int NB, bool COLS_ON_DEVICE, class PR>
+__global__ void __launch_bounds__(QTC_THREADS, 2)
+    quotients_tc_kernel(const __grid_constant__ PR pr, const uint32_t *const *__restrict__ dev_cols, uint32_t n_cols) {
+    constexpr int N = 16 * NB;
+    // two accumulators of N columns, each at a multiple of 32 columns
+    constexpr uint32_t SLOT = N <= 32 ? 32u : 64u, TM_COLS = 2 * SLOT;
+    constexpr uint32_t IDESC = tc::idesc_u8<128, N>();
+    const auto &p = pr.get();
+    extern __shared__ __align__(1024) uint8_t qsm[];
+    const uint32_t C8 = (n_cols + 7) & ~7u;
+    uint8_t *As = qsm;
+    uint8_t *Bs = qsm + QTC_STAGES * QTC_STAGE_BYTES;
+    const uint32_t **s_cols = reinterpret_cast<const uint32_t **>(Bs + qtc_b_bytes(C8, NB));
+    uint64_t *bars = reinterpret_cast<uint64_t *>(s_cols + C8);
+    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + 2 * QTC_STAGES + 5);
+    volatile uint32_t *s_abort = s_tmem + 1;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // ---- B = the bytes of W, from the samples
+    for (uint32_t c = tid; c < C8; c += blockDim.x)
+        s_cols[c] = c < n_cols ? (COLS_ON_DEVICE ? dev_cols[c] : p.cols[c]) : nullptr;
+    unsigned long long *W = reinterpret_cast<unsigned long long *>(As);  // [C8][NB][4], in the stages
+    for (uint32_t i = tid; i < C8 * NB * 4; i += blockDim.x) W[i] = 0;
+    if (tid == 0) *s_abort = 0;
+    __syncthreads();
+    const uint32_t n_samples = p.batch_end[NB - 1];
+    for (uint32_t j = tid; j < n_samples; j += blockDim.x) {
+        uint32_t b = 0;
+#pragma unroll
+        for (int bb = 0; bb + 1 < NB; bb++) b += j >= p.batch_end[bb] ? 1u : 0u;
+        const uint32_t c = p.col_idx[j];
+        if (c >= C8) continue;
+        const qm31 v = p.c2[j];
+        unsigned long long *w = W + ((size_t)c * NB + b) * 4;
+        atomicAdd(w + 0, (unsigned long long)v.a.a);
+        atomicAdd(w + 1, (unsigned long long)v.a.b);
+        atomicAdd(w + 2, (unsigned long long)v.b.a);
+        atomicAdd(w + 3, (unsigned long long)v.b.b);
+    }
+    __syncthreads();
+    for (uint32_t it = tid; it < C8 * NB * 4; it += blockDim.x) {
+        const uint32_t c = it / (NB * 4), bq = it % (NB * 4);  // it = (c * NB + b) * 4 + q, bq = 4 b + q
+        uint8_t *dst = Bs + ((size_t)(c >> 2) * N + bq * 4) * 16 + (c & 3) * 4;
+        uint32_t d = reduce64_p(W[it]);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+#pragma unroll
+            for (int jb = 0; jb < 4; jb++) dst[jb * 16 + i] = (uint8_t)(d >> (8 * jb));
+            const uint64_t s = (uint64_t)d << 8;  // d * 2^8 mod p
+            d = reduce_once((uint32_t)((s & P) + (s >> 31)));
+        }
+    }
+    tc::fence_async_smem();
+    const uint32_t bar0 = tc::smem_addr(bars);
+    if (tid == 0) {
+        for (int s = 0; s < QTC_STAGES; s++) {
+            tc::mbar_init(bar0 + 8 * s, 128);                 // full: the loader threads
+            tc::mbar_init(bar0 + 8 * (QTC_STAGES + s), 1);    // empty: one MMA commit
+        }
+        for (int e = 0; e < 2; e++) {
+            tc::mbar_init(bar0 + 8 * (2 * QTC_STAGES + e), 1);       // accumulator full: one commit
+            tc::mbar_init(bar0 + 8 * (2 * QTC_STAGES + 2 + e), 128); // accumulator empty: 4 warps
+        }
+        tc::mbar_init(bar0 + 8 * (2 * QTC_STAGES + 4), 1);  // all MMAs done
+        tc::mbar_init_fence();
+    }
+    if (warp == 12) tc::tmem_alloc(s_tmem, TM_COLS);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *s_tmem;
+    const uint32_t n_tiles = 1u << (p.log_size - 7);
+    const uint32_t n_chunks = (C8 + 31) / 32;
+    auto FULL = [&](uint32_t s) { return bar0 + 8 * s; };
+    auto EMPTY = [&](uint32_t s) { return bar0 + 8 * (QTC_STAGES + s); };
+    auto TFULL = [&](uint32_t e) { return bar0 + 8 * (2 * QTC_STAGES + e); };
+    auto TEMPTY = [&](uint32_t e) { return bar0 + 8 * (2 * QTC_STAGES + 2 + e); };
+    const uint32_t DONE = bar0 + 8 * (2 * QTC_STAGES + 4);
+    auto give_up = [&]() {
+        if (!*s_abort) {
+            *s_abort = 1;
+            atomicAdd(&g_quot_tc_faults, 1u);
+        }
+    };
+
+    if (warp >= 8 && warp < 12) {
+        // ---- loaders: warp wl copies rows 32 wl .. 32 wl + 31 of the tile, 32 columns a
+        // stage, with 4-byte asynchronous copies (a warp's copy covers 8 rows x 4 columns:
+        // 128 contiguous bytes of the stage); the stage's "full" barrier completes when
+        // all 128 loader threads' copies have landed.
+        const uint32_t wl = warp - 8, ro = lane >> 2, co = lane & 3;
+        const uint32_t st0 = tc::smem_addr(As) + (32 * wl + ro) * 16 + co * 4;
+        uint32_t g = 0;
+        bool ok = true;
+        for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
+            const size_t row0 = (size_t)tile * 128 + 32 * wl + ro;
+            for (uint32_t kc = 0; kc < n_chunks; kc++, g++) {
+                const uint32_t s = g % QTC_STAGES;
+                if (!tc::mbar_wait(EMPTY(s), ((g / QTC_STAGES) & 1) ^ 1, s_abort, QTC_WAIT_NS)) {
+                    give_up();
+                    ok = false;
+                    break;
+                }
+                const uint32_t dst = st0 + s * QTC_STAGE_BYTES;
+#pragma unroll
+                for (int cg = 0; cg < 8; cg++) {
+                    const uint32_t c = kc * 32 + 4 * cg + co;
+                    if (c < n_cols) {
+                        const uint32_t *src = s_cols[c] + row0;
+#pragma unroll
+                        for (int rg = 0; rg < 4; rg++) tc::cp_async4(dst + cg * 2048 + rg * 128, src + 8 * rg);
+                    }
+                }
+                tc::cp_async_arrive(FULL(s));
+            }
+        }
+    } else if (warp == 12) {
+        // ---- the MMA thread
+        if (lane == 0) {
+            const uint32_t a0 = tc::smem_addr(As), b0 = tc::smem_addr(Bs);
+            uint32_t g = 0;
+            bool ok = true;
+            for (uint32_t tl = 0, tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x, tl++) {
+                const uint32_t e = tl & 1;
+                if (!tc::mbar_wait(TEMPTY(e), ((tl >> 1) & 1) ^ 1, s_abort, QTC_WAIT_NS)) {
+                    give_up();
+                    break;
+                }
+                tc::fence_after_sync();
+                for (uint32_t kc = 0; kc < n_chunks; kc++, g++) {
+                    const uint32_t s = g % QTC_STAGES;
+                    if (!tc::mbar_wait(FULL(s), (g / QTC_STAGES) & 1, s_abort, QTC_WAIT_NS)) {
+                        give_up();
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_async_smem();
+                    tc::fence_after_sync();
+                    const uint32_t left = (C8 - kc * 32) / 8, nm = left < 4 ? left : 4u;
+                    for (uint32_t m = 0; m < nm; m++) {
+                        const uint64_t ad = tc::smem_desc(a0 + s * QTC_STAGE_BYTES + m * 4096, 2048, 128);
+                        const uint64_t bd = tc::smem_desc(b0 + (kc * 8 + 2 * m) * N * 16, N * 16, 128);
+                        tc::mma_u8(tmem + e * SLOT, ad, bd, IDESC, (kc | m) != 0);
+                    }
+                    tc::commit(EMPTY(s));
+                }
+                if (ok) tc::commit(TFULL(e));
+            }
+            // every MMA issued here completes before the accumulators are freed
+            tc::commit(DONE);
+            if (!tc::mbar_wait(DONE, 0, nullptr, QTC_WAIT_NS)) give_up();
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue group e: the tiles tl = e, e + 2, ... of this CTA, one row a thread
+        const uint32_t e = warp >> 2, row = 32 * (warp & 3) + lane;
+        const uint32_t lane_base = tmem + ((32 * (warp & 3)) << 16) + e * SLOT;
+        for (uint32_t tl = e, tile = blockIdx.x + e * gridDim.x; tile < n_tiles; tl += 2, tile += 2 * gridDim.x) {
+            if (!tc::mbar_wait(TFULL(e), (tl >> 1) & 1, s_abort, QTC_WAIT_NS)) {
+                give_up();
+                break;
+            }
+            tc::fence_after_sync();
+            uint32_t num[NB][4];
+#pragma unroll
+            for (int b = 0; b < NB; b++) {
+                uint32_t r[16];
+                tc::tmem_ld16(lane_base + 16 * b, r);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    num[b][q] = reduce64_p((uint64_t)r[4 * q] + ((uint64_t)r[4 * q + 1] << 8) +
+                                           ((uint64_t)r[4 * q + 2] << 16) + ((uint64_t)r[4 * q + 3] << 24));
+            }
+            tc::fence_before_sync();
+            tc::mbar_arrive(TEMPTY(e));
+            const uint32_t R = tile * 128 + row, sgn = R & 1;
+            const uint32_t hidx = bit_reverse_bits(R >> 1, p.log_size - 1);
+            const cpoint pt = point_from_tables(p.tab, (p.half_init + p.half_step * hidx) & 0x7fffffffu);
+            cm31 dinv[NB];
+            uint32_t nrm[NB], pre[NB], prefix = 1;
+#pragma unroll
+            for (int b = 0; b < NB; b++) {
+                const cm31 u = cm31_sub(p.den_k[b], cm31_scale(p.piy[b], pt.x));
+                const cm31 v = cm31_scale(p.pix[b], pt.y);
+                dinv[b] = sgn ? cm31_sub(u, v) : cm31_add(u, v);
+                uint64_t n2 = (uint64_t)dinv[b].a * dinv[b].a;
+                mac_wide(n2, dinv[b].b, dinv[b].b);
+                nrm[b] = reduce64_p(n2);
+                prefix = m31_mul(prefix, nrm[b]);
+                pre[b] = prefix;
+            }
+            uint32_t inv = m31_inv(prefix);
+#pragma unroll
+            for (int b = NB - 1; b >= 0; b--) {
+                const uint32_t ni = m31_mul(inv, b > 0 ? pre[b - 1] : 1u);  // 1 / norm
+                inv = m31_mul(inv, nrm[b]);
+                dinv[b] = {m31_mul(dinv[b].a, ni), m31_mul(m31_neg(dinv[b].b), ni)};
+            }
+            qm31 acc = qm31_zero();
+#pragma unroll
+            for (int b = 0; b < NB; b++) {
+                const qm31 ay = qm31_scale(p.a_sum[b], pt.y);
+                const qm31 lin = sgn ? qm31_sub(p.b_sum[b], ay) : qm31_add(p.b_sum[b], ay);
+                const qm31 nb = qm31_sub({{num[b][0], num[b][1]}, {num[b][2], num[b][3]}}, lin);
+                acc = qm31_add(acc, qm31_mul_cm31(nb, dinv[b]));
+            }
+            p.out[0][R] = acc.a.a;
+            p.out[1][R] = acc.a.b;
+            p.out[2][R] = acc.b.a;
+            p.out[3][R] = acc.b.b;
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (warp == 12) tc::tmem_free(tmem, TM_COLS);
+}
+
+// Whether the tensor-core form takes a call: domains of at least 128 rows, 1..4
+// batches, and the byte matrix of W within QTC_MAX_B_BYTES; with the tunable at 1
+// (the default) only calls of two or more batches, where it measured faster (with one
+// batch the CUDA-core kernel's row pairs share their column loads and the tensor form
+// is no faster: 256 columns x 2^21, 0.49 vs 0.47 ms; 8 columns x 2^22, 0.13 vs 0.085
+// ms), with the tunable at 2 every call it can take.
+bool quot_tc_eligible(uint32_t log_size, uint32_t n_batches, uint32_t n_cols) {
+    const uint32_t c8 = (n_cols + 7) & ~7u;
+    const int mode = tunable(TUNE_QUOT_TENSOR);
+    return mode != 0 && (mode == 2 || n_batches >= 2) && log_size >= 7 && log_size <= 31 && n_batches >= 1 &&
+           n_batches <= 4 && n_cols >= 1 && qtc_b_bytes(c8, (int)n_batches) <= QTC_MAX_B_BYTES;
+}
+
+template <int NB, bool COLS_ON_DEVICE, class PR>
+int launch_quot_tc(const PR &pr, const uint32_t *const *dev_cols, uint32_t n_cols, uint32_t log_size, uint32_t jobs,
+                   cudaStream_t st) {
+    static std::atomic<uint64_t> attr_done{0};
+    auto kern = quotients_tc_kernel<NB, COLS_ON_DEVICE, PR>;
+    int rc = once_per_device(attr_done, [&] {
+        STWO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)qtc_smem_bytes(QTC_MAX_B_BYTES / (64 * NB), NB)));
+        return (int)STWO_OK;
+    });
+    if (rc) return rc;
+    const uint32_t c8 = (n_cols + 7) & ~7u;
+    const uint64_t tiles = 1ull << (log_size - 7), cap = 2ull * device_sm_count();
+    const unsigned gx = (unsigned)(tiles < cap ? tiles : cap);
+    kern<<<dim3(gx, jobs), QTC_THREADS, qtc_smem_bytes(c8, NB), st>>>(pr, dev_cols, n_cols);
+    STWO_LAUNCH_CHECK("quotients_tc_kernel");
+    return STWO_OK;
+}
+
+template <bool COLS_ON_DEVICE, class PR>
+int launch_quot_tc_nb(uint32_t nb, const PR &pr, const uint32_t *const *dev_cols, uint32_t n_cols, uint32_t log_size,
+                      uint32_t jobs, cudaStream_t st) {
+    switch (nb) {
+    case 1: return launch_quot_tc<1, COLS_ON_DEVICE>(pr, dev_cols, n_cols, log_size, jobs, st);
+    case 2: return launch_quot_tc<2, COLS_ON_DEVICE>(pr, dev_cols, n_cols, log_size, jobs, st);
+    case 3: return launch_quot_tc<3, COLS_ON_DEVICE>(pr, dev_cols, n_cols, log_size, jobs, st);
+    default: return launch_quot_tc<4, COLS_ON_DEVICE>(pr, dev_cols, n_cols, log_size, jobs, st);
+    }
+}
+
 // The circle-group tables of point_from_tables on the current device: G^i for
 // i < 2^11, G^(2^11 i) for i < 2^11, G^(2^22 i) for i < 2^9 (36 KiB), computed on the
 // host and copied once per device.
@@ -298,6 +595,10 @@ int quotients_async(uint32_t half_init, uint32_t half_step, uint32_t log_size, c
         p->batch_end[b] = off;
     }
     quot_scale_batches(*p, n_batches);
+    if (quot_tc_eligible(log_size, n_batches, n_cols)) {
+        if (cols_on_device) return launch_quot_tc_nb<true>(n_batches, *holder, cols, n_cols, log_size, 1, st);
+        return launch_quot_tc_nb<false>(n_batches, *holder, nullptr, n_cols, log_size, 1, st);
+    }
     uint64_t pairs = 1ull << (log_size - 1);
     uint64_t blocks = (pairs + 255) / 256;
     uint64_t cap = (uint64_t)device_sm_count() * 8;
@@ -332,7 +633,10 @@ int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t 
     STWO_REQUIRE(log_size >= 1 && log_size <= 31, STWO_ERR_UNSUPPORTED_SIZE, "domain log size %u", log_size);
     STWO_REQUIRE(jobs >= 1 && jobs <= 65535, STWO_ERR_INVALID_ARGUMENT, "quotient groups per launch: %u", jobs);
     STWO_REQUIRE(n_samples >= 1 && n_samples <= 1024, STWO_ERR_UNSUPPORTED_SIZE, "%u samples", n_samples);
-    const uint32_t n_stage = quot_padded(n_samples);  // one batch
+    // one batch; column j is sample j
+    if (quot_tc_eligible(log_size, 1, n_samples))
+        return launch_quot_tc<1, false>(QuotByRef{p_dev, js}, nullptr, n_samples, log_size, jobs, st);
+    const uint32_t n_stage = quot_padded(n_samples);
     const size_t smem = (size_t)n_stage * (sizeof(qm31) + sizeof(void *));
     uint64_t pairs = 1ull << (log_size - 1);
     uint64_t blocks = (pairs + 255) / 256;
@@ -349,6 +653,16 @@ int quotients_dev_async(const QuotParamsDev *p_dev, uint32_t log_size, uint32_t 
 using namespace stwo;
 
 extern "C" {
+
+int stwo_quotients_tc_faults(uint32_t *count, int reset) {
+    STWO_REQUIRE(count, STWO_ERR_INVALID_ARGUMENT, "null count");
+    STWO_CUDA_TRY(cudaMemcpyFromSymbol(count, g_quot_tc_faults, sizeof(uint32_t)));
+    if (reset) {
+        const uint32_t zero = 0;
+        STWO_CUDA_TRY(cudaMemcpyToSymbol(g_quot_tc_faults, &zero, sizeof(uint32_t)));
+    }
+    return STWO_OK;
+}
 
 int stwo_accumulate_quotients(uint32_t half_coset_initial_index, uint32_t half_coset_step_size,
                               uint32_t domain_log_size, const uint32_t *const *columns, uint32_t n_columns,

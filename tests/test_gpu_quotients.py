@@ -75,6 +75,69 @@ def test_quotients_config_shape(stwo, oracle):
     _run_quotients(stwo, oracle, 14, 32, [32, 32, 32, 32], 5)
 
 
+@pytest.fixture
+def tensor_cores(stwo):
+    """Sets the quotients_tensor_cores tunable for one test and restores the default."""
+    L = stwo._lib
+
+    def set_(v):
+        L.check(L.lib().stwo_set_tunable(b"quotients_tensor_cores", v))
+    yield set_
+    set_(1)
+
+
+def _faults(stwo):
+    import ctypes as C
+    n = C.c_uint32()
+    stwo._lib.check(stwo._lib.lib().stwo_quotients_tc_faults(C.byref(n), 1))
+    return n.value
+
+
+# (log_size, columns, batch sizes): one tile (2^7 rows) up to many tiles per CTA, 1-4
+# batches, partial column chunks (1, 5, 33, 100 columns), repeated columns within a batch
+# (more samples than columns), the largest byte matrix the tensor form takes (250
+# columns, rounded up to 256, x 4 batches), and 260 x 4, past it (the CUDA cores).
+TC_SHAPES = [(7, 1, [1]), (7, 5, [3, 1, 5]), (8, 33, [33, 33]), (11, 100, [100]), (12, 8, [20, 3, 9, 8]),
+             (13, 32, [32, 7, 1, 19]), (15, 250, [128, 128, 128, 128]), (9, 260, [130, 130, 130, 120]),
+             (18, 64, [64])]
+
+
+@pytest.mark.parametrize("log_size,ncols,batch_sizes", TC_SHAPES)
+@pytest.mark.parametrize("tc", [2, 1, 0])
+def test_quotients_tensor_and_cuda_cores(stwo, oracle, tensor_cores, log_size, ncols, batch_sizes, tc):
+    """Both forms of the quotient kernel equal the oracle, through the native and the
+    reference-compatible entry points (tc: the quotients_tensor_cores tunable; 2 puts
+    one-batch calls on the tensor cores too)."""
+    tensor_cores(tc)
+    _faults(stwo)
+    seed = 100 * log_size + ncols
+    _run_quotients(stwo, oracle, log_size, ncols, batch_sizes, seed)
+    if ncols <= 100:
+        _run_quotients(stwo, oracle, log_size, ncols, batch_sizes, seed + 1, reference_abi=True)
+    assert _faults(stwo) == 0
+
+
+def test_quotients_tensor_cores_full_size(stwo, tensor_cores):
+    """32 columns x 2^22 with 4 points (the kernel sweep's shape): the tensor-core and
+    CUDA-core forms give identical columns (each form is checked against the oracle
+    above on the same per-row formula)."""
+    B = stwo.CudaBackend
+    r = rng(7)
+    lg, nc = 22, 32
+    domain = stwo.CanonicCoset(lg).circle_domain()
+    cols = [stwo.CircleEvaluation(domain, stwo.BaseFieldVec.from_numpy(m31(r, 1 << lg))) for _ in range(nc)]
+    rc = random_qm31(r)
+    batches = [stwo.ColumnSampleBatch(random_circle_point(r), [(c, random_qm31(r)) for c in range(nc)])
+               for _ in range(4)]
+    got = {}
+    for tc in (2, 0):
+        tensor_cores(tc)
+        got[tc] = B.accumulate_quotients(domain, cols, rc, batches).values.to_numpy()
+    for a, b in zip(got[2], got[0]):
+        assert (a == b).all()
+    assert _faults(stwo) == 0
+
+
 @pytest.mark.parametrize("n_cols,log_size", [(3, 1), (8, 5), (64, 13), (256, 8)])
 def test_wide_fib_composition(stwo, oracle, n_cols, log_size):
     L = stwo._lib
