@@ -164,7 +164,7 @@ int stwo_autotune(char *report, size_t report_cap);
  * fft_ept_strided (5 or 6), merkle_sub_threads (128, 256 or 512), merkle_sub_spread
  * (0..5: log2 of the bottom-level nodes each thread hashes), eval_at_point_groups_log
  * (2..4: log2 of the 8192-coefficient groups each eval_at_point CTA folds; 0, the
- * default, chooses per launch), quotients_tensor_cores (0, 1 = the default, 2). */
+ * default, chooses per launch), quotients_tensor_cores (1, the default, or 0). */
 int stwo_set_tunable(const char *name, int value);
 /* Diagnostics (no counterpart in the reference): the integer ceiling of the FFT. One
  * launch runs the FFT passes' own forward butterfly on register-resident operands
@@ -270,12 +270,11 @@ int stwo_accumulate_quotients(uint32_t half_coset_initial_index, uint32_t half_c
                               stwo_qm31 random_coeff, const stwo_spoint *sample_points, const uint32_t *batch_sizes,
                               const uint32_t *column_indices, const stwo_qm31 *sampled_values, uint32_t n_batches,
                               uint32_t *const *out4, void *stream);
-/* Domains of at least 2^7 rows with 2..4 batches (and 64 * n_batches * n_columns <=
+/* Domains of at least 2^8 rows with 1..4 batches (and 64 * n_batches * n_columns <=
  * 65536, columns rounded up to a multiple of 8) are computed on the tensor cores: the
  * batches' column sums as an 8-bit integer matrix product (column bytes x coefficient
- * bytes, 32-bit accumulators in TMEM); other calls on the CUDA cores.
- * stwo_set_tunable("quotients_tensor_cores", v) moves the line: 0 for the CUDA cores
- * always, 2 for the tensor cores with one batch too. Every choice gives the same
+ * bytes, 32-bit accumulators in TMEM); other calls, and every call after
+ * stwo_set_tunable("quotients_tensor_cores", 0), on the CUDA cores. Both give the same
  * values. The tensor-core kernel's barrier waits give up after one second; *count
  * receives how many CTAs gave up since the last reset (0 unless the device
  * misbehaved; their rows are then not written). Synchronises the device. */

@@ -123,7 +123,7 @@ int stwo_set_tunable(const char *name, int value) {
         return STWO_OK;
     }
     if (n == "quotients_tensor_cores") {
-        STWO_REQUIRE(value >= 0 && value <= 2, STWO_ERR_INVALID_ARGUMENT, "quotients_tensor_cores must be 0, 1 or 2");
+        STWO_REQUIRE(value == 0 || value == 1, STWO_ERR_INVALID_ARGUMENT, "quotients_tensor_cores must be 0 or 1");
         set_tunable(TUNE_QUOT_TENSOR, value);
         return STWO_OK;
     }

@@ -113,7 +113,7 @@ enum Tunable {
     TUNE_MERKLE_SUB_SPREAD,     // log2 bottom-level nodes per thread of that kernel (0..5)
     TUNE_EAP_GROUPS_LOG,        // eval_at_point: log2 groups of 8192 coefficients per CTA (2..4), 0 = per launch
     TUNE_FFT_MAX_STRIDED,       // FFT radix split: at most this many layers per strided pass (4..10)
-    TUNE_QUOT_TENSOR,           // DEEP quotients on the tensor cores: 0 never, 1 for 2+ batches, 2 wherever it applies
+    TUNE_QUOT_TENSOR,           // DEEP quotients: 1 = on the tensor cores where the form applies, 0 = CUDA cores
     TUNE_COUNT
 };
 int tunable(Tunable t);

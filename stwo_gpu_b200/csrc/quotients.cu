@@ -230,24 +230,30 @@ __global__ void __launch_bounds__(256, QUOT_MIN_BLOCKS) quotients_kernel(const _
 // D_i = W.q * 2^(8i) mod p = sum_j d_ij 2^(8j),
 //   S_b,q(r) = sum_j 2^(8j) T_j(r) (mod p),  T_j(r) = sum_(c, i) v_i(r) d_ij,
 // a u8 x u8 product with K = 4 C (column c, byte i) and N = 16 NB (batch, component,
-// byte j), accumulated exactly in 32 bits (K * 255^2 < 2^31 for C < 8256). A CTA
-// of 13 warps streams tiles of 128 rows:
-//  * warps 8-11 copy 32 columns of the tile per stage into one of QTC_STAGES K-major
+// byte j), accumulated exactly in 32 bits (K * 255^2 < 2^31 for C < 8256). A tile is
+// 128 row pairs (rows 2k and 2k + 1, at conjugate domain points), one per TMEM lane;
+// the even and the odd rows are two MMAs into adjacent halves of the accumulator, so
+// one thread finishes both rows of its pair as quotients_kernel does (one point, shared
+// denominator products, one inversion for the 2 NB denominators). A CTA of 13 warps
+// streams tiles:
+//  * warps 8-11 copy 16 columns of the tile per stage into one of QTC_STAGES K-major
 //    stages in shared memory (4-byte asynchronous copies, up to QTC_STAGES stages in
-//    flight, each completing its stage's "full" barrier);
-//  * one thread of warp 12 issues the stage's MMAs (four of 128 x N x 32) into one of
-//    two TMEM accumulators and commits them to the stage's "empty" barrier;
+//    flight, each completing its stage's "full" barrier); a stage holds slab 2 g + s
+//    (columns 4g .. 4g + 3 of the rows of parity s) at (2 g + s) * 2048 bytes;
+//  * one thread of warp 12 issues the stage's MMAs (128 x N x 32, one per 8 columns
+//    and parity) into one of two TMEM accumulators and commits them to the stage's
+//    "empty" barrier;
 //  * warps 0-3 and 4-7 take the tiles in turn: each reads its tile's accumulator
-//    (a row a thread), frees it, and finishes the row as quotients_kernel does
-//    (denominators, one inversion for the NB of them, num_b / den_b summed).
+//    (a row pair a thread), frees it, and finishes the pair.
 // B (the byte matrix of W) is built by each CTA in shared memory from the samples.
 // Every barrier wait gives up after QTC_WAIT_NS or once another role has given up;
 // a CTA that gave up counts itself in g_quot_tc_faults (stwo_quotients_tc_faults).
 constexpr int QTC_STAGES = 4;
-constexpr uint32_t QTC_STAGE_BYTES = 128 * 32 * 4;  // 128 rows x 32 columns x 4 bytes
+constexpr uint32_t QTC_STAGE_BYTES = 128 * 2 * 16 * 4;  // 128 row pairs x 16 columns x 4 bytes
 constexpr int QTC_THREADS = 13 * 32;
 constexpr uint64_t QTC_WAIT_NS = 1000000000ull;
 constexpr uint32_t QTC_MAX_B_BYTES = 64 * 1024;
+constexpr size_t QTC_SMEM_FLOOR = 80 * 1024;  // more than a third of an SM's 228 KiB
 
 __device__ uint32_t g_quot_tc_faults;
 
@@ -260,8 +266,9 @@ template <int NB, bool COLS_ON_DEVICE, class PR>
 __global__ void __launch_bounds__(QTC_THREADS, 2)
     quotients_tc_kernel(const __grid_constant__ PR pr, const uint32_t *const *__restrict__ dev_cols, uint32_t n_cols) {
     constexpr int N = 16 * NB;
-    // two accumulators of N columns, each at a multiple of 32 columns
-    constexpr uint32_t SLOT = N <= 32 ? 32u : 64u, TM_COLS = 2 * SLOT;
+    // two accumulators, each an even-row half and an odd-row half of N columns, every
+    // half at a multiple of 32 columns
+    constexpr uint32_t PAR = N <= 32 ? 32u : 64u, SLOT = 2 * PAR, TM_COLS = 2 * SLOT;
     constexpr uint32_t IDESC = tc::idesc_u8<128, N>();
     const auto &p = pr.get();
     extern __shared__ __align__(1024) uint8_t qsm[];
@@ -327,8 +334,8 @@ __global__ void __launch_bounds__(QTC_THREADS, 2)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *s_tmem;
-    const uint32_t n_tiles = 1u << (p.log_size - 7);
-    const uint32_t n_chunks = (C8 + 31) / 32;
+    const uint32_t n_tiles = 1u << (p.log_size - 8);
+    const uint32_t n_chunks = (C8 + 15) / 16;
     auto FULL = [&](uint32_t s) { return bar0 + 8 * s; };
     auto EMPTY = [&](uint32_t s) { return bar0 + 8 * (QTC_STAGES + s); };
     auto TFULL = [&](uint32_t e) { return bar0 + 8 * (2 * QTC_STAGES + e); };
@@ -342,16 +349,16 @@ __global__ void __launch_bounds__(QTC_THREADS, 2)
     };
 
     if (warp >= 8 && warp < 12) {
-        // ---- loaders: warp wl copies rows 32 wl .. 32 wl + 31 of the tile, 32 columns a
-        // stage, with 4-byte asynchronous copies (a warp's copy covers 8 rows x 4 columns:
-        // 128 contiguous bytes of the stage); the stage's "full" barrier completes when
-        // all 128 loader threads' copies have landed.
+        // ---- loaders: warp wl copies row pairs 32 wl .. 32 wl + 31 of the tile, 16
+        // columns a stage, with 4-byte asynchronous copies (a warp's copy covers 8 pairs x
+        // 4 columns of one parity: 128 contiguous bytes of the stage); the stage's "full"
+        // barrier completes when all 128 loader threads' copies have landed.
         const uint32_t wl = warp - 8, ro = lane >> 2, co = lane & 3;
         const uint32_t st0 = tc::smem_addr(As) + (32 * wl + ro) * 16 + co * 4;
         uint32_t g = 0;
         bool ok = true;
         for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
-            const size_t row0 = (size_t)tile * 128 + 32 * wl + ro;
+            const size_t row0 = (size_t)tile * 256 + 2 * (32 * wl + ro);
             for (uint32_t kc = 0; kc < n_chunks; kc++, g++) {
                 const uint32_t s = g % QTC_STAGES;
                 if (!tc::mbar_wait(EMPTY(s), ((g / QTC_STAGES) & 1) ^ 1, s_abort, QTC_WAIT_NS)) {
@@ -361,12 +368,15 @@ __global__ void __launch_bounds__(QTC_THREADS, 2)
                 }
                 const uint32_t dst = st0 + s * QTC_STAGE_BYTES;
 #pragma unroll
-                for (int cg = 0; cg < 8; cg++) {
-                    const uint32_t c = kc * 32 + 4 * cg + co;
+                for (int cg = 0; cg < 4; cg++) {
+                    const uint32_t c = kc * 16 + 4 * cg + co;
                     if (c < n_cols) {
                         const uint32_t *src = s_cols[c] + row0;
 #pragma unroll
-                        for (int rg = 0; rg < 4; rg++) tc::cp_async4(dst + cg * 2048 + rg * 128, src + 8 * rg);
+                        for (int pg = 0; pg < 4; pg++)
+#pragma unroll
+                            for (int par = 0; par < 2; par++)
+                                tc::cp_async4(dst + (2 * cg + par) * 2048 + pg * 128, src + 16 * pg + par);
                     }
                 }
                 tc::cp_async_arrive(FULL(s));
@@ -394,11 +404,15 @@ __global__ void __launch_bounds__(QTC_THREADS, 2)
                     }
                     tc::fence_async_smem();
                     tc::fence_after_sync();
-                    const uint32_t left = (C8 - kc * 32) / 8, nm = left < 4 ? left : 4u;
+                    const uint32_t left = (C8 - kc * 16) / 8, nm = left < 2 ? left : 2u;
                     for (uint32_t m = 0; m < nm; m++) {
-                        const uint64_t ad = tc::smem_desc(a0 + s * QTC_STAGE_BYTES + m * 4096, 2048, 128);
-                        const uint64_t bd = tc::smem_desc(b0 + (kc * 8 + 2 * m) * N * 16, N * 16, 128);
-                        tc::mma_u8(tmem + e * SLOT, ad, bd, IDESC, (kc | m) != 0);
+                        const uint64_t bd = tc::smem_desc(b0 + (kc * 4 + 2 * m) * N * 16, N * 16, 128);
+                        for (uint32_t par = 0; par < 2; par++) {
+                            // slabs 4m + par and 4m + par + 2: columns 8m .. 8m + 7, parity par
+                            const uint64_t ad =
+                                tc::smem_desc(a0 + s * QTC_STAGE_BYTES + (4 * m + par) * 2048, 4096, 128);
+                            tc::mma_u8(tmem + e * SLOT + par * PAR, ad, bd, IDESC, (kc | m) != 0);
+                        }
                     }
                     tc::commit(EMPTY(s));
                 }
@@ -410,8 +424,8 @@ __global__ void __launch_bounds__(QTC_THREADS, 2)
         }
         __syncwarp();
     } else {
-        // ---- epilogue group e: the tiles tl = e, e + 2, ... of this CTA, one row a thread
-        const uint32_t e = warp >> 2, row = 32 * (warp & 3) + lane;
+        // ---- epilogue group e: the tiles tl = e, e + 2, ... of this CTA, a row pair a thread
+        const uint32_t e = warp >> 2, kp = 32 * (warp & 3) + lane;
         const uint32_t lane_base = tmem + ((32 * (warp & 3)) << 16) + e * SLOT;
         for (uint32_t tl = e, tile = blockIdx.x + e * gridDim.x; tile < n_tiles; tl += 2, tile += 2 * gridDim.x) {
             if (!tc::mbar_wait(TFULL(e), (tl >> 1) & 1, s_abort, QTC_WAIT_NS)) {
@@ -419,54 +433,71 @@ __global__ void __launch_bounds__(QTC_THREADS, 2)
                 break;
             }
             tc::fence_after_sync();
-            uint32_t num[NB][4];
+            uint32_t num[2][NB][4];
 #pragma unroll
-            for (int b = 0; b < NB; b++) {
-                uint32_t r[16];
-                tc::tmem_ld16(lane_base + 16 * b, r);
-                tc::tmem_wait_ld();
+            for (int par = 0; par < 2; par++)
 #pragma unroll
-                for (int q = 0; q < 4; q++)
-                    num[b][q] = reduce64_p((uint64_t)r[4 * q] + ((uint64_t)r[4 * q + 1] << 8) +
-                                           ((uint64_t)r[4 * q + 2] << 16) + ((uint64_t)r[4 * q + 3] << 24));
-            }
+                for (int b = 0; b < NB; b++) {
+                    uint32_t r[16];
+                    tc::tmem_ld16(lane_base + par * PAR + 16 * b, r);
+                    tc::tmem_wait_ld();
+                    // sum_j 2^(8j) T_j < 2^56: one fold leaves it below 2^31 + 2^25
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const uint64_t t = (uint64_t)r[4 * q] + ((uint64_t)r[4 * q + 1] << 8) +
+                                           ((uint64_t)r[4 * q + 2] << 16) + ((uint64_t)r[4 * q + 3] << 24);
+                        num[par][b][q] = reduce_once((uint32_t)(t & P) + (uint32_t)(t >> 31));
+                    }
+                }
             tc::fence_before_sync();
             tc::mbar_arrive(TEMPTY(e));
-            const uint32_t R = tile * 128 + row, sgn = R & 1;
-            const uint32_t hidx = bit_reverse_bits(R >> 1, p.log_size - 1);
+            const uint32_t k = tile * 128 + kp;  // rows 2k, 2k + 1
+            const uint32_t hidx = bit_reverse_bits(k, p.log_size - 1);
             const cpoint pt = point_from_tables(p.tab, (p.half_init + p.half_step * hidx) & 0x7fffffffu);
-            cm31 dinv[NB];
-            uint32_t nrm[NB], pre[NB], prefix = 1;
+            cm31 dinv[2][NB];
+            uint32_t nrm[2][NB], pre[2][NB], prefix = 1;
 #pragma unroll
             for (int b = 0; b < NB; b++) {
                 const cm31 u = cm31_sub(p.den_k[b], cm31_scale(p.piy[b], pt.x));
                 const cm31 v = cm31_scale(p.pix[b], pt.y);
-                dinv[b] = sgn ? cm31_sub(u, v) : cm31_add(u, v);
-                uint64_t n2 = (uint64_t)dinv[b].a * dinv[b].a;
-                mac_wide(n2, dinv[b].b, dinv[b].b);
-                nrm[b] = reduce64_p(n2);
-                prefix = m31_mul(prefix, nrm[b]);
-                pre[b] = prefix;
+                dinv[0][b] = cm31_add(u, v);
+                dinv[1][b] = cm31_sub(u, v);
+#pragma unroll
+                for (int sg = 0; sg < 2; sg++) {
+                    uint64_t n2 = (uint64_t)dinv[sg][b].a * dinv[sg][b].a;
+                    mac_wide(n2, dinv[sg][b].b, dinv[sg][b].b);
+                    nrm[sg][b] = reduce64_p(n2);
+                    prefix = m31_mul(prefix, nrm[sg][b]);
+                    pre[sg][b] = prefix;
+                }
             }
             uint32_t inv = m31_inv(prefix);
 #pragma unroll
             for (int b = NB - 1; b >= 0; b--) {
-                const uint32_t ni = m31_mul(inv, b > 0 ? pre[b - 1] : 1u);  // 1 / norm
-                inv = m31_mul(inv, nrm[b]);
-                dinv[b] = {m31_mul(dinv[b].a, ni), m31_mul(m31_neg(dinv[b].b), ni)};
+#pragma unroll
+                for (int sg = 1; sg >= 0; sg--) {
+                    const uint32_t prev = sg == 1 ? pre[0][b] : (b > 0 ? pre[1][b - 1] : 1u);
+                    const uint32_t ni = m31_mul(inv, prev);  // 1 / norm
+                    inv = m31_mul(inv, nrm[sg][b]);
+                    dinv[sg][b] = {m31_mul(dinv[sg][b].a, ni), m31_mul(m31_neg(dinv[sg][b].b), ni)};
+                }
             }
-            qm31 acc = qm31_zero();
+            qm31 acc[2] = {qm31_zero(), qm31_zero()};
 #pragma unroll
             for (int b = 0; b < NB; b++) {
                 const qm31 ay = qm31_scale(p.a_sum[b], pt.y);
-                const qm31 lin = sgn ? qm31_sub(p.b_sum[b], ay) : qm31_add(p.b_sum[b], ay);
-                const qm31 nb = qm31_sub({{num[b][0], num[b][1]}, {num[b][2], num[b][3]}}, lin);
-                acc = qm31_add(acc, qm31_mul_cm31(nb, dinv[b]));
+                const qm31 lin[2] = {qm31_add(p.b_sum[b], ay), qm31_sub(p.b_sum[b], ay)};
+#pragma unroll
+                for (int sg = 0; sg < 2; sg++) {
+                    const qm31 nb =
+                        qm31_sub({{num[sg][b][0], num[sg][b][1]}, {num[sg][b][2], num[sg][b][3]}}, lin[sg]);
+                    acc[sg] = qm31_add(acc[sg], qm31_mul_cm31(nb, dinv[sg][b]));
+                }
             }
-            p.out[0][R] = acc.a.a;
-            p.out[1][R] = acc.a.b;
-            p.out[2][R] = acc.b.a;
-            p.out[3][R] = acc.b.b;
+            reinterpret_cast<uint2 *>(p.out[0])[k] = make_uint2(acc[0].a.a, acc[1].a.a);
+            reinterpret_cast<uint2 *>(p.out[1])[k] = make_uint2(acc[0].a.b, acc[1].a.b);
+            reinterpret_cast<uint2 *>(p.out[2])[k] = make_uint2(acc[0].b.a, acc[1].b.a);
+            reinterpret_cast<uint2 *>(p.out[3])[k] = make_uint2(acc[0].b.b, acc[1].b.b);
         }
     }
     tc::fence_before_sync();
@@ -475,17 +506,13 @@ __global__ void __launch_bounds__(QTC_THREADS, 2)
     if (warp == 12) tc::tmem_free(tmem, TM_COLS);
 }
 
-// Whether the tensor-core form takes a call: domains of at least 128 rows, 1..4
-// batches, and the byte matrix of W within QTC_MAX_B_BYTES; with the tunable at 1
-// (the default) only calls of two or more batches, where it measured faster (with one
-// batch the CUDA-core kernel's row pairs share their column loads and the tensor form
-// is no faster: 256 columns x 2^21, 0.49 vs 0.47 ms; 8 columns x 2^22, 0.13 vs 0.085
-// ms), with the tunable at 2 every call it can take.
+// Whether the tensor-core form takes a call: domains of at least 256 rows, 1..4
+// batches, and the byte matrix of W within QTC_MAX_B_BYTES (unless the
+// quotients_tensor_cores tunable is 0).
 bool quot_tc_eligible(uint32_t log_size, uint32_t n_batches, uint32_t n_cols) {
     const uint32_t c8 = (n_cols + 7) & ~7u;
-    const int mode = tunable(TUNE_QUOT_TENSOR);
-    return mode != 0 && (mode == 2 || n_batches >= 2) && log_size >= 7 && log_size <= 31 && n_batches >= 1 &&
-           n_batches <= 4 && n_cols >= 1 && qtc_b_bytes(c8, (int)n_batches) <= QTC_MAX_B_BYTES;
+    return tunable(TUNE_QUOT_TENSOR) != 0 && log_size >= 8 && log_size <= 31 && n_batches >= 1 && n_batches <= 4 &&
+           n_cols >= 1 && qtc_b_bytes(c8, (int)n_batches) <= QTC_MAX_B_BYTES;
 }
 
 template <int NB, bool COLS_ON_DEVICE, class PR>
@@ -500,9 +527,13 @@ int launch_quot_tc(const PR &pr, const uint32_t *const *dev_cols, uint32_t n_col
     });
     if (rc) return rc;
     const uint32_t c8 = (n_cols + 7) & ~7u;
-    const uint64_t tiles = 1ull << (log_size - 7), cap = 2ull * device_sm_count();
+    const uint64_t tiles = 1ull << (log_size - 8), cap = 2ull * device_sm_count();
     const unsigned gx = (unsigned)(tiles < cap ? tiles : cap);
-    kern<<<dim3(gx, jobs), QTC_THREADS, qtc_smem_bytes(c8, NB), st>>>(pr, dev_cols, n_cols);
+    // With 3 or 4 batches a CTA holds 256 TMEM columns: at least QTC_SMEM_FLOOR bytes of
+    // shared memory keep such CTAs to two an SM, so the SM's 512 columns always suffice.
+    size_t smem = qtc_smem_bytes(c8, NB);
+    if (NB >= 3 && smem < QTC_SMEM_FLOOR) smem = QTC_SMEM_FLOOR;
+    kern<<<dim3(gx, jobs), QTC_THREADS, smem, st>>>(pr, dev_cols, n_cols);
     STWO_LAUNCH_CHECK("quotients_tc_kernel");
     return STWO_OK;
 }
