@@ -164,7 +164,8 @@ int stwo_autotune(char *report, size_t report_cap);
  * fft_ept_strided (5 or 6), merkle_sub_threads (128, 256 or 512), merkle_sub_spread
  * (0..5: log2 of the bottom-level nodes each thread hashes), eval_at_point_groups_log
  * (2..4: log2 of the 8192-coefficient groups each eval_at_point CTA folds; 0, the
- * default, chooses per launch), quotients_tensor_cores (1, the default, or 0). */
+ * default, chooses per launch), quotients_tensor_cores (0, 1 = the default, 2) and
+ * composition_tensor_cores (0 = the default, 1). */
 int stwo_set_tunable(const char *name, int value);
 /* Diagnostics (no counterpart in the reference): the integer ceiling of the FFT. One
  * launch runs the FFT passes' own forward butterfly on register-resident operands
@@ -270,20 +271,30 @@ int stwo_accumulate_quotients(uint32_t half_coset_initial_index, uint32_t half_c
                               stwo_qm31 random_coeff, const stwo_spoint *sample_points, const uint32_t *batch_sizes,
                               const uint32_t *column_indices, const stwo_qm31 *sampled_values, uint32_t n_batches,
                               uint32_t *const *out4, void *stream);
-/* Domains of at least 2^8 rows with 1..4 batches (and 64 * n_batches * n_columns <=
+/* Calls of 2..4 batches over at least 2^16 rows (and 64 * n_batches * n_columns <=
  * 65536, columns rounded up to a multiple of 8) are computed on the tensor cores: the
  * batches' column sums as an 8-bit integer matrix product (column bytes x coefficient
- * bytes, 32-bit accumulators in TMEM); other calls, and every call after
- * stwo_set_tunable("quotients_tensor_cores", 0), on the CUDA cores. Both give the same
- * values. The tensor-core kernel's barrier waits give up after one second; *count
- * receives how many CTAs gave up since the last reset (0 unless the device
- * misbehaved; their rows are then not written). Synchronises the device. */
+ * bytes, 32-bit accumulators in TMEM); other calls on the CUDA cores.
+ * stwo_set_tunable("quotients_tensor_cores", v) moves the line: 0 for the CUDA cores
+ * always, 2 for the tensor cores wherever the form applies (one batch, and domains
+ * down to 2^8 rows). Every choice gives the same values. The tensor-core kernel's
+ * barrier waits give up after one second; *count receives how many CTAs gave up since
+ * the last reset (0 unless the device misbehaved; their rows are then not written).
+ * Synchronises the device. */
 int stwo_quotients_tc_faults(uint32_t *count, int reset);
 
-/* Wide-Fibonacci composition: out = den_inv * sum_i (c_i^2 + c_{i+1}^2 - c_{i+2}) * powers[N-3-i]. */
+/* Wide-Fibonacci composition: out = den_inv * sum_i (c_i^2 + c_{i+1}^2 - c_{i+2}) * powers[N-3-i].
+ * With stwo_set_tunable("composition_tensor_cores", 1), domains of at least 2^7 rows
+ * with 3..512 columns run on the tensor cores (regrouped per column as
+ * sum_j beta_j c_j^2 + gamma_j c_j, an 8-bit integer matrix product of the values' and
+ * squares' bytes with the weights' bytes), with the same values; by default (0) all
+ * run on the CUDA cores. stwo_composition_tc_faults reports the tensor-core kernel's
+ * CTAs that gave up a barrier wait after one second, as stwo_quotients_tc_faults
+ * does. */
 int stwo_wide_fib_composition(const uint32_t *const *trace, uint32_t n_columns, uint32_t ext_log_size,
                               const stwo_qm31 *coeff_powers, const uint32_t *den_inv, uint32_t *const *out4,
                               void *stream);
+int stwo_composition_tc_faults(uint32_t *count, int reset);
 
 /* =====================================================================
  * Tier 3: the wide-Fibonacci STARK prover and the proof server. The reference has
@@ -426,6 +437,11 @@ void stwo_server_destroy(stwo_prover_server *server);
  * kernels are in flight on its stream); it finishes normally. Returns
  * STWO_ERR_INVALID_ARGUMENT when no queued job has that id. */
 int stwo_server_cancel(stwo_prover_server *server, uint64_t job_id);
+/* paused != 0: workers start no queued job (running jobs finish; submissions are
+ * still accepted and queue timeouts still apply); paused == 0: they resume, taking the
+ * queue in arrival order. Holding the queue while a burst of jobs is submitted admits
+ * the burst at once, so that jobs of one shape are proved in full batches. */
+int stwo_server_pause(stwo_prover_server *server, int paused);
 /* Jobs that wait in the queue longer than queue_timeout_ms (0: no limit, the default)
  * are not started: their result carries STWO_ERR_TIMEOUT. Checked whenever a worker
  * looks for work and while stwo_server_poll waits. */

@@ -120,6 +120,7 @@ SIGNATURES = [
     ("stwo_merkle_commit_tree", C.c_int, [vp, vp, u32, u32, vp, vp]),
     ("stwo_accumulate_quotients", C.c_int, [u32, u32, u32, vp, u32, QM31, vp, vp, vp, vp, u32, vp, vp]),
     ("stwo_quotients_tc_faults", C.c_int, [C.POINTER(u32), C.c_int]),
+    ("stwo_composition_tc_faults", C.c_int, [C.POINTER(u32), C.c_int]),
     ("stwo_wide_fib_composition", C.c_int, [vp, u32, u32, vp, vp, vp, vp]),
     ("stwo_kernel_launches", u64, []),
     ("stwo_reserve_device_memory", C.c_int, [u64]),
@@ -151,6 +152,7 @@ SIGNATURES = [
     ("stwo_probe_m31_butterflies", C.c_int, [u32, vp, u64, C.POINTER(u64), vp]),
     ("stwo_server_destroy", None, [vp]),
     ("stwo_server_cancel", C.c_int, [vp, u64]),
+    ("stwo_server_pause", C.c_int, [vp, C.c_int]),
     ("stwo_server_set_queue_timeout", C.c_int, [vp, C.c_double]),
     ("stwo_debug_fail_allocations", None, [u32]),
 ]

@@ -122,8 +122,13 @@ int stwo_set_tunable(const char *name, int value) {
         set_tunable(TUNE_EAP_GROUPS_LOG, value);
         return STWO_OK;
     }
+    if (n == "composition_tensor_cores") {
+        STWO_REQUIRE(value == 0 || value == 1, STWO_ERR_INVALID_ARGUMENT, "composition_tensor_cores must be 0 or 1");
+        set_tunable(TUNE_COMP_TENSOR, value);
+        return STWO_OK;
+    }
     if (n == "quotients_tensor_cores") {
-        STWO_REQUIRE(value == 0 || value == 1, STWO_ERR_INVALID_ARGUMENT, "quotients_tensor_cores must be 0 or 1");
+        STWO_REQUIRE(value >= 0 && value <= 2, STWO_ERR_INVALID_ARGUMENT, "quotients_tensor_cores must be 0, 1 or 2");
         set_tunable(TUNE_QUOT_TENSOR, value);
         return STWO_OK;
     }

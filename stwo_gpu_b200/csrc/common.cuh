@@ -113,7 +113,8 @@ enum Tunable {
     TUNE_MERKLE_SUB_SPREAD,     // log2 bottom-level nodes per thread of that kernel (0..5)
     TUNE_EAP_GROUPS_LOG,        // eval_at_point: log2 groups of 8192 coefficients per CTA (2..4), 0 = per launch
     TUNE_FFT_MAX_STRIDED,       // FFT radix split: at most this many layers per strided pass (4..10)
-    TUNE_QUOT_TENSOR,           // DEEP quotients: 1 = on the tensor cores where the form applies, 0 = CUDA cores
+    TUNE_QUOT_TENSOR,           // DEEP quotients on the tensor cores: 0 never, 1 2+ batches over >= 2^16 rows, 2 always
+    TUNE_COMP_TENSOR,           // wide-Fibonacci composition on the tensor cores: 1 yes, 0 (default) no
     TUNE_COUNT
 };
 int tunable(Tunable t);

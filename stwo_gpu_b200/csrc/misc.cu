@@ -11,9 +11,11 @@
 // parameter block or a device table, each thread does two consecutive rows (8-byte
 // loads per column), and each QM31 coordinate of the sum accumulates unreduced
 // partial products in 64 bits, reduced once per row.
+#include <atomic>
 #include <memory>
 
 #include "common.cuh"
+#include "tc.cuh"
 
 namespace stwo {
 namespace {
@@ -153,8 +155,272 @@ __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant_
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Tensor-core form (tcgen05, 8-bit integer MMA). Regrouped by column, the constraint
+// sum is linear in each column's value and its square:
+//   sum_i P_i (c_i^2 + c_(i+1)^2 - c_(i+2)) = sum_j beta_j c_j^2 + gamma_j c_j,
+//   beta_j = P_j [j <= N-3] + P_(j-1) [1 <= j <= N-2],  gamma_j = -P_(j-2) [j >= 2],
+// with P_i = powers[N-3-i]. Over bytes (as in the tensor-core DEEP quotients) this is a
+// u8 x u8 product with K = 8 bytes a column (the value's 4 bytes, the square's 4) and
+// N = 16 (QM31 coordinate, byte j of the weight times 2^(8i)), exact in 32 bits. A CTA
+// of 13 warps streams tiles of 128 rows, 16 columns a stage:
+//  * warps 8-11 copy the values (4-byte asynchronous copies, 8 rows x 4 columns a warp
+//    copy) into the stage's value slabs and complete its "raw" barrier;
+//  * warps 4-7 read their row's values back, square them into the square slabs and
+//    complete the stage's "full" barrier;
+//  * one thread of warp 12 issues the stage's MMAs (one of 128 x 16 x 32 per 4
+//    columns: a value slab and its square slab) into one of two TMEM accumulators;
+//  * warps 0-3 read a tile's accumulator (a row a thread), release it, fold the four
+//    coordinates mod p and multiply by the row's denominator inverse.
+// Every barrier wait gives up after WTC_WAIT_NS or once another role gave up (counted
+// in g_comp_tc_faults).
+constexpr int WTC_STAGES = 4;
+constexpr uint32_t WTC_STAGE_BYTES = 128 * 16 * 8;  // 128 rows x 16 columns x (value, square)
+constexpr int WTC_THREADS = 13 * 32;
+constexpr uint64_t WTC_WAIT_NS = 1000000000ull;
+constexpr uint32_t WTC_MAX_COLS = 512;
+
+__device__ uint32_t g_comp_tc_faults;
+
+__host__ __device__ constexpr size_t wtc_b_bytes(uint32_t c4) { return (size_t)c4 * 2 * 16 * 16 / 4; }
+__host__ __device__ constexpr size_t wtc_smem_bytes(uint32_t c4) {
+    return (size_t)WTC_STAGES * WTC_STAGE_BYTES + wtc_b_bytes(c4) + (size_t)c4 * 8 + (3 * WTC_STAGES + 5) * 8 + 8;
+}
+
+__device__ __forceinline__ uint32_t qcoord(const qm31 &v, uint32_t q) {
+    return q == 0 ? v.a.a : q == 1 ? v.a.b : q == 2 ? v.b.a : v.b.b;
+}
+
+template <int CAP>
+__global__ void __launch_bounds__(WTC_THREADS, 2) wide_fib_tc_kernel(const __grid_constant__ WideFibParams<CAP> p) {
+    constexpr int N = 16;
+    constexpr uint32_t SLOT = 32, TM_COLS = 64;
+    constexpr uint32_t IDESC = tc::idesc_u8<128, N>();
+    extern __shared__ __align__(1024) uint8_t wsm[];
+    const uint32_t nc = p.n_cols, C4 = (nc + 3) & ~3u;
+    uint8_t *As = wsm;
+    uint8_t *Bs = wsm + WTC_STAGES * WTC_STAGE_BYTES;
+    const uint32_t **s_col = reinterpret_cast<const uint32_t **>(Bs + wtc_b_bytes(C4));
+    uint64_t *bars = reinterpret_cast<uint64_t *>(s_col + C4);
+    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + 3 * WTC_STAGES + 5);
+    volatile uint32_t *s_abort = s_tmem + 1;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, job = blockIdx.y;
+    const uint32_t *const *trace_dev = job_ptr(p.trace_dev, p.js, job);
+    const qm31 *powers = job_ptr(p.powers_dev, p.js, job);
+    const uint32_t *den_inv = job_ptr(p.den_inv, p.js, job);
+
+    for (uint32_t c = tid; c < C4; c += blockDim.x)
+        s_col[c] = c < nc ? (CAP == 1 ? trace_dev[c] : p.trace[c]) : nullptr;
+    if (tid == 0) *s_abort = 0;
+    // B: slab 2g (values of columns 4g .. 4g + 3) holds the bytes of gamma_j * 2^(8i),
+    // slab 2g + 1 (their squares) those of beta_j * 2^(8i); row n = 4 q + byte.
+    for (uint32_t it = tid; it < C4 * 8; it += blockDim.x) {
+        const uint32_t j = it >> 3, t = (it >> 2) & 1, q = it & 3;
+        uint32_t w = 0;
+        if (j < nc) {
+            if (t == 0) {
+                if (j >= 2) w = m31_neg(qcoord(powers[nc - 1 - j], q));  // -P_(j-2)
+            } else {
+                if (j + 3 <= nc) w = qcoord(powers[nc - 3 - j], q);                        // P_j
+                if (j >= 1 && j + 2 <= nc) w = m31_add(w, qcoord(powers[nc - 2 - j], q));  // P_(j-1)
+            }
+        }
+        uint8_t *dst = Bs + ((size_t)(2 * (j >> 2) + t) * N + q * 4) * 16 + (j & 3) * 4;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+#pragma unroll
+            for (int jb = 0; jb < 4; jb++) dst[jb * 16 + i] = (uint8_t)(w >> (8 * jb));
+            const uint64_t sh = (uint64_t)w << 8;  // w * 2^8 mod p
+            w = reduce_once((uint32_t)((sh & P) + (sh >> 31)));
+        }
+    }
+    tc::fence_async_smem();
+    const uint32_t bar0 = tc::smem_addr(bars);
+    auto RAW = [&](uint32_t s) { return bar0 + 8 * s; };
+    auto FULL = [&](uint32_t s) { return bar0 + 8 * (WTC_STAGES + s); };
+    auto EMPTY = [&](uint32_t s) { return bar0 + 8 * (2 * WTC_STAGES + s); };
+    auto TFULL = [&](uint32_t e) { return bar0 + 8 * (3 * WTC_STAGES + e); };
+    auto TEMPTY = [&](uint32_t e) { return bar0 + 8 * (3 * WTC_STAGES + 2 + e); };
+    const uint32_t DONE = bar0 + 8 * (3 * WTC_STAGES + 4);
+    if (tid == 0) {
+        for (int s = 0; s < WTC_STAGES; s++) {
+            tc::mbar_init(RAW(s), 128);   // the loader threads' copies
+            tc::mbar_init(FULL(s), 128);  // the squaring threads
+            tc::mbar_init(EMPTY(s), 1);   // one MMA commit
+        }
+        for (int e = 0; e < 2; e++) {
+            tc::mbar_init(TFULL(e), 1);
+            tc::mbar_init(TEMPTY(e), 128);
+        }
+        tc::mbar_init(DONE, 1);
+        tc::mbar_init_fence();
+    }
+    if (warp == 12) tc::tmem_alloc(s_tmem, TM_COLS);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *s_tmem;
+    const uint32_t n_tiles = 1u << (p.log_size - 7);
+    const uint32_t n_chunks = (C4 + 15) / 16;
+    auto give_up = [&]() {
+        if (!*s_abort) {
+            *s_abort = 1;
+            atomicAdd(&g_comp_tc_faults, 1u);
+        }
+    };
+
+    if (warp >= 8 && warp < 12) {
+        // ---- loaders: rows 32 wl .. 32 wl + 31 of the tile, 16 columns a stage
+        const uint32_t wl = warp - 8, ro = lane >> 2, co = lane & 3;
+        const uint32_t st0 = tc::smem_addr(As) + (32 * wl + ro) * 16 + co * 4;
+        uint32_t g = 0;
+        bool ok = true;
+        for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
+            const size_t row0 = (size_t)tile * 128 + 32 * wl + ro;
+            for (uint32_t kc = 0; kc < n_chunks; kc++, g++) {
+                const uint32_t s = g % WTC_STAGES;
+                if (!tc::mbar_wait(EMPTY(s), ((g / WTC_STAGES) & 1) ^ 1, s_abort, WTC_WAIT_NS)) {
+                    give_up();
+                    ok = false;
+                    break;
+                }
+                const uint32_t dst = st0 + s * WTC_STAGE_BYTES;
+#pragma unroll
+                for (int cg = 0; cg < 4; cg++) {
+                    const uint32_t c = kc * 16 + 4 * cg + co;
+                    if (c < nc) {
+                        const uint32_t *src = s_col[c] + row0;
+#pragma unroll
+                        for (int rg = 0; rg < 4; rg++) tc::cp_async4(dst + (2 * cg) * 2048 + rg * 128, src + 8 * rg);
+                    }
+                }
+                tc::cp_async_arrive(RAW(s));
+            }
+        }
+    } else if (warp >= 4 && warp < 8) {
+        // ---- squaring: row 32 (warp - 4) + lane of every stage
+        const uint32_t r = 32 * (warp - 4) + lane;
+        uint32_t g = 0;
+        bool ok = true;
+        for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
+            for (uint32_t kc = 0; kc < n_chunks; kc++, g++) {
+                const uint32_t s = g % WTC_STAGES;
+                if (!tc::mbar_wait(RAW(s), (g / WTC_STAGES) & 1, s_abort, WTC_WAIT_NS)) {
+                    give_up();
+                    ok = false;
+                    break;
+                }
+                uint8_t *stg = As + s * WTC_STAGE_BYTES + r * 16;
+#pragma unroll
+                for (int cg = 0; cg < 4; cg++) {
+                    const uint4 v = *reinterpret_cast<const uint4 *>(stg + (2 * cg) * 2048);
+                    *reinterpret_cast<uint4 *>(stg + (2 * cg + 1) * 2048) =
+                        make_uint4(m31_sqr(v.x), m31_sqr(v.y), m31_sqr(v.z), m31_sqr(v.w));
+                }
+                tc::fence_async_smem();
+                tc::mbar_arrive(FULL(s));
+            }
+        }
+    } else if (warp == 12) {
+        // ---- the MMA thread
+        if (lane == 0) {
+            const uint32_t a0 = tc::smem_addr(As), b0 = tc::smem_addr(Bs);
+            uint32_t g = 0;
+            bool ok = true;
+            for (uint32_t tl = 0, tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x, tl++) {
+                const uint32_t e = tl & 1;
+                if (!tc::mbar_wait(TEMPTY(e), ((tl >> 1) & 1) ^ 1, s_abort, WTC_WAIT_NS)) {
+                    give_up();
+                    break;
+                }
+                tc::fence_after_sync();
+                for (uint32_t kc = 0; kc < n_chunks; kc++, g++) {
+                    const uint32_t s = g % WTC_STAGES;
+                    if (!tc::mbar_wait(FULL(s), (g / WTC_STAGES) & 1, s_abort, WTC_WAIT_NS)) {
+                        give_up();
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_async_smem();
+                    tc::fence_after_sync();
+                    const uint32_t left = (C4 - kc * 16) / 4, nm = left < 4 ? left : 4u;
+                    for (uint32_t m = 0; m < nm; m++) {
+                        // value slab 2m and square slab 2m + 1: columns 4m .. 4m + 3 of the stage
+                        const uint64_t ad = tc::smem_desc(a0 + s * WTC_STAGE_BYTES + (2 * m) * 2048, 2048, 128);
+                        const uint64_t bd = tc::smem_desc(b0 + (kc * 8 + 2 * m) * N * 16, N * 16, 128);
+                        tc::mma_u8(tmem + e * SLOT, ad, bd, IDESC, (kc | m) != 0);
+                    }
+                    tc::commit(EMPTY(s));
+                }
+                if (ok) tc::commit(TFULL(e));
+            }
+            // every MMA issued here completes before the accumulators are freed
+            tc::commit(DONE);
+            if (!tc::mbar_wait(DONE, 0, nullptr, WTC_WAIT_NS)) give_up();
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: a row a thread, the tiles in turn through the two accumulators
+        const uint32_t row = 32 * warp + lane;
+        const uint32_t lane_base = tmem + ((32 * warp) << 16);
+        uint32_t *out[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) out[c] = job_ptr(p.out[c], p.js, job);
+        for (uint32_t tl = 0, tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, tl++) {
+            const uint32_t e = tl & 1;
+            if (!tc::mbar_wait(TFULL(e), (tl >> 1) & 1, s_abort, WTC_WAIT_NS)) {
+                give_up();
+                break;
+            }
+            tc::fence_after_sync();
+            uint32_t r[16];
+            tc::tmem_ld16(lane_base + e * SLOT, r);
+            tc::tmem_wait_ld();
+            tc::fence_before_sync();
+            tc::mbar_arrive(TEMPTY(e));
+            const uint32_t R = tile * 128 + row;
+            const uint32_t d = den_inv ? __ldg(den_inv + R) : p.den_half[R >> (p.log_size - 1)];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                // sum_j 2^(8j) T_j < 2^56: one fold leaves it below 2^31 + 2^25
+                const uint64_t t = (uint64_t)r[4 * q] + ((uint64_t)r[4 * q + 1] << 8) +
+                                   ((uint64_t)r[4 * q + 2] << 16) + ((uint64_t)r[4 * q + 3] << 24);
+                out[q][R] = m31_mul(reduce_once((uint32_t)(t & P) + (uint32_t)(t >> 31)), d);
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (warp == 12) tc::tmem_free(tmem, TM_COLS);
+}
+
+// The tensor-core form takes domains of at least 128 rows and 3..WTC_MAX_COLS columns
+// when the composition_tensor_cores tunable is 1. It is off by default: at the
+// prover's sizes it is no faster than wide_fib_kernel (256 columns x 2^21: 0.64 vs 0.61
+// ms, 2^20: 0.33 vs 0.31 ms; faster only near 2^17: 54 vs 62 us), since each column's
+// value and its square double the shared memory a loaded byte takes, halving the
+// copies in flight. It needs its dynamic shared memory limit raised once per device.
+template <int CAP>
+bool launch_wf_tc(const WideFibParams<CAP> &p, uint32_t jobs, cudaStream_t st) {
+    if (tunable(TUNE_COMP_TENSOR) != 1 || p.log_size < 7 || p.n_cols < 3 || p.n_cols > WTC_MAX_COLS) return false;
+    static std::atomic<uint64_t> attr_done{0};
+    if (once_per_device(attr_done, [] {
+            STWO_CUDA_TRY(cudaFuncSetAttribute(wide_fib_tc_kernel<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)wtc_smem_bytes(WTC_MAX_COLS)));
+            return (int)STWO_OK;
+        }) != STWO_OK)
+        return false;
+    const uint32_t c4 = (p.n_cols + 3) & ~3u;
+    const uint64_t tiles = 1ull << (p.log_size - 7), cap = 2ull * device_sm_count();
+    const unsigned gx = (unsigned)(tiles < cap ? tiles : cap);
+    wide_fib_tc_kernel<CAP><<<dim3(gx, jobs), WTC_THREADS, wtc_smem_bytes(c4), st>>>(p);
+    return true;
+}
+
 template <int CAP>
 void launch_wf(const WideFibParams<CAP> &p, uint64_t pairs, uint32_t jobs, cudaStream_t st) {
+    if (launch_wf_tc(p, jobs, st)) return;
     // Small domains: 64-thread CTAs so that more SMs share the rows.
     const uint32_t threads = pairs < (uint64_t)device_sm_count() * 256 ? 64 : 256;
     uint64_t blocks = (pairs + threads - 1) / threads, cap = (uint64_t)device_sm_count() * 32;
@@ -276,6 +542,16 @@ int wide_fib_dev_async(const uint32_t *const *trace_dev, uint32_t n_cols, uint32
 using namespace stwo;
 
 extern "C" {
+
+int stwo_composition_tc_faults(uint32_t *count, int reset) {
+    STWO_REQUIRE(count, STWO_ERR_INVALID_ARGUMENT, "null count");
+    STWO_CUDA_TRY(cudaMemcpyFromSymbol(count, g_comp_tc_faults, sizeof(uint32_t)));
+    if (reset) {
+        const uint32_t zero = 0;
+        STWO_CUDA_TRY(cudaMemcpyToSymbol(g_comp_tc_faults, &zero, sizeof(uint32_t)));
+    }
+    return STWO_OK;
+}
 
 int stwo_accumulate(uint32_t *const *left4, const uint32_t *const *right4, uint64_t n, void *stream) {
     return accumulate_async(left4, right4, n, as_stream(stream));

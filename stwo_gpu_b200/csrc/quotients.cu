@@ -507,12 +507,18 @@ __global__ void __launch_bounds__(QTC_THREADS, 2)
 }
 
 // Whether the tensor-core form takes a call: domains of at least 256 rows, 1..4
-// batches, and the byte matrix of W within QTC_MAX_B_BYTES (unless the
-// quotients_tensor_cores tunable is 0).
+// batches, and the byte matrix of W within QTC_MAX_B_BYTES. With the
+// quotients_tensor_cores tunable at 1 (the default) only calls of two or more batches
+// over at least 2^16 rows, where it measured faster (32 columns x 4 points: 2^16 14.3
+// vs 16.7 us, 2^19 34 vs 76 us, 2^22 0.19 vs 0.56 ms); one-batch calls (the prover's)
+// gain 0-19% at 2^18 and above and lose below, and its CTAs (13 warps, 70-140 KiB of
+// shared memory) crowd out concurrent jobs' kernels in the proof server, so they stay
+// on the CUDA cores. At 2 every call it can take; at 0 none.
 bool quot_tc_eligible(uint32_t log_size, uint32_t n_batches, uint32_t n_cols) {
     const uint32_t c8 = (n_cols + 7) & ~7u;
-    return tunable(TUNE_QUOT_TENSOR) != 0 && log_size >= 8 && log_size <= 31 && n_batches >= 1 && n_batches <= 4 &&
-           n_cols >= 1 && qtc_b_bytes(c8, (int)n_batches) <= QTC_MAX_B_BYTES;
+    const int mode = tunable(TUNE_QUOT_TENSOR);
+    return mode != 0 && (mode == 2 || (n_batches >= 2 && log_size >= 16)) && log_size >= 8 && log_size <= 31 &&
+           n_batches >= 1 && n_batches <= 4 && n_cols >= 1 && qtc_b_bytes(c8, (int)n_batches) <= QTC_MAX_B_BYTES;
 }
 
 template <int NB, bool COLS_ON_DEVICE, class PR>

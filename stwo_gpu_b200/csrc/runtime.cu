@@ -27,7 +27,7 @@ void clear_error() { g_last_error[0] = 0; }
 std::atomic<uint64_t> g_kernel_launches{0};
 
 namespace {
-std::atomic<int> g_tunables[TUNE_COUNT] = {{6}, {6}, {6}, {256}, {3}, {0}, {10}, {1}};
+std::atomic<int> g_tunables[TUNE_COUNT] = {{6}, {6}, {6}, {256}, {3}, {0}, {10}, {1}, {0}};
 }
 int tunable(Tunable t) { return g_tunables[t].load(std::memory_order_relaxed); }
 std::atomic<uint64_t> g_tunables_gen{0};

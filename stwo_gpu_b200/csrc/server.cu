@@ -54,6 +54,7 @@ struct stwo_prover_server {
     uint32_t *tw = nullptr, *itw = nullptr;
     uint64_t tree_size = 0;
     bool stopping = false;
+    bool paused = false;          // workers start no job while set (stwo_server_pause)
     double queue_timeout_ms = 0;  // 0: queued jobs wait without limit
     bool blocking_wait = true;  // workers yield their core while waiting on the device...
     uint32_t spin_us = 2000;    // ...after polling this long
@@ -214,7 +215,7 @@ struct stwo_prover_server {
             if (!have_next) {
                 bool got = false;
                 std::unique_lock<std::mutex> lock(mu);
-                cv_work.wait(lock, [&] { return stopping || (!pending.empty() && (got = take(j))); });
+                cv_work.wait(lock, [&] { return stopping || (!paused && !pending.empty() && (got = take(j))); });
                 if (!got) break;  // stopping, nothing taken
                 running++;
             }
@@ -298,7 +299,7 @@ struct stwo_prover_server {
                 std::lock_guard<std::mutex> lock(mu);
                 done.push_back(r);
                 expire();
-                if (cache.valid && !stopping)
+                if (cache.valid && !stopping && !paused)
                     for (auto it = pending.begin(); it != pending.end(); ++it) {
                         if (in_use - j.bytes + it->bytes > budget) continue;  // admission would pass it
                         if (same_shape(it->job, j.job) && it->bytes == j.bytes) {
@@ -516,6 +517,16 @@ int stwo_server_cancel(stwo_prover_server *s, uint64_t job_id) {
         s->pending.erase(it);
     }
     s->cv_done.notify_all();
+    return STWO_OK;
+}
+
+int stwo_server_pause(stwo_prover_server *s, int paused) {
+    STWO_REQUIRE(s, STWO_ERR_INVALID_ARGUMENT, "null server");
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->paused = paused != 0;
+    }
+    if (!paused) s->cv_work.notify_all();
     return STWO_OK;
 }
 

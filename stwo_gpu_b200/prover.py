@@ -195,6 +195,13 @@ class ProofServer:
         raises if the job is running, finished or unknown."""
         L.check(L.lib().stwo_server_cancel(self._s, job_id))
 
+    def pause(self):
+        """Workers start no queued job until resume() (running jobs finish)."""
+        L.check(L.lib().stwo_server_pause(self._s, 1))
+
+    def resume(self):
+        L.check(L.lib().stwo_server_pause(self._s, 0))
+
     def set_queue_timeout(self, ms):
         """Queued jobs that wait longer than ms (0: no limit) are not started; their
         results report STWO_ERR_TIMEOUT."""

@@ -539,6 +539,31 @@ def test_batch_of_one_shape_in_one_launch_sequence(stwo, shape, k):
     stwo.verify(proofs[-1], L, N, log_blowup=B, n_queries=q, pow_bits=pw)
 
 
+def test_server_pause_holds_the_queue():
+    """While paused, the server accepts jobs but starts none; resumed, its one worker
+    takes the first and the 9 queued jobs of its shape behind it as one batch (exactly
+    one launch sequence of 10), every proof equal to the job's proof alone."""
+    stwo = load_package()
+    L = stwo._lib
+    sh = (12, 64, 1, 3, 5)
+    seeds = [1700 + i for i in range(10)]
+    alone = [stwo.prove_wide_fib(job_of(sh), *stwo.wide_fib_inputs(sh[0], sd))[0] for sd in seeds]
+    with stwo.ProofServer(n_workers=1, device_budget_bytes=16 << 30, max_domain_log=21) as srv:
+        srv.pause()
+        for i, sd in enumerate(seeds):
+            srv.submit(i, job_of(sh), *stwo.wide_fib_inputs(sh[0], sd))
+        import time
+        time.sleep(0.2)
+        assert srv.stats()["pending"] == 10 and srv.stats()["running"] == 0
+        assert srv.poll(timeout_ms=0) == []
+        srv.resume()
+        got = _collect(srv, 10)
+        assert srv.batch_stats() == {"batches": 1, "batched_jobs": 10}
+    for i in range(10):
+        assert got[i]["status"] == L.OK, got[i]["error"]
+        assert got[i]["proof"] == alone[i], i
+
+
 @pytest.mark.parametrize("batch", ["32", "5"])
 def test_server_batches_queued_jobs_of_one_shape(batch, monkeypatch):
     """A worker that takes a small job also takes the queued jobs of its shape that

@@ -104,10 +104,11 @@ TC_SHAPES = [(7, 1, [1]), (8, 5, [3, 1, 5]), (8, 33, [33, 33]), (11, 100, [100])
 
 
 @pytest.mark.parametrize("log_size,ncols,batch_sizes", TC_SHAPES)
-@pytest.mark.parametrize("tc", [1, 0])
+@pytest.mark.parametrize("tc", [2, 1, 0])
 def test_quotients_tensor_and_cuda_cores(stwo, oracle, tensor_cores, log_size, ncols, batch_sizes, tc):
     """Both forms of the quotient kernel equal the oracle, through the native and the
-    reference-compatible entry points (tc: the quotients_tensor_cores tunable)."""
+    reference-compatible entry points (tc: the quotients_tensor_cores tunable; 2 takes
+    the tensor cores wherever the form applies)."""
     tensor_cores(tc)
     _faults(stwo)
     seed = 100 * log_size + ncols
@@ -130,16 +131,45 @@ def test_quotients_tensor_cores_full_size(stwo, tensor_cores):
     batches = [stwo.ColumnSampleBatch(random_circle_point(r), [(c, random_qm31(r)) for c in range(nc)])
                for _ in range(4)]
     got = {}
-    for tc in (1, 0):
+    for tc in (2, 0):
         tensor_cores(tc)
         got[tc] = B.accumulate_quotients(domain, cols, rc, batches).values.to_numpy()
-    for a, b in zip(got[1], got[0]):
+    for a, b in zip(got[2], got[0]):
         assert (a == b).all()
     assert _faults(stwo) == 0
 
 
-@pytest.mark.parametrize("n_cols,log_size", [(3, 1), (8, 5), (64, 13), (256, 8)])
-def test_wide_fib_composition(stwo, oracle, n_cols, log_size):
+@pytest.fixture
+def comp_tensor_cores(stwo):
+    """Sets the composition_tensor_cores tunable for one test and restores the default (0)."""
+    L = stwo._lib
+
+    def set_(v):
+        L.check(L.lib().stwo_set_tunable(b"composition_tensor_cores", v))
+    yield set_
+    set_(0)
+
+
+def _comp_faults(stwo):
+    import ctypes as C
+    n = C.c_uint32()
+    stwo._lib.check(stwo._lib.lib().stwo_composition_tc_faults(C.byref(n), 1))
+    return n.value
+
+
+# below one tile (2^6 rows: the CUDA cores), the fewest columns (3), columns not a
+# multiple of 4 or 16, the most the tensor form takes (512) and one past it (513).
+@pytest.mark.parametrize("n_cols,log_size", [(3, 1), (8, 5), (64, 13), (256, 8), (3, 7), (5, 9), (130, 10),
+                                             (512, 8), (513, 8), (256, 12)])
+@pytest.mark.parametrize("tc", [1, 0])
+def test_wide_fib_composition(stwo, oracle, comp_tensor_cores, n_cols, log_size, tc):
+    comp_tensor_cores(tc)
+    _comp_faults(stwo)
+    _wide_fib_composition(stwo, oracle, n_cols, log_size)
+    assert _comp_faults(stwo) == 0
+
+
+def _wide_fib_composition(stwo, oracle, n_cols, log_size):
     L = stwo._lib
     r = rng(n_cols + log_size)
     trace = [m31(r, 1 << log_size) for _ in range(n_cols)]
