@@ -482,7 +482,11 @@ __global__ void __launch_bounds__(QTC_THREADS, 2)
                     dinv[sg][b] = {m31_mul(dinv[sg][b].a, ni), m31_mul(m31_neg(dinv[sg][b].b), ni)};
                 }
             }
-            qm31 acc[2] = {qm31_zero(), qm31_zero()};
+            // sum_b (num_b - lin_b) * dinv_b, the QM31 x CM31 products accumulated unreduced
+            // in 64 bits: (x + y i)(c + d i) = (x c + y (p - d)) + (x d + y c) i; two
+            // products a batch and coordinate, folded after every second batch (a folded
+            // sum plus four products of canonical values stays below 2^64).
+            uint64_t ac[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
 #pragma unroll
             for (int b = 0; b < NB; b++) {
                 const qm31 ay = qm31_scale(p.a_sum[b], pt.y);
@@ -491,13 +495,19 @@ __global__ void __launch_bounds__(QTC_THREADS, 2)
                 for (int sg = 0; sg < 2; sg++) {
                     const qm31 nb =
                         qm31_sub({{num[sg][b][0], num[sg][b][1]}, {num[sg][b][2], num[sg][b][3]}}, lin[sg]);
-                    acc[sg] = qm31_add(acc[sg], qm31_mul_cm31(nb, dinv[sg][b]));
+                    const uint32_t c = dinv[sg][b].a, d = dinv[sg][b].b, nd = P - d;
+                    ac[sg][0] = mac64(mac64(ac[sg][0], nb.a.a, c), nb.a.b, nd);
+                    ac[sg][1] = mac64(mac64(ac[sg][1], nb.a.a, d), nb.a.b, c);
+                    ac[sg][2] = mac64(mac64(ac[sg][2], nb.b.a, c), nb.b.b, nd);
+                    ac[sg][3] = mac64(mac64(ac[sg][3], nb.b.a, d), nb.b.b, c);
+                    if (b & 1)
+#pragma unroll
+                        for (int q = 0; q < 4; q++) ac[sg][q] = fold64_fma(ac[sg][q], 2u);
                 }
             }
-            reinterpret_cast<uint2 *>(p.out[0])[k] = make_uint2(acc[0].a.a, acc[1].a.a);
-            reinterpret_cast<uint2 *>(p.out[1])[k] = make_uint2(acc[0].a.b, acc[1].a.b);
-            reinterpret_cast<uint2 *>(p.out[2])[k] = make_uint2(acc[0].b.a, acc[1].b.a);
-            reinterpret_cast<uint2 *>(p.out[3])[k] = make_uint2(acc[0].b.b, acc[1].b.b);
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                reinterpret_cast<uint2 *>(p.out[q])[k] = make_uint2(reduce64_p(ac[0][q]), reduce64_p(ac[1][q]));
         }
     }
     tc::fence_before_sync();
