@@ -285,10 +285,9 @@ int stwo_quotients_tc_faults(uint32_t *count, int reset);
 
 /* Wide-Fibonacci composition: out = den_inv * sum_i (c_i^2 + c_{i+1}^2 - c_{i+2}) * powers[N-3-i].
  * With stwo_set_tunable("composition_tensor_cores", 1), domains of at least 2^7 rows
- * with 3..512 columns run on the tensor cores (regrouped per column as
- * sum_j beta_j c_j^2 + gamma_j c_j, an 8-bit integer matrix product of the values' and
- * squares' bytes with the weights' bytes), with the same values; by default (0) all
- * run on the CUDA cores. stwo_composition_tc_faults reports the tensor-core kernel's
+ * with 3..1024 columns run on the tensor cores (the constraint values' bytes times the
+ * weights' bytes, an 8-bit integer matrix product), with the same values; by default
+ * (0) all run on the CUDA cores. stwo_composition_tc_faults reports the tensor-core kernel's
  * CTAs that gave up a barrier wait after one second, as stwo_quotients_tc_faults
  * does. */
 int stwo_wide_fib_composition(const uint32_t *const *trace, uint32_t n_columns, uint32_t ext_log_size,

@@ -156,35 +156,38 @@ __global__ void __launch_bounds__(256, 4) wide_fib_kernel(const __grid_constant_
 }
 
 // ---------------------------------------------------------------------------------
-// Tensor-core form (tcgen05, 8-bit integer MMA). Regrouped by column, the constraint
-// sum is linear in each column's value and its square:
-//   sum_i P_i (c_i^2 + c_(i+1)^2 - c_(i+2)) = sum_j beta_j c_j^2 + gamma_j c_j,
-//   beta_j = P_j [j <= N-3] + P_(j-1) [1 <= j <= N-2],  gamma_j = -P_(j-2) [j >= 2],
-// with P_i = powers[N-3-i]. Over bytes (as in the tensor-core DEEP quotients) this is a
-// u8 x u8 product with K = 8 bytes a column (the value's 4 bytes, the square's 4) and
-// N = 16 (QM31 coordinate, byte j of the weight times 2^(8i)), exact in 32 bits. A CTA
-// of 13 warps streams tiles of 128 rows, 16 columns a stage:
-//  * warps 8-11 copy the values (4-byte asynchronous copies, 8 rows x 4 columns a warp
-//    copy) into the stage's value slabs and complete its "raw" barrier;
-//  * warps 4-7 read their row's values back, square them into the square slabs and
-//    complete the stage's "full" barrier;
-//  * one thread of warp 12 issues the stage's MMAs (one of 128 x 16 x 32 per 4
-//    columns: a value slab and its square slab) into one of two TMEM accumulators;
+// Tensor-core form (tcgen05, 8-bit integer MMA). The sum over constraints
+// sum_i P_i e_i (e_i = c_i^2 + c_(i+1)^2 - c_(i+2), P_i = powers[N-3-i]) is, over bytes
+// (as in the tensor-core DEEP quotients), a u8 x u8 product with K = 4 bytes a
+// constraint and N = 16 (QM31 coordinate, byte j of P_i.q * 2^(8b)), exact in 32 bits.
+// A CTA of 13 warps streams tiles of 128 rows, 32 constraints a stage:
+//  * warps 8-11 copy columns 32 kc .. 32 kc + 31 of the tile (4-byte asynchronous
+//    copies, 8 rows x 4 columns a warp copy) into the stage's slabs (slab g: columns
+//    4g .. 4g + 3, row r at r * 16 bytes), and columns 32 kc + 32, 32 kc + 33 into the
+//    stage's look-ahead rows, and complete its "raw" barrier;
+//  * warps 4-7 read their row's 34 values back and overwrite value i with e_i (value
+//    i is no longer needed once e_i is known), then complete the stage's "full" barrier;
+//  * one thread of warp 12 issues the stage's four MMAs (128 x 16 x 32) into one of two
+//    TMEM accumulators;
 //  * warps 0-3 read a tile's accumulator (a row a thread), release it, fold the four
 //    coordinates mod p and multiply by the row's denominator inverse.
-// Every barrier wait gives up after WTC_WAIT_NS or once another role gave up (counted
-// in g_comp_tc_faults).
-constexpr int WTC_STAGES = 4;
-constexpr uint32_t WTC_STAGE_BYTES = 128 * 16 * 8;  // 128 rows x 16 columns x (value, square)
+// Constraints past N-3 read stale values and have zero weights. Every barrier wait
+// gives up after WTC_WAIT_NS or once another role gave up (counted in
+// g_comp_tc_faults).
+constexpr int WTC_STAGES = 3;
+constexpr uint32_t WTC_STAGE_BYTES = 128 * 32 * 4;  // 128 rows x 32 values (then constraints)
+constexpr uint32_t WTC_LA_BYTES = 2 * 128 * 4;      // the next two columns of the 128 rows
 constexpr int WTC_THREADS = 13 * 32;
 constexpr uint64_t WTC_WAIT_NS = 1000000000ull;
-constexpr uint32_t WTC_MAX_COLS = 512;
+constexpr uint32_t WTC_MAX_COLS = 1024;
 
 __device__ uint32_t g_comp_tc_faults;
 
-__host__ __device__ constexpr size_t wtc_b_bytes(uint32_t c4) { return (size_t)c4 * 2 * 16 * 16 / 4; }
-__host__ __device__ constexpr size_t wtc_smem_bytes(uint32_t c4) {
-    return (size_t)WTC_STAGES * WTC_STAGE_BYTES + wtc_b_bytes(c4) + (size_t)c4 * 8 + (3 * WTC_STAGES + 5) * 8 + 8;
+__host__ __device__ constexpr uint32_t wtc_chunks(uint32_t nc) { return (nc - 2 + 31) / 32; }
+__host__ __device__ constexpr size_t wtc_b_bytes(uint32_t nc) { return (size_t)wtc_chunks(nc) * 32 * 4 * 16; }
+__host__ __device__ constexpr size_t wtc_smem_bytes(uint32_t nc) {
+    return (size_t)WTC_STAGES * (WTC_STAGE_BYTES + WTC_LA_BYTES) + wtc_b_bytes(nc) + (size_t)nc * 8 +
+           (3 * WTC_STAGES + 5) * 8 + 8;
 }
 
 __device__ __forceinline__ uint32_t qcoord(const qm31 &v, uint32_t q) {
@@ -192,16 +195,17 @@ __device__ __forceinline__ uint32_t qcoord(const qm31 &v, uint32_t q) {
 }
 
 template <int CAP>
-__global__ void __launch_bounds__(WTC_THREADS, 2) wide_fib_tc_kernel(const __grid_constant__ WideFibParams<CAP> p) {
+__global__ void __launch_bounds__(WTC_THREADS, 3) wide_fib_tc_kernel(const __grid_constant__ WideFibParams<CAP> p) {
     constexpr int N = 16;
     constexpr uint32_t SLOT = 32, TM_COLS = 64;
     constexpr uint32_t IDESC = tc::idesc_u8<128, N>();
     extern __shared__ __align__(1024) uint8_t wsm[];
-    const uint32_t nc = p.n_cols, C4 = (nc + 3) & ~3u;
+    const uint32_t nc = p.n_cols, n_chunks = wtc_chunks(nc);
     uint8_t *As = wsm;
-    uint8_t *Bs = wsm + WTC_STAGES * WTC_STAGE_BYTES;
-    const uint32_t **s_col = reinterpret_cast<const uint32_t **>(Bs + wtc_b_bytes(C4));
-    uint64_t *bars = reinterpret_cast<uint64_t *>(s_col + C4);
+    uint32_t *LA = reinterpret_cast<uint32_t *>(wsm + WTC_STAGES * WTC_STAGE_BYTES);
+    uint8_t *Bs = wsm + WTC_STAGES * (WTC_STAGE_BYTES + WTC_LA_BYTES);
+    const uint32_t **s_col = reinterpret_cast<const uint32_t **>(Bs + wtc_b_bytes(nc));
+    uint64_t *bars = reinterpret_cast<uint64_t *>(s_col + nc);
     uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + 3 * WTC_STAGES + 5);
     volatile uint32_t *s_abort = s_tmem + 1;
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, job = blockIdx.y;
@@ -209,27 +213,18 @@ __global__ void __launch_bounds__(WTC_THREADS, 2) wide_fib_tc_kernel(const __gri
     const qm31 *powers = job_ptr(p.powers_dev, p.js, job);
     const uint32_t *den_inv = job_ptr(p.den_inv, p.js, job);
 
-    for (uint32_t c = tid; c < C4; c += blockDim.x)
-        s_col[c] = c < nc ? (CAP == 1 ? trace_dev[c] : p.trace[c]) : nullptr;
+    for (uint32_t c = tid; c < nc; c += blockDim.x) s_col[c] = CAP == 1 ? trace_dev[c] : p.trace[c];
     if (tid == 0) *s_abort = 0;
-    // B: slab 2g (values of columns 4g .. 4g + 3) holds the bytes of gamma_j * 2^(8i),
-    // slab 2g + 1 (their squares) those of beta_j * 2^(8i); row n = 4 q + byte.
-    for (uint32_t it = tid; it < C4 * 8; it += blockDim.x) {
-        const uint32_t j = it >> 3, t = (it >> 2) & 1, q = it & 3;
-        uint32_t w = 0;
-        if (j < nc) {
-            if (t == 0) {
-                if (j >= 2) w = m31_neg(qcoord(powers[nc - 1 - j], q));  // -P_(j-2)
-            } else {
-                if (j + 3 <= nc) w = qcoord(powers[nc - 3 - j], q);                        // P_j
-                if (j >= 1 && j + 2 <= nc) w = m31_add(w, qcoord(powers[nc - 2 - j], q));  // P_(j-1)
-            }
-        }
-        uint8_t *dst = Bs + ((size_t)(2 * (j >> 2) + t) * N + q * 4) * 16 + (j & 3) * 4;
+    // B: slab g holds constraints 4g .. 4g + 3; row n = 4 q + byte of P_i.q * 2^(8b),
+    // bytes b of constraint i at (i % 4) * 4 + b
+    for (uint32_t it = tid; it < n_chunks * 32 * 4; it += blockDim.x) {
+        const uint32_t i = it >> 2, q = it & 3;
+        uint32_t w = i + 3 <= nc ? qcoord(powers[nc - 3 - i], q) : 0u;
+        uint8_t *dst = Bs + ((size_t)(i >> 2) * N + q * 4) * 16 + (i & 3) * 4;
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
+        for (int b = 0; b < 4; b++) {
 #pragma unroll
-            for (int jb = 0; jb < 4; jb++) dst[jb * 16 + i] = (uint8_t)(w >> (8 * jb));
+            for (int jb = 0; jb < 4; jb++) dst[jb * 16 + b] = (uint8_t)(w >> (8 * jb));
             const uint64_t sh = (uint64_t)w << 8;  // w * 2^8 mod p
             w = reduce_once((uint32_t)((sh & P) + (sh >> 31)));
         }
@@ -245,7 +240,7 @@ __global__ void __launch_bounds__(WTC_THREADS, 2) wide_fib_tc_kernel(const __gri
     if (tid == 0) {
         for (int s = 0; s < WTC_STAGES; s++) {
             tc::mbar_init(RAW(s), 128);   // the loader threads' copies
-            tc::mbar_init(FULL(s), 128);  // the squaring threads
+            tc::mbar_init(FULL(s), 128);  // the constraint threads
             tc::mbar_init(EMPTY(s), 1);   // one MMA commit
         }
         for (int e = 0; e < 2; e++) {
@@ -261,7 +256,6 @@ __global__ void __launch_bounds__(WTC_THREADS, 2) wide_fib_tc_kernel(const __gri
     tc::fence_after_sync();
     const uint32_t tmem = *s_tmem;
     const uint32_t n_tiles = 1u << (p.log_size - 7);
-    const uint32_t n_chunks = (C4 + 15) / 16;
     auto give_up = [&]() {
         if (!*s_abort) {
             *s_abort = 1;
@@ -270,9 +264,10 @@ __global__ void __launch_bounds__(WTC_THREADS, 2) wide_fib_tc_kernel(const __gri
     };
 
     if (warp >= 8 && warp < 12) {
-        // ---- loaders: rows 32 wl .. 32 wl + 31 of the tile, 16 columns a stage
+        // ---- loaders: rows 32 wl .. 32 wl + 31 of the tile
         const uint32_t wl = warp - 8, ro = lane >> 2, co = lane & 3;
         const uint32_t st0 = tc::smem_addr(As) + (32 * wl + ro) * 16 + co * 4;
+        const uint32_t la0 = tc::smem_addr(LA) + (32 * wl + lane) * 4;
         uint32_t g = 0;
         bool ok = true;
         for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
@@ -286,19 +281,25 @@ __global__ void __launch_bounds__(WTC_THREADS, 2) wide_fib_tc_kernel(const __gri
                 }
                 const uint32_t dst = st0 + s * WTC_STAGE_BYTES;
 #pragma unroll
-                for (int cg = 0; cg < 4; cg++) {
-                    const uint32_t c = kc * 16 + 4 * cg + co;
+                for (int cg = 0; cg < 8; cg++) {
+                    const uint32_t c = kc * 32 + 4 * cg + co;
                     if (c < nc) {
                         const uint32_t *src = s_col[c] + row0;
 #pragma unroll
-                        for (int rg = 0; rg < 4; rg++) tc::cp_async4(dst + (2 * cg) * 2048 + rg * 128, src + 8 * rg);
+                        for (int rg = 0; rg < 4; rg++) tc::cp_async4(dst + cg * 2048 + rg * 128, src + 8 * rg);
                     }
+                }
+#pragma unroll
+                for (int t = 0; t < 2; t++) {
+                    const uint32_t c = kc * 32 + 32 + t;
+                    if (c < nc)
+                        tc::cp_async4(la0 + s * WTC_LA_BYTES + t * 512, s_col[c] + (size_t)tile * 128 + 32 * wl + lane);
                 }
                 tc::cp_async_arrive(RAW(s));
             }
         }
     } else if (warp >= 4 && warp < 8) {
-        // ---- squaring: row 32 (warp - 4) + lane of every stage
+        // ---- constraints: row 32 (warp - 4) + lane of every stage, in place
         const uint32_t r = 32 * (warp - 4) + lane;
         uint32_t g = 0;
         bool ok = true;
@@ -311,11 +312,29 @@ __global__ void __launch_bounds__(WTC_THREADS, 2) wide_fib_tc_kernel(const __gri
                     break;
                 }
                 uint8_t *stg = As + s * WTC_STAGE_BYTES + r * 16;
+                uint32_t a[34];
 #pragma unroll
-                for (int cg = 0; cg < 4; cg++) {
-                    const uint4 v = *reinterpret_cast<const uint4 *>(stg + (2 * cg) * 2048);
-                    *reinterpret_cast<uint4 *>(stg + (2 * cg + 1) * 2048) =
-                        make_uint4(m31_sqr(v.x), m31_sqr(v.y), m31_sqr(v.z), m31_sqr(v.w));
+                for (int cg = 0; cg < 8; cg++) {
+                    const uint4 v = *reinterpret_cast<const uint4 *>(stg + cg * 2048);
+                    a[4 * cg] = v.x;
+                    a[4 * cg + 1] = v.y;
+                    a[4 * cg + 2] = v.z;
+                    a[4 * cg + 3] = v.w;
+                }
+                a[32] = LA[(s * WTC_LA_BYTES) / 4 + r];
+                a[33] = LA[(s * WTC_LA_BYTES + 512) / 4 + r];
+                uint32_t sp = m31_sqr(a[0]), sc = m31_sqr(a[1]);
+#pragma unroll
+                for (int cg = 0; cg < 8; cg++) {
+                    uint32_t e4[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const uint32_t x = a[4 * cg + u + 2];
+                        e4[u] = m31_sub(m31_add(sp, sc), x);
+                        sp = sc;
+                        sc = m31_sqr(x);
+                    }
+                    *reinterpret_cast<uint4 *>(stg + cg * 2048) = make_uint4(e4[0], e4[1], e4[2], e4[3]);
                 }
                 tc::fence_async_smem();
                 tc::mbar_arrive(FULL(s));
@@ -343,9 +362,9 @@ __global__ void __launch_bounds__(WTC_THREADS, 2) wide_fib_tc_kernel(const __gri
                     }
                     tc::fence_async_smem();
                     tc::fence_after_sync();
-                    const uint32_t left = (C4 - kc * 16) / 4, nm = left < 4 ? left : 4u;
-                    for (uint32_t m = 0; m < nm; m++) {
-                        // value slab 2m and square slab 2m + 1: columns 4m .. 4m + 3 of the stage
+#pragma unroll
+                    for (uint32_t m = 0; m < 4; m++) {
+                        // slabs 2m, 2m + 1: constraints 8m .. 8m + 7 of the stage
                         const uint64_t ad = tc::smem_desc(a0 + s * WTC_STAGE_BYTES + (2 * m) * 2048, 2048, 128);
                         const uint64_t bd = tc::smem_desc(b0 + (kc * 8 + 2 * m) * N * 16, N * 16, 128);
                         tc::mma_u8(tmem + e * SLOT, ad, bd, IDESC, (kc | m) != 0);
@@ -396,11 +415,12 @@ __global__ void __launch_bounds__(WTC_THREADS, 2) wide_fib_tc_kernel(const __gri
 }
 
 // The tensor-core form takes domains of at least 128 rows and 3..WTC_MAX_COLS columns
-// when the composition_tensor_cores tunable is 1. It is off by default: at the
-// prover's sizes it is no faster than wide_fib_kernel (256 columns x 2^21: 0.64 vs 0.61
-// ms, 2^20: 0.33 vs 0.31 ms; faster only near 2^17: 54 vs 62 us), since each column's
-// value and its square double the shared memory a loaded byte takes, halving the
-// copies in flight. It needs its dynamic shared memory limit raised once per device.
+// when the composition_tensor_cores tunable is 1. It is off by default: against
+// wide_fib_kernel it measured 2-4% faster at the prover's sizes (256 columns x 2^21:
+// 0.578 vs 0.604 ms, 2^20: 0.307 vs 0.313 ms), 19% faster near 2^17, and slower with few
+// columns (16 x 2^22: 0.140 vs 0.100 ms) or a 64 KiB weight matrix (1024 x 2^20: 1.31
+// vs 1.21 ms), too little for its 13-warp CTAs in the proof server's concurrent mix. It
+// needs its dynamic shared memory limit raised once per device.
 template <int CAP>
 bool launch_wf_tc(const WideFibParams<CAP> &p, uint32_t jobs, cudaStream_t st) {
     if (tunable(TUNE_COMP_TENSOR) != 1 || p.log_size < 7 || p.n_cols < 3 || p.n_cols > WTC_MAX_COLS) return false;
@@ -411,10 +431,9 @@ bool launch_wf_tc(const WideFibParams<CAP> &p, uint32_t jobs, cudaStream_t st) {
             return (int)STWO_OK;
         }) != STWO_OK)
         return false;
-    const uint32_t c4 = (p.n_cols + 3) & ~3u;
     const uint64_t tiles = 1ull << (p.log_size - 7), cap = 2ull * device_sm_count();
     const unsigned gx = (unsigned)(tiles < cap ? tiles : cap);
-    wide_fib_tc_kernel<CAP><<<dim3(gx, jobs), WTC_THREADS, wtc_smem_bytes(c4), st>>>(p);
+    wide_fib_tc_kernel<CAP><<<dim3(gx, jobs), WTC_THREADS, wtc_smem_bytes(p.n_cols), st>>>(p);
     return true;
 }
 

@@ -157,10 +157,11 @@ def _comp_faults(stwo):
     return n.value
 
 
-# below one tile (2^6 rows: the CUDA cores), the fewest columns (3), columns not a
-# multiple of 4 or 16, the most the tensor form takes (512) and one past it (513).
-@pytest.mark.parametrize("n_cols,log_size", [(3, 1), (8, 5), (64, 13), (256, 8), (3, 7), (5, 9), (130, 10),
-                                             (512, 8), (513, 8), (256, 12)])
+# below one tile (2^6 rows: the CUDA cores), the fewest columns (3), constraint counts
+# that are not a multiple of 32 (a stage), the most the tensor form takes (1024) and
+# one past it (1025).
+@pytest.mark.parametrize("n_cols,log_size", [(3, 1), (8, 5), (64, 13), (256, 8), (3, 7), (5, 9), (34, 8),
+                                             (35, 8), (130, 10), (512, 8), (1024, 7), (1025, 7), (256, 12)])
 @pytest.mark.parametrize("tc", [1, 0])
 def test_wide_fib_composition(stwo, oracle, comp_tensor_cores, n_cols, log_size, tc):
     comp_tensor_cores(tc)
