@@ -143,17 +143,17 @@ __global__ void __launch_bounds__(BI_THREADS) batch_inverse_qm31_norm_kernel(con
     const uint64_t base = warp_global * (32 * BI_PER_THREAD) + lane;
     qm31 v[BI_PER_THREAD];
     cm31 nrm[BI_PER_THREAD];
-    uint32_t pre[BI_PER_THREAD];
+    uint32_t pre[BI_PER_THREAD], mag[BI_PER_THREAD];
     uint32_t run = 1;
 #pragma unroll
     for (int i = 0; i < BI_PER_THREAD; i++) {
         const uint64_t idx = base + (uint64_t)i * 32;
         v[i] = (idx < n) ? src[idx] : qm31_one();
-        const cm31 a2 = cm31_mul(v[i].a, v[i].a), b2 = cm31_mul(v[i].b, v[i].b);
+        const cm31 a2 = cm31_sqr(v[i].a), b2 = cm31_sqr(v[i].b);
         const cm31 rb2 = {m31_sub(m31_add(b2.a, b2.a), b2.b), m31_add(m31_add(b2.b, b2.b), b2.a)};  // R b^2
         nrm[i] = cm31_sub(a2, rb2);
-        const uint32_t m = reduce64_p((uint64_t)nrm[i].a * nrm[i].a + (uint64_t)nrm[i].b * nrm[i].b);
-        run = m31_mul(run, m);
+        mag[i] = reduce64_p((uint64_t)nrm[i].a * nrm[i].a + (uint64_t)nrm[i].b * nrm[i].b);
+        run = m31_mul(run, mag[i]);
         pre[i] = run;
     }
     // Inclusive scans of the lanes' norm products, forward (prefix) and backward (suffix).
@@ -174,9 +174,16 @@ __global__ void __launch_bounds__(BI_THREADS) batch_inverse_qm31_norm_kernel(con
     for (int i = BI_PER_THREAD - 1; i >= 0; i--) {
         const uint32_t minv = i > 0 ? m31_mul(r, pre[i - 1]) : r;  // 1 / |N_i|^2
         const uint64_t idx = base + (uint64_t)i * 32;
-        r = m31_mul(r, reduce64_p((uint64_t)nrm[i].a * nrm[i].a + (uint64_t)nrm[i].b * nrm[i].b));
-        const cm31 ninv = {m31_mul(nrm[i].a, minv), m31_neg(m31_mul(nrm[i].b, minv))};  // 1 / N_i
-        if (idx < n) dst[idx] = {cm31_mul(v[i].a, ninv), cm31_neg(cm31_mul(v[i].b, ninv))};
+        r = m31_mul(r, mag[i]);
+        // 1 / N_i = c + d i with c = N.a / |N|^2, d = -N.b / |N|^2; the products
+        // (x + y i)(c + d i) = (x c + y (p - d)) + (x d + y c) i reduced once each
+        const uint32_t c = m31_mul(nrm[i].a, minv), nd = m31_mul(nrm[i].b, minv), d = m31_neg(nd);
+        const qm31 z = v[i];
+        const cm31 lo = {reduce64_p((uint64_t)z.a.a * c + (uint64_t)z.a.b * nd),
+                         reduce64_p((uint64_t)z.a.a * d + (uint64_t)z.a.b * c)};
+        const cm31 hi = {reduce64_p((uint64_t)z.b.a * c + (uint64_t)z.b.b * nd),
+                         reduce64_p((uint64_t)z.b.a * d + (uint64_t)z.b.b * c)};
+        if (idx < n) dst[idx] = {lo, cm31_neg(hi)};
     }
 }
 

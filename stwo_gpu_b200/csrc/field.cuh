@@ -127,6 +127,11 @@ __host__ __device__ __forceinline__ cm31 cm31_mul(cm31 x, cm31 y) {
     return {m31_sub(m31_mul(x.a, y.a), m31_mul(x.b, y.b)), m31_add(m31_mul(x.a, y.b), m31_mul(x.b, y.a))};
 }
 __host__ __device__ __forceinline__ cm31 cm31_scale(cm31 x, uint32_t s) { return {m31_mul(x.a, s), m31_mul(x.b, s)}; }
+// (a + b i)^2 = (a + b)(a - b) + 2ab i: two products.
+__host__ __device__ __forceinline__ cm31 cm31_sqr(cm31 x) {
+    const uint32_t ab = m31_mul(x.a, x.b);
+    return {m31_mul(m31_add(x.a, x.b), m31_sub(x.a, x.b)), m31_add(ab, ab)};
+}
 __host__ __device__ inline cm31 cm31_inv(cm31 x) {
     uint32_t f = m31_inv(m31_add(m31_mul(x.a, x.a), m31_mul(x.b, x.b)));
     return {m31_mul(x.a, f), m31_mul(m31_neg(x.b), f)};
