@@ -1337,7 +1337,7 @@ def main():
     ap.add_argument("--cpu-stream-budget", type=float, default=45.0,
                     help="seconds of CPU proving for the cpu_baseline leg at most (32 jobs otherwise)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--detail-out", default=os.path.join("gpurun_out", "bench_detail.json"),
+    ap.add_argument("--detail-out", default=os.path.join("bench_out", "bench_detail.json"),
                     help="where the full record goes (the printed line carries summaries)")
     ap.add_argument("--no-suite", action="store_true", help="skip the config-1 per-kernel sweep")
     ap.add_argument("--profile", default=None,
